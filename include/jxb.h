@@ -1,0 +1,168 @@
+/*
+ * jxb.h -- C ABI of the B200 Galerkin linear-solve library (libjxb.so).
+ *
+ * The library replaces, for single-patch tensor-product NURBS spaces, the
+ * traced stage of JAXIGA's Galerkin solve for linear problems:
+ *
+ *   evaluation at Gauss points   src/jaxiga/space/evaluation.py:95-172, 305-467
+ *   element tangents             src/jaxiga/forms/library.py:54-65, 125-132, 174-181
+ *   matrix-free tangent matvec   src/jaxiga/methods/galerkin.py:207-218
+ *   Jacobi diagonal              src/jaxiga/methods/galerkin.py:221-237
+ *   load vector / rhs            src/jaxiga/methods/galerkin.py:240-245,
+ *                                src/jaxiga/methods/_common.py:280-309
+ *   Krylov solve                 src/jaxiga/solvers/linear.py:399-442
+ *   true-residual diagnostics    src/jaxiga/solvers/diagnostics.py:8-19
+ *
+ * Conventions
+ *   - DOF vectors are FP64 device arrays of length n_dofs = vec * n_cp_total,
+ *     component c of scalar basis i at index vec*i + c (function_space.py:300-312).
+ *   - Control points and elements are numbered with the first parametric
+ *     direction fastest (function_space.py:326-369, nurbs.py conventions).
+ *   - Per-quadrature-point arrays are (n_elem, n_q^dim[, ncomp]) with elements
+ *     and points both first-direction-fastest (pointset.py:104-112).
+ *   - All device work is ordered on the caller's stream; no call blocks except
+ *     jxb_plan_create, jxb_pcg/jxb_refine_solve (which read convergence state
+ *     back to the host) and jxb_plan_destroy.
+ *   - Return value 0 is success; otherwise a jxb_status code, with a message
+ *     retrievable from jxb_last_error() on the calling thread.
+ *   - A plan may be used by one host thread at a time; distinct plans are
+ *     independent. Every device loop has an iteration cap.
+ */
+#ifndef JXB_H
+#define JXB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* jxb_stream; /* a cudaStream_t; NULL = legacy default stream */
+typedef struct jxb_plan jxb_plan;
+
+enum jxb_status {
+  JXB_OK = 0,
+  JXB_ERR_INVALID = 1,      /* bad argument or unsupported configuration */
+  JXB_ERR_CUDA = 2,         /* CUDA runtime error */
+  JXB_ERR_NOT_CONVERGED = 3,/* iteration cap reached before the tolerance */
+  JXB_ERR_NONFINITE = 4,    /* NaN/Inf met in a reduction */
+  JXB_ERR_NOMEM = 5
+};
+
+enum jxb_operator {
+  JXB_OP_POISSON = 0,     /* -div(a grad u) = f   (library.py:40-65)      */
+  JXB_OP_ELASTICITY = 1,  /* small-strain isotropic (library.py:146-203) */
+  JXB_OP_PLATE = 2        /* Kirchhoff plate, biharmonic (library.py:68-143) */
+};
+
+/* Everything a plan needs; arrays are HOST pointers, copied at creation. */
+typedef struct jxb_desc {
+  int dim;                      /* 2 or 3 */
+  int vec;                      /* 1 (Poisson, plate) or dim (elasticity) */
+  int degree;                   /* p, equal in every direction, 1..5 */
+  int n_quad;                   /* Gauss points per direction, p+1 */
+  int n_cp[3];                  /* control points per direction */
+  int n_span[3];                /* non-empty knot spans per direction */
+  const int32_t* first[3];      /* first basis index of each span (bernstein.py:261-284) */
+  const double* span_lo[3];     /* span bounds in [0, 1] */
+  const double* span_hi[3];
+  const double* extraction[3];  /* (n_span, p+1, p+1) row-major Bezier operators (bernstein.py:16-76) */
+  const double* cpts;           /* (n_cp_total, dim) unweighted control points */
+  const double* wgts;           /* (n_cp_total,) NURBS weights */
+  const double* gauss_nodes;    /* (n_quad,) on [-1, 1] */
+  const double* gauss_weights;  /* (n_quad,) */
+  int op;                       /* enum jxb_operator */
+  double coef[4];               /* Poisson: a0 | elasticity: E, nu | plate: E, nu, t */
+  int plane_strain;             /* 2D elasticity: 0 plane stress, 1 plane strain */
+  const double* coef_qp;        /* optional (n_elem, n_quad^dim) per-point a0 (PointField); NULL = coef[0] */
+  const uint8_t* prescribed;    /* optional (n_dofs,) 1 = Dirichlet DOF; NULL = none */
+  int want_f32;                 /* also keep FP32 copies of the point factors (mixed precision) */
+} jxb_desc;
+
+typedef struct jxb_info {
+  int64_t n_dofs, n_free, n_elem, n_qp;
+  int64_t n_bricks;
+  int64_t geo_bytes;            /* bytes of per-point factors read by one apply */
+  int64_t scratch_bytes;        /* brick partial-sum buffer */
+  int ngeo;                     /* factors per quadrature point */
+  int rational;                 /* 1 if weights are not all equal */
+} jxb_info;
+
+typedef struct jxb_solve_opts {
+  double tol;                   /* relative tolerance on ||r|| / ||b|| */
+  double atol;                  /* absolute tolerance (jax semantics), usually 0 */
+  int64_t maxiter;              /* <= 0: 10 * n_free (jax default) */
+  int preconditioner;           /* 0 none, 1 Jacobi */
+  int check_every;              /* iterations per captured graph launch (<= 0: 16) */
+  /* refinement (jxb_refine_solve) */
+  double inner_tol;             /* relative tolerance of each FP32 inner solve */
+  int max_outer;                /* outer FP64 refinement steps cap */
+} jxb_solve_opts;
+
+typedef struct jxb_stats {
+  int64_t iterations;           /* Krylov iterations (inner ones for refinement) */
+  int64_t outer;                /* refinement steps */
+  double residual;              /* ||b - K x|| over free DOFs, recomputed in FP64 */
+  double relative_residual;
+  double b_norm;
+  int converged;                /* finite and residual <= tol * ||b|| */
+  int finite;
+  double seconds;               /* device time of the solve (CUDA events) */
+} jxb_stats;
+
+/* ---- plan lifetime ---------------------------------------------------- */
+int jxb_plan_create(const jxb_desc* desc, jxb_plan** out);
+int jxb_plan_destroy(jxb_plan* plan);
+int jxb_plan_info(const jxb_plan* plan, jxb_info* out);
+const char* jxb_last_error(void);
+int jxb_version(void);
+
+/* ---- operator ----------------------------------------------------------
+ * jxb_apply: y = K x restricted to free DOFs (src/jaxiga/methods/galerkin.py:207-218).
+ *   masked != 0: prescribed entries of x are ignored and y is 0 there,
+ *                i.e. y = P_f K P_f x, the operator the Krylov loop sees.
+ *   masked == 0: the full, unconstrained K x (used for the Dirichlet lift).
+ * jxb_apply_f32: the same operator in FP32 (factors and arithmetic), for
+ *   mixed-precision inner solves; requires want_f32.
+ * jxb_diag: diag(K) on free DOFs, 0 on prescribed (galerkin.py:221-237).
+ */
+int jxb_apply(jxb_plan* plan, jxb_stream stream, const double* x, double* y, int masked);
+int jxb_apply_f32(jxb_plan* plan, jxb_stream stream, const float* x, float* y);
+int jxb_diag(jxb_plan* plan, jxb_stream stream, double* d);
+
+/* ---- fields at quadrature points ---------------------------------------
+ * jxb_qp_coords: physical coordinates of every Gauss point, (n_elem, n_q^dim, dim).
+ * jxb_interpolate: sum_i R_i(x_q) c_i for a control-point field c (n_cp_total, ncomp),
+ *   written as (n_elem, n_q^dim, ncomp) -- Solution.at / PointField construction.
+ * jxb_load: F_i,c = sum_q w_q f_c(x_q) R_i(x_q) for source values f (n_elem, n_q^dim, vec)
+ *   (the source work term of methods/_common.py:280-309), full length n_dofs.
+ */
+int jxb_qp_coords(jxb_plan* plan, jxb_stream stream, double* x);
+int jxb_interpolate(jxb_plan* plan, jxb_stream stream, const double* coef, int ncomp, double* out);
+int jxb_load(jxb_plan* plan, jxb_stream stream, const double* f_qp, double* F);
+/* jxb_qp_weights: integration weights w_hat |J| prod(h/2) at every Gauss point,
+ *   (n_elem, n_q^dim) -- BasisData.w of src/jaxiga/space/evaluation.py:461-463. */
+int jxb_qp_weights(jxb_plan* plan, jxb_stream stream, double* w);
+
+/* ---- solves -------------------------------------------------------------
+ * jxb_pcg: preconditioned CG on the free DOFs, from x = 0, following
+ *   jax.scipy.sparse.linalg.cg (the reference's matrix-free default,
+ *   src/jaxiga/solvers/linear.py:399-442): stop when ||r||^2 <= max(tol^2 ||b||^2, atol^2).
+ *   b is a full-length vector; its prescribed entries are ignored and x is 0
+ *   there on return. Stats carry the FP64 true residual (diagnostics.py:8-19).
+ * jxb_refine_solve: FP64 iterative refinement around FP32 Jacobi-PCG inner solves
+ *   (jxb_apply_f32); the outer residual and correction are FP64.
+ */
+int jxb_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+            const jxb_solve_opts* opts, jxb_stats* stats);
+int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+                     const jxb_solve_opts* opts, jxb_stats* stats);
+
+/* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
+int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JXB_H */

@@ -1,0 +1,34 @@
+"""jaxiga_b200 -- the Galerkin linear-solve path of JAXIGA on NVIDIA B200.
+
+Single-patch tensor-product NURBS spaces; Poisson (incl. per-point
+coefficients), linear elasticity and Kirchhoff plates; matrix-free,
+sum-factorised FP64 operator application with deterministic accumulation and
+device Jacobi-PCG, plus FP32 inner solves inside FP64 iterative refinement.
+All arithmetic runs in the hand-written sm_100a kernels of ``libjxb.so``.
+
+Quick start (the reference's README example)::
+
+    import numpy as np
+    import jaxiga_b200 as jx
+
+    patch = jx.primitives.quadrilateral([[0, 0], [1, 0], [1, 1], [0, 1]]).elevate(3).refine(5)
+    V = jx.FunctionSpace(patch)
+    f = lambda x, p: 8 * np.pi**2 * np.sin(2 * np.pi * x[0]) * np.sin(2 * np.pi * x[1])
+    problem = jx.Poisson(V, dirichlet=[jx.DirichletBC(0.0, where=lambda x: np.full(len(x), True))], source=f)
+    sol = jx.solve(problem, params={"a0": 1.0})
+"""
+
+from .forms import (ClampedBC, DirichletBC, KirchhoffPlate, LinearElasticity, Neumann, PointField, Poisson,
+                    Problem)
+from .geometry import Patch, primitives
+from .operator import Operator
+from .solve import LinearOptions, Solution, errornorm, integrate, norm, solve
+from .space import FunctionSpace, bezier_extraction, element_spans, expand_dofs
+
+__version__ = "0.1.0"
+
+__all__ = [
+    "Patch", "primitives", "FunctionSpace", "expand_dofs", "bezier_extraction", "element_spans",
+    "Problem", "DirichletBC", "ClampedBC", "Neumann", "PointField", "Poisson", "LinearElasticity",
+    "KirchhoffPlate", "solve", "LinearOptions", "Solution", "errornorm", "norm", "integrate", "Operator",
+]

@@ -1,0 +1,142 @@
+"""ctypes binding of libjxb.so (the C ABI declared in include/jxb.h).
+
+The shared library is built in-tree (``jaxiga_b200/libjxb.so``) by
+``jaxiga_b200/build.py``. Loading it needs no GPU; every compute call does.
+There is no CPU fallback: when the library is missing, importing the solver
+path raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libjxb.so")
+
+OP_POISSON, OP_ELASTICITY, OP_PLATE = 0, 1, 2
+
+STATUS = {0: "OK", 1: "invalid argument", 2: "CUDA error", 3: "not converged", 4: "non-finite", 5: "out of memory"}
+
+c_int64_p = ctypes.POINTER(ctypes.c_int64)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("vec", ctypes.c_int),
+        ("degree", ctypes.c_int),
+        ("n_quad", ctypes.c_int),
+        ("n_cp", ctypes.c_int * 3),
+        ("n_span", ctypes.c_int * 3),
+        ("first", c_int32_p * 3),
+        ("span_lo", c_double_p * 3),
+        ("span_hi", c_double_p * 3),
+        ("extraction", c_double_p * 3),
+        ("cpts", c_double_p),
+        ("wgts", c_double_p),
+        ("gauss_nodes", c_double_p),
+        ("gauss_weights", c_double_p),
+        ("op", ctypes.c_int),
+        ("coef", ctypes.c_double * 4),
+        ("plane_strain", ctypes.c_int),
+        ("coef_qp", c_double_p),
+        ("prescribed", ctypes.POINTER(ctypes.c_uint8)),
+        ("want_f32", ctypes.c_int),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("n_dofs", ctypes.c_int64),
+        ("n_free", ctypes.c_int64),
+        ("n_elem", ctypes.c_int64),
+        ("n_qp", ctypes.c_int64),
+        ("n_bricks", ctypes.c_int64),
+        ("geo_bytes", ctypes.c_int64),
+        ("scratch_bytes", ctypes.c_int64),
+        ("ngeo", ctypes.c_int),
+        ("rational", ctypes.c_int),
+    ]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [
+        ("tol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("maxiter", ctypes.c_int64),
+        ("preconditioner", ctypes.c_int),
+        ("check_every", ctypes.c_int),
+        ("inner_tol", ctypes.c_double),
+        ("max_outer", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int64),
+        ("outer", ctypes.c_int64),
+        ("residual", ctypes.c_double),
+        ("relative_residual", ctypes.c_double),
+        ("b_norm", ctypes.c_double),
+        ("converged", ctypes.c_int),
+        ("finite", ctypes.c_int),
+        ("seconds", ctypes.c_double),
+    ]
+
+
+# (name, argtypes) of every exported entry point, in include/jxb.h order
+SIGNATURES = [
+    ("jxb_plan_create", [ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_plan_destroy", [ctypes.c_void_p]),
+    ("jxb_plan_info", [ctypes.c_void_p, ctypes.POINTER(Info)]),
+    ("jxb_last_error", []),
+    ("jxb_version", []),
+    ("jxb_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    ("jxb_apply_f32", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_diag", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_qp_coords", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_interpolate", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("jxb_load", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_qp_weights", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                 ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    ("jxb_refine_solve", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                          ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    ("jxb_dot", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
+]
+
+_lib = None
+
+
+def load():
+    """Load libjxb.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"libjxb.so not found at {LIB_PATH}; build it with `python -m jaxiga_b200.build` "
+            "(the B200 solver has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_char_p if name == "jxb_last_error" else ctypes.c_int
+    _lib = lib
+    return lib
+
+
+class JxbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libjxb error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def check(code):
+    if code != 0:
+        msg = load().jxb_last_error()
+        raise JxbError(code, msg.decode() if msg else "")
+    return code

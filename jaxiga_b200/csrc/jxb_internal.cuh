@@ -1,0 +1,148 @@
+// Internal declarations shared by the libjxb translation units.
+//
+// Data layout in HBM (one plan = one single-patch space + one operator):
+//   * Elements are grouped into bricks. In 3D a brick is TX x TY elements in
+//     (x, y) times CZ element layers in z; in 2D it is TX elements in x times
+//     CY element rows in y. One CTA owns one brick, walks its layers in order
+//     and accumulates element residuals into a shared-memory copy of the
+//     brick's control-point footprint (deterministic, no atomics).
+//   * Per-point factors ("geo") are stored element-slot-major in brick order:
+//     slot = ((brick * layers + layer) * elems_per_layer + e_in_layer), and
+//     per slot [factor k][quadrature point q] with q first-direction fastest.
+//     One layer of a brick is therefore one contiguous tile, which the apply
+//     kernel streams into shared memory with a bulk asynchronous copy.
+//   * The brick's footprint partial sums go to a scratch buffer; a combine
+//     pass sums, per control point, the (at most JXB_MAXC per direction)
+//     bricks that cover it, always in the same order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/jxb.h"
+
+#define JXB_MAXP 5
+#define JXB_MAXQ 6
+#define JXB_MAXC 3          // bricks covering one control point, per direction
+#define JXB_RED_BLOCKS 296  // fixed grid of every deterministic reduction (2 x 148 SMs)
+#define JXB_RED_THREADS 256
+
+namespace jxb {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define JXB_CUDA(call)                                         \
+  do {                                                         \
+    cudaError_t _e = (call);                                   \
+    if (_e != cudaSuccess) return ::jxb::cuda_fail(_e, #call); \
+  } while (0)
+
+// Operator-specific constants handed to kernels by value.
+struct Material {
+  double lam, mu;  // elasticity (effective plane lambda in 2D)
+};
+
+// Solver state for one Krylov loop, resident in device memory.
+struct CgState {
+  double gamma;    // r . z
+  double rr;       // r . r
+  double alpha, beta;
+  double bb;       // b . b
+  double atol2;    // stopping threshold on r . r
+  long long k;     // iterations done
+  long long maxiter;
+  int done;        // 1 once converged, capped or broken down
+  int status;      // JXB_OK, JXB_ERR_NOT_CONVERGED, JXB_ERR_NONFINITE
+};
+
+// Device-side description of the brick grid, passed by value.
+struct Bricks {
+  int dim, vec, p, q;
+  int n_span[3], n_cp[3];
+  int nb[3];          // bricks per direction
+  int te[3];          // elements per brick per direction (tx, ty, layers)
+  int fp[3];          // scratch footprint per direction
+  const int* first[3];   // per span: first control point
+  const int* bcp0[3];    // per brick: first control point of its footprint
+  const int* cover[3];   // per control point: JXB_MAXC (brick, offset) pairs
+  long long n_bricks;
+  long long slots;       // element slots (bricks * elems per brick)
+};
+
+template <typename T>
+struct Tables {  // per direction [span][3][Q][P+1]: values, d/dxi, d2/dxi2
+  const T* t[3];
+};
+
+}  // namespace jxb
+
+struct jxb_plan {
+  int dim, vec, p, q, op, rational, order, plane_strain;
+  int n_span[3], n_cp[3];
+  long long n_elem, n_scalar, n_dofs, n_free, n_qp, nqe;
+  int ngeo;
+  double coef[4];
+  jxb::Material mat;
+  jxb::Bricks br;
+
+  // device buffers
+  int* d_first[3] = {nullptr, nullptr, nullptr};
+  int* d_bcp0[3] = {nullptr, nullptr, nullptr};
+  int* d_cover[3] = {nullptr, nullptr, nullptr};
+  double* d_tab[3] = {nullptr, nullptr, nullptr};
+  float* d_tab32[3] = {nullptr, nullptr, nullptr};
+  double* d_geo = nullptr;    // (slots, ngeo, nqe)
+  float* d_geo32 = nullptr;
+  double* d_wq = nullptr;     // (slots, nqe): omega / W, the load-vector weight
+  double* d_invW = nullptr;   // (slots, nqe): 1 / W (rational only)
+  double* d_cpts = nullptr;   // (n_scalar, dim)
+  double* d_wgts = nullptr;   // (n_scalar)
+  float* d_wgts32 = nullptr;
+  uint8_t* d_keep = nullptr;  // (n_dofs) 1 = free
+  double* d_scratch = nullptr;
+  float* d_scratch32 = nullptr;
+  double* d_red = nullptr;    // reduction partials, 4 x JXB_RED_BLOCKS
+  // Krylov workspace (allocated on first solve)
+  double *d_x = nullptr, *d_b = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr,
+         *d_Ap = nullptr, *d_invdiag = nullptr;
+  float *d_x32 = nullptr, *d_r32 = nullptr, *d_z32 = nullptr, *d_p32 = nullptr, *d_Ap32 = nullptr,
+        *d_invdiag32 = nullptr;
+  jxb::CgState* d_state = nullptr;
+  jxb::CgState* h_state = nullptr;  // pinned
+  bool diag_valid = false;
+  // captured CG iteration graphs: [0] FP64, [1] FP32
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_iters[2] = {0, 0};
+  int graph_precond[2] = {-1, -1};
+  cudaStream_t graph_stream[2] = {nullptr, nullptr};
+  size_t scratch_elems = 0;
+};
+
+namespace jxb {
+
+// geometry.cu
+int build_tables(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s);
+int build_factors(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s);
+int qp_coords(jxb_plan* plan, cudaStream_t s, double* x);
+int interpolate(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
+int qp_weights(jxb_plan* plan, cudaStream_t s, double* w);
+
+// apply.cu
+enum Mode { MODE_APPLY = 0, MODE_LOAD = 1, MODE_DIAG = 2 };
+template <typename T>
+int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const double* f_qp,
+                  const CgState* state, int masked);
+template <typename T>
+int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* dot_with,
+                   double* partials, const CgState* state);
+
+// pcg.cu
+int ensure_workspace(jxb_plan* plan, bool f32);
+int compute_invdiag(jxb_plan* plan, cudaStream_t s);
+int dot(jxb_plan* plan, cudaStream_t s, const double* a, const double* b, double* out_host);
+
+}  // namespace jxb

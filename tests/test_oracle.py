@@ -1,0 +1,135 @@
+"""The oracle pinned against the reference's fixtures (CPU only).
+
+tests/golden/golden.npz was produced by tests/golden/make_golden.py from the
+reference's own setup, evaluation and element-kernel code. Connectivity and
+extraction must match bit for bit; basis data, element tangents, assembled
+operators and solutions to round-off (1e-12 relative or better).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import iga_oracle as O
+from tests.cases import golden
+
+CASES = [("poisson2d", 1, "poisson"), ("patch2d", 1, "poisson"), ("annulus2d", 1, "poisson"),
+         ("elast3d", 3, "elasticity"), ("darcy3d", 1, "poisson"), ("plate2d", 1, "plate")]
+
+
+def space(tag, vec):
+    g = golden()
+    deg = g[tag + "/degree"]
+    return O.Space([g[f"{tag}/knots{d}"] for d in range(len(deg))], deg, g[tag + "/cpts"], g[tag + "/wgts"], vec)
+
+
+def params_and_source(tag, S):
+    g = golden()
+    if tag == "poisson2d":
+        x = O.evaluate(S, np.arange(S.n_elems))["x"]
+        return {"a0": 1.0}, 8 * np.pi**2 * np.sin(2 * np.pi * x[..., 0]) * np.sin(2 * np.pi * x[..., 1])
+    if tag == "patch2d":
+        return {"a0": 1.0}, np.zeros((S.n_elems, 9))
+    if tag == "annulus2d":
+        return {"a0": float(g["annulus2d/a0"])}, O.interpolate_qp(S, g["annulus2d/source_coef"])[..., 0]
+    if tag == "elast3d":
+        return {"E": 1.0, "nu": 0.3}, O.interpolate_qp(S, g["elast3d/eta"]) + np.array([0, 0, -1.0])
+    if tag == "darcy3d":
+        return {"a0_qp": np.exp(O.interpolate_qp(S, g["darcy3d/loga"])[..., 0])}, np.ones((S.n_elems, 64))
+    return {"E": 12 * (1 - 0.09), "nu": 0.3, "t": 1.0}, np.ones((S.n_elems, 25))
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("tag,vec,op", CASES)
+def test_connectivity_and_extraction_are_bit_exact(tag, vec, op):
+    g = golden()
+    S = space(tag, vec)
+    np.testing.assert_array_equal(S.elem_dofs, g[tag + "/elem_dofs"])
+    np.testing.assert_array_equal(S.elem_vertex, g[tag + "/elem_vertex"])
+    for d in range(S.dim):
+        np.testing.assert_array_equal(S.ext1d[d], g[f"{tag}/extraction{d}"])
+        np.testing.assert_array_equal(S.spans[d][2], g[f"{tag}/first{d}"])
+
+
+@pytest.mark.parametrize("tag,vec,op", CASES)
+def test_basis_and_element_tangents(tag, vec, op):
+    g = golden()
+    S = space(tag, vec)
+    sample = g[tag + "/sample"]
+    b = O.evaluate(S, sample, order=2 if op == "plate" else 1)
+    for k in ("R", "dR", "x", "w") + (("d2R",) if op == "plate" else ()):
+        assert rel(b[k], g[f"{tag}/basis_{k}"]) < 1e-12, k
+    params, _ = params_and_source(tag, S)
+    p = dict(params)
+    if "a0_qp" in p:
+        p["a0"] = p.pop("a0_qp")[sample]
+    assert rel(O.element_tangents(op, b, p, vec), g[tag + "/Ke"]) < 1e-13
+
+
+@pytest.mark.parametrize("tag,vec,op", CASES)
+def test_assembly_rhs_and_solution(tag, vec, op):
+    g = golden()
+    S = space(tag, vec)
+    params, f = params_and_source(tag, S)
+    A = O.Assembled(S, op, params, g[tag + "/prescribed"], g[tag + "/prescribed_values"], source_qp=f)
+    assert A.K.nnz == int(g[tag + "/nnz"])
+    assert rel(A.b, g[tag + "/rhs"]) < 1e-13
+    assert rel(A.diag, g[tag + "/diag"]) < 1e-13
+    assert rel(A.K @ g[tag + "/v"], g[tag + "/Kv"]) < 1e-13
+    u = A.lift(O.scipy_superlu(A.K, A.b))
+    assert np.linalg.norm(u - g[tag + "/u"]) <= 1e-12 * np.linalg.norm(g[tag + "/u"])
+
+
+def test_csr_pattern_checksum_matches_reference():
+    import hashlib
+
+    g = golden()
+    S = space("poisson2d", 1)
+    free = np.setdiff1d(np.arange(S.n_dofs), g["poisson2d/prescribed"])
+    indptr, cols, rows, scatter = O.csr_pattern(S.elem_dofs, S.n_dofs, 1, free)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+    assert sha(indptr) + sha(cols) == str(g["poisson2d/csr_sha"])
+
+
+@pytest.mark.parametrize("key", [k for k in golden().files if k.startswith("bezier/") and k.endswith("/C")])
+def test_bezier_extraction_known_answers(key):
+    g = golden()
+    deg = int(key.split("/")[1].split("_")[0][1:])
+    np.testing.assert_array_equal(np.stack(O.bezier_extraction(g[key[:-2] + "/knots"], deg)), g[key])
+
+
+@pytest.mark.parametrize("deg", [1, 2, 3, 4, 5])
+def test_bernstein_known_answers(deg):
+    g = golden()
+    u = np.linspace(-1, 1, 7)
+    np.testing.assert_array_equal(O.bernstein_basis(u, deg), g[f"bernstein/p{deg}/B"])
+    np.testing.assert_allclose(O.bernstein_basis_deriv(u, deg), g[f"bernstein/p{deg}/dB"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(O.bernstein_basis_2nd_deriv(u, deg), g[f"bernstein/p{deg}/d2B"], rtol=0, atol=1e-14)
+
+
+def test_jax_cg_restatement_converges_like_scipy():
+    g = golden()
+    S = space("poisson2d", 1)
+    params, f = params_and_source("poisson2d", S)
+    A = O.Assembled(S, "poisson", params, g["poisson2d/prescribed"], g["poisson2d/prescribed_values"], source_qp=f)
+    x, k = O.jax_cg(lambda v: A.K @ v, A.b, 1e-12, inv_diag=O.jacobi_inverse(A.diag))
+    assert 0 < k < 10 * len(A.b)
+    d = O.linear_diagnostics(lambda v: A.K @ v, x, A.b, 1e-10)
+    assert d["converged"] and d["finite"]
+    u = A.lift(x)
+    assert np.linalg.norm(u - g["poisson2d/u"]) <= 1e-9 * np.linalg.norm(g["poisson2d/u"])
+    xs, used = O.scipy_cg(A.K, A.b, 1e-12)
+    assert np.linalg.norm(A.lift(xs) - g["poisson2d/u"]) <= 1e-9 * np.linalg.norm(g["poisson2d/u"])
+
+
+def test_truncated_cg_reports_non_convergence():
+    """tests/test_solver_robustness.py:85-93 of the reference, on the oracle."""
+    g = golden()
+    S = space("poisson2d", 1)
+    params, f = params_and_source("poisson2d", S)
+    A = O.Assembled(S, "poisson", params, g["poisson2d/prescribed"], g["poisson2d/prescribed_values"], source_qp=f)
+    x, k = O.jax_cg(lambda v: A.K @ v, A.b, 1e-12, maxiter=3, inv_diag=O.jacobi_inverse(A.diag))
+    assert k == 3
+    assert not O.linear_diagnostics(lambda v: A.K @ v, x, A.b, 1e-12)["converged"]
