@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the Galerkin linear-solve path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one matrix-free stiffness application K.u (FP64, masked to the
+free DOFs) of the 3D linear-elasticity workload: unit cube, cubic NURBS,
+64^3 elements, 902,289 DOFs, 16.8M Gauss points. The per-point factors
+(1.34 GB) exceed the 126 MB L2, so consecutive steps stream them from HBM.
+``value`` is whole-job DOF/s (N_dof x steps x n_gpus / max-over-ranks time,
+CUDA events, barrier + synchronize on both sides). ``e2e`` is the same metric
+through the C ABI with host buffers: pinned host u -> device, apply, device
+y -> pinned host, every step. ``time_to_solution`` gives the solves to a
+1e-8 relative residual: plain FP64 Jacobi-PCG and FP32-inner / FP64-refined.
+
+``--impl reference`` times the reference's CPU path for the same metric on a
+bounded sample (SciPy CSR K.u on an assembled 10^3-element instance, the
+matvec inside src/jaxiga/solvers/linear.py:261-321), single-threaded.
+
+With ``--gpus N > 1`` (torchrun) every rank runs an independent replica of
+the workload (weak scaling; the single-patch apply does not exchange data).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-8 residual & K·u DOF/s: mixed+learned vs plain FP64 PCG, 1 B200"
+UNIT = "DOF/s"
+N_SPAN = 64
+CPU_SAMPLE_SPAN = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution runs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--span", type=int, default=N_SPAN, help="elements per direction (default 64)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML reads only)
+# ---------------------------------------------------------------------------
+REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+           0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+           0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    def __init__(self, index, period=0.05):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.period = period
+        self.stop_ev = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+                mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in REASONS.items():
+                    if mask & bit and bit != 0x1:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.nvml:
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_ev.set()
+        if self.nvml:
+            self.t.join()
+
+    def summary(self):
+        med = float(np.median(self.samples)) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the brick kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "apply_dram.json")) as f:
+            d = json.load(f)
+        return d
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's CPU matvec (SciPy CSR) on an assembled sample
+# ---------------------------------------------------------------------------
+def cpu_sample(span=CPU_SAMPLE_SPAN):
+    from jaxiga_b200 import workloads
+    from oracle import iga_oracle as O
+
+    V, problem, params = workloads.config2(n=span)
+    pres, vals = problem.resolve_dirichlet(params)
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, 3)
+    A = O.Assembled(S, "elasticity", {"E": 1.0, "nu": 0.3}, pres, vals, need_full=False)
+    return V, A
+
+
+def time_cpu_matvec(A, n_dofs, seconds=10.0, min_reps=3, max_reps=None):
+    x = np.random.default_rng(0).standard_normal(A.K.shape[0])
+    A.K @ x
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        A.K @ x
+        reps += 1
+        el = time.perf_counter() - t0
+        if (el >= seconds and reps >= min_reps) or (max_reps and reps >= max_reps):
+            break
+    return n_dofs * reps / el, reps, el
+
+
+def cpu_baseline(seconds=10.0):
+    V, A = cpu_sample()
+    v, reps, el = time_cpu_matvec(A, V.n_dofs, seconds)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"3D elasticity, cubic, {CPU_SAMPLE_SPAN}^3 elements ({V.n_dofs} DOFs, nnz {A.K.nnz}); "
+                      f"SciPy CSR K.u of the assembled operator (reference CPU CG matvec), {reps} reps in {el:.1f} s, "
+                      f"1 thread; assembly excluded"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    V, A = cpu_sample()
+    x = np.random.default_rng(0).standard_normal(A.K.shape[0])
+    for _ in range(args.warmup):
+        A.K @ x
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        A.K @ x
+    el = time.perf_counter() - t0
+    value = V.n_dofs * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"elasticity3d_p3_{CPU_SAMPLE_SPAN}^3 (bounded CPU sample of the 64^3 workload)",
+                   "n_dofs": V.n_dofs, "nnz": int(A.K.nnz), "operator": "assembled CSR (SciPy)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"SciPy CSR K.u, {CPU_SAMPLE_SPAN}^3-element elasticity instance, single thread"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import jaxiga_b200 as jx
+    from jaxiga_b200 import workloads
+    from jaxiga_b200.solve import geometry_operator
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    t_setup = time.perf_counter()
+    V, problem, params = workloads.config2(n=args.span)
+    pres, vals = problem.resolve_dirichlet(params)
+    mask = np.zeros(V.n_dofs, bool)
+    mask[pres] = True
+    op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
+    setup_s = time.perf_counter() - t_setup
+    n = V.n_dofs
+    n_qp = V.n_elems * 64
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    x = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
+    y = torch.empty_like(x)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        op.apply(x, out=y)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nvml_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else local_rank
+    with ClockSampler(nvml_index) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.apply(x, out=y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max * 1e-3)
+
+    # per-kernel split for the roofline (CUDA events on the launching stream)
+    ms_bricks, ms_combine = op.profile_apply(x, reps=50)
+    ms_b32, ms_c32 = op.profile_apply(x.float(), reps=50, f32=True)
+    ngeo = op.info["ngeo"]
+    alg_bytes = 8 * 2 * n + 8 * n_qp * ngeo
+    alg_bytes32 = 4 * 2 * n + 4 * n_qp * ngeo
+    p1, q = 4, 4
+    flops = V.n_elems * 3 * (2 * 2 * 9 * p1**3 * q) + n_qp * 2 * 81
+    peaks, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
+    traffic = profile_traffic()
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+        "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+        "kernel": "k_brick3<double,3,4,elasticity> (brick apply)",
+        "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
+        "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
+        "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
+    }
+
+    # e2e through the C ABI with host buffers
+    xh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    xd = torch.empty_like(x)
+    k_e2e = max(10, args.steps // 5)
+    for _ in range(3):
+        xd.copy_(xh, non_blocking=True)
+        op.apply(xd, out=y)
+        yh.copy_(y, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(k_e2e):
+        xd.copy_(xh, non_blocking=True)
+        op.apply(xd, out=y)
+        yh.copy_(y, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * k_e2e / (float(t.item()) * 1e-3)
+
+    tts = None
+    if not args.no_solve:
+        geo = geometry_operator(V)
+        eta = params["eta"]
+        fq = geo.interpolate(eta)
+        fq[..., 2] -= 1.0
+        F = op.load(fq)
+        del fq
+        sol_p, st_p = op.pcg(F, tol=1e-8, preconditioner="jacobi", check_every=32, maxiter=40000)
+        sol_m, st_m = op.refine_solve(F, tol=1e-8, inner_tol=1e-3, check_every=32, maxiter=80000)
+        diff = float(torch.linalg.norm(sol_m - sol_p) / torch.linalg.norm(sol_p))
+        tts = {
+            "tol": 1e-8,
+            "plain_fp64_jacobi_pcg": {"seconds": st_p["seconds"], "iterations": st_p["iterations"],
+                                      "relative_residual": st_p["relative_residual"], "converged": bool(st_p["converged"])},
+            "mixed_fp32_inner_fp64_refinement": {"seconds": st_m["seconds"], "iterations": st_m["iterations"],
+                                                 "outer": st_m["outer"], "relative_residual": st_m["relative_residual"],
+                                                 "converged": bool(st_m["converged"]),
+                                                 "relative_difference_to_plain": diff},
+            "speedup_mixed_vs_plain": st_p["seconds"] / st_m["seconds"] if st_m["seconds"] > 0 else None,
+            "learned_preconditioner": None,
+        }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"elasticity3d_p3_{args.span}^3", "n_dofs": n, "elements": V.n_elems,
+                       "gauss_points": n_qp, "operator": "matrix-free sum-factorised K.u, FP64, masked",
+                       "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),
+                       "parallelism": f"replicas x{world}", "setup_seconds": setup_s},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                    "steps": k_e2e},
+            "gpu_launches": 2 * args.steps,
+            "roofline": roofline,
+            "clocks": clocks.summary(),
+            "time_to_solution": tts,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    op.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

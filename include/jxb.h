@@ -162,6 +162,15 @@ int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double*
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);
 
+/* ---- measurement --------------------------------------------------------
+ * jxb_profile_apply: runs `reps` masked applies (FP64, or FP32 when f32 != 0,
+ *   x/y then being float*) and returns in ms_out[0] / ms_out[1] the average
+ *   device time of one brick launch / one combine launch, measured with CUDA
+ *   events on `stream`. Blocks until done. No counterpart in the reference
+ *   (which has no kernels of its own to time). */
+int jxb_profile_apply(jxb_plan* plan, jxb_stream stream, const void* x, void* y, int reps, int f32,
+                      double* ms_out);
+
 #ifdef __cplusplus
 }
 #endif

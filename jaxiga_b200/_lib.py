@@ -106,6 +106,8 @@ SIGNATURES = [
     ("jxb_refine_solve", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                           ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_dot", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
+    ("jxb_profile_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                           ctypes.c_int, c_double_p]),
 ]
 
 _lib = None

@@ -344,3 +344,41 @@ extern "C" int jxb_qp_weights(jxb_plan* P, jxb_stream stream, double* w) {
   if (!P || !w) return fail(JXB_ERR_INVALID, "jxb_qp_weights: null argument");
   return qp_weights(P, reinterpret_cast<cudaStream_t>(stream), w);
 }
+
+extern "C" int jxb_profile_apply(jxb_plan* P, jxb_stream stream, const void* x, void* y, int reps, int f32,
+                                 double* ms_out) {
+  if (!P || !x || !y || !ms_out || reps < 1) return fail(JXB_ERR_INVALID, "jxb_profile_apply: bad argument");
+  if (f32 && !P->d_geo32) return fail(JXB_ERR_INVALID, "jxb_profile_apply: plan was created without want_f32");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::vector<cudaEvent_t> ev(3 * reps);
+  for (auto& e : ev) JXB_CUDA(cudaEventCreate(&e));
+  int rc = 0;
+  for (int r = 0; r < reps && !rc; ++r) {
+    JXB_CUDA(cudaEventRecord(ev[3 * r], s));
+    if (f32)
+      rc = launch_bricks<float>(P, s, MODE_APPLY, (const float*)x, nullptr, nullptr, 1);
+    else
+      rc = launch_bricks<double>(P, s, MODE_APPLY, (const double*)x, nullptr, nullptr, 1);
+    if (rc) break;
+    JXB_CUDA(cudaEventRecord(ev[3 * r + 1], s));
+    if (f32)
+      rc = launch_combine<float>(P, s, (float*)y, 1, nullptr, nullptr, nullptr);
+    else
+      rc = launch_combine<double>(P, s, (double*)y, 1, nullptr, nullptr, nullptr);
+    JXB_CUDA(cudaEventRecord(ev[3 * r + 2], s));
+  }
+  if (rc) return rc;
+  JXB_CUDA(cudaEventSynchronize(ev[3 * reps - 1]));
+  double tb = 0, tc = 0;
+  for (int r = 0; r < reps; ++r) {
+    float a = 0, b = 0;
+    JXB_CUDA(cudaEventElapsedTime(&a, ev[3 * r], ev[3 * r + 1]));
+    JXB_CUDA(cudaEventElapsedTime(&b, ev[3 * r + 1], ev[3 * r + 2]));
+    tb += a;
+    tc += b;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  ms_out[0] = tb / reps;
+  ms_out[1] = tc / reps;
+  return JXB_OK;
+}

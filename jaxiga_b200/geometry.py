@@ -125,15 +125,11 @@ def _apply_along_dir(coefs, n_per_dir, d, fn):
     dim = len(n_per_dir)
     ncomp = coefs.shape[1]
     grid = np.asarray(coefs, dtype=float).reshape(*reversed(n_per_dir), ncomp)
-    grid = np.moveaxis(grid, dim - 1 - d, -2)  # (..., n_d, comp)
-    rest = grid.shape[:-2]
-    flat = grid.reshape(-1, grid.shape[-2], ncomp)
-    outs, kv = [], None
-    for curve in flat:
-        kv, c = fn(curve)
-        outs.append(c)
-    out = np.stack(outs).reshape(*rest, outs[0].shape[0], ncomp)
-    out = np.moveaxis(out, -2, dim - 1 - d)
+    grid = np.moveaxis(grid, dim - 1 - d, 0)  # (n_d, ..., comp)
+    rest = grid.shape[1:]
+    # every curve along direction d at once: columns of an (n_d, n_curves * comp) matrix
+    kv, out = fn(grid.reshape(grid.shape[0], -1))
+    out = np.moveaxis(out.reshape(out.shape[0], *rest), 0, dim - 1 - d)
     return out.reshape(-1, ncomp), kv
 
 

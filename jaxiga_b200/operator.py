@@ -46,7 +46,7 @@ class Operator:
     OPS = {"poisson": _lib.OP_POISSON, "elasticity": _lib.OP_ELASTICITY, "plate": _lib.OP_PLATE}
 
     def __init__(self, space, op="poisson", coef=(1.0,), prescribed=None, coef_qp=None,
-                 want_f32=False, plane_strain=False):
+                 want_f32=False, plane_strain=False, vec=None):
         import torch
 
         if not torch.cuda.is_available():
@@ -54,13 +54,14 @@ class Operator:
         self.lib = _lib.load()
         self.space = space
         self.op = op
+        self.vec = space.vec if vec is None else int(vec)
         self.device = torch.device("cuda", torch.cuda.current_device())
         p = space.degree[0]
         nodes, weights = np.polynomial.legendre.leggauss(p + 1)
         self._keep = []  # host arrays referenced by the descriptor
         d = _lib.Desc()
         d.dim = space.dim
-        d.vec = space.vec
+        d.vec = self.vec
         d.degree = p
         d.n_quad = p + 1
         for k in range(3):
@@ -98,7 +99,7 @@ class Operator:
             d.coef_qp = _hptr(cq, ctypes.c_double)
         if prescribed is not None:
             pm = np.ascontiguousarray(np.asarray(prescribed).astype(np.uint8))
-            if pm.size != space.n_dofs:
+            if pm.size != space.n_scalar_basis * self.vec:
                 raise ValueError("prescribed mask must have n_dofs entries")
             self._keep.append(pm)
             d.prescribed = _hptr(pm, ctypes.c_uint8)
@@ -168,8 +169,8 @@ class Operator:
         import torch
 
         f = torch.as_tensor(f_qp, dtype=torch.float64, device=self.device).contiguous()
-        if f.numel() != self.n_qp * self.space.vec:
-            raise ValueError(f"source has {f.numel()} values, expected {self.n_qp * self.space.vec}")
+        if f.numel() != self.n_qp * self.vec:
+            raise ValueError(f"source has {f.numel()} values, expected {self.n_qp * self.vec}")
         F = self._empty(self.n_dofs)
         _lib.check(self.lib.jxb_load(self.handle, _stream(), _dptr(f), _dptr(F)))
         return F
@@ -194,6 +195,18 @@ class Operator:
         out = self._empty(self.n_qp * ncomp)
         _lib.check(self.lib.jxb_interpolate(self.handle, _stream(), _dptr(c), ncomp, _dptr(out)))
         return out.view(self.space.n_elems, self.nqe, ncomp)
+
+    def profile_apply(self, x, reps=20, f32=False):
+        """Average device ms of one brick launch and one combine launch (CUDA events)."""
+        import torch
+
+        dt = torch.float32 if f32 else torch.float64
+        x = self._vec(x, dt)
+        y = self._empty(self.n_dofs, dt)
+        ms = (ctypes.c_double * 2)()
+        _lib.check(self.lib.jxb_profile_apply(self.handle, _stream(), _dptr(x), _dptr(y), int(reps),
+                                              1 if f32 else 0, ms))
+        return ms[0], ms[1]
 
     def dot(self, a, b):
         r = ctypes.c_double()

@@ -83,7 +83,7 @@ def geometry_operator(space) -> Operator:
     """Cached evaluation plan of a space (coordinates, weights, interpolation)."""
     op = space._plans.get("geometry")
     if op is None:
-        op = Operator(space, "poisson", (1.0,))
+        op = Operator(space, "poisson", (1.0,), vec=1)
         space._plans["geometry"] = op
     return op
 
@@ -156,7 +156,7 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
             x = qp_points(space)
             f = call_points(problem.source, x, flat_params(params, x.shape[0]))
             f = np.broadcast_to(f.reshape(x.shape[0], -1), (x.shape[0], space.vec))
-            F = op.load(np.ascontiguousarray(f))
+            F = op.load(np.array(f, dtype=np.float64, copy=True))
         b = F
         g = np.zeros(n)
         g[prescribed] = values
@@ -195,8 +195,14 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
 
 
 def _exact_at(exact, x):
-    vals = call_points(lambda xx, p: exact(xx), x, None)
-    return vals.reshape(x.shape[0], -1)
+    """``exact`` over points (n, dim): vectorised over rows, else point by point (norms.py:17-32)."""
+    try:
+        out = np.asarray(exact(x), dtype=float)
+        if out.shape[0] != x.shape[0]:
+            raise ValueError
+    except Exception:
+        out = np.stack([np.asarray(exact(xi), dtype=float) for xi in x])
+    return out.reshape(x.shape[0], -1)
 
 
 def errornorm(sol, exact, norm: str = "L2", exact_grad=None, quad=None, relative: bool = True) -> float:

@@ -131,8 +131,8 @@ def test_pcg_iterations_match_jax_cg(tag):
     V, problem, params, op, pres, vals = make_operator(tag)
     S = O.Space(V.knots, V.degree, V.cpts, V.wgts, V.vec)
     coef, field = problem.operator_coefficients(params)
-    oparams = {"poisson": {"a0": coef[0]}, "elasticity": {"E": coef[0], "nu": coef[1]},
-               "plate": {"E": coef[0], "nu": coef[1], "t": coef[2]}}[OPS[tag]]
+    names = {"poisson": ("a0",), "elasticity": ("E", "nu"), "plate": ("E", "nu", "t")}[OPS[tag]]
+    oparams = dict(zip(names, coef))
     if field is not None:
         oparams["a0_qp"] = np.asarray(field.values)
     A = O.Assembled(S, OPS[tag], oparams, pres, vals, need_full=False)
