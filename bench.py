@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--span", type=int, default=N_SPAN, help="elements per direction (default 64)")
+    ap.add_argument("--span", type=int, default=None, help="elements per direction (default 64, Darcy 96)")
+    ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy"],
+                    help="elasticity: 3D elasticity 64^3 (the headline); darcy: 3D Darcy 96^3")
     return ap.parse_args()
 
 
@@ -198,14 +200,27 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
-    V, problem, params = workloads.config2(n=args.span)
-    pres, vals = problem.resolve_dirichlet(params)
-    mask = np.zeros(V.n_dofs, bool)
-    mask[pres] = True
-    op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
+    darcy = args.workload == "darcy"
+    span = args.span or (96 if darcy else N_SPAN)
+    if darcy:
+        V, problem, params = workloads.config4(n=span)
+        geo0 = geometry_operator(V)
+        a_qp = torch.exp(geo0.interpolate(params["loga"])[..., 0])
+        pres, vals = problem.resolve_dirichlet(params)
+        mask = np.zeros(V.n_dofs, bool)
+        mask[pres] = True
+        op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a_qp.cpu().numpy(), want_f32=True)
+        del a_qp
+    else:
+        V, problem, params = workloads.config2(n=span)
+        pres, vals = problem.resolve_dirichlet(params)
+        mask = np.zeros(V.n_dofs, bool)
+        mask[pres] = True
+        op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
     setup_s = time.perf_counter() - t_setup
     n = V.n_dofs
     n_qp = V.n_elems * 64
+    vec = V.vec
     gen = torch.Generator(device=dev).manual_seed(1234 + rank)
     x = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
     y = torch.empty_like(x)
@@ -243,8 +258,9 @@ def run_ours(args, rank, world, local_rank):
     ngeo = op.info["ngeo"]
     alg_bytes = 8 * 2 * n + 8 * n_qp * ngeo
     alg_bytes32 = 4 * 2 * n + 4 * n_qp * ngeo
+    # survey formula: n_e vec 2*2*d^2 (p+1)^(d+1) + N_qp c_pt, c_pt = 2 d^4 (elasticity) or 2 d^2 (scalar)
     p1, q = 4, 4
-    flops = V.n_elems * 3 * (2 * 2 * 9 * p1**3 * q) + n_qp * 2 * 81
+    flops = V.n_elems * vec * (2 * 2 * 9 * p1**3 * q) + n_qp * (2 * 81 if vec == 3 else 2 * 9)
     peaks, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
     traffic = profile_traffic()
@@ -252,7 +268,7 @@ def run_ours(args, rank, world, local_rank):
         "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
         "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-        "kernel": "k_brick3<double,3,4,elasticity> (brick apply)",
+        "kernel": "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if darcy else "elasticity"),
         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
         "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
         "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
@@ -286,11 +302,13 @@ def run_ours(args, rank, world, local_rank):
     tts = None
     if not args.no_solve:
         geo = geometry_operator(V)
-        eta = params["eta"]
-        fq = geo.interpolate(eta)
-        fq[..., 2] -= 1.0
-        F = op.load(fq)
-        del fq
+        if darcy:
+            F = op.load(torch.ones(n_qp, dtype=torch.float64, device=dev))
+        else:
+            fq = geo.interpolate(params["eta"])
+            fq[..., 2] -= 1.0
+            F = op.load(fq)
+            del fq
         sol_p, st_p = op.pcg(F, tol=1e-8, preconditioner="jacobi", check_every=32, maxiter=40000)
         sol_m, st_m = op.refine_solve(F, tol=1e-8, inner_tol=1e-3, check_every=32, maxiter=80000)
         diff = float(torch.linalg.norm(sol_m - sol_p) / torch.linalg.norm(sol_p))
@@ -315,7 +333,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"elasticity3d_p3_{args.span}^3", "n_dofs": n, "elements": V.n_elems,
+            "config": {"workload": f"{'darcy3d' if darcy else 'elasticity3d'}_p3_{span}^3", "n_dofs": n,
+                       "elements": V.n_elems,
                        "gauss_points": n_qp, "operator": "matrix-free sum-factorised K.u, FP64, masked",
                        "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),
                        "parallelism": f"replicas x{world}", "setup_seconds": setup_s},

@@ -1,0 +1,335 @@
+// 2D brick kernel (included by apply.cu): TX elements per row, TY rows per brick,
+// Q threads per element; x contraction through shared memory, y in registers.
+#pragma once
+
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE>
+__global__ void __launch_bounds__(BrickShape<2, P>::TX* Q) k_brick2(BrickArgs<T> A) {
+  constexpr int P1 = P + 1, PP = P1 * P1;
+  constexpr int TX = BrickShape<2, P>::TX, TY = BrickShape<2, P>::TY;
+  constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
+  constexpr int VEC = OPK == OPK_ELAST ? 2 : 1;
+  constexpr int NG = GeoCount<OPK, RAT, 2>::value;
+  constexpr bool HASV = RAT || MODE == MODE_LOAD;
+  constexpr bool HESS = OPK == OPK_PLATE;
+  constexpr int NK = HESS ? 3 : 2;      // 1D table kinds used
+  constexpr int NCH = HESS ? 6 : 3;     // channels (v, g0, g1[, h00, h01, h11])
+  constexpr int SX = P1 + 1;            // padded q0 stride
+
+  if (A.state && A.state->done) return;
+  const Bricks& br = A.br;
+  const int fp0 = br.fp[0], fp1 = br.fp[1];
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* stx = reinterpret_cast<T*>(smem_raw);   // [TX][3][Q][P1]
+  T* sty = stx + TX * 3 * Q * P1;            // [3][Q][P1]
+  T* bufX = sty + 3 * Q * P1;                // [NE][NK][Q][SX]
+  T* stage = bufX + NE * NK * Q * SX;        // [NE][VEC][PP]
+  T* acc = stage + NE * VEC * PP;            // [VEC][fp1][fp0]
+  int* soff = reinterpret_cast<int*>(acc + VEC * fp0 * fp1);
+
+  const int tid = threadIdx.x;
+  const long long b = blockIdx.x;
+  const int bx = (int)(b % br.nb[0]);
+  const int by = (int)(b / br.nb[0]);
+  const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by];
+  const int el = tid / Q, t = tid % Q;
+  const int ex = bx * TX + el;
+  const bool evalid = ex < br.n_span[0];
+
+  for (int i = tid; i < TX * 3 * Q * P1; i += NT) {
+    int e = i / (3 * Q * P1), r = i % (3 * Q * P1);
+    int sp = min(bx * TX + e, br.n_span[0] - 1);
+    stx[i] = A.tab[0][(size_t)sp * 3 * Q * P1 + r];
+  }
+  if (tid < TX) {
+    int e = bx * TX + tid;
+    soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
+  }
+  const int accn = VEC * fp0 * fp1;
+  for (int i = tid; i < accn; i += NT) acc[i] = T(0);
+  const long long slot_base = b * (long long)TY * NE;
+  const int nlayers = min(TY, br.n_span[1] - by * TY);
+  const T* nx_v = stx + el * 3 * Q * P1;
+
+  for (int ly_ = 0; ly_ < nlayers; ++ly_) {
+    const int ey = by * TY + ly_;
+    const int fy = br.first[1][ey];
+    const int offy = fy - cp0y;
+    for (int i = tid; i < 3 * Q * P1; i += NT) sty[i] = A.tab[1][(size_t)ey * 3 * Q * P1 + i];
+    __syncthreads();
+    const long long slot = slot_base + (long long)ly_ * NE + el;
+    const int fx = evalid ? br.first[0][ex] : 0;
+    T g[VEC][NCH][Q];  // channel order (v, g0, g1, h00, h01, h11) at q1
+
+    if constexpr (MODE == MODE_APPLY) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        if (evalid && t < P1) {  // X: line along x at row i1 = t
+          const int i1 = t;
+          const long long row = (long long)br.n_cp[0] * (fy + i1) + fx;
+          T u[P1];
+#pragma unroll
+          for (int i0 = 0; i0 < P1; ++i0) {
+            long long cp = row + i0;
+            T v = A.x[cp * VEC + c];
+            if (A.masked) v = A.keep[cp * VEC + c] ? v : T(0);
+            if constexpr (RAT) v *= A.wgts[cp];
+            u[i0] = v;
+          }
+          T* dst = bufX + el * NK * Q * SX;
+#pragma unroll
+          for (int k = 0; k < NK; ++k)
+#pragma unroll
+            for (int q0 = 0; q0 < Q; ++q0) {
+              T s = 0;
+#pragma unroll
+              for (int i0 = 0; i0 < P1; ++i0) s += nx_v[(k * Q + q0) * P1 + i0] * u[i0];
+              dst[(k * Q + q0) * SX + i1] = s;
+            }
+        }
+        __syncthreads();
+        if (evalid) {  // Y in registers: q0 = t
+          const int q0 = t;
+          const T* src = bufX + el * NK * Q * SX;
+          T a[NK][P1];
+#pragma unroll
+          for (int k = 0; k < NK; ++k)
+#pragma unroll
+            for (int i1 = 0; i1 < P1; ++i1) a[k][i1] = src[(k * Q + q0) * SX + i1];
+#pragma unroll
+          for (int q1 = 0; q1 < Q; ++q1) {
+            T ch[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int i1 = 0; i1 < P1; ++i1) {
+              T nv = sty[q1 * P1 + i1], nd = sty[(Q + q1) * P1 + i1];
+              ch[0] += nv * a[0][i1];
+              ch[1] += nv * a[1][i1];
+              ch[2] += nd * a[0][i1];
+              if constexpr (HESS) {
+                T nh = sty[(2 * Q + q1) * P1 + i1];
+                ch[3] += nv * a[2][i1];
+                ch[4] += nd * a[1][i1];
+                ch[5] += nh * a[0][i1];
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) g[c][k][q1] = ch[k];
+          }
+        }
+        __syncthreads();
+      }
+      if (evalid) {
+        const T* G = A.geo + (size_t)slot * NG * NQE;
+#pragma unroll
+        for (int q1 = 0; q1 < Q; ++q1) {
+          const int q = t + Q * q1;
+          if constexpr (OPK == OPK_SCALAR) {
+            if constexpr (!RAT) {
+              T k0 = G[q], k1 = G[NQE + q], k2 = G[2 * NQE + q];
+              T gx = g[0][1][q1], gy = g[0][2][q1];
+              g[0][1][q1] = k0 * gx + k1 * gy;
+              g[0][2][q1] = k1 * gx + k2 * gy;
+              g[0][0][q1] = 0;
+            } else {
+              T m[6];
+#pragma unroll
+              for (int k = 0; k < 6; ++k) m[k] = G[k * NQE + q];
+              T v = g[0][0][q1], gx = g[0][1][q1], gy = g[0][2][q1];
+              g[0][0][q1] = m[0] * v + m[1] * gx + m[2] * gy;
+              g[0][1][q1] = m[1] * v + m[3] * gx + m[4] * gy;
+              g[0][2][q1] = m[2] * v + m[4] * gx + m[5] * gy;
+            }
+          } else if constexpr (OPK == OPK_PLATE) {
+            constexpr int n = RAT ? 6 : 5, off = RAT ? 0 : 1;
+            T s[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s[k] = g[0][k][q1];
+            T o[6] = {0, 0, 0, 0, 0, 0};
+            int k = 0;
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+#pragma unroll
+              for (int j = i; j < n; ++j) {
+                T m = G[(k++) * NQE + q];
+                o[i + off] += m * s[j + off];
+                if (j != i) o[j + off] += m * s[i + off];
+              }
+#pragma unroll
+            for (int kk = 0; kk < 6; ++kk) g[0][kk][q1] = o[kk];
+          } else {  // 2D elasticity
+            T Ji[2][2] = {{G[q], G[NQE + q]}, {G[2 * NQE + q], G[3 * NQE + q]}};
+            T om = G[4 * NQE + q];
+            T iW = 1, gW[2] = {0, 0};
+            if constexpr (RAT) {
+              iW = G[5 * NQE + q];
+              gW[0] = G[6 * NQE + q];
+              gW[1] = G[7 * NQE + q];
+            }
+            T gp[2][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+              for (int a = 0; a < 2; ++a) gp[c][a] = RAT ? (g[c][1 + a][q1] - g[c][0][q1] * gW[a]) * iW : g[c][1 + a][q1];
+            T Gx[2][2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+              for (int k = 0; k < 2; ++k) Gx[c][k] = Ji[k][0] * gp[c][0] + Ji[k][1] * gp[c][1];
+            T tr = Gx[0][0] + Gx[1][1];
+            T lam = (T)A.lam, mu = (T)A.mu;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              T S0 = om * (mu * (Gx[c][0] + Gx[0][c]) + (c == 0 ? lam * tr : T(0)));
+              T S1 = om * (mu * (Gx[c][1] + Gx[1][c]) + (c == 1 ? lam * tr : T(0)));
+              T F0 = S0 * Ji[0][0] + S1 * Ji[1][0];
+              T F1 = S0 * Ji[0][1] + S1 * Ji[1][1];
+              if constexpr (RAT) {
+                g[c][0][q1] = -(F0 * gW[0] + F1 * gW[1]) * iW;
+                g[c][1][q1] = F0 * iW;
+                g[c][2][q1] = F1 * iW;
+              } else {
+                g[c][0][q1] = 0;
+                g[c][1][q1] = F0;
+                g[c][2][q1] = F1;
+              }
+            }
+          }
+        }
+      }
+    } else if constexpr (MODE == MODE_LOAD) {
+      if (evalid) {
+        const long long eref = ex + (long long)br.n_span[0] * ey;
+#pragma unroll
+        for (int q1 = 0; q1 < Q; ++q1) {
+          const int q = t + Q * q1;
+          double w = A.wq[slot * NQE + q];
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) {
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) g[c][k][q1] = T(0);
+            g[c][0][q1] = (T)(w * A.f_qp[(eref * NQE + q) * VEC + c]);
+          }
+        }
+      }
+    }
+
+    if constexpr (MODE == MODE_APPLY || MODE == MODE_LOAD) {
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        if (evalid) {  // Y^T: q0 = t -> bufX[k][q0][i1]
+          const int q0 = t;
+          T* dst = bufX + el * NK * Q * SX;
+#pragma unroll
+          for (int i1 = 0; i1 < P1; ++i1) {
+            T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+            for (int q1 = 0; q1 < Q; ++q1) {
+              T nv = sty[q1 * P1 + i1], nd = sty[(Q + q1) * P1 + i1];
+              if constexpr (HASV || HESS) a0 += nv * g[c][0][q1];
+              a0 += nd * g[c][2][q1];
+              a1 += nv * g[c][1][q1];
+              if constexpr (HESS) {
+                T nh = sty[(2 * Q + q1) * P1 + i1];
+                a0 += nh * g[c][5][q1];
+                a1 += nd * g[c][4][q1];
+                a2 += nv * g[c][3][q1];
+              }
+            }
+            dst[(0 * Q + q0) * SX + i1] = a0;
+            dst[(1 * Q + q0) * SX + i1] = a1;
+            if constexpr (HESS) dst[(2 * Q + q0) * SX + i1] = a2;
+          }
+        }
+        __syncthreads();
+        if (evalid && t < P1) {  // X^T: row i1 = t
+          const int i1 = t;
+          const T* src = bufX + el * NK * Q * SX;
+          T* dst = stage + (el * VEC + c) * PP;
+#pragma unroll
+          for (int i0 = 0; i0 < P1; ++i0) {
+            T r = 0;
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+#pragma unroll
+              for (int q0 = 0; q0 < Q; ++q0) r += nx_v[(k * Q + q0) * P1 + i0] * src[(k * Q + q0) * SX + i1];
+            if constexpr (RAT) r *= A.wgts[(long long)br.n_cp[0] * (fy + i1) + fx + i0];
+            dst[i0 * P1 + i1] = r;
+          }
+        }
+        __syncthreads();
+      }
+    } else {  // MODE_DIAG
+      if (evalid) {
+        for (int a = t; a < PP; a += Q) {
+          const int a0 = a % P1, a1 = a / P1;
+          T d[VEC];
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) d[c] = 0;
+          for (int q = 0; q < NQE; ++q) {
+            const int q0 = q % Q, q1 = q / Q;
+            T vx = nx_v[q0 * P1 + a0], dx = nx_v[(Q + q0) * P1 + a0], hx = nx_v[(2 * Q + q0) * P1 + a0];
+            T vy = sty[q1 * P1 + a1], dy = sty[(Q + q1) * P1 + a1], hy = sty[(2 * Q + q1) * P1 + a1];
+            T s[6] = {vx * vy, dx * vy, vx * dy, hx * vy, dx * dy, vx * hy};
+            const T* G = A.geo + (size_t)slot * NG * NQE + q;
+            if constexpr (OPK == OPK_SCALAR || OPK == OPK_PLATE) {
+              constexpr int n = OPK == OPK_SCALAR ? (RAT ? 3 : 2) : (RAT ? 6 : 5);
+              constexpr int off = RAT ? 0 : 1;
+              int k = 0;
+              T acc_ = 0;
+#pragma unroll
+              for (int i = 0; i < n; ++i)
+#pragma unroll
+                for (int j = i; j < n; ++j) {
+                  T m = G[(k++) * NQE];
+                  acc_ += (i == j ? T(1) : T(2)) * m * s[i + off] * s[j + off];
+                }
+              d[0] += acc_;
+            } else {
+              T Ji[2][2] = {{G[0], G[NQE]}, {G[2 * NQE], G[3 * NQE]}};
+              T om = G[4 * NQE];
+              T gp[2] = {s[1], s[2]};
+              if constexpr (RAT) {
+                T iW = G[5 * NQE];
+                gp[0] = (gp[0] - s[0] * G[6 * NQE]) * iW;
+                gp[1] = (gp[1] - s[0] * G[7 * NQE]) * iW;
+              }
+              T gx[2] = {Ji[0][0] * gp[0] + Ji[0][1] * gp[1], Ji[1][0] * gp[0] + Ji[1][1] * gp[1]};
+              T n2 = gx[0] * gx[0] + gx[1] * gx[1];
+#pragma unroll
+              for (int c = 0; c < VEC; ++c) d[c] += om * ((T)(A.lam + A.mu) * gx[c] * gx[c] + (T)A.mu * n2);
+            }
+          }
+          T wsq = 1;
+          if constexpr (RAT) {
+            T w = A.wgts[(long long)br.n_cp[0] * (fy + a1) + fx + a0];
+            wsq = w * w;
+          }
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) stage[(el * VEC + c) * PP + a0 * P1 + a1] = d[c] * wsq;
+        }
+      }
+      __syncthreads();
+    }
+    // gather the row into the brick footprint
+    {
+      const int nfoot = VEC * fp0 * P1;
+      for (int i = tid; i < nfoot; i += NT) {
+        const int jx = i % fp0;
+        const int jyl = (i / fp0) % P1;
+        const int c = i / (fp0 * P1);
+        T s = 0;
+#pragma unroll 4
+        for (int e0 = 0; e0 < TX; ++e0) {
+          const int lx = jx - soff[e0];
+          if (lx < 0 || lx > P) continue;
+          s += stage[(e0 * VEC + c) * PP + lx * P1 + jyl];
+        }
+        acc[(c * fp1 + offy + jyl) * fp0 + jx] += s;
+      }
+    }
+    __syncthreads();
+  }
+  T* out = A.scratch + (size_t)b * accn;
+  for (int i = tid; i < accn; i += NT) out[i] = acc[i];
+}
+
