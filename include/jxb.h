@@ -159,6 +159,43 @@ int jxb_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
 int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                      const jxb_solve_opts* opts, jxb_stats* stats);
 
+/* jxb_pcg_snapshots: jxb_pcg (Jacobi or none, jax CG semantics) that also copies
+ *   the FP64 iterate into snaps[j] (n_dofs doubles each) after every `every`
+ *   iterations, up to max_snaps; *n_snaps receives the number written. With the
+ *   converged x*, (K (x* - x_j), x* - x_j) are the solver's residual/error pairs. */
+int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+                      const jxb_solve_opts* opts, int every, double* snaps, int64_t max_snaps,
+                      int64_t* n_snaps, jxb_stats* stats);
+
+/* ---- learned preconditioner ---------------------------------------------
+ * A 3D convolutional network on the control-point grid (FP32 weights and
+ * activations, hand-written kernels), used inside flexible CG. No counterpart
+ * in the reference, whose only preconditioner is Jacobi
+ * (src/jaxiga/solvers/linear.py:419-431).
+ *   jxb_cnn_create: in_ch input channels (residual components, then features),
+ *     out_ch outputs (= vec), channels[3] per level (each in {4,8,12,16,24,32,48}).
+ *   jxb_cnn_params: device pointer to the flat FP32 parameter vector and its length.
+ *   jxb_cnn_forward: out[out_ch][nz][ny][nx] = N(in[in_ch][nz][ny][nx]).
+ *   jxb_cnn_accumulate: forward, masked MSE against target, backward; adds the
+ *     parameter gradient to the accumulator and returns the loss.
+ *   jxb_cnn_adam: one Adam step with the accumulated gradient times grad_scale.
+ * jxb_fcg_learned: flexible CG, z = ||r|| out_scale N(in_scale r/||r||, features);
+ *   Jacobi directions take over after `stall` non-improving iterations or a
+ *   non-descent direction. stats->outer = iterations that used the network. */
+typedef struct jxb_cnn jxb_cnn;
+int jxb_cnn_create(int in_ch, int out_ch, const int* channels, uint64_t seed, jxb_cnn** out);
+int jxb_cnn_destroy(jxb_cnn* cnn);
+int jxb_cnn_params(jxb_cnn* cnn, float** params, int64_t* n);
+int jxb_cnn_grads(jxb_cnn* cnn, float** grads, int64_t* n);  /* the gradient accumulator */
+int jxb_cnn_forward(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in, float* out);
+int jxb_cnn_zero_grad(jxb_cnn* cnn, jxb_stream stream);
+int jxb_cnn_accumulate(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in,
+                       const float* target, const float* mask, double* loss);
+int jxb_cnn_adam(jxb_cnn* cnn, jxb_stream stream, float lr, float grad_scale);
+int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
+                    const float* features, int n_features, float in_scale, double out_scale, int stall,
+                    const jxb_solve_opts* opts, jxb_stats* stats);
+
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);
 

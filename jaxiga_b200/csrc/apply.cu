@@ -159,10 +159,7 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
   const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
   constexpr unsigned TILE_BYTES = NE * NG * NQE * sizeof(T);
   if constexpr (MODE == MODE_APPLY) {
-    if (tid == 0) {
-      prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, TILE_BYTES);
-      if (nlayers > 1) prefetch_l2(A.geo + (size_t)(slot_base + NE) * NG * NQE, TILE_BYTES);
-    }
+    if (tid == 0) prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, TILE_BYTES);
   }
 
   // x / y tables and footprint offsets of this brick's elements
@@ -197,8 +194,9 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
     const int offz = fz - cp0z;
     const long long slot = slot_base + (long long)lz * NE + el;
     if constexpr (MODE == MODE_APPLY) {
-      if (tid == 0 && lz + 2 < nlayers)
-        prefetch_l2(A.geo + (size_t)(slot_base + (long long)(lz + 2) * NE) * NG * NQE, TILE_BYTES);
+      // one layer ahead: 296 resident CTAs x one tile stays well inside L2
+      if (tid == 0 && lz + 1 < nlayers)
+        prefetch_l2(A.geo + (size_t)(slot_base + (long long)(lz + 1) * NE) * NG * NQE, TILE_BYTES);
     }
     for (int i = tid; i < 2 * Q * P1; i += NT) stz[i] = A.tab[2][(size_t)ez * 3 * Q * P1 + i];
     if constexpr (MODE == MODE_APPLY) {

@@ -358,7 +358,8 @@ static int get_graph(jxb_plan* plan, cudaStream_t s, int iters, int precond, cud
 // Runs CG on the plan-owned vectors (b given as TB*), solution left in plan x.
 template <typename T, typename TB>
 static int run_cg(jxb_plan* plan, cudaStream_t s, const TB* b, double tol, double atol, long long maxiter,
-                  int precond, int check_every, long long* iters, int* status) {
+                  int precond, int check_every, long long* iters, int* status, double* snaps = nullptr,
+                  long long max_snaps = 0, long long* n_snaps = nullptr) {
   constexpr bool F32 = sizeof(T) == 4;
   T* x = F32 ? (T*)plan->d_x32 : (T*)plan->d_x;
   T* r = F32 ? (T*)plan->d_r32 : (T*)plan->d_r;
@@ -375,11 +376,20 @@ static int run_cg(jxb_plan* plan, cudaStream_t s, const TB* b, double tol, doubl
   long long launches = maxiter / check_every + 2;
   JXB_CUDA(cudaMemcpyAsync(plan->h_state, plan->d_state, sizeof(CgState), cudaMemcpyDeviceToHost, s));
   JXB_CUDA(cudaStreamSynchronize(s));
+  long long ns = 0;
   for (long long l = 0; l < launches && !plan->h_state->done; ++l) {
     JXB_CUDA(cudaGraphLaunch(ge, s));
     JXB_CUDA(cudaMemcpyAsync(plan->h_state, plan->d_state, sizeof(CgState), cudaMemcpyDeviceToHost, s));
     JXB_CUDA(cudaStreamSynchronize(s));
+    if constexpr (sizeof(T) == 8) {
+      if (snaps && ns < max_snaps && !plan->h_state->done) {  // iterate after l+1 graph launches
+        JXB_CUDA(cudaMemcpyAsync(snaps + ns * plan->n_dofs, x, plan->n_dofs * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s));
+        ++ns;
+      }
+    }
   }
+  if (n_snaps) *n_snaps = ns;
   *iters = plan->h_state->k;
   *status = plan->h_state->done ? plan->h_state->status : JXB_ERR_NOT_CONVERGED;
   return JXB_OK;
@@ -531,4 +541,47 @@ extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double*
 extern "C" int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host) {
   if (!plan || !a || !b || !out_host) return fail(JXB_ERR_INVALID, "jxb_dot: null argument");
   return dot(plan, reinterpret_cast<cudaStream_t>(stream), a, b, out_host);
+}
+
+// jxb_pcg with the iterates recorded: after every `every` iterations the current
+// FP64 iterate is copied into snaps[j] (n_dofs doubles each), up to max_snaps.
+// With the converged solution x*, e_j = x* - x_j and r_j = K e_j are the
+// (residual, error) pairs of the solve; they train the learned preconditioner.
+extern "C" int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+                                 const jxb_solve_opts* opts, int every, double* snaps, int64_t max_snaps,
+                                 int64_t* n_snaps, jxb_stats* stats) {
+  if (!plan || !b || !x || !opts || !snaps || !n_snaps || every < 1 || max_snaps < 0)
+    return fail(JXB_ERR_INVALID, "jxb_pcg_snapshots: bad argument");
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+  JXB_CUDA(cudaStreamSynchronize(user));
+  if (!plan->graph_stream[0]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[0], cudaStreamNonBlocking));
+  cudaStream_t s = plan->graph_stream[0];
+  int rc = ensure_workspace(plan, false);
+  if (rc) return rc;
+  int precond = opts->preconditioner ? 1 : 0;
+  if (precond && (rc = compute_invdiag(plan, s))) return rc;
+  long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
+  JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, plan->n_dofs * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  long long iters = 0, ns = 0;
+  int status = 0;
+  rc = run_cg<double, double>(plan, s, plan->d_b, opts->tol, opts->atol, maxiter, precond, every, &iters, &status,
+                              snaps, max_snaps, &ns);
+  if (rc) return rc;
+  JXB_CUDA(cudaMemcpyAsync(x, plan->d_x, plan->n_dofs * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  double rn, bn;
+  bool fin;
+  if ((rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin))) return rc;
+  JXB_CUDA(cudaStreamSynchronize(s));
+  *n_snaps = ns;
+  if (stats) {
+    stats->iterations = iters;
+    stats->outer = 0;
+    stats->residual = rn;
+    stats->b_norm = bn;
+    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
+    stats->finite = fin ? 1 : 0;
+    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
+    stats->seconds = 0;
+  }
+  return status == JXB_ERR_NONFINITE ? fail(JXB_ERR_NONFINITE, "jxb_pcg_snapshots: non-finite") : JXB_OK;
 }

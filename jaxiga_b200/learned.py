@@ -1,0 +1,231 @@
+"""Learned preconditioner: a 3D CNN on the control-point grid inside flexible CG.
+
+Pipeline (all arithmetic in libjxb's kernels; torch holds device memory):
+
+1. ``pairs_from_solve``: one plain FP64 Jacobi-PCG solve records its iterates
+   x_j; with the converged x*, e_j = x* - x_j and r_j = K e_j (exact, one
+   operator application each) are the (residual, error) pairs CG actually
+   meets, early rough residuals and late smooth ones alike.
+2. ``train``: masked MSE between N(in_scale * r_j/||r_j||, features) and
+   e_j / (||r_j|| out_scale), forward and backward through the network's own
+   kernels, Adam on the flat parameter vector.
+3. ``solve``: flexible CG with z = ||r|| out_scale N(in_scale r/||r||) and
+   Jacobi-PCG as the fallback (jxb_fcg_learned).
+
+Weights and scales are saved to / resumed from ``.npz`` files.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class _DeviceArray:
+    """Zero-copy torch view of a raw device pointer (CUDA array interface)."""
+
+    def __init__(self, ptr, n, typestr="<f4"):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _s():
+    import torch
+
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class LearnedPreconditioner:
+    """CNN preconditioner for an :class:`~jaxiga_b200.Operator` on a single patch.
+
+    Parameters
+    ----------
+    op : Operator
+        The operator (its Dirichlet mask defines the free DOFs).
+    features : array (n_feat, n_scalar_basis) or None
+        Static per-control-point input channels, e.g. a normalised log-coefficient.
+    channels : (c0, c1, c2)
+        Channels at the three grid levels.
+    """
+
+    def __init__(self, op, features=None, channels=(8, 16, 48), seed=0):
+        import torch
+
+        self.lib = _lib.load()
+        self.op = op
+        self.vec = op.vec
+        sp = op.space
+        self.grid = (sp.n_cp[0], sp.n_cp[1], sp.n_cp[2] if sp.dim == 3 else 1)
+        self.ncp = sp.n_scalar_basis
+        self.dev = op.device
+        if features is not None:
+            f = torch.as_tensor(np.asarray(features), dtype=torch.float32, device=self.dev).reshape(-1, self.ncp)
+            self.features = f.contiguous()
+        else:
+            self.features = None
+        self.n_feat = 0 if self.features is None else self.features.shape[0]
+        self.channels = tuple(int(c) for c in channels)
+        ch = (ctypes.c_int32 * 3)(*self.channels)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.jxb_cnn_create(self.vec + self.n_feat, self.vec, ch, int(seed), ctypes.byref(h)))
+        self.handle = h
+        ptr, n = ctypes.c_void_p(), ctypes.c_int64()
+        _lib.check(self.lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
+        self.params = torch.as_tensor(_DeviceArray(ptr.value, n.value), device=self.dev)
+        self.n_params = n.value
+        self.in_scale = 1.0
+        self.out_scale = 1.0
+        self.history = []
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.jxb_cnn_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- layout helpers ----------------------------------------------------------
+    def _to_grid(self, v):
+        """DOF vector (vec*i + c) -> [vec, ncp] float32."""
+        return v.reshape(self.ncp, self.vec).t().contiguous().float()
+
+    def _input(self, r_grid):
+        import torch
+
+        if self.features is None:
+            return r_grid.contiguous()
+        return torch.cat([r_grid, self.features], 0).contiguous()
+
+    # -- data ------------------------------------------------------------------
+    def pairs_from_solve(self, b, n_pairs=2000, every=1, tol=1e-12, maxiter=None):
+        """Residual/error pairs of one plain FP64 Jacobi-PCG solve of K x = b.
+
+        Returns (R, E, stats): R, E float32 [n, vec, ncp], each pair scaled by
+        1/||r_j||, the solve's stats, and sets in_scale / out_scale.
+        """
+        import torch
+
+        op = self.op
+        b = op._vec(b)
+        x = op._empty(op.n_dofs)
+        snaps = torch.empty((int(n_pairs), op.n_dofs), dtype=torch.float64, device=self.dev)
+        o = op._opts(tol, 0.0, maxiter, "jacobi", every, 0.0, 0)
+        st = _lib.Stats()
+        ns = ctypes.c_int64()
+        _lib.check(self.lib.jxb_pcg_snapshots(op.handle, _s(), _p(b), _p(x), ctypes.byref(o), int(every),
+                                              _p(snaps), int(n_pairs), ctypes.byref(ns), ctypes.byref(st)))
+        m = ns.value
+        R = torch.empty((m, self.vec, self.ncp), dtype=torch.float32, device=self.dev)
+        E = torch.empty_like(R)
+        for j in range(m):
+            # CG iterates are zero on prescribed DOFs, so e_j is too; the masked
+            # operator gives the exact residual r_j = K e_j of iterate j.
+            e = x - snaps[j]
+            r = op.apply(e)
+            rn = float(torch.linalg.norm(r))
+            R[j] = self._to_grid(r / rn)
+            E[j] = self._to_grid(e / rn)
+        del snaps
+        free = int(op.info["n_free"])
+        self.in_scale = float(np.sqrt(free))
+        self.out_scale = float(torch.sqrt((E.double() ** 2).sum() / max(m * free, 1)))
+        stats = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+        return R, E, stats
+
+    @property
+    def mask(self):
+        """Loss mask on the grid: 1 where any component of the control point is free."""
+        import torch
+
+        free = ~self.op.prescribed_mask.reshape(self.ncp, self.vec)
+        return torch.as_tensor(free.any(axis=1).astype(np.float32), device=self.dev)
+
+    # -- training ----------------------------------------------------------------
+    def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, log=None):
+        """Adam on masked MSE; returns the per-epoch mean losses."""
+        import torch
+
+        g = torch.Generator().manual_seed(seed)
+        nx, ny, nz = self.grid
+        m = R.shape[0]
+        mask = self.mask.contiguous()
+        losses = []
+        for ep in range(epochs):
+            order = torch.randperm(m, generator=g).tolist()
+            tot, cnt = 0.0, 0
+            for i0 in range(0, m, batch):
+                _lib.check(self.lib.jxb_cnn_zero_grad(self.handle, _s()))
+                idx = order[i0:i0 + batch]
+                for j in idx:
+                    inp = self._input(R[j] * self.in_scale)
+                    tgt = (E[j] / self.out_scale).contiguous()
+                    loss = ctypes.c_double()
+                    _lib.check(self.lib.jxb_cnn_accumulate(self.handle, _s(), nx, ny, nz, _p(inp), _p(tgt),
+                                                           _p(mask) if mask is not None else None, ctypes.byref(loss)))
+                    tot += loss.value
+                    cnt += 1
+                _lib.check(self.lib.jxb_cnn_adam(self.handle, _s(), float(lr), 1.0 / len(idx)))
+            losses.append(tot / max(cnt, 1))
+            if log:
+                log(f"epoch {ep}: loss {losses[-1]:.4e}")
+        self.history += losses
+        return losses
+
+    def forward(self, r):
+        """z = ||r|| out_scale N(in_scale r / ||r||) for a DOF vector r (the preconditioner map)."""
+        import torch
+
+        nx, ny, nz = self.grid
+        r = self.op._vec(r)
+        rn = float(torch.linalg.norm(r))
+        inp = self._input(self._to_grid(r / rn) * self.in_scale)
+        out = torch.empty((self.vec, self.ncp), dtype=torch.float32, device=self.dev)
+        _lib.check(self.lib.jxb_cnn_forward(self.handle, _s(), nx, ny, nz, _p(inp), _p(out)))
+        return (out.double().t().reshape(-1) * rn * self.out_scale).contiguous()
+
+    # -- solve -------------------------------------------------------------------
+    def solve(self, b, tol=1e-8, maxiter=None, stall=25):
+        """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats)."""
+        op = self.op
+        b = op._vec(b)
+        x = op._empty(op.n_dofs)
+        o = op._opts(tol, 0.0, maxiter, "jacobi", 16, 0.0, 0)
+        st = _lib.Stats()
+        feats = self.features
+        rc = self.lib.jxb_fcg_learned(op.handle, self.handle, _s(), _p(b), _p(x),
+                                      _p(feats) if feats is not None else None, self.n_feat,
+                                      float(self.in_scale), float(self.out_scale), int(stall),
+                                      ctypes.byref(o), ctypes.byref(st))
+        if rc not in (0, 4):
+            _lib.check(rc)
+        out = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+        out["learned_iterations"] = out.pop("outer")
+        return x, out
+
+    # -- checkpoint / resume -------------------------------------------------------
+    def save(self, path):
+        np.savez(path, params=self.params.cpu().numpy(), in_scale=self.in_scale, out_scale=self.out_scale,
+                 channels=np.asarray(self.channels), vec=self.vec, n_feat=self.n_feat,
+                 history=np.asarray(self.history))
+
+    def load(self, path):
+        import torch
+
+        d = np.load(path)
+        if tuple(d["channels"]) != self.channels or int(d["vec"]) != self.vec or int(d["n_feat"]) != self.n_feat:
+            raise ValueError("checkpoint does not match this network's shape")
+        self.params.copy_(torch.as_tensor(d["params"], device=self.dev))
+        self.in_scale = float(d["in_scale"])
+        self.out_scale = float(d["out_scale"])
+        self.history = list(d["history"])

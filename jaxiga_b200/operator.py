@@ -103,6 +103,8 @@ class Operator:
                 raise ValueError("prescribed mask must have n_dofs entries")
             self._keep.append(pm)
             d.prescribed = _hptr(pm, ctypes.c_uint8)
+        self.prescribed_mask = (np.zeros(space.n_scalar_basis * self.vec, bool) if prescribed is None
+                                else np.asarray(prescribed).astype(bool).copy())
         d.want_f32 = 1 if want_f32 else 0
         handle = ctypes.c_void_p()
         _lib.check(self.lib.jxb_plan_create(ctypes.byref(d), ctypes.byref(handle)))
