@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--span", type=int, default=None, help="elements per direction (default 64, Darcy 96)")
-    ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy"],
+    ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy", "plate"],
                     help="elasticity: 3D elasticity 64^3 (the headline); darcy: 3D Darcy 96^3")
     return ap.parse_args()
 
@@ -201,8 +201,15 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
     darcy = args.workload == "darcy"
-    span = args.span or (96 if darcy else N_SPAN)
-    if darcy:
+    plate = args.workload == "plate"
+    span = args.span or (96 if darcy else 256 if plate else N_SPAN)
+    if plate:
+        V, problem, params = workloads.config5(n=span)
+        pres, vals = problem.resolve_dirichlet(params)
+        mask = np.zeros(V.n_dofs, bool)
+        mask[pres] = True
+        op = jx.Operator(V, "plate", problem.operator_coefficients(params)[0], prescribed=mask, want_f32=True)
+    elif darcy:
         V, problem, params = workloads.config4(n=span)
         geo0 = geometry_operator(V)
         a_qp = torch.exp(geo0.interpolate(params["loga"])[..., 0])
@@ -219,7 +226,7 @@ def run_ours(args, rank, world, local_rank):
         op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
     setup_s = time.perf_counter() - t_setup
     n = V.n_dofs
-    n_qp = V.n_elems * 64
+    n_qp = V.n_elems * (25 if plate else 64)
     vec = V.vec
     gen = torch.Generator(device=dev).manual_seed(1234 + rank)
     x = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
@@ -259,8 +266,11 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = 8 * 2 * n + 8 * n_qp * ngeo
     alg_bytes32 = 4 * 2 * n + 4 * n_qp * ngeo
     # survey formula: n_e vec 2*2*d^2 (p+1)^(d+1) + N_qp c_pt, c_pt = 2 d^4 (elasticity) or 2 d^2 (scalar)
-    p1, q = 4, 4
-    flops = V.n_elems * vec * (2 * 2 * 9 * p1**3 * q) + n_qp * (2 * 81 if vec == 3 else 2 * 9)
+    if plate:  # 2D, p = 4: 2*2*d^2*(p+1)^(d+1) x 2.5 for the Hessian channels, 2 * 15 per point
+        flops = int(V.n_elems * 2 * 2 * 4 * 5**3 * 2.5 + n_qp * 2 * 15)
+    else:
+        p1, q = 4, 4
+        flops = V.n_elems * vec * (2 * 2 * 9 * p1**3 * q) + n_qp * (2 * 81 if vec == 3 else 2 * 9)
     peaks, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
     traffic = profile_traffic()
@@ -268,7 +278,8 @@ def run_ours(args, rank, world, local_rank):
         "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
         "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-        "kernel": "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if darcy else "elasticity"),
+        "kernel": ("k_brick2<double,4,5,plate> (brick apply)" if plate else
+                   "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if darcy else "elasticity")),
         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
         "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
         "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
@@ -302,7 +313,7 @@ def run_ours(args, rank, world, local_rank):
     tts = None
     if not args.no_solve:
         geo = geometry_operator(V)
-        if darcy:
+        if darcy or plate:
             F = op.load(torch.ones(n_qp, dtype=torch.float64, device=dev))
         else:
             fq = geo.interpolate(params["eta"])
@@ -333,7 +344,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{'darcy3d' if darcy else 'elasticity3d'}_p3_{span}^3", "n_dofs": n,
+            "config": {"workload": (f"plate2d_p4_{span}^2" if plate else
+                                    f"{'darcy3d' if darcy else 'elasticity3d'}_p3_{span}^3"), "n_dofs": n,
                        "elements": V.n_elems,
                        "gauss_points": n_qp, "operator": "matrix-free sum-factorised K.u, FP64, masked",
                        "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),

@@ -78,6 +78,8 @@ typedef struct jxb_desc {
   const double* coef_qp;        /* optional (n_elem, n_quad^dim) per-point a0 (PointField); NULL = coef[0] */
   const uint8_t* prescribed;    /* optional (n_dofs,) 1 = Dirichlet DOF; NULL = none */
   int want_f32;                 /* also keep FP32 copies of the point factors (mixed precision) */
+  int tile[2];                  /* 2D scalar operator: brick shape (elements per row, rows); {0,0} = default.
+                                   Supported: {32,8} {16,8} {32,16} {64,4} (picked by the batch autotuner) */
 } jxb_desc;
 
 typedef struct jxb_info {
@@ -166,6 +168,22 @@ int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double*
 int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                       const jxb_solve_opts* opts, int every, double* snaps, int64_t max_snaps,
                       int64_t* n_snaps, jxb_stats* stats);
+
+/* ---- batches of independent problems -------------------------------------
+ * The B200 form of the reference's vmap-over-params batching
+ * (tests/test_advanced.py:338-356; host SciPy solves run once per member,
+ * src/jaxiga/solvers/linear.py:147-149): 2D Poisson plans of any degree and
+ * size, their DOF vectors concatenated in plan order (jxb_batch_size gives the
+ * offsets), solved by Jacobi-PCG per instance with per-instance scalars and
+ * convergence, every iteration of the whole batch captured in one CUDA graph.
+ * stats receives one jxb_stats per instance; *seconds the device time. */
+typedef struct jxb_batch jxb_batch;
+int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out);
+int jxb_batch_destroy(jxb_batch* batch);
+int jxb_batch_size(const jxb_batch* batch, int64_t* total_dofs, int64_t* offsets /* n+1 or NULL */);
+int jxb_batch_apply(jxb_batch* batch, jxb_stream stream, const double* x, double* y);
+int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
+                  jxb_stats* stats, double* seconds);
 
 /* ---- learned preconditioner ---------------------------------------------
  * A 3D convolutional network on the control-point grid (FP32 weights and

@@ -45,6 +45,7 @@ class Desc(ctypes.Structure):
         ("coef_qp", c_double_p),
         ("prescribed", ctypes.POINTER(ctypes.c_uint8)),
         ("want_f32", ctypes.c_int),
+        ("tile", ctypes.c_int * 2),
     ]
 
 
@@ -108,6 +109,12 @@ SIGNATURES = [
     ("jxb_pcg_snapshots", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                            ctypes.POINTER(SolveOpts), ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
                            c_int64_p, ctypes.POINTER(Stats)]),
+    ("jxb_batch_create", [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_batch_destroy", [ctypes.c_void_p]),
+    ("jxb_batch_size", [ctypes.c_void_p, c_int64_p, c_int64_p]),
+    ("jxb_batch_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_batch_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats), c_double_p]),
     ("jxb_cnn_create", [ctypes.c_int, ctypes.c_int, c_int32_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_cnn_destroy", [ctypes.c_void_p]),
     ("jxb_cnn_params", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_int64_p]),

@@ -92,25 +92,6 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// ---------------------------------------------------------------------------
-// kernel arguments
-// ---------------------------------------------------------------------------
-template <typename T>
-struct BrickArgs {
-  Bricks br;
-  const T* tab[3];
-  const T* geo;          // (slots, ngeo, nqe)
-  const double* wq;      // load weights (slots, nqe)
-  const T* wgts;         // NURBS weights (rational)
-  const uint8_t* keep;   // (n_dofs) 1 = free
-  const T* x;            // input DOF vector
-  const double* f_qp;    // load: source values, reference order
-  T* scratch;            // (n_bricks, vec, fp2, fp1, fp0)
-  const CgState* state;  // optional: skip all work once done
-  int masked;
-  int* err;
-  double lam, mu;
-};
 
 // ---------------------------------------------------------------------------
 // 3D brick kernel
@@ -644,10 +625,15 @@ static size_t smem3(const Bricks& br) {
   return n * sizeof(T) + (TX + TY) * sizeof(int) + 64;
 }
 
+int tile2_variant(int tx, int ty) {
+  for (int v = 0; v < N_TILE2; ++v)
+    if (TILE2[v][0] == tx && TILE2[v][1] == ty) return v;
+  return -1;
+}
+
 template <typename T, int P, int Q, int OPK, bool RAT, int MODE>
-static size_t smem2(const Bricks& br) {
+static size_t smem2(const Bricks& br, const int TX) {
   constexpr int P1 = P + 1, PP = P1 * P1;
-  constexpr int TX = BrickShape<2, P>::TX;
   constexpr int VEC = OPK == OPK_ELAST ? 2 : 1;
   constexpr int NK = OPK == OPK_PLATE ? 3 : 2;
   constexpr int SX = P1 + 1;
@@ -672,12 +658,27 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
       k<<<(unsigned)br.n_bricks, NT, sm, s>>>(A);
     }
   } else {
-    constexpr int NT = BrickShape<2, P>::TX * Q;
-    size_t sm = smem2<T, P, Q, OPK, RAT, MODE>(br);
-    if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "2D brick does not fit in shared memory");
-    auto k = k_brick2<T, P, Q, OPK, RAT, MODE>;
-    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k<<<(unsigned)br.n_bricks, NT, sm, s>>>(A);
+    const int v = tile2_variant(br.te[0], br.te[1]);
+    if (v < 0) return fail(JXB_ERR_INVALID, "unsupported 2D brick shape");
+    if constexpr (OPK != OPK_SCALAR) {
+      if (v != 0) return fail(JXB_ERR_INVALID, "tile variants are available for the 2D scalar operator only");
+    }
+#define JXB_TILE2(V_)                                                                                   \
+  if (v == V_) {                                                                                        \
+    constexpr int TXv = TILE2[V_][0], TYv = TILE2[V_][1];                                               \
+    size_t sm = smem2<T, P, Q, OPK, RAT, MODE>(br, TXv);                                                \
+    if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "2D brick does not fit in shared memory");        \
+    auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv, TYv>;                                               \
+    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+    k<<<(unsigned)br.n_bricks, TXv * Q, sm, s>>>(A);                                                    \
+  }
+    JXB_TILE2(0)
+    if constexpr (OPK == OPK_SCALAR) {
+      JXB_TILE2(1)
+      JXB_TILE2(2)
+      JXB_TILE2(3)
+    }
+#undef JXB_TILE2
   }
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
@@ -758,6 +759,85 @@ int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* do
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }
+
+// Batched 2D scalar apply: block i runs brick work[i].y of instance work[i].x.
+template <int P, bool RAT>
+static int launch_batch_p(int variant, const BrickArgs<double>* d_args, const int2* d_work, long long n_work,
+                          int fp0, int fp1, const CgState* d_states, cudaStream_t s) {
+  constexpr int Q = P + 1;
+  Bricks br{};
+  br.fp[0] = fp0;
+  br.fp[1] = fp1;
+#define JXB_BTILE(V_)                                                                                   \
+  if (variant == V_) {                                                                                  \
+    constexpr int TXv = TILE2[V_][0], TYv = TILE2[V_][1];                                               \
+    size_t sm = smem2<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY>(br, TXv);                              \
+    if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");   \
+    auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv, TYv>;                       \
+    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+    k<<<(unsigned)n_work, TXv * Q, sm, s>>>(d_args, d_work, d_states);                                  \
+    JXB_CUDA(cudaGetLastError());                                                                       \
+    return JXB_OK;                                                                                      \
+  }
+  JXB_BTILE(0)
+  JXB_BTILE(1)
+  JXB_BTILE(2)
+  JXB_BTILE(3)
+#undef JXB_BTILE
+  return fail(JXB_ERR_INVALID, "unknown tile variant");
+}
+
+int launch_bricks2_batch(int p, bool rational, int variant, const BrickArgs<double>* d_args, const int2* d_work,
+                         long long n_work, int fp0, int fp1, const CgState* d_states, cudaStream_t s) {
+  if (n_work <= 0) return JXB_OK;
+#define JXB_BP(P_) \
+  case P_:         \
+    return rational ? launch_batch_p<P_, true>(variant, d_args, d_work, n_work, fp0, fp1, d_states, s) \
+                    : launch_batch_p<P_, false>(variant, d_args, d_work, n_work, fp0, fp1, d_states, s);
+  switch (p) {
+    JXB_BP(1)
+    JXB_BP(2)
+    JXB_BP(3)
+    JXB_BP(4)
+    JXB_BP(5)
+    default:
+      return fail(JXB_ERR_INVALID, "degree must be in 1..5");
+  }
+#undef JXB_BP
+}
+
+template <typename T>
+BrickArgs<T> make_brick_args(jxb_plan* plan, const T* x, const CgState* state, int masked) {
+  BrickArgs<T> A;
+  A.br = plan->br;
+  constexpr bool F32 = sizeof(T) == 4;
+  for (int d = 0; d < 3; ++d) {
+    if constexpr (F32)
+      A.tab[d] = plan->d_tab32[d];
+    else
+      A.tab[d] = plan->d_tab[d];
+  }
+  if constexpr (F32) {
+    A.geo = plan->d_geo32;
+    A.wgts = plan->d_wgts32;
+    A.scratch = plan->d_scratch32;
+  } else {
+    A.geo = plan->d_geo;
+    A.wgts = plan->d_wgts;
+    A.scratch = plan->d_scratch;
+  }
+  A.wq = plan->d_wq;
+  A.keep = plan->d_keep;
+  A.x = x;
+  A.f_qp = nullptr;
+  A.state = state;
+  A.masked = masked;
+  A.err = reinterpret_cast<int*>(plan->d_red + 4 * JXB_RED_BLOCKS);
+  A.lam = plan->mat.lam;
+  A.mu = plan->mat.mu;
+  return A;
+}
+template BrickArgs<double> make_brick_args<double>(jxb_plan*, const double*, const CgState*, int);
 
 template int launch_bricks<double>(jxb_plan*, cudaStream_t, int, const double*, const double*,
                                    const CgState*, int);

@@ -2,10 +2,12 @@
 // Q threads per element; x contraction through shared memory, y in registers.
 #pragma once
 
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE>
-__global__ void __launch_bounds__(BrickShape<2, P>::TX* Q) k_brick2(BrickArgs<T> A) {
+// The body of one brick (element rows [by*TY, +TY) x columns [bx*TX, +TX)).
+// TX / TY are template parameters so that the autotuner can pick them per
+// degree; the host brick decomposition of the plan must use the same shape.
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+__device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long long b) {
   constexpr int P1 = P + 1, PP = P1 * P1;
-  constexpr int TX = BrickShape<2, P>::TX, TY = BrickShape<2, P>::TY;
   constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
   constexpr int VEC = OPK == OPK_ELAST ? 2 : 1;
   constexpr int NG = GeoCount<OPK, RAT, 2>::value;
@@ -28,7 +30,6 @@ __global__ void __launch_bounds__(BrickShape<2, P>::TX* Q) k_brick2(BrickArgs<T>
   int* soff = reinterpret_cast<int*>(acc + VEC * fp0 * fp1);
 
   const int tid = threadIdx.x;
-  const long long b = blockIdx.x;
   const int bx = (int)(b % br.nb[0]);
   const int by = (int)(b / br.nb[0]);
   const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by];
@@ -331,5 +332,25 @@ __global__ void __launch_bounds__(BrickShape<2, P>::TX* Q) k_brick2(BrickArgs<T>
   }
   T* out = A.scratch + (size_t)b * accn;
   for (int i = tid; i < accn; i += NT) out[i] = acc[i];
+}
+
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+__global__ void __launch_bounds__(TX* Q) k_brick2(BrickArgs<T> A) {
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX, TY>(A, blockIdx.x);
+}
+
+// Many instances in one launch: block i processes brick work[i].y of instance
+// work[i].x, whose arguments are args[work[i].x]; instances already converged
+// (states[inst].done) are skipped.
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+__global__ void __launch_bounds__(TX* Q)
+    k_brick2_batch(const BrickArgs<T>* __restrict__ args, const int2* __restrict__ work,
+                   const CgState* __restrict__ states) {
+  __shared__ BrickArgs<T> sA;
+  const int2 w = work[blockIdx.x];
+  if (states && states[w.x].done) return;
+  if (threadIdx.x == 0) sA = args[w.x];
+  __syncthreads();
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX, TY>(sA, w.y);
 }
 

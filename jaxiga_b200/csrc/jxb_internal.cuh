@@ -73,10 +73,28 @@ struct Bricks {
   long long slots;       // element slots (bricks * elems per brick)
 };
 
+// Arguments of one brick launch (one plan), passed by value or, for batched
+// launches, read by each CTA from a device array.
 template <typename T>
-struct Tables {  // per direction [span][3][Q][P+1]: values, d/dxi, d2/dxi2
-  const T* t[3];
+struct BrickArgs {
+  Bricks br;
+  const T* tab[3];       // per direction [span][3][Q][P+1]: values, d/dxi, d2/dxi2
+  const T* geo;          // (slots, ngeo, nqe)
+  const double* wq;      // load weights (slots, nqe)
+  const T* wgts;         // NURBS weights (rational)
+  const uint8_t* keep;   // (n_dofs) 1 = free
+  const T* x;            // input DOF vector
+  const double* f_qp;    // load: source values, reference order
+  T* scratch;            // (n_bricks, vec, fp2, fp1, fp0)
+  const CgState* state;  // optional: skip all work once done
+  int masked;
+  int* err;
+  double lam, mu;
 };
+
+// 2D brick shapes (elements per row TX, rows per brick TY) the autotuner may pick.
+constexpr int N_TILE2 = 4;
+constexpr int TILE2[N_TILE2][2] = {{32, 8}, {16, 8}, {32, 16}, {64, 4}};
 
 }  // namespace jxb
 
@@ -139,6 +157,12 @@ int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const do
 template <typename T>
 int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* dot_with,
                    double* partials, const CgState* state);
+
+int tile2_variant(int tx, int ty);
+template <typename T>
+BrickArgs<T> make_brick_args(jxb_plan* plan, const T* x, const CgState* state, int masked);
+int launch_bricks2_batch(int p, bool rational, int variant, const BrickArgs<double>* d_args, const int2* d_work,
+                         long long n_work, int fp0, int fp1, const CgState* d_states, cudaStream_t s);
 
 // pcg.cu
 int ensure_workspace(jxb_plan* plan, bool f32);

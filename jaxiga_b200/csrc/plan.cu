@@ -157,6 +157,14 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
   br.p = P->p;
   br.q = P->q;
   host_brick_shape(P->dim, P->p, br.te);
+  if (P->dim == 2 && (desc->tile[0] > 0 || desc->tile[1] > 0)) {
+    if (tile2_variant(desc->tile[0], desc->tile[1]) < 0 || P->op != JXB_OP_POISSON) {
+      delete P;
+      return fail(JXB_ERR_INVALID, "tile: unsupported 2D brick shape (scalar operator only)");
+    }
+    br.te[0] = desc->tile[0];
+    br.te[1] = desc->tile[1];
+  }
   std::vector<int> cover_h[3], bcp0_h[3];
   long long nb_total = 1;
   for (int d = 0; d < 3; ++d) {

@@ -46,7 +46,7 @@ class Operator:
     OPS = {"poisson": _lib.OP_POISSON, "elasticity": _lib.OP_ELASTICITY, "plate": _lib.OP_PLATE}
 
     def __init__(self, space, op="poisson", coef=(1.0,), prescribed=None, coef_qp=None,
-                 want_f32=False, plane_strain=False, vec=None):
+                 want_f32=False, plane_strain=False, vec=None, tile=None):
         import torch
 
         if not torch.cuda.is_available():
@@ -106,6 +106,9 @@ class Operator:
         self.prescribed_mask = (np.zeros(space.n_scalar_basis * self.vec, bool) if prescribed is None
                                 else np.asarray(prescribed).astype(bool).copy())
         d.want_f32 = 1 if want_f32 else 0
+        if tile is not None:
+            d.tile[0], d.tile[1] = int(tile[0]), int(tile[1])
+        self.tile = tuple(tile) if tile is not None else None
         handle = ctypes.c_void_p()
         _lib.check(self.lib.jxb_plan_create(ctypes.byref(d), ctypes.byref(handle)))
         self._keep = []

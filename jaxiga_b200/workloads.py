@@ -76,6 +76,34 @@ def config2(n=64, interpolate=None):
     return V, problem, params
 
 
+def config3(n_instances=256, interpolate=None, span_range=(8, 128)):
+    """Quarter annuli (inner radius 1, outer 2): degree ~ U{2,3,4}, spans per
+    direction log-uniform in span_range, a0 ~ LogNormal(0, 0.5), source
+    sum_k c_k R_k with c ~ N(0, 1) per control point, u = 0 on all four sides.
+
+    Returns (problems, params_list); params carry the source coefficients
+    ("c") and, with ``interpolate(space, coef)``, the source as a PointField.
+    """
+    g = rng(3)
+    problems, params = [], []
+    lo, hi = np.log(span_range[0]), np.log(span_range[1])
+    for _ in range(n_instances):
+        p = int(g.integers(2, 5))
+        n = [int(round(np.exp(g.uniform(lo, hi)))) for _ in range(2)]
+        a0 = float(g.lognormal(0.0, 0.5))
+        patch = primitives.quarter_annulus(1.0, 2.0).elevate(p).insert_knots(uniform_knots(n[0]), uniform_knots(n[1]))
+        V = FunctionSpace(patch)
+        c = g.standard_normal(V.n_scalar_basis)
+        bcs = [DirichletBC(0.0, where=s) for s in ("inner", "outer", "sym_y", "sym_x")]
+        pr = Poisson(V, dirichlet=bcs, source=lambda x, pa: pa["f"])
+        pa = {"a0": a0, "c": c}
+        if interpolate is not None:
+            pa["f"] = PointField(interpolate(V, c)[..., 0])
+        problems.append(pr)
+        params.append(pa)
+    return problems, params
+
+
 def config4(n=96, interpolate=None):
     kn = uniform_knots(n)
     V = FunctionSpace(primitives.cuboid([0, 0, 0], [1, 1, 1]).elevate(3).insert_knots(kn, kn, kn))
