@@ -131,6 +131,18 @@ int jxb_version(void);
  */
 int jxb_apply(jxb_plan* plan, jxb_stream stream, const double* x, double* y, int masked);
 int jxb_apply_f32(jxb_plan* plan, jxb_stream stream, const float* x, float* y);
+/* jxb_apply_static: the same result as jxb_apply, for callers that must not
+ *   allocate device memory when they apply the operator (a handler inside a
+ *   framework that owns every device allocation, a loop where an allocation's
+ *   implicit synchronisation is unacceptable). The brick partial sums go to one
+ *   fixed 16 MiB device array per GPU, present from library load to process
+ *   exit, instead of the plan's scratch; plans needing more are rejected with
+ *   JXB_ERR_INVALID. This call allocates nothing. Its first call on a device
+ *   looks up the array's address (cudaGetSymbolAddress) and should come before
+ *   any stream capture. All calls share the array: calls that overlap on the
+ *   GPU race and must be ordered on one stream. No counterpart in the
+ *   reference, which has no device kernels. */
+int jxb_apply_static(jxb_plan* plan, jxb_stream stream, const double* x, double* y, int masked);
 int jxb_diag(jxb_plan* plan, jxb_stream stream, double* d);
 
 /* ---- fields at quadrature points ---------------------------------------

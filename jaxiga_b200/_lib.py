@@ -97,6 +97,7 @@ SIGNATURES = [
     ("jxb_version", []),
     ("jxb_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     ("jxb_apply_f32", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_apply_static", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     ("jxb_diag", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_qp_coords", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_interpolate", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
