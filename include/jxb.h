@@ -202,29 +202,41 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  * activations, hand-written kernels), used inside flexible CG. No counterpart
  * in the reference, whose only preconditioner is Jacobi
  * (src/jaxiga/solvers/linear.py:419-431).
- *   jxb_cnn_create: in_ch input channels (residual components, then features),
- *     out_ch outputs (= vec), channels[3] per level (each in {4,8,12,16,24,32,48}).
- *   jxb_cnn_params: device pointer to the flat FP32 parameter vector and its length.
+ *   jxb_cnn_create: a U-Net with `levels` (2..6) levels, channels[levels] per
+ *     level (each in {4,8,12,16,24,32,48,64}); in_ch input channels (residual
+ *     components, then features), out_ch outputs (= vec).
+ *   jxb_cnn_params / jxb_cnn_grads: device pointer to the flat FP32 parameter
+ *     vector / gradient accumulator and its length.
  *   jxb_cnn_forward: out[out_ch][nz][ny][nx] = N(in[in_ch][nz][ny][nx]).
- *   jxb_cnn_accumulate: forward, masked MSE against target, backward; adds the
- *     parameter gradient to the accumulator and returns the loss.
+ *   jxb_cnn_backward: adds to the accumulator the parameter gradient of
+ *     sum(gout * N(in)); must follow a forward on the same input and dims.
+ *   jxb_cnn_accumulate: forward, masked MSE against target, backward; returns the loss.
+ *   jxb_cnn_accumulate_energy: forward, then with d = P_f (e - out_scale N(in))
+ *     (grid -> DOF layout, 0 on prescribed DOFs) the loss weight * d^T K d of
+ *     the plan's operator K; adds its parameter gradient and returns the loss.
  *   jxb_cnn_adam: one Adam step with the accumulated gradient times grad_scale.
- * jxb_fcg_learned: flexible CG, z = ||r|| out_scale N(in_scale r/||r||, features);
- *   Jacobi directions take over after `stall` non-improving iterations or a
- *   non-descent direction. stats->outer = iterations that used the network. */
+ * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
+ *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
+ *   Jacobi directions take over after `stall` learned iterations without a new
+ *   lowest residual or a non-descent direction. mixed != 0: FP32 inner solves
+ *   (inner_tol) inside FP64 iterative refinement (plan created with want_f32).
+ *   stats->outer = iterations that used the network. */
 typedef struct jxb_cnn jxb_cnn;
-int jxb_cnn_create(int in_ch, int out_ch, const int* channels, uint64_t seed, jxb_cnn** out);
+int jxb_cnn_create(int in_ch, int out_ch, int levels, const int* channels, uint64_t seed, jxb_cnn** out);
 int jxb_cnn_destroy(jxb_cnn* cnn);
 int jxb_cnn_params(jxb_cnn* cnn, float** params, int64_t* n);
-int jxb_cnn_grads(jxb_cnn* cnn, float** grads, int64_t* n);  /* the gradient accumulator */
+int jxb_cnn_grads(jxb_cnn* cnn, float** grads, int64_t* n);
 int jxb_cnn_forward(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in, float* out);
+int jxb_cnn_backward(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in, const float* gout);
 int jxb_cnn_zero_grad(jxb_cnn* cnn, jxb_stream stream);
 int jxb_cnn_accumulate(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in,
                        const float* target, const float* mask, double* loss);
+int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in, const float* e,
+                              float out_scale, double weight, double* loss);
 int jxb_cnn_adam(jxb_cnn* cnn, jxb_stream stream, float lr, float grad_scale);
 int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                     const float* features, int n_features, float in_scale, double out_scale, int stall,
-                    const jxb_solve_opts* opts, jxb_stats* stats);
+                    int depth, int mixed, const jxb_solve_opts* opts, jxb_stats* stats);
 
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);

@@ -116,19 +116,24 @@ SIGNATURES = [
     ("jxb_batch_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_batch_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats), c_double_p]),
-    ("jxb_cnn_create", [ctypes.c_int, ctypes.c_int, c_int32_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_cnn_create", [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int32_p, ctypes.c_uint64,
+                        ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_cnn_destroy", [ctypes.c_void_p]),
     ("jxb_cnn_params", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_int64_p]),
     ("jxb_cnn_grads", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_int64_p]),
     ("jxb_cnn_forward", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                          ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_cnn_backward", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_cnn_zero_grad", [ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_cnn_accumulate", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
+    ("jxb_cnn_accumulate_energy", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_float, ctypes.c_double, c_double_p]),
     ("jxb_cnn_adam", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float]),
     ("jxb_fcg_learned", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                          ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_int,
-                         ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_dot", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
     ("jxb_profile_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                            ctypes.c_int, c_double_p]),

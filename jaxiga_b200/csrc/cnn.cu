@@ -1,176 +1,260 @@
-// A small 3D convolutional network on the control-point grid, used as a
-// learned preconditioner inside flexible CG (the fourth AI-systems form of
-// the solver; it has no counterpart in the reference, whose preconditioner
-// is Jacobi, src/jaxiga/solvers/linear.py:419-431).
+// A 3D convolutional network on the control-point grid, used as a learned
+// preconditioner inside flexible CG (the fourth AI-systems form of the
+// solver; it has no counterpart in the reference, whose preconditioner is
+// Jacobi, src/jaxiga/solvers/linear.py:419-431).
 //
-// Topology (channels c0, c1, c2; every conv 3x3x3 with zero padding unless
-// marked 1x1; "relu" = rectified output):
+// Topology: a U-Net with L levels (2..6) and channels c[0..L-1]; every conv
+// is 3x3x3 with zero padding unless marked 1x1, "relu" = rectified output:
 //
-//   level 0 (n0)          level 1 (n1 = ceil(n0/2))     level 2 (n2 = ceil(n1/2))
-//   in  -> c0 relu        pool(s0) -> c1 relu           pool(s1) -> c2 relu
-//   c0  -> c0 relu = s0   c1 -> c1 relu = s1            c2 -> c2 relu
-//                                                      c2 -> c2 relu
-//                         up -> 1x1 c2->c1 (+ s1)
-//                         c1 -> c1 relu
-//   up -> 1x1 c1->c0 (+ s0)
-//   c0 -> c0 relu
-//   c0 -> out (linear)
+//   encoder, l = 0..L-2:  x -> c[l] relu;  c[l] -> c[l] relu = s_l;  x = pool(s_l)
+//   bottom, level L-1:    x -> c[L-1] relu;  two more c[L-1] -> c[L-1] relu
+//   decoder, l = L-2..0:  y = up(y);  m_l = 1x1 c[l+1] -> c[l] (y) + s_l;
+//                         y = c[l] -> c[l] relu (m_l)
+//   output:               c[0] -> 4 (linear; the first out_ch channels are used)
 //
-// Pooling averages the (up to eight) children of a coarse voxel; upsampling
-// copies a coarse voxel to its children. All kernels are FP32 with
-// deterministic reductions (fixed partial-sum grids), so training is
-// reproducible run to run. Activations are [channel][z][y][x].
+// Level l has ceil(n/2^l) voxels per direction. Pooling averages the (up to
+// eight) children of a coarse voxel; upsampling copies a coarse voxel to its
+// children. Activations are [channel][z][y][x], FP32.
+//
+// Convolutions (forward and data gradient) use one kernel: a CTA computes a
+// 16 x 8 x 4 voxel tile for a block of up to 16 output channels; each thread
+// owns one (x, y) column of 4 voxels along z, so the three z taps reuse
+// registers and a warp reads consecutive x from shared memory. Input halos
+// and weights are staged in shared memory four input channels at a time.
+// Weight gradients are per-tile partials (one thread per input channel and
+// tap, the block's output channels in registers) summed over tiles in a
+// fixed order, so training is bitwise reproducible run to run.
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
 #include "jxb_internal.cuh"
 
-struct jxb_cnn;
-
 namespace jxb {
 namespace cnn {
 
-constexpr int TXV = 8, TYV = 8, TZV = 4, TV = TXV * TYV * TZV;  // output tile of the conv kernels
+constexpr int CTX = 16, CTY = 8, CTZ = 4;  // voxel tile of the conv kernels
+constexpr int CT = CTX * CTY;              // threads per CTA (one z column of CTZ voxels each)
+constexpr int CIB = 4;                     // input channels staged per pass
+constexpr int MAXL = 6;
+
 struct Dims {
   int nx, ny, nz;
   __host__ __device__ long long vox() const { return (long long)nx * ny * nz; }
 };
 
 static Dims half(Dims d) { return {(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2}; }
+static long long n_tiles(Dims d) {
+  return (long long)((d.nx + CTX - 1) / CTX) * ((d.ny + CTY - 1) / CTY) * ((d.nz + CTZ - 1) / CTZ);
+}
 
 // out[co] = b[co] + sum_ci sum_k w[co][ci][k] in[ci](v + k)   (+ add[co]) (relu)
-// K = 3 (27 taps, zero padding) or K = 1. One thread per output voxel, all
-// output channels in registers; input halo tile and weights of one input
-// channel at a time in shared memory. beta: out = beta * out + result.
-template <int K, int CO>
-__global__ void __launch_bounds__(TV) k_conv(Dims d, int ci_n, const float* __restrict__ in, const float* __restrict__ w,
+// for co in [co0, co0 + COB), co0 = blockIdx.y * COB. K = 3 (27 taps,
+// k = dx + 3 dy + 9 dz) or 1. beta: out = beta * out + result.
+template <int K, int COB>
+__global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __restrict__ in, const float* __restrict__ w,
                                             const float* __restrict__ bias, const float* __restrict__ add, int relu,
                                             float beta, float* __restrict__ out) {
-  constexpr int R = K / 2, HX = TXV + 2 * R, HY = TYV + 2 * R, HZ = TZV + 2 * R, KK = K * K * K;
-  __shared__ __align__(16) float tile[HZ * HY * HX];
-  __shared__ __align__(16) float sw[KK * CO];  // [k][co]
-  const int tx = threadIdx.x % TXV, ty = (threadIdx.x / TXV) % TYV, tz = threadIdx.x / (TXV * TYV);
-  const int ntx = (d.nx + TXV - 1) / TXV, nty = (d.ny + TYV - 1) / TYV;
+  constexpr int R = K / 2, HX = CTX + 2 * R, HY = CTY + 2 * R, HZ = CTZ + 2 * R, KK = K * K * K;
+  constexpr int HV = HX * HY * HZ;
+  __shared__ __align__(16) float tile[CIB * HV];
+  __shared__ __align__(16) float sw[CIB * KK * COB];  // [c][k][co]
+  const int tx = threadIdx.x % CTX, ty = threadIdx.x / CTX;
+  const int ntx = (d.nx + CTX - 1) / CTX, nty = (d.ny + CTY - 1) / CTY;
   const int bx = blockIdx.x % ntx, by = (blockIdx.x / ntx) % nty, bz = blockIdx.x / (ntx * nty);
-  const int x = bx * TXV + tx, y = by * TYV + ty, z = bz * TZV + tz;
-  const bool valid = x < d.nx && y < d.ny && z < d.nz;
+  const int co0 = blockIdx.y * COB;
   const long long vox = d.vox();
-  float acc[CO];
+  float acc[CTZ][COB];
 #pragma unroll
-  for (int co = 0; co < CO; ++co) acc[co] = bias ? bias[co] : 0.f;
-  for (int ci = 0; ci < ci_n; ++ci) {
-    for (int i = threadIdx.x; i < HZ * HY * HX; i += TV) {
-      int hx = i % HX, hy = (i / HX) % HY, hz = i / (HX * HY);
-      int gx = bx * TXV + hx - R, gy = by * TYV + hy - R, gz = bz * TZV + hz - R;
+  for (int c = 0; c < COB; ++c) {
+    const float b0 = bias ? bias[co0 + c] : 0.f;
+#pragma unroll
+    for (int j = 0; j < CTZ; ++j) acc[j][c] = b0;
+  }
+  for (int ci0 = 0; ci0 < ci_n; ci0 += CIB) {
+    const int nc = min(CIB, ci_n - ci0);
+    for (int i = threadIdx.x; i < nc * HV; i += CT) {
+      const int c = i / HV, r = i % HV;
+      const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
+      const int gx = bx * CTX + hx - R, gy = by * CTY + hy - R, gz = bz * CTZ + hz - R;
       float v = 0.f;
       if (gx >= 0 && gy >= 0 && gz >= 0 && gx < d.nx && gy < d.ny && gz < d.nz)
-        v = in[(long long)ci * vox + ((long long)gz * d.ny + gy) * d.nx + gx];
+        v = in[(long long)(ci0 + c) * vox + ((long long)gz * d.ny + gy) * d.nx + gx];
       tile[i] = v;
     }
-    for (int i = threadIdx.x; i < KK * CO; i += TV) {
-      int k = i / CO, co = i % CO;
-      sw[i] = w[((long long)co * ci_n + ci) * KK + k];
+    for (int i = threadIdx.x; i < nc * KK * COB; i += CT) {
+      const int c = i / (KK * COB), k = (i / COB) % KK, o = i % COB;
+      sw[i] = w[((long long)(co0 + o) * ci_n + ci0 + c) * KK + k];
     }
     __syncthreads();
+    for (int c = 0; c < nc; ++c) {
+      const float* tc = tile + c * HV;
+      const float* wc = sw + c * KK * COB;
 #pragma unroll
-    for (int k = 0; k < KK; ++k) {
-      const int dx = k % K, dy = (k / K) % K, dz = k / (K * K);
-      const float v = tile[((tz + dz) * HY + (ty + dy)) * HX + (tx + dx)];
-      const float4* w4 = reinterpret_cast<const float4*>(sw + k * CO);
+      for (int dy = 0; dy < K; ++dy) {
 #pragma unroll
-      for (int c4 = 0; c4 < CO / 4; ++c4) {
-        float4 ww = w4[c4];
-        acc[4 * c4 + 0] += ww.x * v;
-        acc[4 * c4 + 1] += ww.y * v;
-        acc[4 * c4 + 2] += ww.z * v;
-        acc[4 * c4 + 3] += ww.w * v;
+        for (int dx = 0; dx < K; ++dx) {
+          float v[HZ];
+#pragma unroll
+          for (int j = 0; j < HZ; ++j) v[j] = tc[(j * HY + ty + dy) * HX + tx + dx];
+#pragma unroll
+          for (int dz = 0; dz < K; ++dz) {
+            const float4* w4 = reinterpret_cast<const float4*>(wc + ((dz * K + dy) * K + dx) * COB);
+#pragma unroll
+            for (int c4 = 0; c4 < COB / 4; ++c4) {
+              const float4 ww = w4[c4];
+#pragma unroll
+              for (int j = 0; j < CTZ; ++j) {
+                const float a = v[j + dz];
+                acc[j][4 * c4 + 0] = fmaf(ww.x, a, acc[j][4 * c4 + 0]);
+                acc[j][4 * c4 + 1] = fmaf(ww.y, a, acc[j][4 * c4 + 1]);
+                acc[j][4 * c4 + 2] = fmaf(ww.z, a, acc[j][4 * c4 + 2]);
+                acc[j][4 * c4 + 3] = fmaf(ww.w, a, acc[j][4 * c4 + 3]);
+              }
+            }
+          }
+        }
       }
     }
     __syncthreads();
   }
-  if (!valid) return;
-  const long long o = ((long long)z * d.ny + y) * d.nx + x;
+  const int x = bx * CTX + tx, y = by * CTY + ty;
+  if (x >= d.nx || y >= d.ny) return;
 #pragma unroll
-  for (int co = 0; co < CO; ++co) {
-    float v = acc[co];
-    if (add) v += add[co * vox + o];
-    if (relu) v = fmaxf(v, 0.f);
-    float* dst = out + co * vox + o;
-    *dst = beta != 0.f ? beta * *dst + v : v;
+  for (int j = 0; j < CTZ; ++j) {
+    const int z = bz * CTZ + j;
+    if (z >= d.nz) break;
+    const long long o = ((long long)z * d.ny + y) * d.nx + x;
+#pragma unroll
+    for (int c = 0; c < COB; ++c) {
+      float v = acc[j][c];
+      const long long idx = (long long)(co0 + c) * vox + o;
+      if (add) v += add[idx];
+      if (relu) v = fmaxf(v, 0.f);
+      out[idx] = beta != 0.f ? beta * out[idx] + v : v;
+    }
   }
 }
 
-// Weight/bias gradient partials of one tile: dw[co][ci][k] = sum_v g[co](v) in[ci](v+k).
-// Grid: (tiles, ci). Each block writes its partial to part[(tile * ci_n + ci) * (co_n*KK)].
-// Threads loop over (co, k) pairs; gout tile for all co and the input halo in shared memory.
-template <int K>
-__global__ void __launch_bounds__(256) k_conv_wgrad(Dims d, int ci_n, int co_n, const float* __restrict__ in,
+// Weight (and bias) gradient partials of one voxel tile:
+//   part[tile][co][ci][k] = sum_{v in tile} g[co](v) in[ci](v + k),
+//   bpart[tile][co] = sum_{v in tile} g[co](v)   (blockIdx.z == 0 blocks).
+// Grid (tiles, co_n / COB, ceil(ci_n / CIB)). Thread t owns the (ci, k) pair
+// t % (CIB * KK) and the voxels v = t / (CIB * KK) + j * groups of the tile;
+// the groups' sums are added in a fixed order in shared memory.
+template <int K, int COB>
+__global__ void __launch_bounds__(CT) k_conv_wgrad(Dims d, int ci_n, int co_n, const float* __restrict__ in,
                                                   const float* __restrict__ g, float* __restrict__ part,
                                                   float* __restrict__ bpart) {
-  constexpr int R = K / 2, HX = TXV + 2 * R, HY = TYV + 2 * R, HZ = TZV + 2 * R, KK = K * K * K;
-  extern __shared__ float sm[];
-  float* tile = sm;                 // [HZ][HY][HX]
-  float* gt = sm + HZ * HY * HX;    // [co][TV]
-  const int ntx = (d.nx + TXV - 1) / TXV, nty = (d.ny + TYV - 1) / TYV;
-  const int t = blockIdx.x, ci = blockIdx.y;
+  constexpr int R = K / 2, HX = CTX + 2 * R, HY = CTY + 2 * R, HZ = CTZ + 2 * R, KK = K * K * K;
+  constexpr int HV = HX * HY * HZ, TV = CTX * CTY * CTZ;
+  constexpr int NP = CIB * KK;                      // (ci, k) pairs
+  constexpr int GROUPS = NP >= CT ? 1 : CT / NP;    // voxel groups
+  constexpr int NPT = (NP + CT - 1) / CT;           // pairs per thread (K=3: 1)
+  __shared__ __align__(16) float tile[CIB * HV];
+  __shared__ __align__(16) float gt[TV * COB];      // [v][co]
+  __shared__ float red[GROUPS > 1 ? CT * COB : 1];
+  const int ntx = (d.nx + CTX - 1) / CTX, nty = (d.ny + CTY - 1) / CTY;
+  const int t = blockIdx.x;
   const int bx = t % ntx, by = (t / ntx) % nty, bz = t / (ntx * nty);
+  const int co0 = blockIdx.y * COB, ci0 = blockIdx.z * CIB;
+  const int nc = min(CIB, ci_n - ci0);
   const long long vox = d.vox();
-  for (int i = threadIdx.x; i < HZ * HY * HX; i += blockDim.x) {
-    int hx = i % HX, hy = (i / HX) % HY, hz = i / (HX * HY);
-    int gx = bx * TXV + hx - R, gy = by * TYV + hy - R, gz = bz * TZV + hz - R;
+  for (int i = threadIdx.x; i < CIB * HV; i += CT) {
+    const int c = i / HV, r = i % HV;
+    const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
+    const int gx = bx * CTX + hx - R, gy = by * CTY + hy - R, gz = bz * CTZ + hz - R;
     float v = 0.f;
-    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < d.nx && gy < d.ny && gz < d.nz)
-      v = in[(long long)ci * vox + ((long long)gz * d.ny + gy) * d.nx + gx];
+    if (c < nc && gx >= 0 && gy >= 0 && gz >= 0 && gx < d.nx && gy < d.ny && gz < d.nz)
+      v = in[(long long)(ci0 + c) * vox + ((long long)gz * d.ny + gy) * d.nx + gx];
     tile[i] = v;
   }
-  for (int i = threadIdx.x; i < co_n * TV; i += blockDim.x) {
-    int co = i / TV, v = i % TV;
-    int tx = v % TXV, ty = (v / TXV) % TYV, tz = v / (TXV * TYV);
-    int x = bx * TXV + tx, y = by * TYV + ty, z = bz * TZV + tz;
+  for (int i = threadIdx.x; i < TV * COB; i += CT) {
+    const int o = i / TV, v = i % TV;  // coalesced along x for a fixed channel
+    const int vx = v % CTX, vy = (v / CTX) % CTY, vz = v / (CTX * CTY);
+    const int x = bx * CTX + vx, y = by * CTY + vy, z = bz * CTZ + vz;
     float gv = 0.f;
-    if (x < d.nx && y < d.ny && z < d.nz) gv = g[(long long)co * vox + ((long long)z * d.ny + y) * d.nx + x];
-    gt[i] = gv;
+    if (x < d.nx && y < d.ny && z < d.nz) gv = g[(long long)(co0 + o) * vox + ((long long)z * d.ny + y) * d.nx + x];
+    gt[v * COB + o] = gv;
   }
   __syncthreads();
-  float* dst = part + ((long long)t * ci_n + ci) * co_n * KK;
-  for (int p = threadIdx.x; p < co_n * KK; p += blockDim.x) {
-    const int co = p / KK, k = p % KK;
-    const int dx = k % K, dy = (k / K) % K, dz = k / (K * K);
-    const float* gg = gt + co * TV;
-    float s = 0.f;
-    for (int v = 0; v < TV; ++v) {
-      int tx = v % TXV, ty = (v / TXV) % TYV, tz = v / (TXV * TYV);
-      s += gg[v] * tile[((tz + dz) * HY + (ty + dy)) * HX + (tx + dx)];
+  const long long nw = (long long)co_n * ci_n * KK;
+  float* dst = part + (long long)t * nw;
+#pragma unroll
+  for (int pp = 0; pp < NPT; ++pp) {
+    const int pair = (threadIdx.x % NP) + pp * CT;
+    const int grp = GROUPS > 1 ? threadIdx.x / NP : 0;
+    const bool active = pair < NP && grp < GROUPS && (NP >= CT || threadIdx.x < GROUPS * NP);
+    float acc[COB];
+#pragma unroll
+    for (int o = 0; o < COB; ++o) acc[o] = 0.f;
+    if (active) {
+      const int c = pair / KK, k = pair % KK;
+      const int dx = k % K, dy = (k / K) % K, dz = k / (K * K);
+      const float* tc = tile + c * HV + (dz * HY + dy) * HX + dx;
+      for (int v = grp; v < TV; v += GROUPS) {
+        const int vx = v % CTX, vy = (v / CTX) % CTY, vz = v / (CTX * CTY);
+        const float a = tc[(vz * HY + vy) * HX + vx];
+        const float4* g4 = reinterpret_cast<const float4*>(gt + v * COB);
+#pragma unroll
+        for (int c4 = 0; c4 < COB / 4; ++c4) {
+          const float4 gg = g4[c4];
+          acc[4 * c4 + 0] = fmaf(gg.x, a, acc[4 * c4 + 0]);
+          acc[4 * c4 + 1] = fmaf(gg.y, a, acc[4 * c4 + 1]);
+          acc[4 * c4 + 2] = fmaf(gg.z, a, acc[4 * c4 + 2]);
+          acc[4 * c4 + 3] = fmaf(gg.w, a, acc[4 * c4 + 3]);
+        }
+      }
     }
-    dst[p] = s;
+    if (GROUPS > 1) {
+      if (active)
+#pragma unroll
+        for (int o = 0; o < COB; ++o) red[threadIdx.x * COB + o] = acc[o];
+      __syncthreads();
+      if (threadIdx.x < NP) {
+        const int c = threadIdx.x / KK, k = threadIdx.x % KK;
+#pragma unroll
+        for (int o = 0; o < COB; ++o) {
+          float s = 0.f;
+          for (int gi = 0; gi < GROUPS; ++gi) s += red[(gi * NP + threadIdx.x) * COB + o];
+          if (c < nc) dst[((long long)(co0 + o) * ci_n + ci0 + c) * KK + k] = s;
+        }
+      }
+      __syncthreads();
+    } else if (active) {
+      const int c = pair / KK, k = pair % KK;
+      if (c < nc)
+#pragma unroll
+        for (int o = 0; o < COB; ++o) dst[((long long)(co0 + o) * ci_n + ci0 + c) * KK + k] = acc[o];
+    }
   }
-  if (ci == 0 && bpart) {
-    for (int co = threadIdx.x; co < co_n; co += blockDim.x) {
-      float s = 0.f;
-      for (int v = 0; v < TV; ++v) s += gt[co * TV + v];
-      bpart[(long long)t * co_n + co] = s;
-    }
+  if (bpart && blockIdx.z == 0 && threadIdx.x < COB) {
+    float s = 0.f;
+    for (int v = 0; v < TV; ++v) s += gt[v * COB + threadIdx.x];
+    bpart[(long long)t * co_n + co0 + threadIdx.x] = s;
   }
 }
 
-// grad[w] += sum over tiles of part (fixed order); one thread per weight.
-__global__ void k_reduce_parts(long long n_tiles, int ci_n, int co_n, int KK, const float* __restrict__ part,
+// grad[i] += sum over tiles of part[tile][i] in a fixed order: one warp per
+// parameter, lanes striding over tiles, then a fixed shuffle tree.
+__global__ void k_reduce_parts(long long tiles, long long nw, int nb, const float* __restrict__ part,
                                const float* __restrict__ bpart, float* __restrict__ dw, float* __restrict__ db) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long nw = (long long)co_n * ci_n * KK;
-  if (i < nw) {
-    int k = (int)(i % KK), ci = (int)((i / KK) % ci_n), co = (int)(i / ((long long)KK * ci_n));
-    double s = 0.0;
-    for (long long t = 0; t < n_tiles; ++t) s += part[((t * ci_n + ci) * co_n + co) * KK + k];
-    dw[i] += (float)s;
-  } else if (i < nw + co_n && db) {
-    int co = (int)(i - nw);
-    double s = 0.0;
-    for (long long t = 0; t < n_tiles; ++t) s += bpart[t * co_n + co];
-    db[co] += (float)s;
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= nw + nb) return;
+  double s = 0.0;
+  if (wid < nw) {
+    for (long long t = lane; t < tiles; t += 32) s += part[t * nw + wid];
+  } else {
+    for (long long t = lane; t < tiles; t += 32) s += bpart[t * nb + (wid - nw)];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    if (wid < nw) dw[wid] += (float)s;
+    else db[wid - nw] += (float)s;
   }
 }
 
@@ -322,41 +406,51 @@ struct Layer {
 using namespace jxb;
 using namespace jxb::cnn;
 
-// layer indices in the fixed topology
-enum { L0A, L0B, L1A, L1B, L2A, L2B, L2C, L1C, L1D, L0C, L0D, L0E, NLAYERS };
-
 struct jxb_cnn {
-  int in_ch, out_ch, c[3];
-  Layer L[NLAYERS];
+  int in_ch = 0, out_ch = 0, levels = 0, c[MAXL] = {};
+  std::vector<Layer> L;  // encoder pairs, bottom triple, decoder pairs, output
   long long n_params = 0;
   float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   long long adam_t = 0;
-  // activation / gradient buffers sized for `cap` voxels at level 0
-  long long cap = 0;
-  std::vector<float*> bufs;
+  // activations, sized for `cap` (level-0 dims)
+  Dims cap{0, 0, 0};
+  float* arena = nullptr;
+  float *A[MAXL] = {}, *S[MAXL] = {}, *P[MAXL] = {}, *U[MAXL] = {}, *M[MAXL] = {}, *D[MAXL] = {}, *GS[MAXL] = {};
+  float *B0 = nullptr, *B1 = nullptr, *B2 = nullptr, *OUT = nullptr, *G0 = nullptr, *G1 = nullptr;
   float* wt = nullptr;     // transposed weights scratch
   float* part = nullptr;   // weight-gradient partials
   long long part_cap = 0;
   double* red = nullptr;   // loss partials
-  float* h_loss_dummy = nullptr;
 };
 
 namespace {
 
+inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
+
+// layer indices
+inline int enc_a(int l) { return 2 * l; }
+inline int enc_b(int l) { return 2 * l + 1; }
+inline int bot(const jxb_cnn* N, int i) { return 2 * (N->levels - 1) + i; }
+inline int dec_c(const jxb_cnn* N, int l) { return 2 * (N->levels - 1) + 3 + 2 * (N->levels - 2 - l); }
+inline int dec_d(const jxb_cnn* N, int l) { return dec_c(N, l) + 1; }
+inline int out_layer(const jxb_cnn* N) { return 4 * N->levels - 1; }
+
 int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in, const float* add, float beta,
          float* out) {
-  long long tiles = (long long)((d.nx + TXV - 1) / TXV) * ((d.ny + TYV - 1) / TYV) * ((d.nz + TZV - 1) / TZV);
   const float* w = p + L.w_off;
   const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
-  int relu = L.relu ? 1 : 0;
-#define JXB_CONV(KS, CO)                                                                             \
-  if (L.k == KS && L.co == CO) {                                                                     \
-    k_conv<KS, CO><<<(unsigned)tiles, TV, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);           \
-    JXB_CUDA(cudaGetLastError());                                                                    \
-    return JXB_OK;                                                                                   \
+  const int relu = L.relu ? 1 : 0;
+  const long long tiles = n_tiles(d);
+  const int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
+  const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob));
+#define JXB_CONV(KS, C)                                                                         \
+  if (L.k == KS && cob == C) {                                                                  \
+    k_conv<KS, C><<<grid, CT, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);                  \
+    JXB_CUDA(cudaGetLastError());                                                               \
+    return JXB_OK;                                                                              \
   }
-  JXB_CONV(3, 4) JXB_CONV(3, 8) JXB_CONV(3, 12) JXB_CONV(3, 16) JXB_CONV(3, 24) JXB_CONV(3, 32) JXB_CONV(3, 48)
-  JXB_CONV(1, 4) JXB_CONV(1, 8) JXB_CONV(1, 12) JXB_CONV(1, 16) JXB_CONV(1, 24) JXB_CONV(1, 32) JXB_CONV(1, 48)
+  JXB_CONV(3, 4) JXB_CONV(3, 8) JXB_CONV(3, 12) JXB_CONV(3, 16)
+  JXB_CONV(1, 4) JXB_CONV(1, 8) JXB_CONV(1, 12) JXB_CONV(1, 16)
 #undef JXB_CONV
   return fail(JXB_ERR_INVALID, "cnn: unsupported output channel count " + std::to_string(L.co));
 }
@@ -371,167 +465,234 @@ int conv_dgrad(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* 
 }
 
 int conv_wgrad(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* in, const float* g) {
-  long long tiles = (long long)((d.nx + TXV - 1) / TXV) * ((d.ny + TYV - 1) / TYV) * ((d.nz + TZV - 1) / TZV);
-  int KK = L.k * L.k * L.k;
-  long long need = tiles * L.ci * L.co * KK + tiles * L.co;
+  const long long tiles = n_tiles(d);
+  const int KK = L.k * L.k * L.k;
+  const long long nw = (long long)L.co * L.ci * KK;
+  const long long need = tiles * nw + tiles * L.co;
   if (need > N->part_cap) {
     cudaFree(N->part);
+    N->part = nullptr;
+    N->part_cap = 0;
     JXB_CUDA(cudaMalloc(&N->part, need * sizeof(float)));
     N->part_cap = need;
   }
-  float* bpart = N->part + tiles * L.ci * L.co * KK;
-  int R = L.k / 2;
-  size_t sm = ((TXV + 2 * R) * (TYV + 2 * R) * (TZV + 2 * R) + (size_t)L.co * TV) * sizeof(float);
-  dim3 grid((unsigned)tiles, L.ci);
-  if (L.k == 3) {
-    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_conv_wgrad<3><<<grid, 256, sm, s>>>(d, L.ci, L.co, in, g, N->part, L.b_off >= 0 ? bpart : nullptr);
-  } else {
-    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_conv_wgrad<1><<<grid, 256, sm, s>>>(d, L.ci, L.co, in, g, N->part, L.b_off >= 0 ? bpart : nullptr);
+  float* bpart = N->part + tiles * nw;
+  // at most 12 output channels per block keeps the static shared memory under 48 KB
+  const int cob = L.co % 8 == 0 ? 8 : (L.co == 12 ? 12 : 4);
+  const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob), (unsigned)((L.ci + CIB - 1) / CIB));
+  float* bp = L.b_off >= 0 ? bpart : nullptr;
+  bool done = false;
+#define JXB_WGRAD(KS, C)                                                                       \
+  if (!done && L.k == KS && cob == C) {                                                        \
+    k_conv_wgrad<KS, C><<<grid, CT, 0, s>>>(d, L.ci, L.co, in, g, N->part, bp);                \
+    done = true;                                                                               \
   }
+  JXB_WGRAD(3, 4) JXB_WGRAD(3, 8) JXB_WGRAD(3, 12)
+  JXB_WGRAD(1, 4) JXB_WGRAD(1, 8) JXB_WGRAD(1, 12)
+#undef JXB_WGRAD
+  if (!done) return fail(JXB_ERR_INVALID, "cnn: unsupported output channel count " + std::to_string(L.co));
   JXB_CUDA(cudaGetLastError());
-  long long nw = (long long)L.co * L.ci * KK + (L.b_off >= 0 ? L.co : 0);
-  k_reduce_parts<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(tiles, L.ci, L.co, KK, N->part, bpart, N->g + L.w_off,
-                                                             L.b_off >= 0 ? N->g + L.b_off : nullptr);
+  const int nb = L.b_off >= 0 ? L.co : 0;
+  const long long warps = nw + nb;
+  k_reduce_parts<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(tiles, nw, nb, N->part, bpart, N->g + L.w_off,
+                                                                       nb ? N->g + L.b_off : nullptr);
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }
-
-inline unsigned nblk(long long n) { return (unsigned)((n + 255) / 256); }
-
-// buffer indices
-enum { A0A, S0, P1, A1A, S1, P2, A2A, A2B, A2C, U1, M1, A1D, U0, M0, A0D, OUT,
-       G0, G1, G2, G3, NBUF };
 
 int ensure_bufs(jxb_cnn* N, Dims d0) {
-  long long v0 = d0.vox();
-  if (v0 <= N->cap) return JXB_OK;
-  for (float* b : N->bufs) cudaFree(b);
-  N->bufs.assign(NBUF, nullptr);
-  Dims d1 = half(d0), d2 = half(d1);
-  long long v1 = d1.vox(), v2 = d2.vox();
-  int c0 = N->c[0], c1 = N->c[1], c2 = N->c[2];
-  long long sizes[NBUF] = {c0 * v0, c0 * v0, c0 * v1, c1 * v1, c1 * v1, c1 * v2, c2 * v2, c2 * v2, c2 * v2,
-                           c2 * v1, c1 * v1, c1 * v1, c1 * v0, c0 * v0, c0 * v0, (long long)N->L[L0E].co * v0,
-                           0, 0, 0, 0};
-  long long gmax = 0;
-  for (int i = 0; i < OUT + 1; ++i) gmax = std::max(gmax, sizes[i]);
-  gmax = std::max(gmax, (long long)N->in_ch * v0);
-  for (int i = G0; i <= G3; ++i) sizes[i] = gmax;
-  for (int i = 0; i < NBUF; ++i) JXB_CUDA(cudaMalloc(&N->bufs[i], std::max<long long>(sizes[i], 1) * sizeof(float)));
-  N->cap = v0;
+  if (d0.nx == N->cap.nx && d0.ny == N->cap.ny && d0.nz == N->cap.nz) return JXB_OK;
+  cudaFree(N->arena);
+  N->arena = nullptr;
+  N->cap = {0, 0, 0};
+  const int nl = N->levels;
+  Dims d[MAXL];
+  d[0] = d0;
+  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
+  // sizes in floats, each rounded up to 64 floats (256 B)
+  std::vector<std::pair<float**, long long>> want;
+  auto add = [&](float** ptr, long long n) { want.push_back({ptr, (std::max<long long>(n, 1) + 63) / 64 * 64}); };
+  long long gmax = (long long)std::max(N->in_ch, 4) * d0.vox();
+  for (int l = 0; l < nl - 1; ++l) {
+    add(&N->A[l], N->c[l] * d[l].vox());
+    add(&N->S[l], N->c[l] * d[l].vox());
+    add(&N->P[l + 1], N->c[l] * d[l + 1].vox());
+    add(&N->U[l], N->c[l + 1] * d[l].vox());
+    add(&N->M[l], N->c[l] * d[l].vox());
+    add(&N->D[l], N->c[l] * d[l].vox());
+    add(&N->GS[l], N->c[l] * d[l].vox());
+    gmax = std::max(gmax, (long long)std::max(N->c[l], N->c[l + 1]) * d[l].vox());
+  }
+  const long long vb = N->c[nl - 1] * d[nl - 1].vox();
+  add(&N->B0, vb);
+  add(&N->B1, vb);
+  add(&N->B2, vb);
+  gmax = std::max(gmax, vb);
+  add(&N->OUT, 4 * d0.vox());
+  add(&N->G0, gmax);
+  add(&N->G1, gmax);
+  long long total = 0;
+  for (auto& w : want) total += w.second;
+  JXB_CUDA(cudaMalloc(&N->arena, total * sizeof(float)));
+  long long off = 0;
+  for (auto& w : want) {
+    *w.first = N->arena + off;
+    off += w.second;
+  }
+  N->cap = d0;
   return JXB_OK;
 }
 
-int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in, float* out) {
+int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   int rc = ensure_bufs(N, d0);
   if (rc) return rc;
-  Dims d1 = half(d0), d2 = half(d1);
-  auto& B = N->bufs;
+  const int nl = N->levels;
+  Dims d[MAXL];
+  d[0] = d0;
+  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
   const float* p = N->p;
-  if ((rc = conv(s, d0, N->L[L0A], p, in, nullptr, 0.f, B[A0A]))) return rc;
-  if ((rc = conv(s, d0, N->L[L0B], p, B[A0A], nullptr, 0.f, B[S0]))) return rc;
-  k_pool<<<nblk(d1.vox() * N->c[0]), 256, 0, s>>>(d0, d1, N->c[0], B[S0], B[P1]);
-  if ((rc = conv(s, d1, N->L[L1A], p, B[P1], nullptr, 0.f, B[A1A]))) return rc;
-  if ((rc = conv(s, d1, N->L[L1B], p, B[A1A], nullptr, 0.f, B[S1]))) return rc;
-  k_pool<<<nblk(d2.vox() * N->c[1]), 256, 0, s>>>(d1, d2, N->c[1], B[S1], B[P2]);
-  if ((rc = conv(s, d2, N->L[L2A], p, B[P2], nullptr, 0.f, B[A2A]))) return rc;
-  if ((rc = conv(s, d2, N->L[L2B], p, B[A2A], nullptr, 0.f, B[A2B]))) return rc;
-  if ((rc = conv(s, d2, N->L[L2C], p, B[A2B], nullptr, 0.f, B[A2C]))) return rc;
-  k_up<<<nblk(d1.vox() * N->c[2]), 256, 0, s>>>(d1, d2, N->c[2], B[A2C], B[U1]);
-  if ((rc = conv(s, d1, N->L[L1C], p, B[U1], B[S1], 0.f, B[M1]))) return rc;
-  if ((rc = conv(s, d1, N->L[L1D], p, B[M1], nullptr, 0.f, B[A1D]))) return rc;
-  k_up<<<nblk(d0.vox() * N->c[1]), 256, 0, s>>>(d0, d1, N->c[1], B[A1D], B[U0]);
-  if ((rc = conv(s, d0, N->L[L0C], p, B[U0], B[S0], 0.f, B[M0]))) return rc;
-  if ((rc = conv(s, d0, N->L[L0D], p, B[M0], nullptr, 0.f, B[A0D]))) return rc;
-  if ((rc = conv(s, d0, N->L[L0E], p, B[A0D], nullptr, 0.f, out ? out : B[OUT]))) return rc;
+  const float* x = in;
+  for (int l = 0; l < nl - 1; ++l) {
+    if ((rc = conv(s, d[l], N->L[enc_a(l)], p, x, nullptr, 0.f, N->A[l]))) return rc;
+    if ((rc = conv(s, d[l], N->L[enc_b(l)], p, N->A[l], nullptr, 0.f, N->S[l]))) return rc;
+    k_pool<<<nblk(d[l + 1].vox() * N->c[l]), 256, 0, s>>>(d[l], d[l + 1], N->c[l], N->S[l], N->P[l + 1]);
+    x = N->P[l + 1];
+  }
+  const Dims db = d[nl - 1];
+  if ((rc = conv(s, db, N->L[bot(N, 0)], p, x, nullptr, 0.f, N->B0))) return rc;
+  if ((rc = conv(s, db, N->L[bot(N, 1)], p, N->B0, nullptr, 0.f, N->B1))) return rc;
+  if ((rc = conv(s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
+  const float* y = N->B2;
+  for (int l = nl - 2; l >= 0; --l) {
+    k_up<<<nblk(d[l].vox() * N->c[l + 1]), 256, 0, s>>>(d[l], d[l + 1], N->c[l + 1], y, N->U[l]);
+    if ((rc = conv(s, d[l], N->L[dec_c(N, l)], p, N->U[l], N->S[l], 0.f, N->M[l]))) return rc;
+    if ((rc = conv(s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
+    y = N->D[l];
+  }
+  if ((rc = conv(s, d0, N->L[out_layer(N)], p, y, nullptr, 0.f, N->OUT))) return rc;
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }
 
-// Backward through the network for the output gradient in G0 (layout of OUT);
-// accumulates parameter gradients into N->g.
+// Backward through the network for the output gradient in G0 (layout of OUT,
+// 4 channels); accumulates parameter gradients into N->g. Needs the
+// activations of a forward pass on the same input.
 int backward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
-  Dims d1 = half(d0), d2 = half(d1);
-  auto& B = N->bufs;
-  int c0 = N->c[0], c1 = N->c[1], c2 = N->c[2];
-  float *gA = B[G0], *gB = B[G1], *gS0 = B[G2], *gS1 = B[G3];
+  const int nl = N->levels;
+  Dims d[MAXL];
+  d[0] = d0;
+  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
+  float *ga = N->G0, *gb = N->G1;
   int rc;
-  // L0E (linear): gA = dL/dOUT
-  if ((rc = conv_wgrad(N, s, d0, N->L[L0E], B[A0D], gA))) return rc;
-  if ((rc = conv_dgrad(N, s, d0, N->L[L0E], gA, 0.f, gB))) return rc;  // dL/dA0D
-  k_relu_mask<<<nblk(c0 * d0.vox()), 256, 0, s>>>(c0 * d0.vox(), B[A0D], gB);
-  if ((rc = conv_wgrad(N, s, d0, N->L[L0D], B[M0], gB))) return rc;
-  if ((rc = conv_dgrad(N, s, d0, N->L[L0D], gB, 0.f, gA))) return rc;  // dL/dM0 (linear output of L0C + S0)
-  // M0 = L0C(U0) + S0: dS0 = gA, dU0 = L0C^T gA
-  JXB_CUDA(cudaMemcpyAsync(gS0, gA, c0 * d0.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  if ((rc = conv_wgrad(N, s, d0, N->L[L0C], B[U0], gA))) return rc;
-  if ((rc = conv_dgrad(N, s, d0, N->L[L0C], gA, 0.f, gB))) return rc;  // dL/dU0 [c1 @ n0]
-  k_up_bwd<<<nblk(c1 * d1.vox()), 256, 0, s>>>(d0, d1, c1, gB, gA);       // dL/dA1D [c1 @ n1]
-  k_relu_mask<<<nblk(c1 * d1.vox()), 256, 0, s>>>(c1 * d1.vox(), B[A1D], gA);
-  if ((rc = conv_wgrad(N, s, d1, N->L[L1D], B[M1], gA))) return rc;
-  if ((rc = conv_dgrad(N, s, d1, N->L[L1D], gA, 0.f, gB))) return rc;  // dL/dM1
-  JXB_CUDA(cudaMemcpyAsync(gS1, gB, c1 * d1.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
-  if ((rc = conv_wgrad(N, s, d1, N->L[L1C], B[U1], gB))) return rc;
-  if ((rc = conv_dgrad(N, s, d1, N->L[L1C], gB, 0.f, gA))) return rc;  // dL/dU1 [c2 @ n1]
-  k_up_bwd<<<nblk(c2 * d2.vox()), 256, 0, s>>>(d1, d2, c2, gA, gB);       // dL/dA2C
-  k_relu_mask<<<nblk(c2 * d2.vox()), 256, 0, s>>>(c2 * d2.vox(), B[A2C], gB);
-  if ((rc = conv_wgrad(N, s, d2, N->L[L2C], B[A2B], gB))) return rc;
-  if ((rc = conv_dgrad(N, s, d2, N->L[L2C], gB, 0.f, gA))) return rc;
-  k_relu_mask<<<nblk(c2 * d2.vox()), 256, 0, s>>>(c2 * d2.vox(), B[A2B], gA);
-  if ((rc = conv_wgrad(N, s, d2, N->L[L2B], B[A2A], gA))) return rc;
-  if ((rc = conv_dgrad(N, s, d2, N->L[L2B], gA, 0.f, gB))) return rc;
-  k_relu_mask<<<nblk(c2 * d2.vox()), 256, 0, s>>>(c2 * d2.vox(), B[A2A], gB);
-  if ((rc = conv_wgrad(N, s, d2, N->L[L2A], B[P2], gB))) return rc;
-  if ((rc = conv_dgrad(N, s, d2, N->L[L2A], gB, 0.f, gA))) return rc;  // dL/dP2 [c1 @ n2]
-  k_pool_bwd<<<nblk(c1 * d1.vox()), 256, 0, s>>>(d1, d2, c1, gA, 1.f, gS1);  // dS1 += pool^T
-  k_relu_mask<<<nblk(c1 * d1.vox()), 256, 0, s>>>(c1 * d1.vox(), B[S1], gS1);
-  if ((rc = conv_wgrad(N, s, d1, N->L[L1B], B[A1A], gS1))) return rc;
-  if ((rc = conv_dgrad(N, s, d1, N->L[L1B], gS1, 0.f, gA))) return rc;
-  k_relu_mask<<<nblk(c1 * d1.vox()), 256, 0, s>>>(c1 * d1.vox(), B[A1A], gA);
-  if ((rc = conv_wgrad(N, s, d1, N->L[L1A], B[P1], gA))) return rc;
-  if ((rc = conv_dgrad(N, s, d1, N->L[L1A], gA, 0.f, gB))) return rc;  // dL/dP1 [c0 @ n1]
-  k_pool_bwd<<<nblk(c0 * d0.vox()), 256, 0, s>>>(d0, d1, c0, gB, 1.f, gS0);
-  k_relu_mask<<<nblk(c0 * d0.vox()), 256, 0, s>>>(c0 * d0.vox(), B[S0], gS0);
-  if ((rc = conv_wgrad(N, s, d0, N->L[L0B], B[A0A], gS0))) return rc;
-  if ((rc = conv_dgrad(N, s, d0, N->L[L0B], gS0, 0.f, gA))) return rc;
-  k_relu_mask<<<nblk(c0 * d0.vox()), 256, 0, s>>>(c0 * d0.vox(), B[A0A], gA);
-  if ((rc = conv_wgrad(N, s, d0, N->L[L0A], in, gA))) return rc;
+  // output layer
+  if ((rc = conv_wgrad(N, s, d0, N->L[out_layer(N)], N->D[0], ga))) return rc;
+  if ((rc = conv_dgrad(N, s, d0, N->L[out_layer(N)], ga, 0.f, gb))) return rc;  // dL/dD0
+  std::swap(ga, gb);
+  // decoder, level 0 upwards: ga = dL/dD_l
+  for (int l = 0; l < nl - 1; ++l) {
+    const long long n = (long long)N->c[l] * d[l].vox();
+    k_relu_mask<<<nblk(n), 256, 0, s>>>(n, N->D[l], ga);
+    if ((rc = conv_wgrad(N, s, d[l], N->L[dec_d(N, l)], N->M[l], ga))) return rc;
+    if ((rc = conv_dgrad(N, s, d[l], N->L[dec_d(N, l)], ga, 0.f, N->GS[l]))) return rc;  // dL/dM_l = dL/ds_l (skip part)
+    if ((rc = conv_wgrad(N, s, d[l], N->L[dec_c(N, l)], N->U[l], N->GS[l]))) return rc;
+    if ((rc = conv_dgrad(N, s, d[l], N->L[dec_c(N, l)], N->GS[l], 0.f, gb))) return rc;  // dL/dU_l
+    k_up_bwd<<<nblk((long long)N->c[l + 1] * d[l + 1].vox()), 256, 0, s>>>(d[l], d[l + 1], N->c[l + 1], gb, ga);
+  }
+  // bottom: ga = dL/dB2
+  const Dims db = d[nl - 1];
+  const long long nbv = (long long)N->c[nl - 1] * db.vox();
+  k_relu_mask<<<nblk(nbv), 256, 0, s>>>(nbv, N->B2, ga);
+  if ((rc = conv_wgrad(N, s, db, N->L[bot(N, 2)], N->B1, ga))) return rc;
+  if ((rc = conv_dgrad(N, s, db, N->L[bot(N, 2)], ga, 0.f, gb))) return rc;
+  k_relu_mask<<<nblk(nbv), 256, 0, s>>>(nbv, N->B1, gb);
+  if ((rc = conv_wgrad(N, s, db, N->L[bot(N, 1)], N->B0, gb))) return rc;
+  if ((rc = conv_dgrad(N, s, db, N->L[bot(N, 1)], gb, 0.f, ga))) return rc;
+  k_relu_mask<<<nblk(nbv), 256, 0, s>>>(nbv, N->B0, ga);
+  const float* bot_in = N->P[nl - 1];
+  if ((rc = conv_wgrad(N, s, db, N->L[bot(N, 0)], bot_in, ga))) return rc;
+  if ((rc = conv_dgrad(N, s, db, N->L[bot(N, 0)], ga, 0.f, gb))) return rc;  // dL/dP_{L-1}
+  std::swap(ga, gb);
+  // encoder, deepest first: ga = dL/dP_{l+1}
+  for (int l = nl - 2; l >= 0; --l) {
+    const long long n = (long long)N->c[l] * d[l].vox();
+    k_pool_bwd<<<nblk(n), 256, 0, s>>>(d[l], d[l + 1], N->c[l], ga, 1.f, N->GS[l]);  // dL/ds_l
+    k_relu_mask<<<nblk(n), 256, 0, s>>>(n, N->S[l], N->GS[l]);
+    if ((rc = conv_wgrad(N, s, d[l], N->L[enc_b(l)], N->A[l], N->GS[l]))) return rc;
+    if ((rc = conv_dgrad(N, s, d[l], N->L[enc_b(l)], N->GS[l], 0.f, gb))) return rc;  // dL/dA_l
+    k_relu_mask<<<nblk(n), 256, 0, s>>>(n, N->A[l], gb);
+    const float* xin = l > 0 ? N->P[l] : in;
+    if ((rc = conv_wgrad(N, s, d[l], N->L[enc_a(l)], xin, gb))) return rc;
+    if (l > 0) {
+      if ((rc = conv_dgrad(N, s, d[l], N->L[enc_a(l)], gb, 0.f, ga))) return rc;  // dL/dP_l
+    }
+  }
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }
 
-bool supported_co(int c) { return c == 4 || c == 8 || c == 12 || c == 16 || c == 24 || c == 32 || c == 48; }
+bool supported_co(int c) { return c == 4 || c == 8 || c == 12 || c == 16 || c == 24 || c == 32 || c == 48 || c == 64; }
 
 }  // namespace
 
-extern "C" int jxb_cnn_create(int in_ch, int out_ch, const int* channels, uint64_t seed, jxb_cnn** out) {
-  if (!out || !channels || in_ch < 1 || in_ch > 8 || out_ch < 1 || out_ch > 3)
-    return fail(JXB_ERR_INVALID, "jxb_cnn_create: bad argument");
-  for (int i = 0; i < 3; ++i)
-    if (!supported_co(channels[i])) return fail(JXB_ERR_INVALID, "jxb_cnn_create: channels must be in {4,8,12,16,24,32,48}");
+namespace jxb {
+
+int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4) {
+  int rc = forward(N, s, Dims{nx, ny, nz}, in);
+  if (rc) return rc;
+  if (out4) *out4 = N->OUT;
+  return JXB_OK;
+}
+
+float* cnn_grad_out(jxb_cnn* N) { return N->G0; }
+
+int cnn_backward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in) {
+  return backward(N, s, Dims{nx, ny, nz}, in);
+}
+
+int cnn_out_channels(const jxb_cnn* N) { return N->out_ch; }
+
+}  // namespace jxb
+
+extern "C" int jxb_cnn_create(int in_ch, int out_ch, int levels, const int* channels, uint64_t seed, jxb_cnn** out) {
+  if (!out || !channels || in_ch < 1 || in_ch > 8 || out_ch < 1 || out_ch > 3 || levels < 2 || levels > MAXL)
+    return fail(JXB_ERR_INVALID, "jxb_cnn_create: bad argument (in_ch 1..8, out_ch 1..3, levels 2..6)");
+  for (int i = 0; i < levels; ++i)
+    if (!supported_co(channels[i]))
+      return fail(JXB_ERR_INVALID, "jxb_cnn_create: channels must be in {4,8,12,16,24,32,48,64}");
   jxb_cnn* N = new jxb_cnn();
   N->in_ch = in_ch;
   N->out_ch = out_ch;
-  for (int i = 0; i < 3; ++i) N->c[i] = channels[i];
-  int c0 = channels[0], c1 = channels[1], c2 = channels[2];
-  // the output layer's channel count must be a multiple of 4 for the conv kernel: pad to 4
-  struct Spec { int ci, co, k; bool relu; } spec[NLAYERS] = {
-      {in_ch, c0, 3, true}, {c0, c0, 3, true}, {c0, c1, 3, true}, {c1, c1, 3, true}, {c1, c2, 3, true},
-      {c2, c2, 3, true},    {c2, c2, 3, true}, {c2, c1, 1, false}, {c1, c1, 3, true}, {c1, c0, 1, false},
-      {c0, c0, 3, true},    {c0, 4, 3, false}};
+  N->levels = levels;
+  for (int i = 0; i < levels; ++i) N->c[i] = channels[i];
+  struct Spec { int ci, co, k; bool relu; };
+  std::vector<Spec> spec;
+  int prev = in_ch;
+  for (int l = 0; l < levels - 1; ++l) {
+    spec.push_back({prev, channels[l], 3, true});
+    spec.push_back({channels[l], channels[l], 3, true});
+    prev = channels[l];
+  }
+  const int cb = channels[levels - 1];
+  spec.push_back({prev, cb, 3, true});
+  spec.push_back({cb, cb, 3, true});
+  spec.push_back({cb, cb, 3, true});
+  for (int l = levels - 2; l >= 0; --l) {
+    spec.push_back({channels[l + 1], channels[l], 1, false});
+    spec.push_back({channels[l], channels[l], 3, true});
+  }
+  spec.push_back({channels[0], 4, 3, false});  // output padded to 4 channels for the conv kernel
   long long off = 0;
-  for (int i = 0; i < NLAYERS; ++i) {
-    Layer& L = N->L[i];
-    L.ci = spec[i].ci;
-    L.co = spec[i].co;
-    L.k = spec[i].k;
-    L.relu = spec[i].relu;
+  for (const Spec& sp : spec) {
+    Layer L;
+    L.ci = sp.ci;
+    L.co = sp.co;
+    L.k = sp.k;
+    L.relu = sp.relu;
     L.w_off = off;
     off += (long long)L.co * L.ci * L.k * L.k * L.k;
     L.b_off = off;
     off += L.co;
+    N->L.push_back(L);
   }
   N->n_params = off;
   auto bail = [&](cudaError_t e) {
@@ -551,27 +712,27 @@ extern "C" int jxb_cnn_create(int in_ch, int out_ch, const int* channels, uint64
   if ((e = cudaMalloc(&N->m, off * sizeof(float))) != cudaSuccess) return bail(e);
   if ((e = cudaMalloc(&N->v, off * sizeof(float))) != cudaSuccess) return bail(e);
   long long wmax = 0;
-  for (int i = 0; i < NLAYERS; ++i) wmax = std::max(wmax, (long long)N->L[i].co * N->L[i].ci * 27);
+  for (const Layer& L : N->L) wmax = std::max(wmax, (long long)L.co * L.ci * 27);
   if ((e = cudaMalloc(&N->wt, wmax * sizeof(float))) != cudaSuccess) return bail(e);
   if ((e = cudaMalloc(&N->red, 2 * JXB_RED_BLOCKS * sizeof(double))) != cudaSuccess) return bail(e);
   cudaMemset(N->g, 0, off * sizeof(float));
   cudaMemset(N->m, 0, off * sizeof(float));
   cudaMemset(N->v, 0, off * sizeof(float));
   // He-uniform weights, zero biases; the output layer starts small
-  for (int i = 0; i < NLAYERS; ++i) {
+  const int last = out_layer(N);
+  for (int i = 0; i <= last; ++i) {
     const Layer& L = N->L[i];
     long long nw = (long long)L.co * L.ci * L.k * L.k * L.k;
     float fan_in = (float)(L.ci * L.k * L.k * L.k);
-    float a = sqrtf(6.f / fan_in) * (i == L0E ? 0.1f : 1.f);
+    float a = sqrtf(6.f / fan_in) * (i == last ? 0.1f : 1.f);
     k_init<<<nblk(nw), 256>>>(nw, seed * 1000003ull + i, a, N->p + L.w_off);
     cudaMemset(N->p + L.b_off, 0, L.co * sizeof(float));
   }
   // zero the padding output channels of the last layer (only out_ch are used)
   {
-    const Layer& L = N->L[L0E];
+    const Layer& L = N->L[last];
     long long per = (long long)L.ci * 27;
-    if (out_ch < L.co)
-      cudaMemset(N->p + L.w_off + out_ch * per, 0, (L.co - out_ch) * per * sizeof(float));
+    if (out_ch < L.co) cudaMemset(N->p + L.w_off + out_ch * per, 0, (L.co - out_ch) * per * sizeof(float));
   }
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return bail(e);
@@ -589,7 +750,7 @@ extern "C" int jxb_cnn_destroy(jxb_cnn* N) {
   cudaFree(N->wt);
   cudaFree(N->part);
   cudaFree(N->red);
-  for (float* b : N->bufs) cudaFree(b);
+  cudaFree(N->arena);
   delete N;
   return JXB_OK;
 }
@@ -612,10 +773,23 @@ extern "C" int jxb_cnn_forward(jxb_cnn* N, jxb_stream stream, int nx, int ny, in
   if (!N || !in || !out || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_forward: bad argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
-  int rc = forward(N, s, d, in, nullptr);
+  int rc = forward(N, s, d, in);
   if (rc) return rc;
-  JXB_CUDA(cudaMemcpyAsync(out, N->bufs[OUT], (size_t)N->out_ch * d.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaMemcpyAsync(out, N->OUT, (size_t)N->out_ch * d.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
   return JXB_OK;
+}
+
+extern "C" int jxb_cnn_backward(jxb_cnn* N, jxb_stream stream, int nx, int ny, int nz, const float* in,
+                                const float* gout) {
+  if (!N || !in || !gout || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_backward: bad argument");
+  if (N->cap.nx != nx || N->cap.ny != ny || N->cap.nz != nz)
+    return fail(JXB_ERR_INVALID, "jxb_cnn_backward: no forward pass on these dimensions precedes it");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  Dims d{nx, ny, nz};
+  const size_t vb = (size_t)d.vox() * sizeof(float);
+  JXB_CUDA(cudaMemcpyAsync(N->G0, gout, N->out_ch * vb, cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaMemsetAsync(N->G0 + (size_t)N->out_ch * d.vox(), 0, (4 - N->out_ch) * vb, s));
+  return backward(N, s, d, in);
 }
 
 extern "C" int jxb_cnn_zero_grad(jxb_cnn* N, jxb_stream stream) {
@@ -629,12 +803,11 @@ extern "C" int jxb_cnn_accumulate(jxb_cnn* N, jxb_stream stream, int nx, int ny,
   if (!N || !in || !target) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate: null argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
-  int rc = forward(N, s, d, in, nullptr);
+  int rc = forward(N, s, d, in);
   if (rc) return rc;
   // loss on the first out_ch channels of the (4-channel padded) output
-  k_mse<<<JXB_RED_BLOCKS, 256, 0, s>>>(d.vox(), N->out_ch, N->bufs[OUT], target, mask, N->bufs[G0], N->red);
-  JXB_CUDA(cudaMemsetAsync(N->bufs[G0] + (size_t)N->out_ch * d.vox(), 0,
-                           (size_t)(N->L[L0E].co - N->out_ch) * d.vox() * sizeof(float), s));
+  k_mse<<<JXB_RED_BLOCKS, 256, 0, s>>>(d.vox(), N->out_ch, N->OUT, target, mask, N->G0, N->red);
+  JXB_CUDA(cudaMemsetAsync(N->G0 + (size_t)N->out_ch * d.vox(), 0, (size_t)(4 - N->out_ch) * d.vox() * sizeof(float), s));
   std::vector<double> h(2 * JXB_RED_BLOCKS);
   JXB_CUDA(cudaMemcpyAsync(h.data(), N->red, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   JXB_CUDA(cudaStreamSynchronize(s));
@@ -644,7 +817,7 @@ extern "C" int jxb_cnn_accumulate(jxb_cnn* N, jxb_stream stream, int nx, int ny,
     m += h[2 * i + 1];
   }
   double denom = m > 0 ? m : 1.0;
-  k_scale<<<nblk((long long)N->out_ch * d.vox()), 256, 0, s>>>((long long)N->out_ch * d.vox(), (float)(1.0 / denom), N->bufs[G0]);
+  k_scale<<<nblk((long long)N->out_ch * d.vox()), 256, 0, s>>>((long long)N->out_ch * d.vox(), (float)(1.0 / denom), N->G0);
   rc = backward(N, s, d, in);
   if (rc) return rc;
   if (loss) *loss = a / denom;

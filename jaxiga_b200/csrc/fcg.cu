@@ -1,198 +1,601 @@
-// Flexible CG with a learned (CNN) preconditioner.
+// Flexible CG with a learned (CNN) preconditioner, and the energy-norm
+// training step of that network.
 //
-// FCG(1) in the form of Notay (SIAM J. Sci. Comput. 22, 2000): the search
-// direction is the preconditioned residual made A-orthogonal to the previous
-// direction only, p_k = z_k - (z_k . A p_{k-1} / p_{k-1} . A p_{k-1}) p_{k-1},
-// alpha_k = (p_k . r_k) / (p_k . A p_k). It tolerates a preconditioner that is
-// not a fixed linear SPD map, which a ReLU network is not.
+// Truncated flexible CG, FCG(m) in the form of Notay (SIAM J. Sci. Comput.
+// 22, 2000): the search direction is the preconditioned residual made
+// A-orthogonal to the last m directions,
+//   p_k = z_k - sum_{j=k-m}^{k-1} (z_k . A p_j / p_j . A p_j) p_j,
+//   alpha_k = (p_k . r_k) / (p_k . A p_k).
+// It tolerates a preconditioner that is not a fixed linear SPD map, which a
+// ReLU network is not; m > 1 keeps the global A-orthogonality that a varying
+// preconditioner otherwise loses.
 //
-// The preconditioner maps the residual r to z = ||r|| * out_scale * N(r / ||r|| * in_scale, features),
-// N the network applied on the control-point grid (channels: the vec residual
-// components, then the caller's static feature channels such as a
-// log-coefficient field). Scaling by ||r|| makes the map homogeneous of degree
-// one. Jacobi-PCG is the fallback: if a learned direction is not a descent
-// direction (p . A p <= 0) or the residual stops decreasing for `stall`
-// iterations, the remaining iterations use z = D^-1 r. Stopping rule and
-// true-residual diagnostics are those of jxb_pcg.
+// The preconditioner maps r to z = ||r|| out_scale N(in_scale r/||r||, features),
+// N the network on the control-point grid (channels: the vec residual
+// components, then static features such as a log-coefficient). Scaling by
+// ||r|| makes the map homogeneous of degree one. Jacobi is the fallback: a
+// learned direction with p . A p <= 0, or `stall` learned iterations without
+// a new lowest residual, restart the recurrence with z = D^-1 r (which, with
+// a fixed SPD preconditioner, is plain PCG). Stopping rule and true-residual
+// diagnostics are those of jxb_pcg (src/jaxiga/solvers/linear.py:399-442,
+// src/jaxiga/solvers/diagnostics.py:8-19).
+//
+// Device-resident: every scalar of the recurrence lives in a device state
+// block; one iteration is pack, network, unpack (or Jacobi), multi-dot,
+// direction, brick apply, combine (+ p.Ap partials), p.r partials and ring
+// copies, x/r update (+ r.r partials), finish. It is captured once into a
+// CUDA graph (one iteration per launch for the learned mode, `check_every`
+// for Jacobi) and every kernel but the network's returns at once when the
+// device `done` flag is set. Reductions use a fixed grid and order.
 #include <math.h>
 
 #include <vector>
 
 #include "jxb_internal.cuh"
 
-extern "C" int jxb_cnn_forward(struct jxb_cnn* N, jxb_stream stream, int nx, int ny, int nz, const float* in, float* out);
-
 namespace jxb {
 
-__global__ void k_pack_in(long long ncp, int vec, const double* __restrict__ r, const uint8_t* __restrict__ keep,
-                          float s, float* __restrict__ in) {
+constexpr int FCG_MMAX = 8;
+
+struct FcgState {
+  CgState cg;              // rr, alpha, atol2, k (= iterations), maxiter, done, status
+  double pAp[FCG_MMAX];    // ring: p_j . A p_j of the stored directions
+  long long nd;            // directions stored since the last restart
+  int bad;                 // the last direction had p . A p <= 0 or was not finite
+  int m;                   // ring length
+};
+
+template <typename T>
+__global__ void k_fpack(long long ncp, int vec, const T* __restrict__ r, const uint8_t* __restrict__ keep,
+                        float in_scale, const FcgState* st, float* __restrict__ in) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ncp * vec) return;
-  long long cp = i / vec;
-  int c = (int)(i % vec);
-  in[(long long)c * ncp + cp] = keep[i] ? (float)(r[i] * s) : 0.f;
+  const double rr = st->cg.rr;
+  const float s = (!st->cg.done && rr > 0) ? (float)(in_scale / sqrt(rr)) : 0.f;
+  const long long cp = i / vec;
+  const int c = (int)(i % vec);
+  in[(long long)c * ncp + cp] = keep[i] ? (float)r[i] * s : 0.f;
 }
 
-__global__ void k_unpack_out(long long ncp, int vec, const float* __restrict__ out, const uint8_t* __restrict__ keep,
-                             double s, double* __restrict__ z) {
+template <typename T>
+__global__ void k_funpack(long long ncp, int vec, const float* __restrict__ out, const uint8_t* __restrict__ keep,
+                          double out_scale, const FcgState* st, T* __restrict__ z) {
+  if (st->cg.done) return;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ncp * vec) return;
-  long long cp = i / vec;
-  int c = (int)(i % vec);
-  z[i] = keep[i] ? s * (double)out[(long long)c * ncp + cp] : 0.0;
+  const long long cp = i / vec;
+  const int c = (int)(i % vec);
+  z[i] = keep[i] ? (T)(sqrt(st->cg.rr) * out_scale * (double)out[(long long)c * ncp + cp]) : T(0);
 }
 
-__global__ void k_jacobi(long long n, const double* __restrict__ inv, const double* __restrict__ r, double* __restrict__ z) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) z[i] = inv[i] * r[i];
+template <typename T>
+__global__ void k_fjac(long long n, const T* __restrict__ inv, const T* __restrict__ r, const FcgState* st,
+                       T* __restrict__ z) {
+  if (st->cg.done) return;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = inv[i] * r[i];
 }
 
-__global__ void k_dir(long long n, const double* __restrict__ z, double beta, const double* __restrict__ pp,
-                      double* __restrict__ p) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = z[i] - beta * pp[i];
-}
+// ring slot of stored direction d (0-based since the last restart)
+__device__ __forceinline__ int fcg_slot(long long d, int m) { return (int)(d % m); }
 
-__global__ void k_step(long long n, double alpha, const double* __restrict__ p, const double* __restrict__ Ap,
-                       double* __restrict__ x, double* __restrict__ r) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
-    x[i] += alpha * p[i];
-    r[i] -= alpha * Ap[i];
+// partials[j][block] = z . A p_{nd-1-j}, j < min(nd, m)
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fmdot(long long n, const FcgState* st, const T* __restrict__ z,
+                                                           const T* __restrict__ APr, double* __restrict__ partials) {
+  if (st->cg.done) return;
+  const int m = st->m;
+  const long long nd = st->nd;
+  const int jn = (int)(nd < m ? nd : m);
+  double acc[FCG_MMAX];
+#pragma unroll
+  for (int j = 0; j < FCG_MMAX; ++j) acc[j] = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double zi = (double)z[i];
+#pragma unroll
+    for (int j = 0; j < FCG_MMAX; ++j)
+      if (j < jn) acc[j] += zi * (double)APr[(long long)fcg_slot(nd - 1 - j, m) * n + i];
+  }
+#pragma unroll
+  for (int j = 0; j < FCG_MMAX; ++j) {
+    if (j >= jn) break;  // jn is uniform across the block
+    const double s = block_sum_all(acc[j]);
+    if (threadIdx.x == 0) partials[j * JXB_RED_BLOCKS + blockIdx.x] = s;
   }
 }
 
-__global__ void k_resid(long long n, const double* __restrict__ b, const double* __restrict__ Ax,
-                        const uint8_t* __restrict__ keep, double* __restrict__ out) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = keep[i] ? b[i] - Ax[i] : 0.0;
+// p = z - sum_j beta_j p_{nd-1-j}, beta_j = (z . A p_j) / (p_j . A p_j)
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fdir(long long n, const FcgState* st, const T* __restrict__ z,
+                                                          const T* __restrict__ Pr, const double* __restrict__ partials,
+                                                          T* __restrict__ p) {
+  if (st->cg.done) return;
+  const int m = st->m;
+  const long long nd = st->nd;
+  const int jn = (int)(nd < m ? nd : m);
+  T beta[FCG_MMAX];
+#pragma unroll
+  for (int j = 0; j < FCG_MMAX; ++j) {
+    beta[j] = T(0);
+    if (j < jn) beta[j] = (T)(reduce_partials(partials + j * JXB_RED_BLOCKS) / st->pAp[fcg_slot(nd - 1 - j, m)]);
+  }
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T v = z[i];
+#pragma unroll
+    for (int j = 0; j < FCG_MMAX; ++j)
+      if (j < jn) v -= beta[j] * Pr[(long long)fcg_slot(nd - 1 - j, m) * n + i];
+    p[i] = v;
+  }
 }
 
-__global__ void k_mask_copy(long long n, const double* __restrict__ b, const uint8_t* __restrict__ keep, double* __restrict__ r) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) r[i] = keep[i] ? b[i] : 0.0;
+// p.r partials; p and A p copied into ring slot nd % m
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fpr(long long n, const FcgState* st, const T* __restrict__ p,
+                                                         const T* __restrict__ Ap, const T* __restrict__ r,
+                                                         T* __restrict__ Pr, T* __restrict__ APr,
+                                                         double* __restrict__ partials) {
+  if (st->cg.done) return;
+  const long long off = (long long)fcg_slot(st->nd, st->m) * n;
+  double acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T pi = p[i];
+    Pr[off + i] = pi;
+    APr[off + i] = Ap[i];
+    acc += (double)pi * (double)r[i];
+  }
+  const double s = block_sum_all(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
+// x += alpha p, r -= alpha A p (+ r.r partials); skipped for a bad direction
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fupdate(long long n, const FcgState* st, const double* __restrict__ pap_part,
+                                                             const double* __restrict__ pr_part, const T* __restrict__ p,
+                                                             const T* __restrict__ Ap, T* __restrict__ x, T* __restrict__ r,
+                                                             double* __restrict__ rr_part) {
+  if (st->cg.done) return;
+  const double pAp = reduce_partials(pap_part), pr = reduce_partials(pr_part);
+  if (!(pAp > 0) || !isfinite(pAp) || !isfinite(pr)) return;
+  const T alpha = (T)(pr / pAp);
+  double acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    const T ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    acc += (double)ri * (double)ri;
+  }
+  const double s = block_sum_all(acc);
+  if (threadIdx.x == 0) rr_part[blockIdx.x] = s;
+}
+
+__global__ void k_ffin(FcgState* st, const double* __restrict__ pap_part, const double* __restrict__ pr_part,
+                       const double* __restrict__ rr_part) {
+  if (st->cg.done) return;
+  const double pAp = reduce_partials(pap_part), pr = reduce_partials(pr_part);
+  const bool bad = !(pAp > 0) || !isfinite(pAp) || !isfinite(pr);
+  const double rr = bad ? 0.0 : reduce_partials(rr_part);
+  if (threadIdx.x != 0) return;
+  if (bad) {
+    st->bad = 1;
+    st->cg.done = 1;
+    return;
+  }
+  st->pAp[fcg_slot(st->nd, st->m)] = pAp;
+  st->nd += 1;
+  st->cg.k += 1;
+  st->cg.alpha = pr / pAp;
+  st->cg.rr = rr;
+  if (!isfinite(rr)) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NONFINITE;
+  } else if (!(rr > st->cg.atol2)) {
+    st->cg.done = 1;
+  } else if (st->cg.k >= st->cg.maxiter) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NOT_CONVERGED;
+  }
+}
+
+template <typename T, typename TB>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_finit(long long n, const TB* __restrict__ b, const uint8_t* __restrict__ keep,
+                                                           T* __restrict__ x, T* __restrict__ r, double* __restrict__ part) {
+  double acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T bi = keep[i] ? (T)b[i] : T(0);
+    x[i] = T(0);
+    r[i] = bi;
+    acc += (double)bi * (double)bi;
+  }
+  const double s = block_sum_all(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_finit_fin(FcgState* st, const double* __restrict__ part, double tol, double atol, long long maxiter, int m) {
+  const double bb = reduce_partials(part);
+  if (threadIdx.x != 0) return;
+  st->cg.rr = bb;
+  st->cg.bb = bb;
+  st->cg.gamma = 0;
+  st->cg.alpha = st->cg.beta = 0;
+  st->cg.atol2 = fmax(tol * tol * bb, atol * atol);
+  st->cg.k = 0;
+  st->cg.maxiter = maxiter;
+  st->cg.status = JXB_OK;
+  st->cg.done = 0;
+  st->nd = 0;
+  st->bad = 0;
+  st->m = m;
+  if (!isfinite(bb)) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NONFINITE;
+  } else if (!(bb > st->cg.atol2)) {
+    st->cg.done = 1;
+  } else if (maxiter <= 0) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NOT_CONVERGED;
+  }
+}
+
+// restart the recurrence (after a bad learned direction or a stall)
+__global__ void k_frestart(FcgState* st) {
+  st->nd = 0;
+  st->bad = 0;
+  if (st->cg.status == JXB_OK && st->cg.k < st->cg.maxiter && st->cg.rr > st->cg.atol2) st->cg.done = 0;
+}
+
+template <typename T>
+__global__ void k_ediff(long long ncp, int vec, const float* __restrict__ e, const float* __restrict__ out,
+                        float out_scale, const uint8_t* __restrict__ keep, T* __restrict__ d) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncp * vec) return;
+  const long long cp = i / vec;
+  const int c = (int)(i % vec);
+  const long long g = (long long)c * ncp + cp;
+  d[i] = keep[i] ? (T)e[g] - (T)out_scale * (T)out[g] : T(0);
+}
+
+template <typename T>
+__global__ void k_egrad(long long ncp, int vec, const T* __restrict__ Kd, const uint8_t* __restrict__ keep, double s,
+                        float* __restrict__ g) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncp * 4) return;
+  const int c = (int)(i / ncp);
+  const long long cp = i % ncp;
+  float v = 0.f;
+  if (c < vec) {
+    const long long dof = cp * vec + c;
+    v = keep[dof] ? (float)(s * (double)Kd[dof]) : 0.f;
+  }
+  g[i] = v;
+}
+
+__global__ void k_to_f32(long long n, const double* __restrict__ r, double s, float* __restrict__ out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)(r[i] * s);
+}
+
+__global__ void k_axpy_f32(long long n, double a, const float* __restrict__ d, double* __restrict__ x) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += a * (double)d[i];
+}
+
+namespace {
+
+inline unsigned nb256(long long n) { return (unsigned)((n + 255) / 256); }
+
+// One FCG run's buffers and settings.
+struct FcgRun {
+  jxb_plan* plan;
+  jxb_cnn* cnn;
+  const float* features;
+  int n_features;
+  float in_scale;
+  double out_scale;
+  int stall, m, every;
+  FcgState *d_st = nullptr, *h_st = nullptr;
+  double* part = nullptr;  // (FCG_MMAX + 3) x JXB_RED_BLOCKS
+  float* in = nullptr;
+  void *Pr = nullptr, *APr = nullptr;
+  long long learned_iters = 0;
+  ~FcgRun() {
+    cudaFree(d_st);
+    cudaFreeHost(h_st);
+    cudaFree(part);
+    cudaFree(in);
+    cudaFree(Pr);
+    cudaFree(APr);
+  }
+};
+
+template <typename T>
+int record_iteration(FcgRun& R, cudaStream_t s, bool learned, int iters) {
+  jxb_plan* plan = R.plan;
+  constexpr bool F32 = sizeof(T) == 4;
+  T* x = F32 ? (T*)plan->d_x32 : (T*)plan->d_x;
+  T* r = F32 ? (T*)plan->d_r32 : (T*)plan->d_r;
+  T* z = F32 ? (T*)plan->d_z32 : (T*)plan->d_z;
+  T* p = F32 ? (T*)plan->d_p32 : (T*)plan->d_p;
+  T* Ap = F32 ? (T*)plan->d_Ap32 : (T*)plan->d_Ap;
+  const T* inv = F32 ? (const T*)plan->d_invdiag32 : (const T*)plan->d_invdiag;
+  const long long n = plan->n_dofs, ncp = plan->n_scalar;
+  const int vec = plan->vec;
+  double* pm = R.part;
+  double* pap = R.part + FCG_MMAX * JXB_RED_BLOCKS;
+  double* ppr = pap + JXB_RED_BLOCKS;
+  double* prr = ppr + JXB_RED_BLOCKS;
+  const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
+  for (int it = 0; it < iters; ++it) {
+    if (learned) {
+      k_fpack<T><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, r, plan->d_keep, R.in_scale, R.d_st, R.in);
+      const float* out4 = nullptr;
+      int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, &out4);
+      if (rc) return rc;
+      k_funpack<T><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, out4, plan->d_keep, R.out_scale, R.d_st, z);
+    } else {
+      k_fjac<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, inv, r, R.d_st, z);
+    }
+    k_fmdot<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, z, (const T*)R.APr, pm);
+    k_fdir<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, z, (const T*)R.Pr, pm, p);
+    int rc = launch_bricks<T>(plan, s, MODE_APPLY, p, nullptr, &R.d_st->cg, 1);
+    if (rc) return rc;
+    rc = launch_combine<T>(plan, s, Ap, 1, p, pap, &R.d_st->cg);
+    if (rc) return rc;
+    k_fpr<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, p, Ap, r, (T*)R.Pr, (T*)R.APr, ppr);
+    k_fupdate<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, pap, ppr, p, Ap, x, r, prr);
+    k_ffin<<<1, JXB_RED_THREADS, 0, s>>>(R.d_st, pap, ppr, prr);
+  }
+  JXB_CUDA(cudaGetLastError());
+  return JXB_OK;
+}
+
+template <typename T>
+int capture(FcgRun& R, cudaStream_t s, bool learned, int iters, cudaGraphExec_t* out) {
+  cudaGraph_t g;
+  JXB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  int rc = record_iteration<T>(R, s, learned, iters);
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return JXB_OK;
+}
+
+struct GraphPair {
+  cudaGraphExec_t learned = nullptr, jacobi = nullptr;
+  ~GraphPair() {
+    if (learned) cudaGraphExecDestroy(learned);
+    if (jacobi) cudaGraphExecDestroy(jacobi);
+  }
+};
+
+// Allocates the run's buffers for vectors of type T (the network input keeps
+// the feature channels after the vec residual channels).
+template <typename T>
+int fcg_setup(FcgRun& R, cudaStream_t s) {
+  jxb_plan* plan = R.plan;
+  const long long n = plan->n_dofs, ncp = plan->n_scalar;
+  JXB_CUDA(cudaMalloc(&R.d_st, sizeof(FcgState)));
+  JXB_CUDA(cudaMallocHost(&R.h_st, sizeof(FcgState)));
+  JXB_CUDA(cudaMalloc(&R.part, (FCG_MMAX + 3) * JXB_RED_BLOCKS * sizeof(double)));
+  JXB_CUDA(cudaMalloc(&R.Pr, (size_t)R.m * n * sizeof(T)));
+  JXB_CUDA(cudaMalloc(&R.APr, (size_t)R.m * n * sizeof(T)));
+  if (R.cnn) {
+    JXB_CUDA(cudaMalloc(&R.in, (size_t)(plan->vec + R.n_features) * ncp * sizeof(float)));
+    JXB_CUDA(cudaMemsetAsync(R.in, 0, (size_t)plan->vec * ncp * sizeof(float), s));
+    if (R.n_features)
+      JXB_CUDA(cudaMemcpyAsync(R.in + (size_t)plan->vec * ncp, R.features, (size_t)R.n_features * ncp * sizeof(float),
+                               cudaMemcpyDeviceToDevice, s));
+    // one forward outside capture sizes the network's activation buffers
+    const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
+    int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, nullptr);
+    if (rc) return rc;
+  }
+  return JXB_OK;
+}
+
+// Runs FCG on rhs b (type TB) into the plan's T-typed x. Returns the status
+// (JXB_OK, NOT_CONVERGED, NONFINITE) in *status and the iteration count.
+template <typename T, typename TB>
+int fcg_run(FcgRun& R, GraphPair& G, cudaStream_t s, const TB* b, double tol, double atol, long long maxiter,
+            long long* iters, int* status) {
+  jxb_plan* plan = R.plan;
+  constexpr bool F32 = sizeof(T) == 4;
+  T* x = F32 ? (T*)plan->d_x32 : (T*)plan->d_x;
+  T* r = F32 ? (T*)plan->d_r32 : (T*)plan->d_r;
+  const long long n = plan->n_dofs;
+  k_finit<T, TB><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, b, plan->d_keep, x, r, R.part);
+  k_finit_fin<<<1, JXB_RED_THREADS, 0, s>>>(R.d_st, R.part, tol, atol, maxiter, R.m);
+  JXB_CUDA(cudaGetLastError());
+  bool learned = R.cnn != nullptr;
+  if (learned && !G.learned) {
+    int rc = capture<T>(R, s, true, 1, &G.learned);
+    if (rc) return rc;
+  }
+  if (!G.jacobi) {
+    int rc = capture<T>(R, s, false, R.every, &G.jacobi);
+    if (rc) return rc;
+  }
+  JXB_CUDA(cudaMemcpyAsync(R.h_st, R.d_st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+  JXB_CUDA(cudaStreamSynchronize(s));
+  double best = R.h_st->cg.rr;
+  long long since = 0;
+  const long long cap = maxiter + 2;  // every launch advances k unless done; bounded in any case
+  for (long long l = 0; l < cap && !R.h_st->cg.done; ++l) {
+    const long long k0 = R.h_st->cg.k;
+    JXB_CUDA(cudaGraphLaunch(learned ? G.learned : G.jacobi, s));
+    JXB_CUDA(cudaMemcpyAsync(R.h_st, R.d_st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+    JXB_CUDA(cudaStreamSynchronize(s));
+    const FcgState& h = *R.h_st;
+    if (learned) {
+      R.learned_iters += h.cg.k - k0;
+      if (h.cg.rr < best) {
+        best = h.cg.rr;
+        since = 0;
+      } else {
+        since += h.cg.k - k0;
+      }
+      if (h.bad || since >= R.stall) {  // fall back to Jacobi directions
+        learned = false;
+        k_frestart<<<1, 1, 0, s>>>(R.d_st);
+        JXB_CUDA(cudaGetLastError());
+        JXB_CUDA(cudaMemcpyAsync(R.h_st, R.d_st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+        JXB_CUDA(cudaStreamSynchronize(s));
+      }
+    } else if (h.bad) {  // Jacobi direction without descent: breakdown
+      *iters = h.cg.k;
+      *status = JXB_ERR_NONFINITE;
+      return JXB_OK;
+    }
+  }
+  *iters = R.h_st->cg.k;
+  *status = R.h_st->cg.done ? R.h_st->cg.status : JXB_ERR_NOT_CONVERGED;
+  if (R.h_st->cg.done && R.h_st->cg.status == JXB_OK && R.h_st->cg.rr > R.h_st->cg.atol2)
+    *status = JXB_ERR_NOT_CONVERGED;
+  return JXB_OK;
+}
+
+}  // namespace
 }  // namespace jxb
 
 using namespace jxb;
 
-extern "C" int jxb_fcg_learned(jxb_plan* plan, struct jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
+extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                                const float* features, int n_features, float in_scale, double out_scale, int stall,
-                               const jxb_solve_opts* opts, jxb_stats* stats) {
-  if (!plan || !cnn || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: null argument");
+                               int depth, int mixed, const jxb_solve_opts* opts, jxb_stats* stats) {
+  if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: null argument");
   if (n_features < 0 || (n_features > 0 && !features)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: bad features");
-  if (!(opts->tol > 0)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: tol must be positive");
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  int rc = ensure_workspace(plan, false);
+  if (cnn && cnn_out_channels(cnn) != plan->vec)
+    return fail(JXB_ERR_INVALID, "jxb_fcg_learned: the network's outputs must equal the plan's vec");
+  if (!(opts->tol > 0) || !isfinite(opts->tol)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: tol must be finite and positive");
+  if (depth < 1 || depth > FCG_MMAX) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: depth must be in 1..8");
+  if (mixed && !plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: mixed needs a plan created with want_f32");
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+  if (!plan->graph_stream[1]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[1], cudaStreamNonBlocking));
+  cudaStream_t s = plan->graph_stream[1];
+  cudaEvent_t e0, e1, evu;
+  JXB_CUDA(cudaEventCreate(&e0));
+  JXB_CUDA(cudaEventCreate(&e1));
+  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
+  JXB_CUDA(cudaEventRecord(evu, user));
+  JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
+  int rc = ensure_workspace(plan, mixed != 0);
   if (rc) return rc;
   rc = compute_invdiag(plan, s);
   if (rc) return rc;
-  const long long n = plan->n_dofs, ncp = plan->n_scalar;
-  const int vec = plan->vec;
-  double *tmp1 = nullptr, *tmp2 = nullptr;
-  float *in = nullptr, *out = nullptr;
-  JXB_CUDA(cudaMalloc(&tmp1, n * sizeof(double)));
-  JXB_CUDA(cudaMalloc(&tmp2, n * sizeof(double)));
-  JXB_CUDA(cudaMalloc(&in, (size_t)(vec + n_features) * ncp * sizeof(float)));
-  JXB_CUDA(cudaMalloc(&out, (size_t)vec * ncp * sizeof(float)));
-  if (n_features)
-    JXB_CUDA(cudaMemcpyAsync(in + (size_t)vec * ncp, features, (size_t)n_features * ncp * sizeof(float),
-                             cudaMemcpyDeviceToDevice, s));
-  double *xv = plan->d_x, *r = plan->d_r, *z = plan->d_z;
-  double *p = plan->d_p, *Ap = plan->d_Ap, *pp = tmp1, *App = tmp2;  // current / previous direction
-  const unsigned nb = (unsigned)((n + 255) / 256);
-  cudaEvent_t e0, e1;
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
-  JXB_CUDA(cudaEventRecord(e0, s));
-  JXB_CUDA(cudaMemsetAsync(xv, 0, n * sizeof(double), s));
-  k_mask_copy<<<nb, 256, 0, s>>>(n, b, plan->d_keep, r);
-  double bb = 0;
-  if ((rc = dot(plan, s, r, r, &bb))) return rc;
-  const double atol2 = fmax(opts->tol * opts->tol * bb, opts->atol * opts->atol);
+  const long long n = plan->n_dofs;
+  FcgRun R;
+  R.plan = plan;
+  R.cnn = cnn;
+  R.features = features;
+  R.n_features = n_features;
+  R.in_scale = in_scale;
+  R.out_scale = out_scale;
+  R.stall = stall > 0 ? stall : 1 << 30;
+  R.m = depth;
+  R.every = opts->check_every > 0 ? opts->check_every : 16;
+  GraphPair G;
+  rc = mixed ? fcg_setup<float>(R, s) : fcg_setup<double>(R, s);
+  if (rc) return rc;
   const long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
-  double rr = bb, best = bb, pAp_prev = 0;
-  long long k = 0, since_best = 0, learned_iters = 0;
-  bool use_learned = true, fresh = true;
+  JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaEventRecord(e0, s));
+  long long total = 0, outer = 0;
   int status = JXB_OK;
-  const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
-  while (rr > atol2 && k < maxiter) {
-    const double rn = sqrt(rr);
-    if (use_learned) {
-      k_pack_in<<<(unsigned)((ncp * vec + 255) / 256), 256, 0, s>>>(ncp, vec, r, plan->d_keep, (float)(in_scale / rn), in);
-      if ((rc = jxb_cnn_forward(cnn, stream, nx, ny, nz, in, out))) return rc;
-      k_unpack_out<<<(unsigned)((ncp * vec + 255) / 256), 256, 0, s>>>(ncp, vec, out, plan->d_keep, rn * out_scale, z);
-    } else {
-      k_jacobi<<<nb, 256, 0, s>>>(n, plan->d_invdiag, r, z);
-    }
-    if (!fresh) {
-      double zAp = 0;
-      if ((rc = dot(plan, s, z, App, &zAp))) return rc;
-      k_dir<<<nb, 256, 0, s>>>(n, z, zAp / pAp_prev, pp, p);
-    } else {
-      JXB_CUDA(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    }
-    if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, p, nullptr, nullptr, 1))) return rc;
-    if ((rc = launch_combine<double>(plan, s, Ap, 1, nullptr, nullptr, nullptr))) return rc;
-    double pAp = 0, pr = 0;
-    if ((rc = dot(plan, s, p, Ap, &pAp))) return rc;
-    if ((rc = dot(plan, s, p, r, &pr))) return rc;
-    if (!(pAp > 0) || !isfinite(pAp) || !isfinite(pr)) {
-      if (use_learned) {  // the learned direction is unusable: continue with Jacobi
-        use_learned = false;
-        fresh = true;
-        ++k;
-        continue;
+  double rn = 0, bn = 0;
+  bool fin = true;
+  if (!mixed) {
+    rc = fcg_run<double, double>(R, G, s, plan->d_b, opts->tol, opts->atol, maxiter, &total, &status);
+    if (rc) return rc;
+    JXB_CUDA(cudaEventRecord(e1, s));
+    JXB_CUDA(cudaMemcpyAsync(x, plan->d_x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin);
+    if (rc) return rc;
+  } else {
+    // FP64 iterative refinement: the FP64 residual, normalised, is the rhs of
+    // an FP32 FCG solve to inner_tol; the correction is added in FP64.
+    double* xb = plan->d_z;
+    double* res = plan->d_r;
+    JXB_CUDA(cudaMemsetAsync(xb, 0, n * sizeof(double), s));
+    const double inner = opts->inner_tol > 0 ? opts->inner_tol : 1e-4;
+    const int max_outer = opts->max_outer > 0 ? opts->max_outer : 30;
+    rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+    if (rc) return rc;
+    while (outer < max_outer && fin && rn > opts->tol * bn && total < maxiter) {
+      float* rhs32 = plan->d_Ap32;  // copied into r32 by the FCG init before Ap32 is reused
+      k_to_f32<<<nb256(n), 256, 0, s>>>(n, res, 1.0 / rn, rhs32);
+      // the inner tolerance never asks for more than the outer target needs
+      const double itol = fmax(inner, 0.5 * opts->tol * bn / rn);
+      long long it = 0;
+      int st = 0;
+      rc = fcg_run<float, float>(R, G, s, rhs32, itol, 0.0, maxiter - total, &it, &st);
+      if (rc) return rc;
+      total += it;
+      k_axpy_f32<<<nb256(n), 256, 0, s>>>(n, rn, plan->d_x32, xb);
+      JXB_CUDA(cudaGetLastError());
+      const double prev = rn;
+      rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+      if (rc) return rc;
+      ++outer;
+      if (st == JXB_ERR_NONFINITE) {
+        status = JXB_ERR_NONFINITE;
+        break;
       }
-      status = JXB_ERR_NONFINITE;
-      break;
+      if (!(rn < prev)) break;  // stagnation: stop, the stats report it
     }
-    k_step<<<nb, 256, 0, s>>>(n, pr / pAp, p, Ap, xv, r);
-    std::swap(p, pp);
-    std::swap(Ap, App);
-    pAp_prev = pAp;
-    fresh = false;
-    if ((rc = dot(plan, s, r, r, &rr))) return rc;
-    ++k;
-    if (use_learned) ++learned_iters;
-    if (rr < best) {
-      best = rr;
-      since_best = 0;
-    } else if (++since_best >= stall && use_learned) {
-      use_learned = false;  // stagnation: finish with Jacobi directions
-      fresh = true;
-      since_best = 0;
-    }
+    JXB_CUDA(cudaEventRecord(e1, s));
+    JXB_CUDA(cudaMemcpyAsync(x, xb, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
-  if (status == JXB_OK && rr > atol2) status = JXB_ERR_NOT_CONVERGED;
-  JXB_CUDA(cudaEventRecord(e1, s));
-  JXB_CUDA(cudaMemcpyAsync(x, xv, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  // FP64 true residual (the check of src/jaxiga/solvers/diagnostics.py:8-19)
-  if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, xv, nullptr, nullptr, 1))) return rc;
-  if ((rc = launch_combine<double>(plan, s, tmp1, 1, nullptr, nullptr, nullptr))) return rc;
-  k_resid<<<nb, 256, 0, s>>>(n, b, tmp1, plan->d_keep, tmp2);
-  double res2 = 0;
-  if ((rc = dot(plan, s, tmp2, tmp2, &res2))) return rc;
+  JXB_CUDA(cudaEventRecord(evu, s));
+  JXB_CUDA(cudaStreamWaitEvent(user, evu, 0));
+  JXB_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
   JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(tmp1);
-  cudaFree(tmp2);
-  cudaFree(in);
-  cudaFree(out);
+  cudaEventDestroy(evu);
   if (stats) {
-    const double res = sqrt(res2), bn = sqrt(bb);
-    stats->iterations = k;
-    stats->outer = learned_iters;
-    stats->residual = res;
+    stats->iterations = total;
+    stats->outer = R.learned_iters;
+    stats->residual = rn;
     stats->b_norm = bn;
-    stats->relative_residual = res / (bn > 0 ? bn : 1.0);
-    stats->finite = isfinite(res) ? 1 : 0;
-    stats->converged = (isfinite(res) && res <= opts->tol * bn) ? 1 : 0;
+    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
+    stats->finite = (fin && isfinite(rn)) ? 1 : 0;
+    stats->converged = (stats->finite && rn <= opts->tol * bn) ? 1 : 0;
     stats->seconds = ms * 1e-3;
   }
-  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_fcg_learned: non-finite value");
+  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_fcg_learned: non-finite value or breakdown");
+  return JXB_OK;
+}
+
+extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in,
+                                         const float* e, float out_scale, double weight, double* loss) {
+  if (!plan || !cnn || !in || !e) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: null argument");
+  if (cnn_out_channels(cnn) != plan->vec)
+    return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: the network's outputs must equal the plan's vec");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int rc = ensure_workspace(plan, false);
+  if (rc) return rc;
+  const long long ncp = plan->n_scalar;
+  const int vec = plan->vec;
+  const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
+  const float* out4 = nullptr;
+  if ((rc = cnn_forward(cnn, s, nx, ny, nz, in, &out4))) return rc;
+  double* d = plan->d_p;
+  double* Kd = plan->d_Ap;
+  k_ediff<double><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, e, out4, out_scale, plan->d_keep, d);
+  if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, d, nullptr, nullptr, 1))) return rc;
+  if ((rc = launch_combine<double>(plan, s, Kd, 1, d, plan->d_red, nullptr))) return rc;
+  k_egrad<double><<<nb256(ncp * 4), 256, 0, s>>>(ncp, vec, Kd, plan->d_keep, -2.0 * weight * out_scale,
+                                                  cnn_grad_out(cnn));
+  JXB_CUDA(cudaGetLastError());
+  std::vector<double> h(JXB_RED_BLOCKS);
+  JXB_CUDA(cudaMemcpyAsync(h.data(), plan->d_red, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if ((rc = cnn_backward(cnn, s, nx, ny, nz, in))) return rc;
+  JXB_CUDA(cudaStreamSynchronize(s));
+  double dkd = 0;
+  for (int i = 0; i < JXB_RED_BLOCKS; ++i) dkd += h[i];
+  if (loss) *loss = weight * dkd;
   return JXB_OK;
 }

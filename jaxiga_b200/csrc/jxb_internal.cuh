@@ -41,6 +41,39 @@ int cuda_fail(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return ::jxb::cuda_fail(_e, #call); \
   } while (0)
 
+// Deterministic reductions: warp shuffle tree, then the warps of a block in
+// index order; partials of a fixed JXB_RED_BLOCKS grid summed the same way.
+static __device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum returned to every thread (fixed order).
+static __device__ double block_sum_all(double v) {
+  __shared__ double part[32];
+  __shared__ double total;
+  v = warp_sum(v);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) part[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) s += part[i];
+    total = s;
+  }
+  __syncthreads();
+  double r = total;
+  __syncthreads();
+  return r;
+}
+
+// Sum of the JXB_RED_BLOCKS partials in a fixed order, identical in every block.
+static __device__ double reduce_partials(const double* part) {
+  double v = 0;
+  for (int i = threadIdx.x; i < JXB_RED_BLOCKS; i += blockDim.x) v += part[i];
+  return block_sum_all(v);
+}
+
 // Operator-specific constants handed to kernels by value.
 struct Material {
   double lam, mu;  // elasticity (effective plane lambda in 2D)
@@ -168,5 +201,15 @@ int launch_bricks2_batch(int p, bool rational, int variant, const BrickArgs<doub
 int ensure_workspace(jxb_plan* plan, bool f32);
 int compute_invdiag(jxb_plan* plan, cudaStream_t s);
 int dot(jxb_plan* plan, cudaStream_t s, const double* a, const double* b, double* out_host);
+// ||b - K x|| over free DOFs (FP64, masked); the residual goes to res_out when
+// not null; blocks until the norms are on the host
+int true_residual(jxb_plan* plan, cudaStream_t s, const double* b, const double* x, double* res_out, double* rnorm,
+                  double* bnorm, bool* finite);
+
+// cnn.cu (the network of the learned preconditioner)
+int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4);
+float* cnn_grad_out(jxb_cnn* N);  // the 4-channel output-gradient buffer read by cnn_backward
+int cnn_backward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in);
+int cnn_out_channels(const jxb_cnn* N);
 
 }  // namespace jxb

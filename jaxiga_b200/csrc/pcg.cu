@@ -20,37 +20,6 @@
 
 namespace jxb {
 
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Block-wide sum returned to every thread (fixed order).
-__device__ double block_sum_all(double v) {
-  __shared__ double part[32];
-  __shared__ double total;
-  v = warp_sum(v);
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) part[w] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) s += part[i];
-    total = s;
-  }
-  __syncthreads();
-  double r = total;
-  __syncthreads();
-  return r;
-}
-
-// Sum of the JXB_RED_BLOCKS partials in a fixed order, identical in every block.
-__device__ double reduce_partials(const double* part) {
-  double v = 0;
-  for (int i = threadIdx.x; i < JXB_RED_BLOCKS; i += blockDim.x) v += part[i];
-  return block_sum_all(v);
-}
-
 template <typename T, typename TB>
 __global__ void __launch_bounds__(JXB_RED_THREADS) k_cg_init(long long n, const TB* __restrict__ b, const uint8_t* __restrict__ keep,
                           const T* __restrict__ invdiag, int precond, T* x, T* r, T* z, T* p,
@@ -286,8 +255,8 @@ int dot(jxb_plan* plan, cudaStream_t s, const double* a, const double* b, double
 }
 
 // ||b - A x|| over free DOFs (FP64 apply); optionally keeps the residual vector.
-static int true_residual(jxb_plan* plan, cudaStream_t s, const double* b, const double* x,
-                         double* res_out, double* rnorm, double* bnorm, bool* finite) {
+int true_residual(jxb_plan* plan, cudaStream_t s, const double* b, const double* x,
+                  double* res_out, double* rnorm, double* bnorm, bool* finite) {
   int rc = launch_bricks<double>(plan, s, MODE_APPLY, x, nullptr, nullptr, 1);
   if (rc) return rc;
   rc = launch_combine<double>(plan, s, plan->d_Ap, 1, nullptr, nullptr, nullptr);

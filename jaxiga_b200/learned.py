@@ -1,4 +1,4 @@
-"""Learned preconditioner: a 3D CNN on the control-point grid inside flexible CG.
+"""Learned preconditioner: a 3D U-Net on the control-point grid inside flexible CG.
 
 Pipeline (all arithmetic in libjxb's kernels; torch holds device memory):
 
@@ -6,11 +6,16 @@ Pipeline (all arithmetic in libjxb's kernels; torch holds device memory):
    x_j; with the converged x*, e_j = x* - x_j and r_j = K e_j (exact, one
    operator application each) are the (residual, error) pairs CG actually
    meets, early rough residuals and late smooth ones alike.
-2. ``train``: masked MSE between N(in_scale * r_j/||r_j||, features) and
-   e_j / (||r_j|| out_scale), forward and backward through the network's own
-   kernels, Adam on the flat parameter vector.
-3. ``solve``: flexible CG with z = ||r|| out_scale N(in_scale r/||r||) and
-   Jacobi-PCG as the fallback (jxb_fcg_learned).
+2. ``train``: the energy norm of the preconditioner's error,
+   (e - z)^T K (e - z) / e^T K e with z = out_scale N(in_scale r/||r||) for the
+   normalised pair, forward and backward through the network's own kernels
+   and the operator apply, Adam on the flat parameter vector. The energy norm
+   weighs the error the way CG convergence does (a plain MSE on e favours the
+   smooth components and leaves the rough ones to chance). A masked-MSE loss
+   is kept for comparison.
+3. ``solve``: truncated flexible CG with z = ||r|| out_scale N(in_scale r/||r||)
+   and Jacobi-PCG as the fallback (jxb_fcg_learned), optionally as FP32 inner
+   solves inside FP64 iterative refinement.
 
 Weights and scales are saved to / resumed from ``.npz`` files.
 """
@@ -51,11 +56,12 @@ class LearnedPreconditioner:
         The operator (its Dirichlet mask defines the free DOFs).
     features : array (n_feat, n_scalar_basis) or None
         Static per-control-point input channels, e.g. a normalised log-coefficient.
-    channels : (c0, c1, c2)
-        Channels at the three grid levels.
+    channels : sequence of int or None
+        Channels per U-Net level (2..6 levels, each in {4,8,12,16,24,32,48,64});
+        None picks :func:`default_channels` for the grid.
     """
 
-    def __init__(self, op, features=None, channels=(8, 16, 48), seed=0):
+    def __init__(self, op, features=None, channels=None, seed=0):
         import torch
 
         self.lib = _lib.load()
@@ -71,10 +77,13 @@ class LearnedPreconditioner:
         else:
             self.features = None
         self.n_feat = 0 if self.features is None else self.features.shape[0]
+        if channels is None:
+            channels = default_channels(self.grid)
         self.channels = tuple(int(c) for c in channels)
-        ch = (ctypes.c_int32 * 3)(*self.channels)
+        ch = (ctypes.c_int32 * len(self.channels))(*self.channels)
         h = ctypes.c_void_p()
-        _lib.check(self.lib.jxb_cnn_create(self.vec + self.n_feat, self.vec, ch, int(seed), ctypes.byref(h)))
+        _lib.check(self.lib.jxb_cnn_create(self.vec + self.n_feat, self.vec, len(self.channels), ch, int(seed),
+                                           ctypes.byref(h)))
         self.handle = h
         ptr, n = ctypes.c_void_p(), ctypes.c_int64()
         _lib.check(self.lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
@@ -152,14 +161,19 @@ class LearnedPreconditioner:
         return torch.as_tensor(free.any(axis=1).astype(np.float32), device=self.dev)
 
     # -- training ----------------------------------------------------------------
-    def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, log=None):
-        """Adam on masked MSE; returns the per-epoch mean losses."""
+    def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, loss="energy", log=None):
+        """Adam on the energy-norm (or masked-MSE) loss; returns the per-epoch mean losses."""
         import torch
 
+        if loss not in ("energy", "mse"):
+            raise ValueError("loss must be 'energy' or 'mse'")
         g = torch.Generator().manual_seed(seed)
         nx, ny, nz = self.grid
         m = R.shape[0]
         mask = self.mask.contiguous()
+        if loss == "energy":
+            # e^T K e of each normalised pair is e . r (r = K e exactly)
+            w = (1.0 / (E.double() * R.double()).sum(dim=(1, 2))).cpu().tolist()
         losses = []
         for ep in range(epochs):
             order = torch.randperm(m, generator=g).tolist()
@@ -169,11 +183,16 @@ class LearnedPreconditioner:
                 idx = order[i0:i0 + batch]
                 for j in idx:
                     inp = self._input(R[j] * self.in_scale)
-                    tgt = (E[j] / self.out_scale).contiguous()
-                    loss = ctypes.c_double()
-                    _lib.check(self.lib.jxb_cnn_accumulate(self.handle, _s(), nx, ny, nz, _p(inp), _p(tgt),
-                                                           _p(mask) if mask is not None else None, ctypes.byref(loss)))
-                    tot += loss.value
+                    val = ctypes.c_double()
+                    if loss == "energy":
+                        _lib.check(self.lib.jxb_cnn_accumulate_energy(
+                            self.op.handle, self.handle, _s(), _p(inp), _p(E[j].contiguous()),
+                            float(self.out_scale), float(w[j]), ctypes.byref(val)))
+                    else:
+                        tgt = (E[j] / self.out_scale).contiguous()
+                        _lib.check(self.lib.jxb_cnn_accumulate(self.handle, _s(), nx, ny, nz, _p(inp), _p(tgt),
+                                                               _p(mask), ctypes.byref(val)))
+                    tot += val.value
                     cnt += 1
                 _lib.check(self.lib.jxb_cnn_adam(self.handle, _s(), float(lr), 1.0 / len(idx)))
             losses.append(tot / max(cnt, 1))
@@ -192,21 +211,28 @@ class LearnedPreconditioner:
         inp = self._input(self._to_grid(r / rn) * self.in_scale)
         out = torch.empty((self.vec, self.ncp), dtype=torch.float32, device=self.dev)
         _lib.check(self.lib.jxb_cnn_forward(self.handle, _s(), nx, ny, nz, _p(inp), _p(out)))
-        return (out.double().t().reshape(-1) * rn * self.out_scale).contiguous()
+        z = out.double().t().reshape(-1) * rn * self.out_scale
+        return (z * torch.as_tensor(~self.op.prescribed_mask, device=self.dev)).contiguous()
 
     # -- solve -------------------------------------------------------------------
-    def solve(self, b, tol=1e-8, maxiter=None, stall=25):
-        """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats)."""
+    def solve(self, b, tol=1e-8, maxiter=None, stall=20, depth=4, mixed=False, inner_tol=1e-4, check_every=16,
+              use_network=True):
+        """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats).
+
+        ``mixed``: FP32 inner solves to ``inner_tol`` inside FP64 refinement.
+        ``use_network=False`` runs the same FCG with Jacobi only (the baseline
+        the network is measured against).
+        """
         op = self.op
         b = op._vec(b)
         x = op._empty(op.n_dofs)
-        o = op._opts(tol, 0.0, maxiter, "jacobi", 16, 0.0, 0)
+        o = op._opts(tol, 0.0, maxiter, "jacobi", check_every, inner_tol, 0)
         st = _lib.Stats()
         feats = self.features
-        rc = self.lib.jxb_fcg_learned(op.handle, self.handle, _s(), _p(b), _p(x),
+        rc = self.lib.jxb_fcg_learned(op.handle, self.handle if use_network else None, _s(), _p(b), _p(x),
                                       _p(feats) if feats is not None else None, self.n_feat,
-                                      float(self.in_scale), float(self.out_scale), int(stall),
-                                      ctypes.byref(o), ctypes.byref(st))
+                                      float(self.in_scale), float(self.out_scale), int(stall), int(depth),
+                                      1 if mixed else 0, ctypes.byref(o), ctypes.byref(st))
         if rc not in (0, 4):
             _lib.check(rc)
         out = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
@@ -229,3 +255,14 @@ class LearnedPreconditioner:
         self.in_scale = float(d["in_scale"])
         self.out_scale = float(d["out_scale"])
         self.history = list(d["history"])
+
+
+def default_channels(grid):
+    """Channels per level for a control-point grid: enough levels that the
+    coarsest grid has at most 8 points per direction (2..6 levels), 8 channels
+    on the finest level growing to 48."""
+    n = max(grid)
+    levels = 2
+    while levels < 6 and -(-n // 2 ** (levels - 1)) > 8:
+        levels += 1
+    return (8, 16, 24, 32, 48, 48)[:levels]

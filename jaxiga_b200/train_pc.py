@@ -1,13 +1,17 @@
 """Train the learned preconditioner for a benchmark workload on the GPU.
 
-    python -m jaxiga_b200.train_pc --workload elasticity --out pc.npz [--pairs 2000] [--seconds 600]
+    python -m jaxiga_b200.train_pc --workload darcy --out pc.npz [--pairs 2000] [--seconds 600]
 
 Pairs come from plain FP64 Jacobi-PCG solves of the workload itself (the load
 vector first, then seeded random right-hand sides), one (residual, error)
-pair per iteration; training runs the network's own forward/backward kernels
-and Adam until the time budget is spent; the checkpoint (weights, scales,
-loss history) is written to ``--out``. A JSON line with the training record
-is printed.
+pair per iteration; training minimises the energy norm of the
+preconditioner's error with the network's own forward/backward kernels and
+Adam until the time budget is spent; the checkpoint (weights, scales, loss
+history) is written to ``--out``. Then the workload is solved to 1e-8 by
+plain FP64 Jacobi-PCG, by flexible CG with the network (FP64), by the same
+with FP32 inner solves inside FP64 refinement, and by the flexible CG
+without the network, and one JSON line with the training record and the
+solves is printed.
 """
 
 from __future__ import annotations
@@ -36,6 +40,14 @@ def build(workload, span=None):
         fq[..., 2] -= 1.0
         F = op.load(fq)
         features = None
+    elif workload == "plate":
+        V, problem, params = workloads.config5(n=span or 256)
+        pres, _ = problem.resolve_dirichlet(params)
+        mask = np.zeros(V.n_dofs, bool)
+        mask[pres] = True
+        op = jx.Operator(V, "plate", problem.operator_coefficients(params)[0], prescribed=mask, want_f32=True)
+        F = op.load(torch.ones(V.n_elems * 25, dtype=torch.float64, device=op.device))
+        features = None
     else:
         V, problem, params = workloads.config4(n=span or 96)
         a = torch.exp(geometry_operator(V).interpolate(params["loga"])[..., 0]).cpu().numpy()
@@ -55,21 +67,23 @@ def main():
     from jaxiga_b200.learned import LearnedPreconditioner
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["elasticity", "darcy"], default="elasticity")
+    ap.add_argument("--workload", choices=["elasticity", "darcy", "plate"], default="elasticity")
     ap.add_argument("--span", type=int, default=None)
     ap.add_argument("--pairs", type=int, default=2000)
     ap.add_argument("--seconds", type=float, default=600.0)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--channels", default="8,16,48")
+    ap.add_argument("--channels", default=None, help="per-level channels, e.g. 8,16,24,32,48 (default: by grid)")
+    ap.add_argument("--epochs", type=int, default=1000)
+    ap.add_argument("--depth", type=int, default=4)
     ap.add_argument("--out", required=True)
     ap.add_argument("--seed", type=int, default=20260901)
     args = ap.parse_args()
     t0 = time.time()
     V, op, F, features = build(args.workload, args.span)
-    lp = LearnedPreconditioner(op, features=features, channels=tuple(int(c) for c in args.channels.split(",")),
-                               seed=args.seed)
+    channels = None if args.channels is None else tuple(int(c) for c in args.channels.split(","))
+    lp = LearnedPreconditioner(op, features=features, channels=channels, seed=args.seed)
     gen = torch.Generator(device=op.device).manual_seed(args.seed)
-    Rs, Es, solves = [], [], []
+    Rs, Es, solves_data = [], [], []
     have = 0
     k = 0
     while have < args.pairs:
@@ -78,7 +92,7 @@ def main():
         Rs.append(R)
         Es.append(E)
         have += R.shape[0]
-        solves.append({"iterations": st["iterations"], "pairs": int(R.shape[0])})
+        solves_data.append({"iterations": st["iterations"], "pairs": int(R.shape[0])})
         k += 1
     R = torch.cat(Rs)
     E = torch.cat(Es)
@@ -88,14 +102,38 @@ def main():
     t_data = time.time() - t0
     t1 = time.time()
     ep = 0
-    while time.time() - t1 < args.seconds:
+    while time.time() - t1 < args.seconds and ep < args.epochs:
         lr = args.lr if ep < 4 else args.lr / 3
         lp.train(R, E, epochs=1, lr=lr, batch=4, seed=ep)
         ep += 1
+    t_train = time.time() - t1
     lp.save(args.out)
-    print(json.dumps({"workload": args.workload, "n_dofs": V.n_dofs, "pairs": int(R.shape[0]), "solves": solves,
-                      "data_seconds": t_data, "train_seconds": time.time() - t1, "epochs": ep,
-                      "loss_first": lp.history[0], "loss_last": lp.history[-1], "params": lp.n_params,
+    del R, E
+    solves = {}
+    x_ref, st = op.pcg(F, tol=1e-8, preconditioner="jacobi")
+    solves["plain_fp64_jacobi_pcg"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth)
+    solves["learned_fcg_fp64"] = st
+    x_m, st = lp.solve(F, tol=1e-8, depth=args.depth, mixed=True, inner_tol=1e-4)
+    st["relative_difference_to_plain"] = float(torch.linalg.norm(x_m - x_ref) / torch.linalg.norm(x_ref))
+    solves["learned_fcg_mixed"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, use_network=False)
+    solves["fcg_jacobi_only"] = st
+    # network inference time on its own
+    r = torch.randn(V.n_dofs, dtype=torch.float64, device=op.device)
+    for _ in range(3):
+        lp.forward(r)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        lp.forward(r)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": args.workload, "n_dofs": V.n_dofs, "pairs": int(have), "channels": lp.channels,
+                      "solves_for_pairs": solves_data, "data_seconds": t_data, "train_seconds": t_train,
+                      "epochs": ep, "loss_first": lp.history[0], "loss_last": lp.history[-1],
+                      "params": lp.n_params, "forward_ms": e0.elapsed_time(e1) / 10, "solves": solves,
                       "checkpoint": args.out}))
 
 

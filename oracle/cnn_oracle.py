@@ -1,35 +1,42 @@
 """CPU oracle of the learned-preconditioner network (NumPy, FP64).
 
 TEST INFRASTRUCTURE ONLY: the GPU network (libjxb's cnn kernels) is checked
-against this restatement -- forward output and parameter gradients of the
-masked mean-squared-error loss. The reference has no learned preconditioner
-(its only preconditioner is Jacobi, src/jaxiga/solvers/linear.py:419-431), so
-this oracle restates the network the way libjxb defines it:
+against this restatement -- forward output and parameter gradients for a
+given output gradient (masked mean-squared error, or any other loss). The
+reference has no learned preconditioner (its only preconditioner is Jacobi,
+src/jaxiga/solvers/linear.py:419-431), so this oracle restates the network
+the way libjxb defines it: a U-Net with L levels and channels c[0..L-1],
 
-    level 0: in -> c0 relu; c0 -> c0 relu = s0
-    level 1: pool(s0) -> c1 relu; c1 -> c1 relu = s1
-    level 2: pool(s1) -> c2 relu; c2 -> c2 relu; c2 -> c2 relu
-    level 1: up -> 1x1 c2 -> c1 (+ s1); c1 -> c1 relu
-    level 0: up -> 1x1 c1 -> c0 (+ s0); c0 -> c0 relu; c0 -> 4 (linear; first out_ch used)
+    encoder, l = 0..L-2:  x -> c[l] relu; c[l] -> c[l] relu = s_l; x = pool(s_l)
+    bottom (level L-1):   x -> c[L-1] relu; two more c[L-1] -> c[L-1] relu
+    decoder, l = L-2..0:  y = up(y); m_l = 1x1 c[l+1] -> c[l] (y) + s_l;
+                          y = c[l] -> c[l] relu (m_l)
+    output:               c[0] -> 4 (linear; the first out_ch channels are used)
 
 3x3x3 convolutions use zero padding, tap index k = dx + 3 dy + 9 dz; pooling
 averages the existing children of a coarse voxel (odd sizes round up);
 upsampling copies a coarse voxel to its children. Parameters are one flat
-vector: per layer the weights [co][ci][k] then the biases [co].
+vector: per layer (in the order above) the weights [co][ci][k] then the
+biases [co].
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-SPECS = ["L0A", "L0B", "L1A", "L1B", "L2A", "L2B", "L2C", "L1C", "L1D", "L0C", "L0D", "L0E"]
-
-
 def layer_shapes(in_ch, channels):
-    c0, c1, c2 = channels
-    return [(in_ch, c0, 3, True), (c0, c0, 3, True), (c0, c1, 3, True), (c1, c1, 3, True), (c1, c2, 3, True),
-            (c2, c2, 3, True), (c2, c2, 3, True), (c2, c1, 1, False), (c1, c1, 3, True), (c1, c0, 1, False),
-            (c0, c0, 3, True), (c0, 4, 3, False)]
+    """(ci, co, k, relu) of every layer, in parameter order."""
+    c = [int(v) for v in channels]
+    n = len(c)
+    out, prev = [], in_ch
+    for lv in range(n - 1):
+        out += [(prev, c[lv], 3, True), (c[lv], c[lv], 3, True)]
+        prev = c[lv]
+    out += [(prev, c[-1], 3, True), (c[-1], c[-1], 3, True), (c[-1], c[-1], 3, True)]
+    for lv in range(n - 2, -1, -1):
+        out += [(c[lv + 1], c[lv], 1, False), (c[lv], c[lv], 3, True)]
+    out.append((c[0], 4, 3, False))
+    return out
 
 
 def unpack(params, in_ch, channels):
@@ -128,73 +135,84 @@ def up_grad(gf, coarse_shape):
 def forward(params, x, in_ch, channels):
     """Returns (output [4, ...], cache)."""
     L = unpack(np.asarray(params, dtype=np.float64), in_ch, channels)
+    n = len(channels)
     relu = lambda v: np.maximum(v, 0.0)  # noqa: E731
-    a = {}
-    a["in"] = x
-    a["A0A"] = relu(conv(x, *L[0][:2]))
-    a["S0"] = relu(conv(a["A0A"], *L[1][:2]))
-    a["P1"] = pool(a["S0"])
-    a["A1A"] = relu(conv(a["P1"], *L[2][:2]))
-    a["S1"] = relu(conv(a["A1A"], *L[3][:2]))
-    a["P2"] = pool(a["S1"])
-    a["A2A"] = relu(conv(a["P2"], *L[4][:2]))
-    a["A2B"] = relu(conv(a["A2A"], *L[5][:2]))
-    a["A2C"] = relu(conv(a["A2B"], *L[6][:2]))
-    a["U1"] = up(a["A2C"], a["S1"].shape[1:])
-    a["M1"] = conv(a["U1"], *L[7][:2]) + a["S1"]
-    a["A1D"] = relu(conv(a["M1"], *L[8][:2]))
-    a["U0"] = up(a["A1D"], a["S0"].shape[1:])
-    a["M0"] = conv(a["U0"], *L[9][:2]) + a["S0"]
-    a["A0D"] = relu(conv(a["M0"], *L[10][:2]))
-    out = conv(a["A0D"], *L[11][:2])
+    a = {"in": x, "enc_in": [], "A": [], "S": [], "D": [None] * (n - 1)}
+    i = 0
+    h = x
+    for lv in range(n - 1):
+        a["enc_in"].append(h)
+        a["A"].append(relu(conv(h, *L[i][:2])))
+        a["S"].append(relu(conv(a["A"][-1], *L[i + 1][:2])))
+        h = pool(a["S"][-1])
+        i += 2
+    a["bot_in"] = h
+    a["B0"] = relu(conv(h, *L[i][:2]))
+    a["B1"] = relu(conv(a["B0"], *L[i + 1][:2]))
+    a["B2"] = relu(conv(a["B1"], *L[i + 2][:2]))
+    i += 3
+    y = a["B2"]
+    a["U"] = [None] * (n - 1)
+    a["M"] = [None] * (n - 1)
+    for lv in range(n - 2, -1, -1):
+        a["U"][lv] = up(y, a["S"][lv].shape[1:])
+        a["M"][lv] = conv(a["U"][lv], *L[i][:2]) + a["S"][lv]
+        a["D"][lv] = relu(conv(a["M"][lv], *L[i + 1][:2]))
+        y = a["D"][lv]
+        i += 2
+    out = conv(y, *L[i][:2])
     return out, (L, a)
+
+
+def backward(params, x, gout, in_ch, channels):
+    """Flat parameter gradient of sum(gout * forward(x)[:gout.shape[0]])."""
+    out, (L, a) = forward(params, x, in_ch, channels)
+    n = len(channels)
+    g = np.zeros_like(out)
+    g[: gout.shape[0]] = gout
+    grads = [None] * len(L)
+    mask_relu = lambda gg, act: gg * (act > 0)  # noqa: E731
+    i = len(L) - 1
+    gx, gw, gb = conv_grads(a["D"][0], L[i][0], g)
+    grads[i] = (gw, gb)
+    gskip = [None] * (n - 1)
+    i -= 2  # the level-0 decoder 1x1 layer; its 3x3 partner is i + 1
+    for lv in range(n - 1):
+        gx = mask_relu(gx, a["D"][lv])
+        gx, gw, gb = conv_grads(a["M"][lv], L[i + 1][0], gx)
+        grads[i + 1] = (gw, gb)
+        gskip[lv] = gx.copy()
+        gx, gw, gb = conv_grads(a["U"][lv], L[i][0], gx)
+        grads[i] = (gw, gb)
+        coarse = a["D"][lv + 1] if lv + 1 < n - 1 else a["B2"]
+        gx = up_grad(gx, coarse.shape[1:])
+        i -= 2
+    ib = 2 * (n - 1)  # first bottom layer
+    gx = mask_relu(gx, a["B2"])
+    gx, gw, gb = conv_grads(a["B1"], L[ib + 2][0], gx)
+    grads[ib + 2] = (gw, gb)
+    gx = mask_relu(gx, a["B1"])
+    gx, gw, gb = conv_grads(a["B0"], L[ib + 1][0], gx)
+    grads[ib + 1] = (gw, gb)
+    gx = mask_relu(gx, a["B0"])
+    gx, gw, gb = conv_grads(a["bot_in"], L[ib][0], gx)
+    grads[ib] = (gw, gb)
+    for lv in range(n - 2, -1, -1):
+        gs = mask_relu(gskip[lv] + pool_grad(gx, a["S"][lv].shape[1:]), a["S"][lv])
+        gx, gw, gb = conv_grads(a["A"][lv], L[2 * lv + 1][0], gs)
+        grads[2 * lv + 1] = (gw, gb)
+        gx = mask_relu(gx, a["A"][lv])
+        gx, gw, gb = conv_grads(a["enc_in"][lv], L[2 * lv][0], gx)
+        grads[2 * lv] = (gw, gb)
+    return np.concatenate([np.concatenate([gw.reshape(-1), gb]) for gw, gb in grads])
 
 
 def loss_and_grads(params, x, target, mask, in_ch, out_ch, channels):
     """Masked MSE over the first out_ch outputs and its parameter gradient (flat)."""
-    out, (L, a) = forward(params, x, in_ch, channels)
+    out, _ = forward(params, x, in_ch, channels)
     m = np.ones(x.shape[1:]) if mask is None else mask
     diff = out[:out_ch] - target
     denom = m.sum() * out_ch
     loss = float((m * diff**2).sum() / denom)
-    g = np.zeros_like(out)
-    g[:out_ch] = 2 * m * diff / denom
-    grads = [None] * len(L)
-    mask_relu = lambda gg, act: gg * (act > 0)  # noqa: E731
-    gx, gw, gb = conv_grads(a["A0D"], L[11][0], g)
-    grads[11] = (gw, gb)
-    gx = mask_relu(gx, a["A0D"])
-    gx, gw, gb = conv_grads(a["M0"], L[10][0], gx)
-    grads[10] = (gw, gb)
-    gS0 = gx.copy()
-    gx, gw, gb = conv_grads(a["U0"], L[9][0], gx)
-    grads[9] = (gw, gb)
-    gx = mask_relu(up_grad(gx, a["A1D"].shape[1:]), a["A1D"])
-    gx, gw, gb = conv_grads(a["M1"], L[8][0], gx)
-    grads[8] = (gw, gb)
-    gS1 = gx.copy()
-    gx, gw, gb = conv_grads(a["U1"], L[7][0], gx)
-    grads[7] = (gw, gb)
-    gx = mask_relu(up_grad(gx, a["A2C"].shape[1:]), a["A2C"])
-    gx, gw, gb = conv_grads(a["A2B"], L[6][0], gx)
-    grads[6] = (gw, gb)
-    gx = mask_relu(gx, a["A2B"])
-    gx, gw, gb = conv_grads(a["A2A"], L[5][0], gx)
-    grads[5] = (gw, gb)
-    gx = mask_relu(gx, a["A2A"])
-    gx, gw, gb = conv_grads(a["P2"], L[4][0], gx)
-    grads[4] = (gw, gb)
-    gS1 = mask_relu(gS1 + pool_grad(gx, a["S1"].shape[1:]), a["S1"])
-    gx, gw, gb = conv_grads(a["A1A"], L[3][0], gS1)
-    grads[3] = (gw, gb)
-    gx = mask_relu(gx, a["A1A"])
-    gx, gw, gb = conv_grads(a["P1"], L[2][0], gx)
-    grads[2] = (gw, gb)
-    gS0 = mask_relu(gS0 + pool_grad(gx, a["S0"].shape[1:]), a["S0"])
-    gx, gw, gb = conv_grads(a["A0A"], L[1][0], gS0)
-    grads[1] = (gw, gb)
-    gx = mask_relu(gx, a["A0A"])
-    gx, gw, gb = conv_grads(x, L[0][0], gx)
-    grads[0] = (gw, gb)
-    flat = np.concatenate([np.concatenate([gw.reshape(-1), gb]) for gw, gb in grads])
-    return loss, out, flat
+    g = 2 * m * diff / denom
+    return loss, out, backward(params, x, g, in_ch, channels)

@@ -1,7 +1,9 @@
 """The learned preconditioner on the GPU: network forward and gradients against
 the NumPy oracle (FP32 kernels vs FP64 oracle: 2e-4 relative on outputs, 2e-3
-relative to the largest entry on gradients), and flexible CG with the trained
-network against plain Jacobi-PCG (same tolerance, same answer, fewer iterations)."""
+relative to the largest entry on gradients) for 2-4 level U-Nets, the
+energy-norm training step against the oracle network plus the assembled
+oracle operator, and truncated flexible CG with the trained network against
+plain Jacobi-PCG (same tolerance, same answer, fewer iterations)."""
 
 import ctypes
 
@@ -11,6 +13,7 @@ import pytest
 import jaxiga_b200 as jx
 from jaxiga_b200 import _lib
 from jaxiga_b200.learned import LearnedPreconditioner, _DeviceArray
+from jaxiga_b200.space import expand_dofs
 from oracle import cnn_oracle
 
 pytestmark = pytest.mark.gpu
@@ -26,20 +29,40 @@ def _s():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-@pytest.mark.parametrize("grid,in_ch,out_ch,channels", [((9, 7, 5), 2, 1, (4, 8, 12)), ((6, 6, 1), 3, 3, (8, 8, 16))])
+def _make_net(lib, in_ch, out_ch, channels, seed, rng):
+    import torch
+
+    h = ctypes.c_void_p()
+    _lib.check(lib.jxb_cnn_create(in_ch, out_ch, len(channels), (ctypes.c_int32 * len(channels))(*channels), seed,
+                                  ctypes.byref(h)))
+    ptr, n = ctypes.c_void_p(), ctypes.c_int64()
+    _lib.check(lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
+    params = torch.as_tensor(_DeviceArray(ptr.value, n.value), device="cuda")
+    params.copy_(torch.as_tensor(rng.uniform(-0.3, 0.3, n.value), dtype=torch.float32))
+    return h, params.cpu().numpy().astype(np.float64)
+
+
+def _grads(lib, h):
+    import torch
+
+    gp, gn = ctypes.c_void_p(), ctypes.c_int64()
+    _lib.check(lib.jxb_cnn_grads(h, ctypes.byref(gp), ctypes.byref(gn)))
+    return torch.as_tensor(_DeviceArray(gp.value, gn.value), device="cuda").cpu().numpy()
+
+
+@pytest.mark.parametrize("grid,in_ch,out_ch,channels", [
+    ((9, 7, 5), 2, 1, (4, 8, 12)),
+    ((6, 6, 1), 3, 3, (8, 8, 16)),
+    ((19, 18, 17), 2, 1, (8, 16, 24, 32)),
+    ((11, 9, 7), 4, 3, (12, 24)),
+    ((21, 5, 3), 1, 1, (16, 32, 48)),
+])
 def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels):
     import torch
 
     lib = _lib.load()
-    h = ctypes.c_void_p()
-    _lib.check(lib.jxb_cnn_create(in_ch, out_ch, (ctypes.c_int32 * 3)(*channels), 5, ctypes.byref(h)))
-    ptr, n = ctypes.c_void_p(), ctypes.c_int64()
-    _lib.check(lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
-    params = torch.as_tensor(_DeviceArray(ptr.value, n.value), device="cuda")
     rng = np.random.default_rng(3)
-    p = rng.uniform(-0.3, 0.3, n.value)
-    params.copy_(torch.as_tensor(p, dtype=torch.float32))
-    p32 = params.cpu().numpy().astype(np.float64)
+    h, p32 = _make_net(lib, in_ch, out_ch, channels, 5, rng)
     nx, ny, nz = grid
     x = rng.standard_normal((in_ch, nz, ny, nx))
     t = rng.standard_normal((out_ch, nz, ny, nx))
@@ -47,9 +70,9 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
     xd = torch.as_tensor(x, dtype=torch.float32, device="cuda").contiguous()
     out = torch.empty((out_ch, nz, ny, nx), dtype=torch.float32, device="cuda")
     _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out)))
-    loss_ref, out_ref, g_ref = cnn_oracle.loss_and_grads(p32, x.astype(np.float32).astype(np.float64),
-                                                         t.astype(np.float32).astype(np.float64), mask, in_ch,
-                                                         out_ch, channels)
+    x32 = x.astype(np.float32).astype(np.float64)
+    loss_ref, out_ref, g_ref = cnn_oracle.loss_and_grads(p32, x32, t.astype(np.float32).astype(np.float64), mask,
+                                                         in_ch, out_ch, channels)
     o = out.cpu().numpy()
     assert np.abs(o - out_ref[:out_ch]).max() <= 2e-4 * np.abs(out_ref[:out_ch]).max()
     _lib.check(lib.jxb_cnn_zero_grad(h, _s()))
@@ -57,12 +80,69 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
     td = torch.as_tensor(t, dtype=torch.float32, device="cuda").contiguous()
     md = torch.as_tensor(mask, dtype=torch.float32, device="cuda").contiguous()
     _lib.check(lib.jxb_cnn_accumulate(h, _s(), nx, ny, nz, _p(xd), _p(td), _p(md), ctypes.byref(loss)))
-    gp, gn = ctypes.c_void_p(), ctypes.c_int64()
-    _lib.check(lib.jxb_cnn_grads(h, ctypes.byref(gp), ctypes.byref(gn)))
-    g = torch.as_tensor(_DeviceArray(gp.value, gn.value), device="cuda").cpu().numpy()
+    g = _grads(lib, h)
+    assert abs(loss.value - loss_ref) <= 1e-4 * abs(loss_ref)
+    assert np.abs(g - g_ref).max() <= 2e-3 * np.abs(g_ref).max()
+    # backward from an arbitrary output gradient
+    gout = rng.standard_normal((out_ch, nz, ny, nx))
+    god = torch.as_tensor(gout, dtype=torch.float32, device="cuda").contiguous()
+    _lib.check(lib.jxb_cnn_zero_grad(h, _s()))
+    _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out)))
+    _lib.check(lib.jxb_cnn_backward(h, _s(), nx, ny, nz, _p(xd), _p(god)))
+    g2 = _grads(lib, h)
+    g2_ref = cnn_oracle.backward(p32, x32, gout.astype(np.float32).astype(np.float64), in_ch, channels)
+    assert np.abs(g2 - g2_ref).max() <= 2e-3 * np.abs(g2_ref).max()
+    lib.jxb_cnn_destroy(h)
+
+
+@pytest.mark.parametrize("op_name", ["poisson", "elasticity"])
+def test_energy_loss_gradient_matches_oracle(op_name):
+    """loss = w d^T K d, d = P_f (e - s N(in)), against the oracle network and assembled K."""
+    import torch
+
+    from oracle import iga_oracle as O
+
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    kn = np.linspace(0, 1, 4)[1:-1]
+    vec = 3 if op_name == "elasticity" else 1
+    V = jx.FunctionSpace(jx.primitives.cuboid([0, 0, 0], [1, 1, 1]).elevate(3).insert_knots(kn, kn, kn), vec=vec)
+    pres = np.unique(expand_dofs(V.side_indices("u0"), vec))
+    mask = np.zeros(V.n_dofs, bool)
+    mask[pres] = True
+    coef = (1.0, 0.3) if vec == 3 else (1.0,)
+    op = jx.Operator(V, op_name, coef, prescribed=mask)
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, vec)
+    params = {"E": 1.0, "nu": 0.3} if vec == 3 else {"a0": 1.0}
+    A = O.Assembled(S, op_name, params, pres, np.zeros(len(pres)), need_full=False)
+    nx, ny, nz = V.n_cp
+    ncp = V.n_scalar_basis
+    in_ch = vec + 1
+    h, p32 = _make_net(lib, in_ch, vec, (4, 8, 12), 7, rng)
+    x = rng.standard_normal((in_ch, nz, ny, nx))
+    e = rng.standard_normal((vec, nz, ny, nx))
+    s, w = 0.7, 0.3
+    xd = torch.as_tensor(x, dtype=torch.float32, device="cuda").contiguous()
+    ed = torch.as_tensor(e, dtype=torch.float32, device="cuda").contiguous()
+    _lib.check(lib.jxb_cnn_zero_grad(h, _s()))
+    loss = ctypes.c_double()
+    _lib.check(lib.jxb_cnn_accumulate_energy(op.handle, h, _s(), _p(xd), _p(ed), s, w, ctypes.byref(loss)))
+    g = _grads(lib, h)
+    # oracle: grid [c][cp] <-> DOF vec*cp + c
+    x32 = x.astype(np.float32).astype(np.float64)
+    out, _ = cnn_oracle.forward(p32, x32, in_ch, (4, 8, 12))
+    e32 = e.astype(np.float32).astype(np.float64)
+    d = (e32 - s * out[:vec]).reshape(vec, ncp).T.reshape(-1)
+    d[mask] = 0.0
+    Kd = np.zeros(V.n_dofs)
+    Kd[A.free] = A.K @ d[A.free]
+    loss_ref = w * float(d @ Kd)
+    gout = (-2.0 * w * s * Kd).reshape(ncp, vec).T.reshape(vec, nz, ny, nx)
+    g_ref = cnn_oracle.backward(p32, x32, gout, in_ch, (4, 8, 12))
     assert abs(loss.value - loss_ref) <= 1e-4 * abs(loss_ref)
     assert np.abs(g - g_ref).max() <= 2e-3 * np.abs(g_ref).max()
     lib.jxb_cnn_destroy(h)
+    op.close()
 
 
 def _darcy(n=16, seed=4):
@@ -78,7 +158,7 @@ def _darcy(n=16, seed=4):
     geo.close()
     mask = np.zeros(V.n_dofs, bool)
     mask[np.unique(np.concatenate([V.side_indices(s) for s in ("u0", "u1", "v0", "v1", "w0", "w1")]))] = True
-    op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a)
+    op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a, want_f32=True)
     feat = ((loga - loga.mean()) / loga.std())[None, :]
     return V, op, feat
 
@@ -88,22 +168,30 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
 
     V, op, feat = _darcy(16)
     b = op.load(torch.ones(V.n_elems * 64, dtype=torch.float64, device="cuda"))
-    lp = LearnedPreconditioner(op, features=feat, channels=(8, 16, 32), seed=1)
+    lp = LearnedPreconditioner(op, features=feat, seed=1)
     R, E, st = lp.pairs_from_solve(b, n_pairs=400, every=1, tol=1e-12)
     assert st["converged"] and R.shape[0] > 50
-    losses = lp.train(R, E, epochs=6, lr=3e-3, batch=4)
+    losses = lp.train(R, E, epochs=8, lr=3e-3, batch=4)
     assert losses[-1] < losses[0]
     x_ref, st_ref = op.pcg(b, tol=1e-8, preconditioner="jacobi")
     x, st_l = lp.solve(b, tol=1e-8)
     assert st_l["converged"] and st_ref["converged"]
     rel = float(torch.linalg.norm(x - x_ref) / torch.linalg.norm(x_ref))
     assert rel < 1e-6
-    # the trained network takes fewer Krylov iterations than Jacobi
+    # the trained network takes fewer Krylov iterations than Jacobi-PCG, and
+    # the same flexible CG without the network matches Jacobi-PCG
+    _, st_j = lp.solve(b, tol=1e-8, use_network=False)
+    assert st_j["converged"] and abs(st_j["iterations"] - st_ref["iterations"]) <= 2, (st_j, st_ref)
+    assert st_l["learned_iterations"] == st_l["iterations"], st_l
     assert st_l["iterations"] < st_ref["iterations"], (st_l, st_ref)
+    # mixed precision: FP32 inner flexible CG inside FP64 refinement
+    x_m, st_m = lp.solve(b, tol=1e-8, mixed=True, inner_tol=1e-4)
+    assert st_m["converged"], st_m
+    assert float(torch.linalg.norm(x_m - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
     # checkpoint / resume reproduces the preconditioner
     path = tmp_path / "pc.npz"
     lp.save(path)
-    lp2 = LearnedPreconditioner(op, features=feat, channels=(8, 16, 32), seed=9)
+    lp2 = LearnedPreconditioner(op, features=feat, seed=9)
     lp2.load(path)
     r = torch.randn(V.n_dofs, dtype=torch.float64, device="cuda") * torch.as_tensor(~op.prescribed_mask, device="cuda")
     assert torch.equal(lp.forward(r), lp2.forward(r))
