@@ -24,6 +24,7 @@
 // hit L2. Keeping the tile out of shared memory is what lets two 256-thread
 // CTAs share an SM.
 #include <math.h>
+#include <stdlib.h>
 
 #include "jxb_internal.cuh"
 
@@ -544,6 +545,17 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
 }
 
 #include "brick2d.cuh"
+#include "brick3_mma.cuh"
+
+// The FP64 tensor-core brick kernel runs the degree-3 scalar apply unless the
+// environment sets JXB_BRICK3_MMA=0 (the FMA kernel then runs, e.g. to compare).
+static bool use_brick3_mma() {
+  static const bool on = [] {
+    const char* e = getenv("JXB_BRICK3_MMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 // ---------------------------------------------------------------------------
 // combine: y_i = sum over covering bricks (fixed order); optional p.y partials
@@ -650,6 +662,16 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
     if constexpr (OPK == OPK_PLATE) {
       return fail(JXB_ERR_INVALID, "plate operator is 2D only");
     } else {
+      if constexpr (sizeof(T) == 8 && P == 3 && OPK == OPK_SCALAR && !RAT && MODE == MODE_APPLY) {
+        if (use_brick3_mma()) {
+          const size_t sm = smem3_mma(br);
+          if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory");
+          JXB_CUDA(cudaFuncSetAttribute(k_brick3_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          k_brick3_mma<<<(unsigned)br.n_bricks, bm::NT, sm, s>>>(A);
+          JXB_CUDA(cudaGetLastError());
+          return JXB_OK;
+        }
+      }
       constexpr int NT = BrickShape<3, P>::TX * BrickShape<3, P>::TY * Q * Q;
       size_t sm = smem3<T, P, Q, OPK, RAT, MODE>(br);
       if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory for this degree/operator");

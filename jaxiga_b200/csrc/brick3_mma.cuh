@@ -1,0 +1,288 @@
+// FP64 tensor-core variant of the 3D brick apply for the scalar operator
+// (Poisson / Darcy, polynomial weights) at degree 3 with 4 Gauss points per
+// direction. Included by apply.cu inside namespace jxb.
+//
+// At p = 3 every 1D contraction of the sum factorisation is a product of the
+// 8 x 4 table [N; N'] (rows: 4 points x value/derivative, columns: the 4
+// Bernstein functions) with a 4-row slab of element data, i.e. exactly the
+// shape of mma.sync.m8n8k4.f64: one instruction does the 256 multiply-adds
+// that take 256 scalar FMAs (and as many table loads) otherwise. The
+// backward contractions use the transposed tables [N^T; N'^T] (or the halves
+// swapped, so the needed product lands in rows 0-3).
+//
+// Work split: the CTA owns one 4 x 4 x 8 element brick as in the scalar
+// kernel; each of its 16 warps owns one element of the current layer and
+// runs the element's whole pipeline warp-synchronously (forward x, y, z;
+// point operator; backward z, y, x -- 28 MMAs), handing data between stages
+// through a private, padded shared-memory area (__syncwarp between stages).
+// Element residuals go to the layer stage and the same fixed-order gather
+// as the scalar kernel sums them into the brick footprint, so the result is
+// bitwise reproducible.
+//
+// Fragment layouts of m8n8k4 (lane l, g = l >> 2, t = l & 3):
+//   A (8x4, row): a = A[g][t];  B (4x8, col): b = B[t][g];  C/D (8x8): d_i = D[g][2t + i].
+
+namespace bm {
+constexpr int P1 = 4, Q = 4, NQE = 64, NG = 6;
+constexpr int TX = 4, TY = 4, CZ = 8, NE = TX * TY, NT = NE * 32;
+constexpr int XS = 20;               // XB[rX (8)][c (16)], c = i1 + 4 i2
+constexpr int YR = 8, Y2 = 68;       // YB[i2 (4)][rY (8)][rX (8)]
+constexpr int F2 = 20, FC = 4 * F2;  // FB[channel (3)][q2 (4)][n (16)], n = q0 + 4 q1
+constexpr int T2 = 24, TC = 4 * T2;  // TB[channel (3)][i2 (4)][n (16)]
+constexpr int S1 = 20, SC = 4 * S1;  // SB[type (2)][i1 (4)][m (16)], m = q0 + 4 i2
+constexpr int RA = 3 * FC;           // region A (XB, FB, SB): 240 doubles
+constexpr int RB = 3 * TC;           // region B (YB, TB): 288 doubles
+constexpr int WB = RA + RB;          // per-warp doubles
+constexpr int SU0 = 12;              // row stride of the layer input tile
+constexpr int SPL = 6;               // line stride of the element residual stage
+constexpr int SST = 16 * SPL;        // element stride of the stage
+static_assert(8 * XS <= RA && 2 * SC <= RA && 4 * Y2 <= RB, "per-warp regions");
+}  // namespace bm
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0, double c1) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
+      : "=d"(d0), "=d"(d1)
+      : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+static size_t smem3_mma(const Bricks& br) {
+  using namespace bm;
+  const size_t acc = ((size_t)br.fp[0] * br.fp[1] * br.fp[2] + 1) / 2 * 2;
+  const size_t n = (size_t)NE * WB + (TX + TY + 1) * 32 + (size_t)NE * SST + acc + (size_t)P1 * br.fp[1] * SU0;
+  return n * sizeof(double) + (TX + TY) * sizeof(int) + 64;
+}
+
+__global__ void __launch_bounds__(bm::NT, 2) k_brick3_mma(BrickArgs<double> A) {
+  using namespace bm;
+  if (A.state && A.state->done) return;
+  const Bricks& br = A.br;
+  const int fp0 = br.fp[0], fp1 = br.fp[1], fp2 = br.fp[2];
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* wbuf = reinterpret_cast<double*>(smem_raw);  // [NE][WB]
+  double* stx = wbuf + NE * WB;                          // [TX][32]: [2][Q][P1] per element column
+  double* sty = stx + TX * 32;                           // [TY][32]
+  double* stz = sty + TY * 32;                           // [32]
+  double* stage = stz + 32;                              // [NE][16 lines][SPL]
+  double* acc = stage + NE * SST;                        // [fp2][fp1][fp0]
+  const int accn = fp0 * fp1 * fp2;
+  double* su = acc + (accn + 1) / 2 * 2;                 // [P1][fp1][SU0]
+  int* soff = reinterpret_cast<int*>(su + P1 * fp1 * SU0);
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const long long b = blockIdx.x;
+  const int bx = (int)(b % br.nb[0]);
+  const int by = (int)((b / br.nb[0]) % br.nb[1]);
+  const int bz = (int)(b / ((long long)br.nb[0] * br.nb[1]));
+  const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by], cp0z = br.bcp0[2][bz];
+  const int exl = w % TX, eyl = w / TX;
+  const int ex = bx * TX + exl, ey = by * TY + eyl;
+  const bool evalid = ex < br.n_span[0] && ey < br.n_span[1];
+  const long long slot_base = b * (long long)CZ * NE;
+  const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
+  constexpr unsigned TILE_BYTES = NE * NG * NQE * sizeof(double);
+  if (tid == 0) prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, TILE_BYTES);
+
+  for (int i = tid; i < TX * 32; i += NT) {
+    const int e = i >> 5, r = i & 31;
+    const int sp = min(bx * TX + e, br.n_span[0] - 1);
+    stx[i] = A.tab[0][(size_t)sp * 3 * Q * P1 + r];
+  }
+  for (int i = tid; i < TY * 32; i += NT) {
+    const int e = i >> 5, r = i & 31;
+    const int sp = min(by * TY + e, br.n_span[1] - 1);
+    sty[i] = A.tab[1][(size_t)sp * 3 * Q * P1 + r];
+  }
+  if (tid < TX) {
+    const int e = bx * TX + tid;
+    soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
+  }
+  if (tid < TY) {
+    const int e = by * TY + tid;
+    soff[TX + tid] = e < br.n_span[1] ? br.first[1][e] - cp0y : -100000;
+  }
+  for (int i = tid; i < accn; i += NT) acc[i] = 0.0;
+  __syncthreads();
+
+  // A fragments of this warp's element that stay fixed across layers
+  const double* tx_ = stx + exl * 32;
+  const double* ty_ = sty + eyl * 32;
+  const int bo = t * 4 + (g & 3);        // [q = t][i = g & 3] of a [2][Q][P1] table
+  const int ty0 = (g >> 2) * 16, ty1 = (1 - (g >> 2)) * 16;
+  const double ax = tx_[lane], ay = ty_[lane];
+  const double axb = tx_[ty0 + bo], axb2 = tx_[ty1 + bo];
+  const double ayb = ty_[ty0 + bo], ayb2 = ty_[ty1 + bo];
+  const int ox = evalid ? br.first[0][ex] - cp0x : 0, oy = evalid ? br.first[1][ey] - cp0y : 0;
+  double* RA_ = wbuf + w * WB;
+  double* RB_ = RA_ + RA;
+  const long long nxy = (long long)br.n_cp[0] * br.n_cp[1];
+  const bool hi = lane >= 16;
+  const int hh = hi ? 1 : 0;
+
+  for (int lz = 0; lz < nlayers; ++lz) {
+    const int ez = bz * CZ + lz;
+    const int fz = br.first[2][ez];
+    const int offz = fz - cp0z;
+    const long long slot = slot_base + (long long)lz * NE + w;
+    if (tid == 0 && lz + 1 < nlayers)
+      prefetch_l2(A.geo + (size_t)(slot_base + (long long)(lz + 1) * NE) * NG * NQE, TILE_BYTES);
+    if (tid < 32) stz[tid] = A.tab[2][(size_t)ez * 3 * Q * P1 + tid];
+    for (int i = tid; i < P1 * fp1 * fp0; i += NT) {
+      const int jx = i % fp0, rest = i / fp0;
+      const int jy = rest % fp1, jz = rest / fp1;
+      const int gx = cp0x + jx, gy = cp0y + jy;
+      double v = 0.0;
+      if (gx < br.n_cp[0] && gy < br.n_cp[1]) {
+        const long long dof = gx + (long long)br.n_cp[0] * gy + nxy * (fz + jz);
+        v = A.x[dof];
+        if (A.masked && !A.keep[dof]) v = 0.0;
+      }
+      su[(jz * fp1 + jy) * SU0 + jx] = v;
+    }
+    __syncthreads();
+
+    if (evalid) {
+      const double az = stz[lane];
+      const double azb = stz[ty0 + bo], azb2 = stz[ty1 + bo];
+      // ---- forward x: D[rX = (type, q0)][c = i1 + 4 i2] -> XB
+      const double* ue = su + oy * SU0 + ox;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const double bv = ue[((2 * j + (g >> 2)) * fp1 + (g & 3)) * SU0 + t];
+        double d0, d1;
+        dmma(d0, d1, ax, bv, 0.0, 0.0);
+        st2(RA_ + g * XS + 8 * j + 2 * t, d0, d1);
+      }
+      __syncwarp();
+      // ---- forward y (i2 = jj): D[rY = (type, q1)][rX] -> YB[i2][rY][rX]
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const double bv = RA_[g * XS + t + 4 * jj];
+        double d0, d1;
+        dmma(d0, d1, ay, bv, 0.0, 0.0);
+        st2(RB_ + jj * Y2 + g * YR + 2 * t, d0, d1);
+      }
+      __syncwarp();
+      // ---- geometric factors of this lane's two points (issued early)
+      const double* G = A.geo + (size_t)slot * NG * NQE + 16 * (g & 3) + 8 * hh + 2 * t;
+      double2 kf[NG];
+#pragma unroll
+      for (int k = 0; k < NG; ++k) kf[k] = __ldg(reinterpret_cast<const double2*>(G + k * NQE));
+      // ---- forward z, columns n = 8h + g -> (q0, q1) = (g & 3, 2h + (g >> 2))
+      double gxr[2][2], gyr[2][2], gzr[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double* yb = RB_ + t * Y2 + (2 * h + (g >> 2)) * YR + (g & 3);
+        const double bdv = yb[4];           // rY = (v, q1), rX = (d, q0): x-derivative
+        const double bvd = yb[4 * YR];      // rY = (d, q1), rX = (v, q0): y-derivative
+        const double bvv = yb[0];           // both values
+        dmma(gxr[h][0], gxr[h][1], az, bdv, 0.0, 0.0);  // rows 0-3: gx
+        dmma(gyr[h][0], gyr[h][1], az, bvd, 0.0, 0.0);  // rows 0-3: gy
+        dmma(gzr[h][0], gzr[h][1], az, bvv, 0.0, 0.0);  // rows 4-7: gz
+      }
+      // lanes 0-15 keep the points of h = 0, lanes 16-31 those of h = 1
+      double GX[2], GY[2], GZ[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double r1 = __shfl_xor_sync(0xffffffffu, hi ? gzr[0][i] : gxr[1][i], 16);
+        const double r2 = __shfl_xor_sync(0xffffffffu, gyr[1][i], 16);
+        GX[i] = hi ? r1 : gxr[0][i];
+        GY[i] = hi ? r2 : gyr[0][i];
+        GZ[i] = hi ? gzr[1][i] : r1;
+      }
+      // ---- point operator: flux = M_q grad u (symmetric 3 x 3 metric)
+      {
+        const double k0[2] = {kf[0].x, kf[0].y}, k1[2] = {kf[1].x, kf[1].y}, k2[2] = {kf[2].x, kf[2].y};
+        const double k3[2] = {kf[3].x, kf[3].y}, k4[2] = {kf[4].x, kf[4].y}, k5[2] = {kf[5].x, kf[5].y};
+        double fx[2], fy[2], fz_[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          fx[i] = k0[i] * GX[i] + k1[i] * GY[i] + k2[i] * GZ[i];
+          fy[i] = k1[i] * GX[i] + k3[i] * GY[i] + k4[i] * GZ[i];
+          fz_[i] = k2[i] * GX[i] + k4[i] * GY[i] + k5[i] * GZ[i];
+        }
+        double* fb = RA_ + (g & 3) * F2 + 8 * hh + 2 * t;
+        st2(fb, fx[0], fx[1]);
+        st2(fb + FC, fy[0], fy[1]);
+        st2(fb + 2 * FC, fz_[0], fz_[1]);
+      }
+      __syncwarp();
+      // ---- backward z: T[channel][i2][n] (rows 0-3 of each product)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double* fb = RA_ + t * F2 + 8 * h + g;
+        double a0, a1, b0, b1, c0, c1;
+        dmma(a0, a1, azb, fb[0], 0.0, 0.0);        // Nz^T fx  -> T_dv
+        dmma(b0, b1, azb, fb[FC], 0.0, 0.0);       // Nz^T fy  -> T_vd
+        dmma(c0, c1, azb2, fb[2 * FC], 0.0, 0.0);  // Nz'^T fz -> T_vv
+        if (!hi) {
+          double* tb = RB_ + g * T2 + 8 * h + 2 * t;
+          st2(tb, a0, a1);
+          st2(tb + TC, b0, b1);
+          st2(tb + 2 * TC, c0, c1);
+        }
+      }
+      __syncwarp();
+      // ---- backward y: columns m = 8h + g -> (q0, i2) = (g & 3, 2h + (g >> 2))
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double* tb = RB_ + (2 * h + (g >> 2)) * T2 + (g & 3) + 4 * t;
+        double v0, v1, d0, d1;
+        dmma(v0, v1, ayb2, tb[TC], 0.0, 0.0);      // Ny'^T T_vd
+        dmma(v0, v1, ayb, tb[2 * TC], v0, v1);     // + Ny^T T_vv
+        dmma(d0, d1, ayb, tb[0], 0.0, 0.0);        // Ny^T T_dv
+        if (!hi) {
+          double* sb = RA_ + g * S1 + 8 * h + 2 * t;
+          st2(sb, v0, v1);
+          st2(sb + SC, d0, d1);
+        }
+      }
+      __syncwarp();
+      // ---- backward x: columns n = 8h + g -> (i1, i2) = (g & 3, 2h + (g >> 2))
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double* sb = RA_ + (g & 3) * S1 + t + 8 * h + 4 * (g >> 2);
+        double r0, r1;
+        dmma(r0, r1, axb2, sb[SC], 0.0, 0.0);      // Nx'^T S_d
+        dmma(r0, r1, axb, sb[0], r0, r1);          // + Nx^T S_v
+        if (!hi) {  // res[i0 = g][line = i1 + 4 i2 = 8h + 2t + i]
+          double* st = stage + w * SST + (8 * h + 2 * t) * SPL + g;
+          st[0] = r0;
+          st[SPL] = r1;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- deterministic gather of the layer into the brick footprint
+    {
+      const int nfoot = fp0 * fp1 * P1;
+      for (int i = tid; i < nfoot; i += NT) {
+        const int jx = i % fp0;
+        const int jy = (i / fp0) % fp1;
+        const int jzl = i / (fp0 * fp1);
+        double s = 0.0;
+#pragma unroll
+        for (int e1 = 0; e1 < TY; ++e1) {
+          const int ly = jy - soff[TX + e1];
+          if (ly < 0 || ly >= P1) continue;
+#pragma unroll
+          for (int e0 = 0; e0 < TX; ++e0) {
+            const int lx = jx - soff[e0];
+            if (lx < 0 || lx >= P1) continue;
+            s += stage[(e1 * TX + e0) * SST + (ly + P1 * jzl) * SPL + lx];
+          }
+        }
+        acc[((offz + jzl) * fp1 + jy) * fp0 + jx] += s;
+      }
+    }
+    // the next layer's first barrier orders these accumulator updates
+  }
+  __syncthreads();
+  double* out = A.scratch + (size_t)b * accn;
+  for (int i = tid; i < accn; i += NT) out[i] = acc[i];
+}

@@ -152,6 +152,29 @@ class LearnedPreconditioner:
         stats = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
         return R, E, stats
 
+    def pairs_random(self, n_pairs, tol=1e-10, seed=0, maxiter=None):
+        """Pairs (r, K^-1 r) for seeded r ~ N(0, I) on the free DOFs.
+
+        Each e = K^-1 r comes from a plain FP64 Jacobi-PCG solve to ``tol``.
+        White-noise residuals cover the whole spectrum, which the iterates of a
+        few Krylov solves do not. Returns float32 [n, vec, ncp] R, E normalised
+        by ||r|| (the scales of ``pairs_from_solve`` are left unchanged).
+        """
+        import torch
+
+        op = self.op
+        gen = torch.Generator(device=self.dev).manual_seed(int(seed))
+        free = torch.as_tensor(~op.prescribed_mask, device=self.dev)
+        R = torch.empty((int(n_pairs), self.vec, self.ncp), dtype=torch.float32, device=self.dev)
+        E = torch.empty_like(R)
+        for j in range(int(n_pairs)):
+            r = torch.randn(op.n_dofs, dtype=torch.float64, device=self.dev, generator=gen) * free
+            e, st = op.pcg(r, tol=tol, maxiter=maxiter, preconditioner="jacobi")
+            rn = float(torch.linalg.norm(r))
+            R[j] = self._to_grid(r / rn)
+            E[j] = self._to_grid(e / rn)
+        return R, E
+
     @property
     def mask(self):
         """Loss mask on the grid: 1 where any component of the control point is free."""
@@ -215,7 +238,7 @@ class LearnedPreconditioner:
         return (z * torch.as_tensor(~self.op.prescribed_mask, device=self.dev)).contiguous()
 
     # -- solve -------------------------------------------------------------------
-    def solve(self, b, tol=1e-8, maxiter=None, stall=20, depth=4, mixed=False, inner_tol=1e-4, check_every=16,
+    def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=1e-4, check_every=16,
               use_network=True):
         """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats).
 

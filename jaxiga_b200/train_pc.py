@@ -4,7 +4,7 @@
 
 Pairs come from plain FP64 Jacobi-PCG solves of the workload itself (the load
 vector first, then seeded random right-hand sides), one (residual, error)
-pair per iteration; training minimises the energy norm of the
+pair per iteration, plus ``--random`` pairs (r ~ N(0, I), e = K^-1 r); training minimises the energy norm of the
 preconditioner's error with the network's own forward/backward kernels and
 Adam until the time budget is spent; the checkpoint (weights, scales, loss
 history) is written to ``--out``. Then the workload is solved to 1e-8 by
@@ -69,7 +69,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["elasticity", "darcy", "plate"], default="elasticity")
     ap.add_argument("--span", type=int, default=None)
-    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--pairs", type=int, default=2000, help="pairs from the iterates of Jacobi-PCG solves")
+    ap.add_argument("--random", type=int, default=0, help="extra pairs (r ~ N(0, I), K^-1 r)")
     ap.add_argument("--seconds", type=float, default=600.0)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--channels", default=None, help="per-level channels, e.g. 8,16,24,32,48 (default: by grid)")
@@ -94,6 +95,11 @@ def main():
         have += R.shape[0]
         solves_data.append({"iterations": st["iterations"], "pairs": int(R.shape[0])})
         k += 1
+    if args.random > 0:  # white-noise residuals r ~ N(0, I), e = K^-1 r
+        R2, E2 = lp.pairs_random(args.random, tol=1e-10, seed=args.seed)
+        Rs.append(R2)
+        Es.append(E2)
+        have += R2.shape[0]
     R = torch.cat(Rs)
     E = torch.cat(Es)
     # one global output scale over all solves
