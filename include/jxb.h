@@ -211,9 +211,13 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  *   jxb_cnn_backward: adds to the accumulator the parameter gradient of
  *     sum(gout * N(in)); must follow a forward on the same input and dims.
  *   jxb_cnn_accumulate: forward, masked MSE against target, backward; returns the loss.
- *   jxb_cnn_accumulate_energy: forward, then with d = P_f (e - out_scale N(in))
- *     (grid -> DOF layout, 0 on prescribed DOFs) the loss weight * d^T K d of
- *     the plan's operator K; adds its parameter gradient and returns the loss.
+ *   jxb_cnn_accumulate_energy: forward, then, with z = P_f out_scale N(in) in DOF
+ *     layout (0 on prescribed DOFs) and the plan's operator K, the loss
+ *     angle == 0: weight * d^T K d, d = P_f e - z (energy norm of the error);
+ *     angle != 0: weight * (1 - (z.r)^2 / ((z^T K z)(e.r))) for the pair r = K e
+ *     (energy-norm angle between z and e: blind to the scale of z, which
+ *     flexible CG does not use). e and r are grids [vec][nz][ny][nx]; adds the
+ *     parameter gradient and returns the loss.
  *   jxb_cnn_adam: one Adam step with the accumulated gradient times grad_scale.
  * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
  *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
@@ -232,7 +236,7 @@ int jxb_cnn_zero_grad(jxb_cnn* cnn, jxb_stream stream);
 int jxb_cnn_accumulate(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in,
                        const float* target, const float* mask, double* loss);
 int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in, const float* e,
-                              float out_scale, double weight, double* loss);
+                              const float* r, float out_scale, double weight, int angle, double* loss);
 int jxb_cnn_adam(jxb_cnn* cnn, jxb_stream stream, float lr, float grad_scale);
 int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                     const float* features, int n_features, float in_scale, double out_scale, int stall,

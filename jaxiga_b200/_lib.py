@@ -129,7 +129,8 @@ SIGNATURES = [
     ("jxb_cnn_accumulate", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
     ("jxb_cnn_accumulate_energy", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                   ctypes.c_void_p, ctypes.c_float, ctypes.c_double, c_double_p]),
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_double, ctypes.c_int,
+                                   c_double_p]),
     ("jxb_cnn_adam", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float]),
     ("jxb_fcg_learned", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                          ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_int,

@@ -11,13 +11,16 @@
 // swapped, so the needed product lands in rows 0-3).
 //
 // Work split: the CTA owns one 4 x 4 x 8 element brick as in the scalar
-// kernel; each of its 16 warps owns one element of the current layer and
-// runs the element's whole pipeline warp-synchronously (forward x, y, z;
-// point operator; backward z, y, x -- 28 MMAs), handing data between stages
-// through a private, padded shared-memory area (__syncwarp between stages).
-// Element residuals go to the layer stage and the same fixed-order gather
-// as the scalar kernel sums them into the brick footprint, so the result is
-// bitwise reproducible.
+// kernel, and each of its 16 warps owns one column of 8 elements along z.
+// A warp runs each element's whole pipeline warp-synchronously (forward x,
+// y, z; point operator; backward z, y, x -- 28 MMAs), handing data between
+// stages through a private, padded shared-memory area (__syncwarp between
+// stages), and adds the element residual into its column's footprint in
+// shared memory, layer after layer in order. Warps never wait for each other
+// until the brick is done; then one fixed-order gather sums the 16 column
+// footprints into the brick footprint (no atomics), so the result is bitwise
+// reproducible. Input fragments come straight from the DOF vector (read one
+// layer ahead), factor tiles are prefetched into L2 one layer ahead.
 //
 // Fragment layouts of m8n8k4 (lane l, g = l >> 2, t = l & 3):
 //   A (8x4, row): a = A[g][t];  B (4x8, col): b = B[t][g];  C/D (8x8): d_i = D[g][2t + i].
@@ -33,9 +36,7 @@ constexpr int S1 = 20, SC = 4 * S1;  // SB[type (2)][i1 (4)][m (16)], m = q0 + 4
 constexpr int RA = 3 * FC;           // region A (XB, FB, SB): 240 doubles
 constexpr int RB = 3 * TC;           // region B (YB, TB): 288 doubles
 constexpr int WB = RA + RB;          // per-warp doubles
-constexpr int SU0 = 12;              // row stride of the layer input tile
-constexpr int SPL = 6;               // line stride of the element residual stage
-constexpr int SST = 16 * SPL;        // element stride of the stage
+constexpr int CF = P1 * P1;         // one z row of a column footprint: [i1][i0]
 static_assert(8 * XS <= RA && 2 * SC <= RA && 4 * Y2 <= RB, "per-warp regions");
 }  // namespace bm
 
@@ -51,8 +52,7 @@ __device__ __forceinline__ void st2(double* p, double a, double b) {
 
 static size_t smem3_mma(const Bricks& br) {
   using namespace bm;
-  const size_t acc = ((size_t)br.fp[0] * br.fp[1] * br.fp[2] + 1) / 2 * 2;
-  const size_t n = (size_t)NE * WB + (TX + TY + 1) * 32 + (size_t)NE * SST + acc + (size_t)P1 * br.fp[1] * SU0;
+  const size_t n = (size_t)NE * WB + (size_t)NE * br.fp[2] * CF;
   return n * sizeof(double) + (TX + TY) * sizeof(int) + 64;
 }
 
@@ -63,15 +63,9 @@ __global__ void __launch_bounds__(bm::NT, 2) k_brick3_mma(BrickArgs<double> A) {
   const int fp0 = br.fp[0], fp1 = br.fp[1], fp2 = br.fp[2];
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  double* wbuf = reinterpret_cast<double*>(smem_raw);  // [NE][WB]
-  double* stx = wbuf + NE * WB;                          // [TX][32]: [2][Q][P1] per element column
-  double* sty = stx + TX * 32;                           // [TY][32]
-  double* stz = sty + TY * 32;                           // [32]
-  double* stage = stz + 32;                              // [NE][16 lines][SPL]
-  double* acc = stage + NE * SST;                        // [fp2][fp1][fp0]
-  const int accn = fp0 * fp1 * fp2;
-  double* su = acc + (accn + 1) / 2 * 2;                 // [P1][fp1][SU0]
-  int* soff = reinterpret_cast<int*>(su + P1 * fp1 * SU0);
+  double* wbuf = reinterpret_cast<double*>(smem_raw);  // [NE][WB] stage hand-off areas
+  double* colf = wbuf + NE * WB;                         // [NE][fp2][i1][i0] column footprints
+  int* soff = reinterpret_cast<int*>(colf + NE * fp2 * CF);
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -85,19 +79,6 @@ __global__ void __launch_bounds__(bm::NT, 2) k_brick3_mma(BrickArgs<double> A) {
   const bool evalid = ex < br.n_span[0] && ey < br.n_span[1];
   const long long slot_base = b * (long long)CZ * NE;
   const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
-  constexpr unsigned TILE_BYTES = NE * NG * NQE * sizeof(double);
-  if (tid == 0) prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, TILE_BYTES);
-
-  for (int i = tid; i < TX * 32; i += NT) {
-    const int e = i >> 5, r = i & 31;
-    const int sp = min(bx * TX + e, br.n_span[0] - 1);
-    stx[i] = A.tab[0][(size_t)sp * 3 * Q * P1 + r];
-  }
-  for (int i = tid; i < TY * 32; i += NT) {
-    const int e = i >> 5, r = i & 31;
-    const int sp = min(by * TY + e, br.n_span[1] - 1);
-    sty[i] = A.tab[1][(size_t)sp * 3 * Q * P1 + r];
-  }
   if (tid < TX) {
     const int e = bx * TX + tid;
     soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
@@ -106,56 +87,52 @@ __global__ void __launch_bounds__(bm::NT, 2) k_brick3_mma(BrickArgs<double> A) {
     const int e = by * TY + tid;
     soff[TX + tid] = e < br.n_span[1] ? br.first[1][e] - cp0y : -100000;
   }
-  for (int i = tid; i < accn; i += NT) acc[i] = 0.0;
-  __syncthreads();
+  double* cf = colf + w * fp2 * CF;
+  for (int i = lane; i < fp2 * CF; i += 32) cf[i] = 0.0;
 
-  // A fragments of this warp's element that stay fixed across layers
-  const double* tx_ = stx + exl * 32;
-  const double* ty_ = sty + eyl * 32;
-  const int bo = t * 4 + (g & 3);        // [q = t][i = g & 3] of a [2][Q][P1] table
-  const int ty0 = (g >> 2) * 16, ty1 = (1 - (g >> 2)) * 16;
-  const double ax = tx_[lane], ay = ty_[lane];
-  const double axb = tx_[ty0 + bo], axb2 = tx_[ty1 + bo];
-  const double ayb = ty_[ty0 + bo], ayb2 = ty_[ty1 + bo];
-  const int ox = evalid ? br.first[0][ex] - cp0x : 0, oy = evalid ? br.first[1][ey] - cp0y : 0;
-  double* RA_ = wbuf + w * WB;
-  double* RB_ = RA_ + RA;
-  const long long nxy = (long long)br.n_cp[0] * br.n_cp[1];
-  const bool hi = lane >= 16;
-  const int hh = hi ? 1 : 0;
-
-  for (int lz = 0; lz < nlayers; ++lz) {
-    const int ez = bz * CZ + lz;
-    const int fz = br.first[2][ez];
-    const int offz = fz - cp0z;
-    const long long slot = slot_base + (long long)lz * NE + w;
-    if (tid == 0 && lz + 1 < nlayers)
-      prefetch_l2(A.geo + (size_t)(slot_base + (long long)(lz + 1) * NE) * NG * NQE, TILE_BYTES);
-    if (tid < 32) stz[tid] = A.tab[2][(size_t)ez * 3 * Q * P1 + tid];
-    for (int i = tid; i < P1 * fp1 * fp0; i += NT) {
-      const int jx = i % fp0, rest = i / fp0;
-      const int jy = rest % fp1, jz = rest / fp1;
-      const int gx = cp0x + jx, gy = cp0y + jy;
-      double v = 0.0;
-      if (gx < br.n_cp[0] && gy < br.n_cp[1]) {
-        const long long dof = gx + (long long)br.n_cp[0] * gy + nxy * (fz + jz);
-        v = A.x[dof];
-        if (A.masked && !A.keep[dof]) v = 0.0;
+  if (evalid) {
+    // A fragments of the column's x / y tables ([2][Q][P1] per span)
+    const double* tx_ = A.tab[0] + (size_t)ex * 3 * Q * P1;
+    const double* ty_ = A.tab[1] + (size_t)ey * 3 * Q * P1;
+    const int bo = t * 4 + (g & 3);  // [q = t][i = g & 3]
+    const int ty0 = (g >> 2) * 16, ty1 = (1 - (g >> 2)) * 16;
+    const double ax = tx_[lane], ay = ty_[lane];
+    const double axb = tx_[ty0 + bo], axb2 = tx_[ty1 + bo];
+    const double ayb = ty_[ty0 + bo], ayb2 = ty_[ty1 + bo];
+    double* RA_ = wbuf + w * WB;
+    double* RB_ = RA_ + RA;
+    const bool hi = lane >= 16;
+    const int hh = hi ? 1 : 0;
+    const long long ncx = br.n_cp[0], nxy = (long long)br.n_cp[0] * br.n_cp[1];
+    // this lane's input entries (x-stage B fragments): i0 = t, i1 = g & 3, i2 = 2j + (g >> 2)
+    const long long dxy = (long long)(br.first[0][ex] + t) + ncx * (br.first[1][ey] + (g & 3));
+    auto load_in = [&](int ez_, double& u0, double& u1) {
+      const long long d0 = dxy + nxy * (br.first[2][ez_] + (g >> 2));
+      const long long d1 = d0 + 2 * nxy;
+      u0 = A.x[d0];
+      u1 = A.x[d1];
+      if (A.masked) {
+        if (!A.keep[d0]) u0 = 0.0;
+        if (!A.keep[d1]) u1 = 0.0;
       }
-      su[(jz * fp1 + jy) * SU0 + jx] = v;
-    }
-    __syncthreads();
-
-    if (evalid) {
-      const double az = stz[lane];
-      const double azb = stz[ty0 + bo], azb2 = stz[ty1 + bo];
+    };
+    if (lane == 0) prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
+    double un0, un1;
+    load_in(bz * CZ, un0, un1);
+    for (int lz = 0; lz < nlayers; ++lz) {
+      const int ez = bz * CZ + lz;
+      const int offz = br.first[2][ez] - cp0z;
+      const long long slot = slot_base + (long long)lz * NE + w;
+      if (lane == 0 && lz + 1 < nlayers) prefetch_l2(A.geo + (size_t)(slot + NE) * NG * NQE, NG * NQE * sizeof(double));
+      const double u0 = un0, u1 = un1;
+      if (lz + 1 < nlayers) load_in(ez + 1, un0, un1);
+      const double* tz_ = A.tab[2] + (size_t)ez * 3 * Q * P1;
+      const double az = tz_[lane], azb = tz_[ty0 + bo], azb2 = tz_[ty1 + bo];
       // ---- forward x: D[rX = (type, q0)][c = i1 + 4 i2] -> XB
-      const double* ue = su + oy * SU0 + ox;
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const double bv = ue[((2 * j + (g >> 2)) * fp1 + (g & 3)) * SU0 + t];
         double d0, d1;
-        dmma(d0, d1, ax, bv, 0.0, 0.0);
+        dmma(d0, d1, ax, j ? u1 : u0, 0.0, 0.0);
         st2(RA_ + g * XS + 8 * j + 2 * t, d0, d1);
       }
       __syncwarp();
@@ -250,39 +227,37 @@ __global__ void __launch_bounds__(bm::NT, 2) k_brick3_mma(BrickArgs<double> A) {
         double r0, r1;
         dmma(r0, r1, axb2, sb[SC], 0.0, 0.0);      // Nx'^T S_d
         dmma(r0, r1, axb, sb[0], r0, r1);          // + Nx^T S_v
-        if (!hi) {  // res[i0 = g][line = i1 + 4 i2 = 8h + 2t + i]
-          double* st = stage + w * SST + (8 * h + 2 * t) * SPL + g;
-          st[0] = r0;
-          st[SPL] = r1;
-        }
-      }
-    }
-    __syncthreads();
-    // ---- deterministic gather of the layer into the brick footprint
-    {
-      const int nfoot = fp0 * fp1 * P1;
-      for (int i = tid; i < nfoot; i += NT) {
-        const int jx = i % fp0;
-        const int jy = (i / fp0) % fp1;
-        const int jzl = i / (fp0 * fp1);
-        double s = 0.0;
+        if (!hi) {  // res[i0 = g][i1 + 4 i2 = 8h + 2t + i] into the column footprint
 #pragma unroll
-        for (int e1 = 0; e1 < TY; ++e1) {
-          const int ly = jy - soff[TX + e1];
-          if (ly < 0 || ly >= P1) continue;
-#pragma unroll
-          for (int e0 = 0; e0 < TX; ++e0) {
-            const int lx = jx - soff[e0];
-            if (lx < 0 || lx >= P1) continue;
-            s += stage[(e1 * TX + e0) * SST + (ly + P1 * jzl) * SPL + lx];
+          for (int i = 0; i < 2; ++i) {
+            const int n = 8 * h + 2 * t + i;
+            cf[((offz + (n >> 2)) * P1 + (n & 3)) * P1 + g] += i ? r1 : r0;
           }
         }
-        acc[((offz + jzl) * fp1 + jy) * fp0 + jx] += s;
       }
+      __syncwarp();
     }
-    // the next layer's first barrier orders these accumulator updates
   }
   __syncthreads();
-  double* out = A.scratch + (size_t)b * accn;
-  for (int i = tid; i < accn; i += NT) out[i] = acc[i];
+  // ---- deterministic gather of the column footprints into the brick footprint
+  const int nfoot = fp0 * fp1 * fp2;
+  double* out = A.scratch + (size_t)b * nfoot;
+  for (int i = tid; i < nfoot; i += NT) {
+    const int jx = i % fp0;
+    const int jy = (i / fp0) % fp1;
+    const int jz = i / (fp0 * fp1);
+    double s = 0.0;
+#pragma unroll
+    for (int e1 = 0; e1 < TY; ++e1) {
+      const int ly = jy - soff[TX + e1];
+      if (ly < 0 || ly >= P1) continue;
+#pragma unroll
+      for (int e0 = 0; e0 < TX; ++e0) {
+        const int lx = jx - soff[e0];
+        if (lx < 0 || lx >= P1) continue;
+        s += colf[((e1 * TX + e0) * fp2 + jz) * CF + ly * P1 + lx];
+      }
+    }
+    out[i] = s;
+  }
 }

@@ -269,6 +269,51 @@ __global__ void k_egrad(long long ncp, int vec, const T* __restrict__ Kd, const 
   g[i] = v;
 }
 
+// z = keep ? out_scale * out : 0 in DOF layout
+__global__ void k_zdof(long long ncp, int vec, const float* __restrict__ out, float out_scale,
+                       const uint8_t* __restrict__ keep, double* __restrict__ z) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncp * vec) return;
+  const long long cp = i / vec;
+  const int c = (int)(i % vec);
+  z[i] = keep[i] ? (double)out_scale * (double)out[(long long)c * ncp + cp] : 0.0;
+}
+
+// partials of z . r and e . r over free DOFs (r, e: grid layout [vec][ncp])
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_angle_dots(long long ncp, int vec, const double* __restrict__ z,
+                                                                const float* __restrict__ r, const float* __restrict__ e,
+                                                                const uint8_t* __restrict__ keep, double* __restrict__ part) {
+  double zr = 0, er = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ncp * vec;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (!keep[i]) continue;
+    const long long g = (long long)(i % vec) * ncp + i / vec;
+    const double ri = (double)r[g];
+    zr += z[i] * ri;
+    er += (double)e[g] * ri;
+  }
+  const double s0 = block_sum_all(zr), s1 = block_sum_all(er);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s0;
+    part[JXB_RED_BLOCKS + blockIdx.x] = s1;
+  }
+}
+
+// gout[c][cp] = keep ? s1 * Kz - s2 * r : 0 (4 channels, the extra ones 0)
+__global__ void k_angle_grad(long long ncp, int vec, const double* __restrict__ Kz, const float* __restrict__ r,
+                             const uint8_t* __restrict__ keep, double s1, double s2, float* __restrict__ g) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncp * 4) return;
+  const int c = (int)(i / ncp);
+  const long long cp = i % ncp;
+  float v = 0.f;
+  if (c < vec) {
+    const long long dof = cp * vec + c;
+    v = keep[dof] ? (float)(s1 * Kz[dof] - s2 * (double)r[i]) : 0.f;
+  }
+  g[i] = v;
+}
+
 __global__ void k_to_f32(long long n, const double* __restrict__ r, double s, float* __restrict__ out) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (float)(r[i] * s);
@@ -570,8 +615,9 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
 }
 
 extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in,
-                                         const float* e, float out_scale, double weight, double* loss) {
-  if (!plan || !cnn || !in || !e) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: null argument");
+                                         const float* e, const float* r, float out_scale, double weight, int angle,
+                                         double* loss) {
+  if (!plan || !cnn || !in || !e || (angle && !r)) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: null argument");
   if (cnn_out_channels(cnn) != plan->vec)
     return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: the network's outputs must equal the plan's vec");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -584,18 +630,48 @@ extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_strea
   if ((rc = cnn_forward(cnn, s, nx, ny, nz, in, &out4))) return rc;
   double* d = plan->d_p;
   double* Kd = plan->d_Ap;
-  k_ediff<double><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, e, out4, out_scale, plan->d_keep, d);
-  if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, d, nullptr, nullptr, 1))) return rc;
-  if ((rc = launch_combine<double>(plan, s, Kd, 1, d, plan->d_red, nullptr))) return rc;
-  k_egrad<double><<<nb256(ncp * 4), 256, 0, s>>>(ncp, vec, Kd, plan->d_keep, -2.0 * weight * out_scale,
-                                                  cnn_grad_out(cnn));
-  JXB_CUDA(cudaGetLastError());
-  std::vector<double> h(JXB_RED_BLOCKS);
-  JXB_CUDA(cudaMemcpyAsync(h.data(), plan->d_red, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  std::vector<double> h(3 * JXB_RED_BLOCKS);
+  double value = 0;
+  if (!angle) {
+    // loss = weight d^T K d, d = P_f (e - s N(in)); dL/dN = -2 weight s K d
+    k_ediff<double><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, e, out4, out_scale, plan->d_keep, d);
+    if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, d, nullptr, nullptr, 1))) return rc;
+    if ((rc = launch_combine<double>(plan, s, Kd, 1, d, plan->d_red, nullptr))) return rc;
+    k_egrad<double><<<nb256(ncp * 4), 256, 0, s>>>(ncp, vec, Kd, plan->d_keep, -2.0 * weight * out_scale,
+                                                    cnn_grad_out(cnn));
+    JXB_CUDA(cudaGetLastError());
+    JXB_CUDA(cudaMemcpyAsync(h.data(), plan->d_red, JXB_RED_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    JXB_CUDA(cudaStreamSynchronize(s));
+    double dkd = 0;
+    for (int i = 0; i < JXB_RED_BLOCKS; ++i) dkd += h[i];
+    value = weight * dkd;
+  } else {
+    // scale-free: loss = weight (1 - (z.r)^2 / ((z^T K z)(e.r))), z = P_f s N(in), r = K e;
+    // dL/dz = weight 2a/(b c) ((a/b) K z - r), a = z.r, b = z^T K z, c = e.r
+    k_zdof<<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, out4, out_scale, plan->d_keep, d);
+    if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, d, nullptr, nullptr, 1))) return rc;
+    if ((rc = launch_combine<double>(plan, s, Kd, 1, d, plan->d_red, nullptr))) return rc;
+    k_angle_dots<<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(ncp, vec, d, r, e, plan->d_keep,
+                                                             plan->d_red + JXB_RED_BLOCKS);
+    JXB_CUDA(cudaGetLastError());
+    JXB_CUDA(cudaMemcpyAsync(h.data(), plan->d_red, 3 * JXB_RED_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    JXB_CUDA(cudaStreamSynchronize(s));
+    double bq = 0, a = 0, c = 0;
+    for (int i = 0; i < JXB_RED_BLOCKS; ++i) {
+      bq += h[i];
+      a += h[JXB_RED_BLOCKS + i];
+      c += h[2 * JXB_RED_BLOCKS + i];
+    }
+    if (!(bq > 0) || !(c > 0) || !isfinite(a)) return fail(JXB_ERR_NONFINITE, "jxb_cnn_accumulate_energy: degenerate pair or output");
+    value = weight * (1.0 - a * a / (bq * c));
+    const double f = weight * 2.0 * a / (bq * c);
+    // chain rule through z = s N: dL/dN = s dL/dz
+    k_angle_grad<<<nb256(ncp * 4), 256, 0, s>>>(ncp, vec, Kd, r, plan->d_keep, f * (a / bq) * out_scale, f * out_scale,
+                                                cnn_grad_out(cnn));
+    JXB_CUDA(cudaGetLastError());
+  }
   if ((rc = cnn_backward(cnn, s, nx, ny, nz, in))) return rc;
   JXB_CUDA(cudaStreamSynchronize(s));
-  double dkd = 0;
-  for (int i = 0; i < JXB_RED_BLOCKS; ++i) dkd += h[i];
-  if (loss) *loss = weight * dkd;
+  if (loss) *loss = value;
   return JXB_OK;
 }

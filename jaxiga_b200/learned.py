@@ -6,13 +6,15 @@ Pipeline (all arithmetic in libjxb's kernels; torch holds device memory):
    x_j; with the converged x*, e_j = x* - x_j and r_j = K e_j (exact, one
    operator application each) are the (residual, error) pairs CG actually
    meets, early rough residuals and late smooth ones alike.
-2. ``train``: the energy norm of the preconditioner's error,
-   (e - z)^T K (e - z) / e^T K e with z = out_scale N(in_scale r/||r||) for the
-   normalised pair, forward and backward through the network's own kernels
-   and the operator apply, Adam on the flat parameter vector. The energy norm
-   weighs the error the way CG convergence does (a plain MSE on e favours the
-   smooth components and leaves the rough ones to chance). A masked-MSE loss
-   is kept for comparison.
+2. ``train``: by default the energy-norm angle between the network's output
+   z = N(in_scale r/||r||) and the error e, 1 - (z.r)^2 / ((z^T K z)(e^T K e))
+   (r = K e), forward and backward through the network's own kernels and the
+   operator apply, Adam on the flat parameter vector. The energy norm weighs
+   the error the way CG convergence does, and the angle ignores the scale of
+   z, which flexible CG does not use: for a smooth residual the error is
+   orders of magnitude larger than for a rough one of the same norm, a range
+   a network fed unit-norm inputs cannot span. The scaled energy norm
+   (e - z)^T K (e - z) / e^T K e and a masked MSE are kept for comparison.
 3. ``solve``: truncated flexible CG with z = ||r|| out_scale N(in_scale r/||r||)
    and Jacobi-PCG as the fallback (jxb_fcg_learned), optionally as FP32 inner
    solves inside FP64 iterative refinement.
@@ -184,12 +186,13 @@ class LearnedPreconditioner:
         return torch.as_tensor(free.any(axis=1).astype(np.float32), device=self.dev)
 
     # -- training ----------------------------------------------------------------
-    def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, loss="energy", log=None):
-        """Adam on the energy-norm (or masked-MSE) loss; returns the per-epoch mean losses."""
+    def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, loss="angle", log=None):
+        """Adam on the energy-norm angle (or scaled energy norm, or masked-MSE) loss;
+        returns the per-epoch mean losses."""
         import torch
 
-        if loss not in ("energy", "mse"):
-            raise ValueError("loss must be 'energy' or 'mse'")
+        if loss not in ("angle", "energy", "mse"):
+            raise ValueError("loss must be 'angle', 'energy' or 'mse'")
         g = torch.Generator().manual_seed(seed)
         nx, ny, nz = self.grid
         m = R.shape[0]
@@ -207,10 +210,12 @@ class LearnedPreconditioner:
                 for j in idx:
                     inp = self._input(R[j] * self.in_scale)
                     val = ctypes.c_double()
-                    if loss == "energy":
+                    if loss in ("energy", "angle"):
+                        angle = loss == "angle"
                         _lib.check(self.lib.jxb_cnn_accumulate_energy(
                             self.op.handle, self.handle, _s(), _p(inp), _p(E[j].contiguous()),
-                            float(self.out_scale), float(w[j]), ctypes.byref(val)))
+                            _p(R[j].contiguous()) if angle else None, float(self.out_scale),
+                            1.0 if angle else float(w[j]), 1 if angle else 0, ctypes.byref(val)))
                     else:
                         tgt = (E[j] / self.out_scale).contiguous()
                         _lib.check(self.lib.jxb_cnn_accumulate(self.handle, _s(), nx, ny, nz, _p(inp), _p(tgt),

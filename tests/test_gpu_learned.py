@@ -95,9 +95,11 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
     lib.jxb_cnn_destroy(h)
 
 
-@pytest.mark.parametrize("op_name", ["poisson", "elasticity"])
-def test_energy_loss_gradient_matches_oracle(op_name):
-    """loss = w d^T K d, d = P_f (e - s N(in)), against the oracle network and assembled K."""
+@pytest.mark.parametrize("op_name,angle", [("poisson", 0), ("elasticity", 0), ("poisson", 1), ("elasticity", 1)])
+def test_energy_loss_gradient_matches_oracle(op_name, angle):
+    """Energy-norm losses against the oracle network and the assembled K:
+    w d^T K d with d = P_f (e - s N(in)), and w (1 - (z.r)^2 / ((z^T K z)(e.r)))
+    with z = P_f s N(in), r = K e."""
     import torch
 
     from oracle import iga_oracle as O
@@ -120,24 +122,46 @@ def test_energy_loss_gradient_matches_oracle(op_name):
     in_ch = vec + 1
     h, p32 = _make_net(lib, in_ch, vec, (4, 8, 12), 7, rng)
     x = rng.standard_normal((in_ch, nz, ny, nx))
-    e = rng.standard_normal((vec, nz, ny, nx))
+    e = rng.standard_normal((vec, nz, ny, nx)).astype(np.float32).astype(np.float64)
     s, w = 0.7, 0.3
+    to_dof = lambda v: v.reshape(vec, ncp).T.reshape(-1)  # noqa: E731  grid [c][cp] -> DOF vec*cp + c
+    to_grid = lambda v: v.reshape(ncp, vec).T.reshape(vec, nz, ny, nx)  # noqa: E731
+
+    def K(v):
+        out = np.zeros(V.n_dofs)
+        out[A.free] = A.K @ v[A.free]
+        return out
+
+    ed_ = to_dof(e)
+    ed_[mask] = 0.0
+    r = to_grid(K(ed_)).astype(np.float32).astype(np.float64)  # the pair's residual r = K e
     xd = torch.as_tensor(x, dtype=torch.float32, device="cuda").contiguous()
     ed = torch.as_tensor(e, dtype=torch.float32, device="cuda").contiguous()
+    rd = torch.as_tensor(r, dtype=torch.float32, device="cuda").contiguous()
     _lib.check(lib.jxb_cnn_zero_grad(h, _s()))
     loss = ctypes.c_double()
-    _lib.check(lib.jxb_cnn_accumulate_energy(op.handle, h, _s(), _p(xd), _p(ed), s, w, ctypes.byref(loss)))
+    _lib.check(lib.jxb_cnn_accumulate_energy(op.handle, h, _s(), _p(xd), _p(ed), _p(rd), s, w, angle,
+                                             ctypes.byref(loss)))
     g = _grads(lib, h)
-    # oracle: grid [c][cp] <-> DOF vec*cp + c
     x32 = x.astype(np.float32).astype(np.float64)
     out, _ = cnn_oracle.forward(p32, x32, in_ch, (4, 8, 12))
-    e32 = e.astype(np.float32).astype(np.float64)
-    d = (e32 - s * out[:vec]).reshape(vec, ncp).T.reshape(-1)
-    d[mask] = 0.0
-    Kd = np.zeros(V.n_dofs)
-    Kd[A.free] = A.K @ d[A.free]
-    loss_ref = w * float(d @ Kd)
-    gout = (-2.0 * w * s * Kd).reshape(ncp, vec).T.reshape(vec, nz, ny, nx)
+    if not angle:
+        d = to_dof(e - s * out[:vec])
+        d[mask] = 0.0
+        Kd = K(d)
+        loss_ref = w * float(d @ Kd)
+        gout = to_grid(-2.0 * w * s * Kd)
+    else:
+        z = to_dof(s * out[:vec])
+        z[mask] = 0.0
+        rdof = to_dof(r)
+        rdof[mask] = 0.0
+        Kz = K(z)
+        a, bq, c = float(z @ rdof), float(z @ Kz), float(ed_ @ rdof)
+        loss_ref = w * (1.0 - a * a / (bq * c))
+        gz = w * 2.0 * a / (bq * c) * (a / bq * Kz - rdof)
+        gz[mask] = 0.0
+        gout = to_grid(s * gz)
     g_ref = cnn_oracle.backward(p32, x32, gout, in_ch, (4, 8, 12))
     assert abs(loss.value - loss_ref) <= 1e-4 * abs(loss_ref)
     assert np.abs(g - g_ref).max() <= 2e-3 * np.abs(g_ref).max()
