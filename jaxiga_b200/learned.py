@@ -120,7 +120,8 @@ class LearnedPreconditioner:
 
     # -- data ------------------------------------------------------------------
     def pairs_from_solve(self, b, n_pairs=2000, every=1, tol=1e-12, maxiter=None):
-        """Residual/error pairs of one plain FP64 Jacobi-PCG solve of K x = b.
+        """Residual/error pairs of one plain FP64 Jacobi-PCG solve of K x = b:
+        the starting point x_0 = 0, then the iterate after every ``every`` steps.
 
         Returns (R, E, stats): R, E float32 [n, vec, ncp], each pair scaled by
         1/||r_j||, the solve's stats, and sets in_scale / out_scale.
@@ -136,13 +137,14 @@ class LearnedPreconditioner:
         ns = ctypes.c_int64()
         _lib.check(self.lib.jxb_pcg_snapshots(op.handle, _s(), _p(b), _p(x), ctypes.byref(o), int(every),
                                               _p(snaps), int(n_pairs), ctypes.byref(ns), ctypes.byref(st)))
-        m = ns.value
+        m = min(ns.value + 1, int(n_pairs))
         R = torch.empty((m, self.vec, self.ncp), dtype=torch.float32, device=self.dev)
         E = torch.empty_like(R)
         for j in range(m):
-            # CG iterates are zero on prescribed DOFs, so e_j is too; the masked
-            # operator gives the exact residual r_j = K e_j of iterate j.
-            e = x - snaps[j]
+            # pair 0 is the starting iterate x_0 = 0 (e_0 = x*, r_0 = b on the
+            # free DOFs); CG iterates are zero on prescribed DOFs, so e_j is too,
+            # and the masked operator gives the exact residual r_j = K e_j.
+            e = x if j == 0 else x - snaps[j - 1]
             r = op.apply(e)
             rn = float(torch.linalg.norm(r))
             R[j] = self._to_grid(r / rn)
