@@ -547,14 +547,18 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
 #include "brick2d.cuh"
 #include "brick3_mma.cuh"
 
-// The FP64 tensor-core brick kernel runs the degree-3 scalar apply unless the
-// environment sets JXB_BRICK3_MMA=0 (the FMA kernel then runs, e.g. to compare).
-static bool use_brick3_mma() {
-  static const bool on = [] {
+// The FP64 tensor-core brick kernel runs the degree-3 scalar apply. The
+// environment variable JXB_BRICK3_MMA selects the variant: 0 = the FMA kernel
+// (to compare), 2 = the MMA kernel built for one CTA per SM, anything else =
+// the MMA kernel built for two CTAs per SM.
+static int brick3_mma_mode() {
+  static const int mode = [] {
     const char* e = getenv("JXB_BRICK3_MMA");
-    return !(e && e[0] == '0');
+    if (e && e[0] == '0') return 0;
+    if (e && e[0] == '2') return 1;
+    return 2;
   }();
-  return on;
+  return mode;
 }
 
 // ---------------------------------------------------------------------------
@@ -663,11 +667,12 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
       return fail(JXB_ERR_INVALID, "plate operator is 2D only");
     } else {
       if constexpr (sizeof(T) == 8 && P == 3 && OPK == OPK_SCALAR && !RAT && MODE == MODE_APPLY) {
-        if (use_brick3_mma()) {
+        if (const int minb = brick3_mma_mode()) {
           const size_t sm = smem3_mma(br);
           if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory");
-          JXB_CUDA(cudaFuncSetAttribute(k_brick3_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-          k_brick3_mma<<<(unsigned)br.n_bricks, bm::NT, sm, s>>>(A);
+          auto k = minb == 2 ? k_brick3_mma<2> : k_brick3_mma<1>;
+          JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          k<<<(unsigned)br.n_bricks, bm::NT, sm, s>>>(A);
           JXB_CUDA(cudaGetLastError());
           return JXB_OK;
         }

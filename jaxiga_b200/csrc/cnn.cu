@@ -139,6 +139,50 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
   }
 }
 
+// The same convolution for grids too small to fill the GPU with voxel tiles:
+// one thread per (output channel, voxel), blockIdx.y = output channel, input
+// channels and taps summed in order by the thread (inputs from L1/L2, weights
+// uniform across the warp).
+template <int K>
+__global__ void __launch_bounds__(128) k_conv_small(Dims d, int ci_n, const float* __restrict__ in,
+                                                    const float* __restrict__ w, const float* __restrict__ bias,
+                                                    const float* __restrict__ add, int relu, float beta,
+                                                    float* __restrict__ out) {
+  constexpr int R = K / 2, KK = K * K * K;
+  const int co = blockIdx.y;
+  const int vox = (int)d.vox();
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= vox) return;
+  const int nxy = d.nx * d.ny;
+  const int x = v % d.nx, y = (v / d.nx) % d.ny, z = v / nxy;
+  float acc = bias ? bias[co] : 0.f;
+  const float* wc = w + (long long)co * ci_n * KK;
+  for (int ci = 0; ci < ci_n; ++ci) {
+    const float* ic = in + (long long)ci * vox;
+    const float* wk = wc + ci * KK;
+#pragma unroll
+    for (int dz = 0; dz < K; ++dz) {
+      const int zz = z + dz - R;
+      if (zz < 0 || zz >= d.nz) continue;
+#pragma unroll
+      for (int dy = 0; dy < K; ++dy) {
+        const int yy = y + dy - R;
+        if (yy < 0 || yy >= d.ny) continue;
+#pragma unroll
+        for (int dx = 0; dx < K; ++dx) {
+          const int xx = x + dx - R;
+          if (xx < 0 || xx >= d.nx) continue;
+          acc = fmaf(__ldg(wk + (dz * K + dy) * K + dx), __ldg(ic + zz * nxy + yy * d.nx + xx), acc);
+        }
+      }
+    }
+  }
+  const long long idx = (long long)co * vox + v;
+  if (add) acc += add[idx];
+  if (relu) acc = fmaxf(acc, 0.f);
+  out[idx] = beta != 0.f ? beta * out[idx] + acc : acc;
+}
+
 // Weight (and bias) gradient partials of one voxel tile:
 //   part[tile][co][ci][k] = sum_{v in tile} g[co](v) in[ci](v + k),
 //   bpart[tile][co] = sum_{v in tile} g[co](v)   (blockIdx.z == 0 blocks).
@@ -271,22 +315,22 @@ __global__ void k_relu_mask(long long n, const float* __restrict__ act, float* _
   if (i < n && !(act[i] > 0.f)) g[i] = 0.f;
 }
 
-// average of the children (ceil division of odd sizes)
+// average of the children (ceil division of odd sizes); activation counts stay below 2^31
 __global__ void k_pool(Dims f, Dims c, int ch, const float* __restrict__ in, float* __restrict__ out) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long cv = c.vox();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cv = (int)c.vox(), fv = (int)f.vox();
   if (i >= cv * ch) return;
-  long long o = i % cv;
-  int k = (int)(i / cv);
-  int x = (int)(o % c.nx), y = (int)((o / c.nx) % c.ny), z = (int)(o / ((long long)c.nx * c.ny));
+  const int k = i / cv, o = i - k * cv;
+  const int x = o % c.nx, y = (o / c.nx) % c.ny, z = o / (c.nx * c.ny);
+  const float* src = in + (long long)k * fv;
   float s = 0.f;
   int n = 0;
   for (int dz = 0; dz < 2; ++dz)
     for (int dy = 0; dy < 2; ++dy)
       for (int dx = 0; dx < 2; ++dx) {
-        int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+        const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
         if (X < f.nx && Y < f.ny && Z < f.nz) {
-          s += in[(long long)k * f.vox() + ((long long)Z * f.ny + Y) * f.nx + X];
+          s += src[(Z * f.ny + Y) * f.nx + X];
           ++n;
         }
       }
@@ -295,41 +339,39 @@ __global__ void k_pool(Dims f, Dims c, int ch, const float* __restrict__ in, flo
 
 // backward of k_pool: each fine voxel receives g_coarse / (children of its parent); beta accumulates
 __global__ void k_pool_bwd(Dims f, Dims c, int ch, const float* __restrict__ gc, float beta, float* __restrict__ gf) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long fv = f.vox();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fv = (int)f.vox(), cv = (int)c.vox();
   if (i >= fv * ch) return;
-  long long o = i % fv;
-  int k = (int)(i / fv);
-  int X = (int)(o % f.nx), Y = (int)((o / f.nx) % f.ny), Z = (int)(o / ((long long)f.nx * f.ny));
-  int x = X / 2, y = Y / 2, z = Z / 2;
-  int nxc = min(2, f.nx - 2 * x), nyc = min(2, f.ny - 2 * y), nzc = min(2, f.nz - 2 * z);
-  float v = gc[(long long)k * c.vox() + ((long long)z * c.ny + y) * c.nx + x] / (nxc * nyc * nzc);
+  const int k = i / fv, o = i - k * fv;
+  const int X = o % f.nx, Y = (o / f.nx) % f.ny, Z = o / (f.nx * f.ny);
+  const int x = X / 2, y = Y / 2, z = Z / 2;
+  const int nxc = min(2, f.nx - 2 * x), nyc = min(2, f.ny - 2 * y), nzc = min(2, f.nz - 2 * z);
+  const float v = gc[(long long)k * cv + (z * c.ny + y) * c.nx + x] / (nxc * nyc * nzc);
   gf[i] = beta != 0.f ? beta * gf[i] + v : v;
 }
 
 __global__ void k_up(Dims f, Dims c, int ch, const float* __restrict__ in, float* __restrict__ out) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long fv = f.vox();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fv = (int)f.vox(), cv = (int)c.vox();
   if (i >= fv * ch) return;
-  long long o = i % fv;
-  int k = (int)(i / fv);
-  int X = (int)(o % f.nx), Y = (int)((o / f.nx) % f.ny), Z = (int)(o / ((long long)f.nx * f.ny));
-  out[i] = in[(long long)k * c.vox() + ((long long)(Z / 2) * c.ny + Y / 2) * c.nx + X / 2];
+  const int k = i / fv, o = i - k * fv;
+  const int X = o % f.nx, Y = (o / f.nx) % f.ny, Z = o / (f.nx * f.ny);
+  out[i] = in[(long long)k * cv + ((Z / 2) * c.ny + Y / 2) * c.nx + X / 2];
 }
 
 __global__ void k_up_bwd(Dims f, Dims c, int ch, const float* __restrict__ gf, float* __restrict__ gc) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long cv = c.vox();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cv = (int)c.vox(), fv = (int)f.vox();
   if (i >= cv * ch) return;
-  long long o = i % cv;
-  int k = (int)(i / cv);
-  int x = (int)(o % c.nx), y = (int)((o / c.nx) % c.ny), z = (int)(o / ((long long)c.nx * c.ny));
+  const int k = i / cv, o = i - k * cv;
+  const int x = o % c.nx, y = (o / c.nx) % c.ny, z = o / (c.nx * c.ny);
+  const float* src = gf + (long long)k * fv;
   float s = 0.f;
   for (int dz = 0; dz < 2; ++dz)
     for (int dy = 0; dy < 2; ++dy)
       for (int dx = 0; dx < 2; ++dx) {
-        int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
-        if (X < f.nx && Y < f.ny && Z < f.nz) s += gf[(long long)k * f.vox() + ((long long)Z * f.ny + Y) * f.nx + X];
+        const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+        if (X < f.nx && Y < f.ny && Z < f.nz) s += src[(Z * f.ny + Y) * f.nx + X];
       }
   gc[i] = s;
 }
@@ -442,6 +484,15 @@ int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in
   const int relu = L.relu ? 1 : 0;
   const long long tiles = n_tiles(d);
   const int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
+  if (tiles * (L.co / cob) < 2 * 148) {  // fewer tile CTAs than two per SM: one thread per (channel, voxel)
+    const dim3 g2((unsigned)((d.vox() + 127) / 128), (unsigned)L.co);
+    if (L.k == 3)
+      k_conv_small<3><<<g2, 128, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
+    else
+      k_conv_small<1><<<g2, 128, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
+    JXB_CUDA(cudaGetLastError());
+    return JXB_OK;
+  }
   const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob));
 #define JXB_CONV(KS, C)                                                                         \
   if (L.k == KS && cob == C) {                                                                  \
@@ -513,6 +564,7 @@ int ensure_bufs(jxb_cnn* N, Dims d0) {
   std::vector<std::pair<float**, long long>> want;
   auto add = [&](float** ptr, long long n) { want.push_back({ptr, (std::max<long long>(n, 1) + 63) / 64 * 64}); };
   long long gmax = (long long)std::max(N->in_ch, 4) * d0.vox();
+  if ((long long)64 * d0.vox() >= (1ll << 31)) return fail(JXB_ERR_INVALID, "cnn: grid too large (activation indices are 32-bit)");
   for (int l = 0; l < nl - 1; ++l) {
     add(&N->A[l], N->c[l] * d[l].vox());
     add(&N->S[l], N->c[l] * d[l].vox());
