@@ -119,37 +119,19 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         if (!A.keep[d1]) u1 = 0.0;
       }
     };
-    if (lane == 0) prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
-    // factors of this lane's two points and the z-table fragments of a layer,
-    // loaded one layer ahead (after the point operator of the layer before)
     const int qoff = 16 * (g & 3) + 8 * hh + 2 * t;
-    auto load_kf = [&](int lz_, double2* kf_) {
-      const double* G = A.geo + (size_t)(slot_base + (long long)lz_ * NE + w) * NG * NQE + qoff;
-#pragma unroll
-      for (int k = 0; k < NG; ++k) kf_[k] = __ldg(reinterpret_cast<const double2*>(G + k * NQE));
-    };
-    auto load_tz = [&](int ez_, double& a0, double& a1, double& a2) {
-      const double* tz_ = A.tab[2] + (size_t)ez_ * 3 * Q * P1;
-      a0 = tz_[lane];
-      a1 = tz_[ty0 + bo];
-      a2 = tz_[ty1 + bo];
-    };
-    double un0, un1, azn, azbn, azb2n;
-    double2 kf[NG];
+    if (lane == 0) prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
+    double un0, un1;
     load_in(bz * CZ, un0, un1);
-    load_tz(bz * CZ, azn, azbn, azb2n);
-    load_kf(0, kf);
     for (int lz = 0; lz < nlayers; ++lz) {
       const int ez = bz * CZ + lz;
       const int offz = br.first[2][ez] - cp0z;
-      if (lane == 0 && lz + 1 < nlayers)
-        prefetch_l2(A.geo + (size_t)(slot_base + (long long)(lz + 1) * NE + w) * NG * NQE, NG * NQE * sizeof(double));
+      const long long slot = slot_base + (long long)lz * NE + w;
+      if (lane == 0 && lz + 1 < nlayers) prefetch_l2(A.geo + (size_t)(slot + NE) * NG * NQE, NG * NQE * sizeof(double));
       const double u0 = un0, u1 = un1;
-      const double az = azn, azb = azbn, azb2 = azb2n;
-      if (lz + 1 < nlayers) {
-        load_in(ez + 1, un0, un1);
-        load_tz(ez + 1, azn, azbn, azb2n);
-      }
+      if (lz + 1 < nlayers) load_in(ez + 1, un0, un1);
+      const double* tz_ = A.tab[2] + (size_t)ez * 3 * Q * P1;
+      const double az = tz_[lane], azb = tz_[ty0 + bo], azb2 = tz_[ty1 + bo];
       // ---- forward x: D[rX = (type, q0)][c = i1 + 4 i2] -> XB
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
@@ -167,6 +149,11 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         st2(RB_ + jj * Y2 + g * YR + 2 * t, d0, d1);
       }
       __syncwarp();
+      // ---- geometric factors of this lane's two points (L2 hits after the prefetch)
+      const double* G = A.geo + (size_t)slot * NG * NQE + qoff;
+      double2 kf[NG];
+#pragma unroll
+      for (int k = 0; k < NG; ++k) kf[k] = __ldg(reinterpret_cast<const double2*>(G + k * NQE));
       // ---- forward z, columns n = 8h + g -> (q0, q1) = (g & 3, 2h + (g >> 2))
       double gxr[2][2], gyr[2][2], gzr[2][2];
 #pragma unroll
@@ -205,7 +192,6 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         st2(fb + FC, fy[0], fy[1]);
         st2(fb + 2 * FC, fz_[0], fz_[1]);
       }
-      if (lz + 1 < nlayers) load_kf(lz + 1, kf);  // in flight during the backward stages
       __syncwarp();
       // ---- backward z: T[channel][i2][n] (rows 0-3 of each product)
 #pragma unroll
