@@ -11,7 +11,10 @@ free DOFs) of the 3D linear-elasticity workload: unit cube, cubic NURBS,
 CUDA events, barrier + synchronize on both sides). ``e2e`` is the same metric
 through the C ABI with host buffers: pinned host u -> device, apply, device
 y -> pinned host, every step. ``time_to_solution`` gives the solves to a
-1e-8 relative residual: plain FP64 Jacobi-PCG and FP32-inner / FP64-refined.
+1e-8 relative residual: plain FP64 Jacobi-PCG and FP32-inner / FP64-refined,
+and, when jaxiga_b200/checkpoints holds a trained network for the workload
+(``python -m jaxiga_b200.train_pc``), flexible CG with the learned
+preconditioner in FP64 and as FP32 inner solves in FP64 refinement.
 
 ``--impl reference`` times the reference's CPU path for the same metric on a
 bounded sample (SciPy CSR K.u on an assembled 10^3-element instance, the
@@ -115,12 +118,15 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def profile_traffic():
-    """dram bytes per launch of the brick kernel from the committed ncu summary, if any."""
+def profile_traffic(workload, span):
+    """DRAM bytes per launch of the workload's brick kernel from the committed ncu
+    summary (profiles/apply_dram.json), scaled from the captured size by the
+    element count when the capture was smaller; None when there is none."""
     try:
         with open(os.path.join(ROOT, "profiles", "apply_dram.json")) as f:
-            d = json.load(f)
-        return d
+            d = json.load(f)[workload]
+        scale = (span / d["span"]) ** (2 if workload == "plate" else 3)
+        return {"dram_bytes_per_launch": d["dram_bytes_per_launch"] * scale, "captured_span": d["span"]}
     except Exception:
         return None
 
@@ -273,7 +279,7 @@ def run_ours(args, rank, world, local_rank):
         flops = V.n_elems * vec * (2 * 2 * 9 * p1**3 * q) + n_qp * (2 * 81 if vec == 3 else 2 * 9)
     peaks, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
-    traffic = profile_traffic()
+    traffic = profile_traffic(args.workload, span)
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
@@ -336,6 +342,29 @@ def run_ours(args, rank, world, local_rank):
             "speedup_mixed_vs_plain": st_p["seconds"] / st_m["seconds"] if st_m["seconds"] > 0 else None,
             "learned_preconditioner": None,
         }
+        ckpt = os.path.join(ROOT, "jaxiga_b200", "checkpoints", f"{args.workload}{span}.npz")
+        if os.path.exists(ckpt):
+            from jaxiga_b200.learned import LearnedPreconditioner
+
+            feats = None
+            if darcy:
+                loga = params["loga"]
+                feats = ((loga - loga.mean()) / loga.std())[None, :]
+            lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
+            rows = {}
+            for key, mixed in (("learned_fcg_fp64", False), ("mixed_learned_fcg", True)):
+                lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4)  # first call captures the graphs
+                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4)
+                rows[key] = {"seconds": st_l["seconds"], "iterations": st_l["iterations"],
+                             "learned_iterations": st_l["learned_iterations"],
+                             "relative_residual": st_l["relative_residual"], "converged": bool(st_l["converged"]),
+                             "relative_difference_to_plain": float(torch.linalg.norm(x_l - sol_p) / torch.linalg.norm(sol_p))}
+            tts["learned_preconditioner"] = {
+                "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
+                "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **rows,
+                "speedup_learned_vs_plain": st_p["seconds"] / rows["learned_fcg_fp64"]["seconds"],
+                "speedup_mixed_learned_vs_plain": st_p["seconds"] / rows["mixed_learned_fcg"]["seconds"]}
+            lp.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -140,26 +140,34 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
 }
 
 // The same convolution for grids too small to fill the GPU with voxel tiles:
-// one thread per (output channel, voxel), blockIdx.y = output channel, input
-// channels and taps summed in order by the thread (inputs from L1/L2, weights
-// uniform across the warp).
-template <int K>
+// one thread per (voxel, group of COS output channels), blockIdx.y = channel
+// group; the group's weights [ci][k][COS] are staged in shared memory, each
+// input value feeds COS accumulators, and every thread sums its input
+// channels and taps in a fixed order.
+template <int K, int COS>
 __global__ void __launch_bounds__(128) k_conv_small(Dims d, int ci_n, const float* __restrict__ in,
                                                     const float* __restrict__ w, const float* __restrict__ bias,
                                                     const float* __restrict__ add, int relu, float beta,
                                                     float* __restrict__ out) {
   constexpr int R = K / 2, KK = K * K * K;
-  const int co = blockIdx.y;
+  extern __shared__ __align__(16) float swc[];  // [ci][k][COS]
+  const int co0 = blockIdx.y * COS;
+  for (int i = threadIdx.x; i < ci_n * KK * COS; i += blockDim.x) {
+    const int o = i % COS, rest = i / COS;  // rest = ci * KK + k
+    swc[i] = w[(long long)(co0 + o) * ci_n * KK + rest];
+  }
+  __syncthreads();
   const int vox = (int)d.vox();
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= vox) return;
   const int nxy = d.nx * d.ny;
   const int x = v % d.nx, y = (v / d.nx) % d.ny, z = v / nxy;
-  float acc = bias ? bias[co] : 0.f;
-  const float* wc = w + (long long)co * ci_n * KK;
+  float acc[COS];
+#pragma unroll
+  for (int o = 0; o < COS; ++o) acc[o] = bias ? bias[co0 + o] : 0.f;
   for (int ci = 0; ci < ci_n; ++ci) {
     const float* ic = in + (long long)ci * vox;
-    const float* wk = wc + ci * KK;
+    const float4* wk = reinterpret_cast<const float4*>(swc + ci * KK * COS);
 #pragma unroll
     for (int dz = 0; dz < K; ++dz) {
       const int zz = z + dz - R;
@@ -172,15 +180,28 @@ __global__ void __launch_bounds__(128) k_conv_small(Dims d, int ci_n, const floa
         for (int dx = 0; dx < K; ++dx) {
           const int xx = x + dx - R;
           if (xx < 0 || xx >= d.nx) continue;
-          acc = fmaf(__ldg(wk + (dz * K + dy) * K + dx), __ldg(ic + zz * nxy + yy * d.nx + xx), acc);
+          const float a = __ldg(ic + zz * nxy + yy * d.nx + xx);
+          const int k = (dz * K + dy) * K + dx;
+#pragma unroll
+          for (int o4 = 0; o4 < COS / 4; ++o4) {
+            const float4 ww = wk[k * (COS / 4) + o4];
+            acc[4 * o4 + 0] = fmaf(ww.x, a, acc[4 * o4 + 0]);
+            acc[4 * o4 + 1] = fmaf(ww.y, a, acc[4 * o4 + 1]);
+            acc[4 * o4 + 2] = fmaf(ww.z, a, acc[4 * o4 + 2]);
+            acc[4 * o4 + 3] = fmaf(ww.w, a, acc[4 * o4 + 3]);
+          }
         }
       }
     }
   }
-  const long long idx = (long long)co * vox + v;
-  if (add) acc += add[idx];
-  if (relu) acc = fmaxf(acc, 0.f);
-  out[idx] = beta != 0.f ? beta * out[idx] + acc : acc;
+#pragma unroll
+  for (int o = 0; o < COS; ++o) {
+    const long long idx = (long long)(co0 + o) * vox + v;
+    float r = acc[o];
+    if (add) r += add[idx];
+    if (relu) r = fmaxf(r, 0.f);
+    out[idx] = beta != 0.f ? beta * out[idx] + r : r;
+  }
 }
 
 // Weight (and bias) gradient partials of one voxel tile:
@@ -484,12 +505,15 @@ int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in
   const int relu = L.relu ? 1 : 0;
   const long long tiles = n_tiles(d);
   const int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
-  if (tiles * (L.co / cob) < 2 * 148) {  // fewer tile CTAs than two per SM: one thread per (channel, voxel)
-    const dim3 g2((unsigned)((d.vox() + 127) / 128), (unsigned)L.co);
-    if (L.k == 3)
-      k_conv_small<3><<<g2, 128, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
-    else
-      k_conv_small<1><<<g2, 128, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
+  if (tiles * (L.co / cob) < 2 * 148) {  // fewer tile CTAs than two per SM: one thread per (voxel, 4 channels)
+    const dim3 g2((unsigned)((d.vox() + 127) / 128), (unsigned)(L.co / 4));
+    const size_t sm = (size_t)L.ci * L.k * L.k * L.k * 4 * sizeof(float);
+    if (L.k == 3) {
+      if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k_conv_small<3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_conv_small<3, 4><<<g2, 128, sm, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
+    } else {
+      k_conv_small<1, 4><<<g2, 128, sm, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
+    }
     JXB_CUDA(cudaGetLastError());
     return JXB_OK;
   }

@@ -275,6 +275,14 @@ class LearnedPreconditioner:
                  channels=np.asarray(self.channels), vec=self.vec, n_feat=self.n_feat,
                  history=np.asarray(self.history))
 
+    @classmethod
+    def from_checkpoint(cls, op, path, features=None):
+        """A preconditioner with the network shape, weights and scales stored in ``path``."""
+        d = np.load(path)
+        lp = cls(op, features=features, channels=tuple(int(c) for c in d["channels"]))
+        lp.load(path)
+        return lp
+
     def load(self, path):
         import torch
 
