@@ -304,3 +304,56 @@ def default_channels(grid):
     while levels < 6 and -(-n // 2 ** (levels - 1)) > 8:
         levels += 1
     return (8, 16, 24, 32, 48, 48)[:levels]
+
+
+def time_network(n=99, channels=None, reps=10, in_ch=2, once=False):
+    """Device time (ms) of the network's forward and backward on an n^3 grid of
+    random inputs, CUDA events on the current stream. ``once``: one forward and
+    one backward after three warm-up forwards (for a profiler launch list)."""
+    import torch
+
+    lib = _lib.load()
+    channels = tuple(channels or default_channels((n, n, n)))
+    h = ctypes.c_void_p()
+    _lib.check(lib.jxb_cnn_create(in_ch, 1, len(channels), (ctypes.c_int32 * len(channels))(*channels), 1,
+                                  ctypes.byref(h)))
+    try:
+        x = torch.randn(in_ch, n, n, n, device="cuda")
+        out = torch.empty(1, n, n, n, device="cuda")
+        g = torch.randn(1, n, n, n, device="cuda")
+        fwd = lambda: _lib.check(lib.jxb_cnn_forward(h, _s(), n, n, n, _p(x), _p(out)))  # noqa: E731
+        bwd = lambda: _lib.check(lib.jxb_cnn_backward(h, _s(), n, n, n, _p(x), _p(g)))  # noqa: E731
+        for _ in range(3):
+            fwd()
+        if once:
+            fwd()
+            bwd()
+            torch.cuda.synchronize()
+            return None
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        for _ in range(reps):
+            fwd()
+        e1.record()
+        for _ in range(reps):
+            fwd()
+            bwd()
+        e2.record()
+        torch.cuda.synchronize()
+        f = e0.elapsed_time(e1) / reps
+        return {"grid": n, "channels": channels, "forward_ms": f, "backward_ms": e1.elapsed_time(e2) / reps - f}
+    finally:
+        lib.jxb_cnn_destroy(h)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="time the learned preconditioner's network on an n^3 grid")
+    ap.add_argument("--grid", type=int, default=99)
+    ap.add_argument("--channels", default=None, help="per-level channels, e.g. 8,16,24,32,48")
+    ap.add_argument("--once", action="store_true", help="3 warm-up forwards, then one forward and one backward")
+    a = ap.parse_args()
+    ch = None if a.channels is None else [int(c) for c in a.channels.split(",")]
+    print(json.dumps(time_network(a.grid, ch, once=a.once)))
