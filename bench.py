@@ -285,8 +285,8 @@ def run_ours(args, rank, world, local_rank):
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
         "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
         "kernel": ("k_brick2<double,4,5,plate> (brick apply)" if plate else
-                   "k_brick3_mma (FP64 mma.sync brick apply, poisson p=3)"
-                   if darcy and os.environ.get("JXB_BRICK3_MMA", "1") != "0" else
+                   "k_brick3_mma (FP64 mma.sync brick apply, %s p=3)" % ("poisson" if darcy else "elasticity")
+                   if os.environ.get("JXB_BRICK3_MMA", "1") != "0" else
                    "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if darcy else "elasticity")),
         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
         "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,

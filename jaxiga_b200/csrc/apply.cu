@@ -547,10 +547,10 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
 #include "brick2d.cuh"
 #include "brick3_mma.cuh"
 
-// The FP64 tensor-core brick kernel runs the degree-3 scalar apply. The
-// environment variable JXB_BRICK3_MMA selects the variant: 0 = the FMA kernel
-// (to compare), 2 = the MMA kernel built for one CTA per SM, anything else =
-// the MMA kernel built for two CTAs per SM.
+// The FP64 tensor-core brick kernel runs the degree-3 scalar and elasticity
+// applies. The environment variable JXB_BRICK3_MMA selects the variant: 0 =
+// the FMA kernel (to compare), 2 = the scalar MMA kernel built for one CTA per
+// SM, anything else = the default (scalar: two CTAs per SM; elasticity: one).
 static int brick3_mma_mode() {
   static const int mode = [] {
     const char* e = getenv("JXB_BRICK3_MMA");
@@ -666,11 +666,16 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
     if constexpr (OPK == OPK_PLATE) {
       return fail(JXB_ERR_INVALID, "plate operator is 2D only");
     } else {
-      if constexpr (sizeof(T) == 8 && P == 3 && OPK == OPK_SCALAR && !RAT && MODE == MODE_APPLY) {
-        if (const int minb = brick3_mma_mode()) {
-          const size_t sm = smem3_mma(br);
+      if constexpr (sizeof(T) == 8 && P == 3 && (OPK == OPK_SCALAR || OPK == OPK_ELAST) && !RAT &&
+                    MODE == MODE_APPLY) {
+        if (const int mode = brick3_mma_mode()) {
+          const size_t sm = smem3_mma<OPK>(br);
           if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory");
-          auto k = minb == 2 ? k_brick3_mma<2> : k_brick3_mma<1>;
+          // elasticity needs the registers of the one-CTA-per-SM build
+          auto k = k_brick3_mma<OPK, 1>;
+          if constexpr (OPK == OPK_SCALAR) {
+            if (mode == 2) k = k_brick3_mma<OPK, 2>;
+          }
           JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
           k<<<(unsigned)br.n_bricks, bm::NT, sm, s>>>(A);
           JXB_CUDA(cudaGetLastError());

@@ -1,6 +1,7 @@
-// FP64 tensor-core variant of the 3D brick apply for the scalar operator
-// (Poisson / Darcy, polynomial weights) at degree 3 with 4 Gauss points per
-// direction. Included by apply.cu inside namespace jxb.
+// FP64 tensor-core variant of the 3D brick apply at degree 3 with 4 Gauss
+// points per direction, for the scalar operator (Poisson / Darcy) and for
+// linear elasticity, polynomial weights. Included by apply.cu inside
+// namespace jxb.
 //
 // At p = 3 every 1D contraction of the sum factorisation is a product of the
 // 8 x 4 table [N; N'] (rows: 4 points x value/derivative, columns: the 4
@@ -10,23 +11,25 @@
 // backward contractions use the transposed tables [N^T; N'^T] (or the halves
 // swapped, so the needed product lands in rows 0-3).
 //
-// Work split: the CTA owns one 4 x 4 x 8 element brick as in the scalar
+// Work split: the CTA owns one 4 x 4 x 8 element brick as in the FMA
 // kernel, and each of its 16 warps owns one column of 8 elements along z.
-// A warp runs each element's whole pipeline warp-synchronously (forward x,
-// y, z; point operator; backward z, y, x -- 28 MMAs), handing data between
-// stages through a private, padded shared-memory area (__syncwarp between
-// stages), and adds the element residual into its column's footprint in
-// shared memory, layer after layer in order. Warps never wait for each other
-// until the brick is done; then one fixed-order gather sums the 16 column
-// footprints into the brick footprint (no atomics), so the result is bitwise
-// reproducible. Input fragments come straight from the DOF vector (read one
-// layer ahead), factor tiles are prefetched into L2 one layer ahead.
+// A warp runs each element's whole pipeline warp-synchronously -- per
+// displacement component the forward x, y, z contractions, then the point
+// operator on all components, then per component the backward z, y, x
+// (28 MMAs per component) -- handing data between stages through a private,
+// padded shared-memory area (__syncwarp between stages), and adds the element
+// residual into its column's footprint in shared memory, layer after layer in
+// order. Warps never wait for each other until the brick is done; then one
+// fixed-order gather sums the 16 column footprints into the brick footprint
+// (no atomics), so the result is bitwise reproducible. Input fragments come
+// straight from the DOF vector (read one layer ahead), factor tiles are
+// prefetched into L2 one layer ahead.
 //
 // Fragment layouts of m8n8k4 (lane l, g = l >> 2, t = l & 3):
 //   A (8x4, row): a = A[g][t];  B (4x8, col): b = B[t][g];  C/D (8x8): d_i = D[g][2t + i].
 
 namespace bm {
-constexpr int P1 = 4, Q = 4, NQE = 64, NG = 6;
+constexpr int P1 = 4, Q = 4, NQE = 64;
 constexpr int TX = 4, TY = 4, CZ = 8, NE = TX * TY, NT = NE * 32;
 constexpr int XS = 20;               // XB[rX (8)][c (16)], c = i1 + 4 i2
 constexpr int YR = 8, Y2 = 68;       // YB[i2 (4)][rY (8)][rX (8)]
@@ -36,7 +39,7 @@ constexpr int S1 = 20, SC = 4 * S1;  // SB[type (2)][i1 (4)][m (16)], m = q0 + 4
 constexpr int RA = 3 * FC;           // region A (XB, FB, SB): 240 doubles
 constexpr int RB = 3 * TC;           // region B (YB, TB): 288 doubles
 constexpr int WB = RA + RB;          // per-warp doubles
-constexpr int CF = P1 * P1;         // one z row of a column footprint: [i1][i0]
+constexpr int CF = P1 * P1;          // one z row of a column footprint: [i1][i0]
 static_assert(8 * XS <= RA && 2 * SC <= RA && 4 * Y2 <= RB, "per-warp regions");
 }  // namespace bm
 
@@ -50,25 +53,29 @@ __device__ __forceinline__ void st2(double* p, double a, double b) {
   *reinterpret_cast<double2*>(p) = make_double2(a, b);
 }
 
+template <int OPK>
 static size_t smem3_mma(const Bricks& br) {
   using namespace bm;
-  const size_t n = (size_t)NE * WB + (size_t)NE * br.fp[2] * CF;
+  constexpr int VEC = OPK == OPK_ELAST ? 3 : 1;
+  const size_t n = (size_t)NE * WB + (size_t)NE * VEC * br.fp[2] * CF;
   return n * sizeof(double) + (TX + TY) * sizeof(int) + 64;
 }
 
 // MINB resident CTAs per SM the kernel is built for: 2 caps registers at 64
 // per thread, 1 allows 128 with half the warps.
-template <int MINB>
+template <int OPK, int MINB>
 __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A) {
   using namespace bm;
+  constexpr int VEC = OPK == OPK_ELAST ? 3 : 1;
+  constexpr int NG = OPK == OPK_ELAST ? 10 : 6;  // factors per point: J^-1 and w|J| / the symmetric metric
   if (A.state && A.state->done) return;
   const Bricks& br = A.br;
   const int fp0 = br.fp[0], fp1 = br.fp[1], fp2 = br.fp[2];
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* wbuf = reinterpret_cast<double*>(smem_raw);  // [NE][WB] stage hand-off areas
-  double* colf = wbuf + NE * WB;                         // [NE][fp2][i1][i0] column footprints
-  int* soff = reinterpret_cast<int*>(colf + NE * fp2 * CF);
+  double* colf = wbuf + NE * WB;                         // [NE][VEC][fp2][i1][i0] column footprints
+  int* soff = reinterpret_cast<int*>(colf + NE * VEC * fp2 * CF);
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -90,8 +97,8 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
     const int e = by * TY + tid;
     soff[TX + tid] = e < br.n_span[1] ? br.first[1][e] - cp0y : -100000;
   }
-  double* cf = colf + w * fp2 * CF;
-  for (int i = lane; i < fp2 * CF; i += 32) cf[i] = 0.0;
+  double* cf = colf + w * VEC * fp2 * CF;
+  for (int i = lane; i < VEC * fp2 * CF; i += 32) cf[i] = 0.0;
 
   if (evalid) {
     // A fragments of the column's x / y tables ([2][Q][P1] per span)
@@ -108,148 +115,195 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
     const int hh = hi ? 1 : 0;
     const long long ncx = br.n_cp[0], nxy = (long long)br.n_cp[0] * br.n_cp[1];
     // this lane's input entries (x-stage B fragments): i0 = t, i1 = g & 3, i2 = 2j + (g >> 2)
-    const long long dxy = (long long)(br.first[0][ex] + t) + ncx * (br.first[1][ey] + (g & 3));
-    auto load_in = [&](int ez_, double& u0, double& u1) {
-      const long long d0 = dxy + nxy * (br.first[2][ez_] + (g >> 2));
-      const long long d1 = d0 + 2 * nxy;
-      u0 = A.x[d0];
-      u1 = A.x[d1];
-      if (A.masked) {
-        if (!A.keep[d0]) u0 = 0.0;
-        if (!A.keep[d1]) u1 = 0.0;
+    const long long cxy = (long long)(br.first[0][ex] + t) + ncx * (br.first[1][ey] + (g & 3));
+    auto load_in = [&](int ez_, double (&u)[VEC][2]) {
+      const long long c0 = cxy + nxy * (br.first[2][ez_] + (g >> 2));
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const long long cp = c0 + 2 * j * nxy;
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+          const long long dof = cp * VEC + c;
+          double v = A.x[dof];
+          if (A.masked && !A.keep[dof]) v = 0.0;
+          u[c][j] = v;
+        }
       }
     };
     const int qoff = 16 * (g & 3) + 8 * hh + 2 * t;
     if (lane == 0) prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
-    double un0, un1;
-    load_in(bz * CZ, un0, un1);
+    double un[VEC][2];
+    load_in(bz * CZ, un);
     for (int lz = 0; lz < nlayers; ++lz) {
       const int ez = bz * CZ + lz;
       const int offz = br.first[2][ez] - cp0z;
       const long long slot = slot_base + (long long)lz * NE + w;
       if (lane == 0 && lz + 1 < nlayers) prefetch_l2(A.geo + (size_t)(slot + NE) * NG * NQE, NG * NQE * sizeof(double));
-      const double u0 = un0, u1 = un1;
-      if (lz + 1 < nlayers) load_in(ez + 1, un0, un1);
+      double u[VEC][2];
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        u[c][0] = un[c][0];
+        u[c][1] = un[c][1];
+      }
+      if (lz + 1 < nlayers) load_in(ez + 1, un);
       const double* tz_ = A.tab[2] + (size_t)ez * 3 * Q * P1;
       const double az = tz_[lane], azb = tz_[ty0 + bo], azb2 = tz_[ty1 + bo];
-      // ---- forward x: D[rX = (type, q0)][c = i1 + 4 i2] -> XB
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        double d0, d1;
-        dmma(d0, d1, ax, j ? u1 : u0, 0.0, 0.0);
-        st2(RA_ + g * XS + 8 * j + 2 * t, d0, d1);
-      }
-      __syncwarp();
-      // ---- forward y (i2 = jj): D[rY = (type, q1)][rX] -> YB[i2][rY][rX]
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const double bv = RA_[g * XS + t + 4 * jj];
-        double d0, d1;
-        dmma(d0, d1, ay, bv, 0.0, 0.0);
-        st2(RB_ + jj * Y2 + g * YR + 2 * t, d0, d1);
-      }
-      __syncwarp();
-      // ---- geometric factors of this lane's two points (L2 hits after the prefetch)
       const double* G = A.geo + (size_t)slot * NG * NQE + qoff;
       double2 kf[NG];
+      // gradients of each component at this lane's two points
+      double GX[VEC][2], GY[VEC][2], GZ[VEC][2];
 #pragma unroll
-      for (int k = 0; k < NG; ++k) kf[k] = __ldg(reinterpret_cast<const double2*>(G + k * NQE));
-      // ---- forward z, columns n = 8h + g -> (q0, q1) = (g & 3, 2h + (g >> 2))
-      double gxr[2][2], gyr[2][2], gzr[2][2];
+      for (int c = 0; c < VEC; ++c) {
+        // ---- forward x: D[rX = (type, q0)][c = i1 + 4 i2] -> XB
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double* yb = RB_ + t * Y2 + (2 * h + (g >> 2)) * YR + (g & 3);
-        const double bdv = yb[4];           // rY = (v, q1), rX = (d, q0): x-derivative
-        const double bvd = yb[4 * YR];      // rY = (d, q1), rX = (v, q0): y-derivative
-        const double bvv = yb[0];           // both values
-        dmma(gxr[h][0], gxr[h][1], az, bdv, 0.0, 0.0);  // rows 0-3: gx
-        dmma(gyr[h][0], gyr[h][1], az, bvd, 0.0, 0.0);  // rows 0-3: gy
-        dmma(gzr[h][0], gzr[h][1], az, bvv, 0.0, 0.0);  // rows 4-7: gz
-      }
-      // lanes 0-15 keep the points of h = 0, lanes 16-31 those of h = 1
-      double GX[2], GY[2], GZ[2];
+        for (int j = 0; j < 2; ++j) {
+          double d0, d1;
+          dmma(d0, d1, ax, u[c][j], 0.0, 0.0);
+          st2(RA_ + g * XS + 8 * j + 2 * t, d0, d1);
+        }
+        __syncwarp();
+        // ---- forward y (i2 = jj): D[rY = (type, q1)][rX] -> YB[i2][rY][rX]
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const double r1 = __shfl_xor_sync(0xffffffffu, hi ? gzr[0][i] : gxr[1][i], 16);
-        const double r2 = __shfl_xor_sync(0xffffffffu, gyr[1][i], 16);
-        GX[i] = hi ? r1 : gxr[0][i];
-        GY[i] = hi ? r2 : gyr[0][i];
-        GZ[i] = hi ? gzr[1][i] : r1;
-      }
-      // ---- point operator: flux = M_q grad u (symmetric 3 x 3 metric)
-      {
-        const double k0[2] = {kf[0].x, kf[0].y}, k1[2] = {kf[1].x, kf[1].y}, k2[2] = {kf[2].x, kf[2].y};
-        const double k3[2] = {kf[3].x, kf[3].y}, k4[2] = {kf[4].x, kf[4].y}, k5[2] = {kf[5].x, kf[5].y};
-        double fx[2], fy[2], fz_[2];
+        for (int jj = 0; jj < 4; ++jj) {
+          const double bv = RA_[g * XS + t + 4 * jj];
+          double d0, d1;
+          dmma(d0, d1, ay, bv, 0.0, 0.0);
+          st2(RB_ + jj * Y2 + g * YR + 2 * t, d0, d1);
+        }
+        __syncwarp();
+        if (c == VEC - 1) {  // the factors (L2 hits after the prefetch), in flight during the last z stage
+#pragma unroll
+          for (int k = 0; k < NG; ++k) kf[k] = __ldg(reinterpret_cast<const double2*>(G + k * NQE));
+        }
+        // ---- forward z, columns n = 8h + g -> (q0, q1) = (g & 3, 2h + (g >> 2))
+        double gxr[2][2], gyr[2][2], gzr[2][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double* yb = RB_ + t * Y2 + (2 * h + (g >> 2)) * YR + (g & 3);
+          const double bdv = yb[4];       // rY = (v, q1), rX = (d, q0): x-derivative
+          const double bvd = yb[4 * YR];  // rY = (d, q1), rX = (v, q0): y-derivative
+          const double bvv = yb[0];       // both values
+          dmma(gxr[h][0], gxr[h][1], az, bdv, 0.0, 0.0);  // rows 0-3: d/dxi
+          dmma(gyr[h][0], gyr[h][1], az, bvd, 0.0, 0.0);  // rows 0-3: d/deta
+          dmma(gzr[h][0], gzr[h][1], az, bvv, 0.0, 0.0);  // rows 4-7: d/dzeta
+        }
+        // lanes 0-15 keep the points of h = 0, lanes 16-31 those of h = 1
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-          fx[i] = k0[i] * GX[i] + k1[i] * GY[i] + k2[i] * GZ[i];
-          fy[i] = k1[i] * GX[i] + k3[i] * GY[i] + k4[i] * GZ[i];
-          fz_[i] = k2[i] * GX[i] + k4[i] * GY[i] + k5[i] * GZ[i];
+          const double r1 = __shfl_xor_sync(0xffffffffu, hi ? gzr[0][i] : gxr[1][i], 16);
+          const double r2 = __shfl_xor_sync(0xffffffffu, gyr[1][i], 16);
+          GX[c][i] = hi ? r1 : gxr[0][i];
+          GY[c][i] = hi ? r2 : gyr[0][i];
+          GZ[c][i] = hi ? gzr[1][i] : r1;
         }
-        double* fb = RA_ + (g & 3) * F2 + 8 * hh + 2 * t;
-        st2(fb, fx[0], fx[1]);
-        st2(fb + FC, fy[0], fy[1]);
-        st2(fb + 2 * FC, fz_[0], fz_[1]);
+        __syncwarp();  // the next component's y stage overwrites YB
       }
-      __syncwarp();
-      // ---- backward z: T[channel][i2][n] (rows 0-3 of each product)
+      // ---- point operator at this lane's two points: fluxes F[c][a] (a = xi, eta, zeta)
+      double F[VEC][3][2];
+      if constexpr (OPK == OPK_ELAST) {
+        const double lam = A.lam, mu = A.mu;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double* fb = RA_ + t * F2 + 8 * h + g;
-        double a0, a1, b0, b1, c0, c1;
-        dmma(a0, a1, azb, fb[0], 0.0, 0.0);        // Nz^T fx  -> T_dv
-        dmma(b0, b1, azb, fb[FC], 0.0, 0.0);       // Nz^T fy  -> T_vd
-        dmma(c0, c1, azb2, fb[2 * FC], 0.0, 0.0);  // Nz'^T fz -> T_vv
-        if (!hi) {
-          double* tb = RB_ + g * T2 + 8 * h + 2 * t;
-          st2(tb, a0, a1);
-          st2(tb + TC, b0, b1);
-          st2(tb + 2 * TC, c0, c1);
-        }
-      }
-      __syncwarp();
-      // ---- backward y: columns m = 8h + g -> (q0, i2) = (g & 3, 2h + (g >> 2))
+        for (int i = 0; i < 2; ++i) {
+          double Ji[3][3];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double* tb = RB_ + (2 * h + (g >> 2)) * T2 + (g & 3) + 4 * t;
-        double v0, v1, d0, d1;
-        dmma(v0, v1, ayb2, tb[TC], 0.0, 0.0);      // Ny'^T T_vd
-        dmma(v0, v1, ayb, tb[2 * TC], v0, v1);     // + Ny^T T_vv
-        dmma(d0, d1, ayb, tb[0], 0.0, 0.0);        // Ny^T T_dv
-        if (!hi) {
-          double* sb = RA_ + g * S1 + 8 * h + 2 * t;
-          st2(sb, v0, v1);
-          st2(sb + SC, d0, d1);
-        }
-      }
-      __syncwarp();
-      // ---- backward x: columns n = 8h + g -> (i1, i2) = (g & 3, 2h + (g >> 2))
+          for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double* sb = RA_ + (g & 3) * S1 + t + 8 * h + 4 * (g >> 2);
-        double r0, r1;
-        dmma(r0, r1, axb2, sb[SC], 0.0, 0.0);      // Nx'^T S_d
-        dmma(r0, r1, axb, sb[0], r0, r1);          // + Nx^T S_v
-        if (!hi) {  // res[i0 = g][i1 + 4 i2 = 8h + 2t + i] into the column footprint
+            for (int a = 0; a < 3; ++a) Ji[k][a] = i ? kf[k * 3 + a].y : kf[k * 3 + a].x;
+          const double om = i ? kf[9].y : kf[9].x;
+          double Gx[3][3];  // du_c / dx_k
 #pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const int n = 8 * h + 2 * t + i;
-            cf[((offz + (n >> 2)) * P1 + (n & 3)) * P1 + g] += i ? r1 : r0;
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Gx[c][k] = Ji[k][0] * GX[c][i] + Ji[k][1] * GY[c][i] + Ji[k][2] * GZ[c][i];
+          const double tr = Gx[0][0] + Gx[1][1] + Gx[2][2];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double Sr[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Sr[k] = om * (mu * (Gx[c][k] + Gx[k][c]) + (c == k ? lam * tr : 0.0));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) F[c][a][i] = Sr[0] * Ji[0][a] + Sr[1] * Ji[1][a] + Sr[2] * Ji[2][a];
           }
         }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const double k0 = i ? kf[0].y : kf[0].x, k1 = i ? kf[1].y : kf[1].x, k2 = i ? kf[2].y : kf[2].x;
+          const double k3 = i ? kf[3].y : kf[3].x, k4 = i ? kf[4].y : kf[4].x, k5 = i ? kf[5].y : kf[5].x;
+          F[0][0][i] = k0 * GX[0][i] + k1 * GY[0][i] + k2 * GZ[0][i];
+          F[0][1][i] = k1 * GX[0][i] + k3 * GY[0][i] + k4 * GZ[0][i];
+          F[0][2][i] = k2 * GX[0][i] + k4 * GY[0][i] + k5 * GZ[0][i];
+        }
       }
-      __syncwarp();
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        {
+          double* fb = RA_ + (g & 3) * F2 + 8 * hh + 2 * t;
+          st2(fb, F[c][0][0], F[c][0][1]);
+          st2(fb + FC, F[c][1][0], F[c][1][1]);
+          st2(fb + 2 * FC, F[c][2][0], F[c][2][1]);
+        }
+        __syncwarp();
+        // ---- backward z: T[channel][i2][n] (rows 0-3 of each product)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double* fb = RA_ + t * F2 + 8 * h + g;
+          double a0, a1, b0, b1, c0, c1;
+          dmma(a0, a1, azb, fb[0], 0.0, 0.0);        // Nz^T F_xi   -> T_dv
+          dmma(b0, b1, azb, fb[FC], 0.0, 0.0);       // Nz^T F_eta  -> T_vd
+          dmma(c0, c1, azb2, fb[2 * FC], 0.0, 0.0);  // Nz'^T F_zeta -> T_vv
+          if (!hi) {
+            double* tb = RB_ + g * T2 + 8 * h + 2 * t;
+            st2(tb, a0, a1);
+            st2(tb + TC, b0, b1);
+            st2(tb + 2 * TC, c0, c1);
+          }
+        }
+        __syncwarp();
+        // ---- backward y: columns m = 8h + g -> (q0, i2) = (g & 3, 2h + (g >> 2))
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double* tb = RB_ + (2 * h + (g >> 2)) * T2 + (g & 3) + 4 * t;
+          double v0, v1, d0, d1;
+          dmma(v0, v1, ayb2, tb[TC], 0.0, 0.0);   // Ny'^T T_vd
+          dmma(v0, v1, ayb, tb[2 * TC], v0, v1);  // + Ny^T T_vv
+          dmma(d0, d1, ayb, tb[0], 0.0, 0.0);     // Ny^T T_dv
+          if (!hi) {
+            double* sb = RA_ + g * S1 + 8 * h + 2 * t;
+            st2(sb, v0, v1);
+            st2(sb + SC, d0, d1);
+          }
+        }
+        __syncwarp();
+        // ---- backward x: columns n = 8h + g -> (i1, i2) = (g & 3, 2h + (g >> 2))
+        double* cfc = cf + c * fp2 * CF;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double* sb = RA_ + (g & 3) * S1 + t + 8 * h + 4 * (g >> 2);
+          double r0, r1;
+          dmma(r0, r1, axb2, sb[SC], 0.0, 0.0);  // Nx'^T S_d
+          dmma(r0, r1, axb, sb[0], r0, r1);      // + Nx^T S_v
+          if (!hi) {  // res[i0 = g][i1 + 4 i2 = 8h + 2t + i] into the column footprint
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int n = 8 * h + 2 * t + i;
+              cfc[((offz + (n >> 2)) * P1 + (n & 3)) * P1 + g] += i ? r1 : r0;
+            }
+          }
+        }
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
   // ---- deterministic gather of the column footprints into the brick footprint
   const int nfoot = fp0 * fp1 * fp2;
-  double* out = A.scratch + (size_t)b * nfoot;
-  for (int i = tid; i < nfoot; i += NT) {
+  double* out = A.scratch + (size_t)b * VEC * nfoot;
+  for (int i = tid; i < VEC * nfoot; i += NT) {
     const int jx = i % fp0;
     const int jy = (i / fp0) % fp1;
-    const int jz = i / (fp0 * fp1);
+    const int jz = (i / (fp0 * fp1)) % fp2;
+    const int c = i / nfoot;
     double s = 0.0;
 #pragma unroll
     for (int e1 = 0; e1 < TY; ++e1) {
@@ -259,7 +313,7 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
       for (int e0 = 0; e0 < TX; ++e0) {
         const int lx = jx - soff[e0];
         if (lx < 0 || lx >= P1) continue;
-        s += colf[((e1 * TX + e0) * fp2 + jz) * CF + ly * P1 + lx];
+        s += colf[(((e1 * TX + e0) * VEC + c) * fp2 + jz) * CF + ly * P1 + lx];
       }
     }
     out[i] = s;
