@@ -17,7 +17,7 @@
 // displacement component the forward x, y, z contractions, then the point
 // operator on all components, then per component the backward z, y, x
 // (28 MMAs per component) -- handing data between stages through a private,
-// padded shared-memory area (__syncwarp between stages), and adds the element
+// bank-conflict-free shared-memory area (__syncwarp between stages), and adds the element
 // residual into its column's footprint in shared memory, layer after layer in
 // order. Warps never wait for each other until the brick is done; then one
 // fixed-order gather sums the 16 column footprints into the brick footprint
@@ -31,16 +31,19 @@
 namespace bm {
 constexpr int P1 = 4, Q = 4, NQE = 64;
 constexpr int TX = 4, TY = 4, CZ = 8, NE = TX * TY, NT = NE * 32;
-constexpr int XS = 20;               // XB[rX (8)][c (16)], c = i1 + 4 i2
+// XB, FB and SB are rows of 16 doubles stored XOR-swizzled (swz below), which
+// keeps both the 16-byte fragment stores and the 8-byte operand loads free of
+// bank conflicts; YB and TB get the same from padding.
 constexpr int YR = 8, Y2 = 68;       // YB[i2 (4)][rY (8)][rX (8)]
-constexpr int F2 = 20, FC = 4 * F2;  // FB[channel (3)][q2 (4)][n (16)], n = q0 + 4 q1
+constexpr int FC = 64;               // FB[channel (3)][q2 (4)][n (16)], n = q0 + 4 q1   (swizzled rows)
 constexpr int T2 = 24, TC = 4 * T2;  // TB[channel (3)][i2 (4)][n (16)]
-constexpr int S1 = 20, SC = 4 * S1;  // SB[type (2)][i1 (4)][m (16)], m = q0 + 4 i2
-constexpr int RA = 3 * FC;           // region A (XB, FB, SB): 240 doubles
+constexpr int SC = 64;               // SB[type (2)][i1 (4)][m (16)], m = q0 + 4 i2      (swizzled rows)
+                                     // XB[rX (8)][c (16)], c = i1 + 4 i2                 (swizzled rows)
+constexpr int RA = 3 * FC;           // region A (XB, FB, SB): 192 doubles
 constexpr int RB = 3 * TC;           // region B (YB, TB): 288 doubles
 constexpr int WB = RA + RB;          // per-warp doubles
 constexpr int CF = P1 * P1;          // one z row of a column footprint: [i1][i0]
-static_assert(8 * XS <= RA && 2 * SC <= RA && 4 * Y2 <= RB, "per-warp regions");
+static_assert(8 * 16 <= RA && 2 * SC <= RA && 4 * Y2 <= RB, "per-warp regions");
 }  // namespace bm
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0, double c1) {
@@ -48,6 +51,10 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b,
       : "=d"(d0), "=d"(d1)
       : "d"(a), "d"(b), "d"(c0), "d"(c1));
 }
+
+// position of (row r, column c) in a swizzled buffer of 16-double rows: the
+// row's two low bits flip column bits 3 and 2 (pairs c, c+1 stay adjacent)
+__device__ __forceinline__ int swz(int r, int c) { return r * 16 + (c ^ (((r & 1) << 3) | ((r & 2) << 1))); }
 
 __device__ __forceinline__ void st2(double* p, double a, double b) {
   *reinterpret_cast<double2*>(p) = make_double2(a, b);
@@ -159,13 +166,13 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         for (int j = 0; j < 2; ++j) {
           double d0, d1;
           dmma(d0, d1, ax, u[c][j], 0.0, 0.0);
-          st2(RA_ + g * XS + 8 * j + 2 * t, d0, d1);
+          st2(RA_ + swz(g, 8 * j + 2 * t), d0, d1);
         }
         __syncwarp();
         // ---- forward y (i2 = jj): D[rY = (type, q1)][rX] -> YB[i2][rY][rX]
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-          const double bv = RA_[g * XS + t + 4 * jj];
+          const double bv = RA_[swz(g, t + 4 * jj)];
           double d0, d1;
           dmma(d0, d1, ay, bv, 0.0, 0.0);
           st2(RB_ + jj * Y2 + g * YR + 2 * t, d0, d1);
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
 #pragma unroll
       for (int c = 0; c < VEC; ++c) {
         {
-          double* fb = RA_ + (g & 3) * F2 + 8 * hh + 2 * t;
+          double* fb = RA_ + swz(g & 3, 8 * hh + 2 * t);
           st2(fb, F[c][0][0], F[c][0][1]);
           st2(fb + FC, F[c][1][0], F[c][1][1]);
           st2(fb + 2 * FC, F[c][2][0], F[c][2][1]);
@@ -247,7 +254,7 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         // ---- backward z: T[channel][i2][n] (rows 0-3 of each product)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const double* fb = RA_ + t * F2 + 8 * h + g;
+          const double* fb = RA_ + swz(t, 8 * h + g);
           double a0, a1, b0, b1, c0, c1;
           dmma(a0, a1, azb, fb[0], 0.0, 0.0);        // Nz^T F_xi   -> T_dv
           dmma(b0, b1, azb, fb[FC], 0.0, 0.0);       // Nz^T F_eta  -> T_vd
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
           dmma(v0, v1, ayb, tb[2 * TC], v0, v1);  // + Ny^T T_vv
           dmma(d0, d1, ayb, tb[0], 0.0, 0.0);     // Ny^T T_dv
           if (!hi) {
-            double* sb = RA_ + g * S1 + 8 * h + 2 * t;
+            double* sb = RA_ + swz(g, 8 * h + 2 * t);
             st2(sb, v0, v1);
             st2(sb + SC, d0, d1);
           }
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
         double* cfc = cf + c * fp2 * CF;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const double* sb = RA_ + (g & 3) * S1 + t + 8 * h + 4 * (g >> 2);
+          const double* sb = RA_ + swz(g & 3, t + 8 * h + 4 * (g >> 2));
           double r0, r1;
           dmma(r0, r1, axb2, sb[SC], 0.0, 0.0);  // Nx'^T S_d
           dmma(r0, r1, axb, sb[0], r0, r1);      // + Nx^T S_v
