@@ -222,8 +222,10 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
  *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
  *   Jacobi directions take over after `stall` learned iterations without a new
- *   lowest residual or a non-descent direction. mixed != 0: FP32 inner solves
- *   (inner_tol) inside FP64 iterative refinement (plan created with want_f32).
+ *   lowest residual or a non-descent direction. `mode` bit 0: FP32 inner solves
+ *   (inner_tol) inside FP64 iterative refinement (plan created with want_f32);
+ *   bit 1: two-level preconditioner z = a n + D^-1 (r - a K n), n the network
+ *   output, a = (n.r)/(n^T K n) (one more operator apply per iteration).
  *   stats->outer = iterations that used the network. */
 typedef struct jxb_cnn jxb_cnn;
 int jxb_cnn_create(int in_ch, int out_ch, int levels, const int* channels, uint64_t seed, jxb_cnn** out);
@@ -240,7 +242,7 @@ int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, c
 int jxb_cnn_adam(jxb_cnn* cnn, jxb_stream stream, float lr, float grad_scale);
 int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                     const float* features, int n_features, float in_scale, double out_scale, int stall,
-                    int depth, int mixed, const jxb_solve_opts* opts, jxb_stats* stats);
+                    int depth, int mode, const jxb_solve_opts* opts, jxb_stats* stats);
 
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);

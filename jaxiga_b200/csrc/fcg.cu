@@ -76,6 +76,32 @@ __global__ void k_fjac(long long n, const T* __restrict__ inv, const T* __restri
     z[i] = inv[i] * r[i];
 }
 
+// partials of z . r (two-level mode)
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fzr(long long n, const FcgState* st, const T* __restrict__ z,
+                                                         const T* __restrict__ r, double* __restrict__ partials) {
+  if (st->cg.done) return;
+  double acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc += (double)z[i] * (double)r[i];
+  const double s = block_sum_all(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// two-level preconditioner: z <- a z + D^-1 (r - a K z), a = (z.r)/(z.Kz), the
+// network output taken as a coarse correction with its own line search and
+// followed by one Jacobi step on the remaining residual
+template <typename T>
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_ftwolevel(long long n, const FcgState* st, const double* __restrict__ zkz_part,
+                                                               const double* __restrict__ zr_part, const T* __restrict__ Kz,
+                                                               const T* __restrict__ r, const T* __restrict__ inv, T* __restrict__ z) {
+  if (st->cg.done) return;
+  const double zkz = reduce_partials(zkz_part), zr = reduce_partials(zr_part);
+  const T a = (zkz > 0 && isfinite(zkz) && isfinite(zr)) ? (T)(zr / zkz) : T(0);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = a * z[i] + inv[i] * (r[i] - a * Kz[i]);
+}
+
 // ring slot of stored direction d (0-based since the last restart)
 __device__ __forceinline__ int fcg_slot(long long d, int m) { return (int)(d % m); }
 
@@ -337,6 +363,7 @@ struct FcgRun {
   float in_scale;
   double out_scale;
   int stall, m, every;
+  bool two_level = false;
   FcgState *d_st = nullptr, *h_st = nullptr;
   double* part = nullptr;  // (FCG_MMAX + 3) x JXB_RED_BLOCKS
   float* in = nullptr;
@@ -376,6 +403,14 @@ int record_iteration(FcgRun& R, cudaStream_t s, bool learned, int iters) {
       int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, &out4);
       if (rc) return rc;
       k_funpack<T><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, out4, plan->d_keep, R.out_scale, R.d_st, z);
+      if (R.two_level) {  // K z into Ap (free until the direction's apply), z.Kz and z.r partials
+        int rc2 = launch_bricks<T>(plan, s, MODE_APPLY, z, nullptr, &R.d_st->cg, 1);
+        if (rc2) return rc2;
+        rc2 = launch_combine<T>(plan, s, Ap, 1, z, pap, &R.d_st->cg);
+        if (rc2) return rc2;
+        k_fzr<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, z, r, ppr);
+        k_ftwolevel<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, pap, ppr, Ap, r, inv, z);
+      }
     } else {
       k_fjac<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, inv, r, R.d_st, z);
     }
@@ -508,7 +543,8 @@ using namespace jxb;
 
 extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                                const float* features, int n_features, float in_scale, double out_scale, int stall,
-                               int depth, int mixed, const jxb_solve_opts* opts, jxb_stats* stats) {
+                               int depth, int mode, const jxb_solve_opts* opts, jxb_stats* stats) {
+  const int mixed = mode & 1;
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: null argument");
   if (n_features < 0 || (n_features > 0 && !features)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: bad features");
   if (cnn && cnn_out_channels(cnn) != plan->vec)
@@ -540,6 +576,7 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
   R.stall = stall > 0 ? stall : 1 << 30;
   R.m = depth;
   R.every = opts->check_every > 0 ? opts->check_every : 16;
+  R.two_level = (mode & 2) != 0;
   GraphPair G;
   rc = mixed ? fcg_setup<float>(R, s) : fcg_setup<double>(R, s);
   if (rc) return rc;

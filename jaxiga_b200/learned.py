@@ -246,10 +246,12 @@ class LearnedPreconditioner:
 
     # -- solve -------------------------------------------------------------------
     def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=1e-4, check_every=16,
-              use_network=True):
+              use_network=True, two_level=False):
         """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats).
 
         ``mixed``: FP32 inner solves to ``inner_tol`` inside FP64 refinement.
+        ``two_level``: the network output n as a coarse correction with its own
+        line search, then one Jacobi step: z = a n + D^-1 (r - a K n).
         ``use_network=False`` runs the same FCG with Jacobi only (the baseline
         the network is measured against).
         """
@@ -262,7 +264,7 @@ class LearnedPreconditioner:
         rc = self.lib.jxb_fcg_learned(op.handle, self.handle if use_network else None, _s(), _p(b), _p(x),
                                       _p(feats) if feats is not None else None, self.n_feat,
                                       float(self.in_scale), float(self.out_scale), int(stall), int(depth),
-                                      1 if mixed else 0, ctypes.byref(o), ctypes.byref(st))
+                                      (1 if mixed else 0) | (2 if two_level else 0), ctypes.byref(o), ctypes.byref(st))
         if rc not in (0, 4):
             _lib.check(rc)
         out = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}

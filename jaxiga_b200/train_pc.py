@@ -123,6 +123,10 @@ def main():
     x_m, st = lp.solve(F, tol=1e-8, depth=args.depth, mixed=True, inner_tol=1e-4)
     st["relative_difference_to_plain"] = float(torch.linalg.norm(x_m - x_ref) / torch.linalg.norm(x_ref))
     solves["learned_fcg_mixed"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True)
+    solves["learned_fcg_two_level"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True, mixed=True, inner_tol=1e-4)
+    solves["learned_fcg_two_level_mixed"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth, use_network=False)
     solves["fcg_jacobi_only"] = st
     # network inference time on its own

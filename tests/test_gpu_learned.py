@@ -212,6 +212,10 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     assert st_j["converged"] and abs(st_j["iterations"] - st_ref["iterations"]) <= 2, (st_j, st_ref)
     assert st_l["learned_iterations"] == st_l["iterations"], st_l
     assert st_l["iterations"] < st_ref["iterations"], (st_l, st_ref)
+    # two-level: the network as a line-searched coarse correction plus one Jacobi step
+    x_t, st_t = lp.solve(b, tol=1e-8, two_level=True)
+    assert st_t["converged"] and st_t["iterations"] < st_ref["iterations"], (st_t, st_ref)
+    assert float(torch.linalg.norm(x_t - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
     # mixed precision: FP32 inner flexible CG inside FP64 refinement
     x_m, st_m = lp.solve(b, tol=1e-8, mixed=True, inner_tol=1e-4)
     assert st_m["converged"], st_m
