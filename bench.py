@@ -352,9 +352,10 @@ def run_ours(args, rank, world, local_rank):
                 feats = ((loga - loga.mean()) / loga.std())[None, :]
             lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
             rows = {}
-            for key, mixed in (("learned_fcg_fp64", False), ("mixed_learned_fcg", True)):
-                lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4)  # first call captures the graphs
-                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4)
+            for key, mixed, two in (("learned_fcg_fp64", False, False), ("mixed_learned_fcg", True, False),
+                                    ("learned_two_level_fp64", False, True), ("mixed_learned_two_level", True, True)):
+                lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4, two_level=two)  # first call captures the graphs
+                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4, two_level=two)
                 rows[key] = {"seconds": st_l["seconds"], "iterations": st_l["iterations"],
                              "learned_iterations": st_l["learned_iterations"],
                              "relative_residual": st_l["relative_residual"], "converged": bool(st_l["converged"]),
@@ -362,8 +363,7 @@ def run_ours(args, rank, world, local_rank):
             tts["learned_preconditioner"] = {
                 "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
                 "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **rows,
-                "speedup_learned_vs_plain": st_p["seconds"] / rows["learned_fcg_fp64"]["seconds"],
-                "speedup_mixed_learned_vs_plain": st_p["seconds"] / rows["mixed_learned_fcg"]["seconds"]}
+                **{"speedup_%s_vs_plain" % k: st_p["seconds"] / v["seconds"] for k, v in rows.items()}}
             lp.close()
 
     cpu = None
