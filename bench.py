@@ -53,8 +53,9 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--span", type=int, default=None, help="elements per direction (default 64, Darcy 96)")
-    ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy", "plate"],
-                    help="elasticity: 3D elasticity 64^3 (the headline); darcy: 3D Darcy 96^3")
+    ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy", "plate", "batch"],
+                    help="elasticity: 3D elasticity 64^3 (the headline); darcy: 3D Darcy 96^3; plate: Kirchhoff "
+                         "plate 256^2; batch: 256 uneven quarter-annulus Poisson instances in one graph")
     return ap.parse_args()
 
 
@@ -393,6 +394,108 @@ def run_ours(args, rank, world, local_rank):
     op.close()
 
 
+def run_batch(args, rank, world, local_rank):
+    """256 uneven 2D Poisson instances (quarter annuli, p in {2,3,4}, 8-128 spans per
+    direction): one batched K.u over all instances per step, then the time to a
+    1e-8 residual of the batched PCG (one captured graph) against the instances
+    solved one after another (the reference loops over its solves)."""
+    import torch
+    import torch.distributed as dist
+
+    from jaxiga_b200 import _lib, workloads
+    from jaxiga_b200.batch import BatchSolver
+
+    torch.cuda.set_device(local_rank)
+    t0 = time.perf_counter()
+    problems, params = workloads.config3()
+    bs = BatchSolver(problems, params, tiles="auto")
+    setup_s = time.perf_counter() - t0
+    b = bs.batch
+    n = b.total
+    x = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1234 + rank))
+    y = torch.empty_like(x)
+    apply = lambda xx, yy: _lib.check(b.lib.jxb_batch_apply(b.handle, torch.cuda.current_stream().cuda_stream,  # noqa: E731
+                                                            xx.data_ptr(), yy.data_ptr()))
+    for _ in range(max(args.warmup, 3)):
+        apply(x, y)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            apply(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * n * args.steps / (ms * 1e-3)
+    # algorithmic bytes: u and y once, 6 factors per point (rational 2D scalar metric)
+    n_qp = sum(pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems)
+    alg = 8 * 2 * n + 8 * 6 * n_qp
+    peaks, peak_kind = measured_peaks()
+    achieved = alg / (ms / args.steps * 1e-3) / 1e9
+    # end to end: pinned host x -> device, batched apply, device y -> pinned host
+    xh = torch.empty(n, dtype=torch.float64).pin_memory()
+    yh = torch.empty(n, dtype=torch.float64).pin_memory()
+    xh.copy_(x.cpu())
+    k_e2e = max(10, args.steps // 5)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(k_e2e):
+        x.copy_(xh, non_blocking=True)
+        apply(x, y)
+        yh.copy_(y, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e = world * n * k_e2e / (e0.elapsed_time(e1) * 1e-3)
+    tts = None
+    if not args.no_solve:
+        bs.solve(tol=1e-8)  # captures the graph
+        xs, sts, secs = bs.solve(tol=1e-8)
+        seq_s, seq_it = 0.0, 0
+        for op, bb in zip(bs.ops, torch.split(bs.b, [op.n_dofs for op in bs.ops])):
+            _, st = op.pcg(bb.contiguous(), tol=1e-8, preconditioner="jacobi")
+            seq_s += st["seconds"]
+            seq_it += st["iterations"]
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for op, bb in zip(bs.ops, torch.split(bs.b, [op.n_dofs for op in bs.ops])):
+            op.pcg(bb.contiguous(), tol=1e-8, preconditioner="jacobi")
+        torch.cuda.synchronize()
+        seq_wall = time.perf_counter() - t1
+        tts = {"tol": 1e-8, "batched_pcg_one_graph": {"seconds": secs, "converged": int(sum(s["converged"] for s in sts)),
+                                                       "max_iterations": int(max(s["iterations"] for s in sts))},
+               "sequential_pcg_loop": {"device_seconds": seq_s, "wall_seconds": seq_wall, "iterations": seq_it},
+               "speedup_batched_vs_sequential_wall": seq_wall / secs if secs > 0 else None}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched_quarter_annuli_256", "instances": len(problems), "n_dofs": n,
+                       "elements": sum(pr.space.n_elems for pr in problems), "gauss_points": n_qp,
+                       "degrees": sorted({pr.space.degree[0] for pr in problems}), "tiles": {str(k): v for k, v in bs.tiles.items()},
+                       "operator": "batched matrix-free K.u, FP64, masked, one launch per degree group",
+                       "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * 6 * n_qp / 1e9),
+                       "parallelism": "replicas x%d" % world, "setup_seconds": setup_s},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n, "steps": k_e2e},
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                         "traffic": None, "kernel": "k_brick2_batch (batched 2D brick apply) + k_combine_batch",
+                         "algorithmic_bytes_per_launch": alg},
+            "clocks": clk.summary(), "time_to_solution": tts, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    bs.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -410,7 +513,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "batch":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
