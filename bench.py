@@ -68,7 +68,7 @@ REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_c
 
 
 class ClockSampler:
-    def __init__(self, index, period=0.05):
+    def __init__(self, index, period=0.005):
         self.samples, self.reasons, self.max_mhz = [], set(), None
         self.period = period
         self.stop_ev = threading.Event()
@@ -404,10 +404,13 @@ def run_batch(args, rank, world, local_rank):
 
     from jaxiga_b200 import _lib, workloads
     from jaxiga_b200.batch import BatchSolver
+    from jaxiga_b200.solve import geometry_operator
 
     torch.cuda.set_device(local_rank)
     t0 = time.perf_counter()
-    problems, params = workloads.config3()
+    # source sum_k c_k R_k evaluated at the Gauss points by each space's geometry plan
+    problems, params = workloads.config3(
+        interpolate=lambda V, c: geometry_operator(V).interpolate(c).cpu().numpy())
     bs = BatchSolver(problems, params, tiles="auto")
     setup_s = time.perf_counter() - t0
     b = bs.batch

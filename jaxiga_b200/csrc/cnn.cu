@@ -17,7 +17,8 @@
 // children. Activations are [channel][z][y][x], FP32.
 //
 // Convolutions (forward and data gradient) use one kernel: a CTA computes a
-// 16 x 8 x 4 voxel tile for a block of up to 16 output channels; each thread
+// 16 x 8 x 4 voxel tile for a block of up to 16 output channels (narrower on
+// small grids, so that the grid still fills the GPU); each thread
 // owns one (x, y) column of 4 voxels along z, so the three z taps reuse
 // registers and a warp reads consecutive x from shared memory. Input halos
 // and weights are staged in shared memory four input channels at a time.
@@ -136,71 +137,6 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
       if (relu) v = fmaxf(v, 0.f);
       out[idx] = beta != 0.f ? beta * out[idx] + v : v;
     }
-  }
-}
-
-// The same convolution for grids too small to fill the GPU with voxel tiles:
-// one thread per (voxel, group of COS output channels), blockIdx.y = channel
-// group; the group's weights [ci][k][COS] are staged in shared memory, each
-// input value feeds COS accumulators, and every thread sums its input
-// channels and taps in a fixed order.
-template <int K, int COS>
-__global__ void __launch_bounds__(128) k_conv_small(Dims d, int ci_n, const float* __restrict__ in,
-                                                    const float* __restrict__ w, const float* __restrict__ bias,
-                                                    const float* __restrict__ add, int relu, float beta,
-                                                    float* __restrict__ out) {
-  constexpr int R = K / 2, KK = K * K * K;
-  extern __shared__ __align__(16) float swc[];  // [ci][k][COS]
-  const int co0 = blockIdx.y * COS;
-  for (int i = threadIdx.x; i < ci_n * KK * COS; i += blockDim.x) {
-    const int o = i % COS, rest = i / COS;  // rest = ci * KK + k
-    swc[i] = w[(long long)(co0 + o) * ci_n * KK + rest];
-  }
-  __syncthreads();
-  const int vox = (int)d.vox();
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= vox) return;
-  const int nxy = d.nx * d.ny;
-  const int x = v % d.nx, y = (v / d.nx) % d.ny, z = v / nxy;
-  float acc[COS];
-#pragma unroll
-  for (int o = 0; o < COS; ++o) acc[o] = bias ? bias[co0 + o] : 0.f;
-  for (int ci = 0; ci < ci_n; ++ci) {
-    const float* ic = in + (long long)ci * vox;
-    const float4* wk = reinterpret_cast<const float4*>(swc + ci * KK * COS);
-#pragma unroll
-    for (int dz = 0; dz < K; ++dz) {
-      const int zz = z + dz - R;
-      if (zz < 0 || zz >= d.nz) continue;
-#pragma unroll
-      for (int dy = 0; dy < K; ++dy) {
-        const int yy = y + dy - R;
-        if (yy < 0 || yy >= d.ny) continue;
-#pragma unroll
-        for (int dx = 0; dx < K; ++dx) {
-          const int xx = x + dx - R;
-          if (xx < 0 || xx >= d.nx) continue;
-          const float a = __ldg(ic + zz * nxy + yy * d.nx + xx);
-          const int k = (dz * K + dy) * K + dx;
-#pragma unroll
-          for (int o4 = 0; o4 < COS / 4; ++o4) {
-            const float4 ww = wk[k * (COS / 4) + o4];
-            acc[4 * o4 + 0] = fmaf(ww.x, a, acc[4 * o4 + 0]);
-            acc[4 * o4 + 1] = fmaf(ww.y, a, acc[4 * o4 + 1]);
-            acc[4 * o4 + 2] = fmaf(ww.z, a, acc[4 * o4 + 2]);
-            acc[4 * o4 + 3] = fmaf(ww.w, a, acc[4 * o4 + 3]);
-          }
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 0; o < COS; ++o) {
-    const long long idx = (long long)(co0 + o) * vox + v;
-    float r = acc[o];
-    if (add) r += add[idx];
-    if (relu) r = fmaxf(r, 0.f);
-    out[idx] = beta != 0.f ? beta * out[idx] + r : r;
   }
 }
 
@@ -504,19 +440,11 @@ int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in
   const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
   const int relu = L.relu ? 1 : 0;
   const long long tiles = n_tiles(d);
-  const int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
-  if (tiles * (L.co / cob) < 2 * 148) {  // fewer tile CTAs than two per SM: one thread per (voxel, 4 channels)
-    const dim3 g2((unsigned)((d.vox() + 127) / 128), (unsigned)(L.co / 4));
-    const size_t sm = (size_t)L.ci * L.k * L.k * L.k * 4 * sizeof(float);
-    if (L.k == 3) {
-      if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k_conv_small<3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      k_conv_small<3, 4><<<g2, 128, sm, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
-    } else {
-      k_conv_small<1, 4><<<g2, 128, sm, s>>>(d, L.ci, in, w, b, add, relu, beta, out);
-    }
-    JXB_CUDA(cudaGetLastError());
-    return JXB_OK;
-  }
+  int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
+  // small grids: narrower output-channel blocks until there are two CTAs per SM
+  // (every output still sums its inputs in the same order, so results do not change)
+  for (const int c : {12, 8, 4})
+    if (tiles * (L.co / cob) < 2 * 148 && c < cob && L.co % c == 0) cob = c;
   const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob));
 #define JXB_CONV(KS, C)                                                                         \
   if (L.k == KS && cob == C) {                                                                  \

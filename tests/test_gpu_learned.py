@@ -56,7 +56,7 @@ def _grads(lib, h):
     ((19, 18, 17), 2, 1, (8, 16, 24, 32)),
     ((11, 9, 7), 4, 3, (12, 24)),
     ((21, 5, 3), 1, 1, (16, 32, 48)),
-    ((66, 64, 40), 2, 1, (8, 16)),  # level 0 large enough for the tiled kernel, level 1 for the small one
+    ((66, 64, 40), 2, 1, (8, 16)),  # level 0 with wide channel blocks, level 1 with narrow ones
 ])
 def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels):
     import torch
