@@ -423,13 +423,13 @@ def element_tangents(op, basis, params, vec=1):
         dim = basis["dR"].shape[2]
         C = isotropic(params["E"], params["nu"], dim, params.get("plane", "stress"))
         B = strain_displacement(basis["dR"])
-        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, C, B)
+        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, C, B, optimize=True)
     if op == "plate":
         E, nu, t = params["E"], params["nu"], params["t"]
         D = E * t**3 / (12 * (1 - nu**2)) * np.array([[1, nu, 0], [nu, 1, 0], [0, 0, (1 - nu) / 2]])
         d2R = basis["d2R"]
         B = -np.stack([d2R[:, :, 0], d2R[:, :, 2], 2.0 * d2R[:, :, 1]], axis=2)
-        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, D, B)
+        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, D, B, optimize=True)
     raise ValueError(op)
 
 
