@@ -21,7 +21,7 @@
  *   - Per-quadrature-point arrays are (n_elem, n_q^dim[, ncomp]) with elements
  *     and points both first-direction-fastest (pointset.py:104-112).
  *   - All device work is ordered on the caller's stream; no call blocks except
- *     jxb_plan_create, jxb_pcg/jxb_refine_solve (which read convergence state
+ *     jxb_plan_create, the solves (which read convergence state
  *     back to the host) and jxb_plan_destroy.
  *   - Return value 0 is success; otherwise a jxb_status code, with a message
  *     retrievable from jxb_last_error() on the calling thread.
@@ -97,9 +97,10 @@ typedef struct jxb_solve_opts {
   int64_t maxiter;              /* <= 0: 10 * n_free (jax default) */
   int preconditioner;           /* 0 none, 1 Jacobi */
   int check_every;              /* iterations per captured graph launch (<= 0: 16) */
-  /* refinement (jxb_refine_solve) */
-  double inner_tol;             /* relative tolerance of each FP32 inner solve */
-  int max_outer;                /* outer FP64 refinement steps cap */
+  /* refinement (jxb_refine_solve, jxb_mixed_pcg) */
+  double inner_tol;             /* relative tolerance of each FP32 inner solve;
+                                   jxb_mixed_pcg: residual drop between updates */
+  int max_outer;                /* cap on outer FP64 steps / updates */
 } jxb_solve_opts;
 
 typedef struct jxb_stats {
@@ -167,11 +168,20 @@ int jxb_qp_weights(jxb_plan* plan, jxb_stream stream, double* w);
  *   there on return. Stats carry the FP64 true residual (diagnostics.py:8-19).
  * jxb_refine_solve: FP64 iterative refinement around FP32 Jacobi-PCG inner solves
  *   (jxb_apply_f32); the outer residual and correction are FP64.
+ * jxb_mixed_pcg: FP32 Jacobi-PCG with reliable FP64 updates. The FP32 iterate
+ *   is folded into the FP64 solution and the residual recomputed in FP64 each
+ *   time the FP32 residual has fallen by opts->inner_tol (default 1e-2), and
+ *   at the target; the search direction is kept across updates. Stats: outer =
+ *   number of updates, iterations = FP32 iterations. Same stopping rule and
+ *   true-residual stats as jxb_pcg; the plan needs want_f32. No counterpart in
+ *   the reference (its solves are FP64 only).
  */
 int jxb_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
             const jxb_solve_opts* opts, jxb_stats* stats);
 int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                      const jxb_solve_opts* opts, jxb_stats* stats);
+int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+                  const jxb_solve_opts* opts, jxb_stats* stats);
 
 /* jxb_pcg_snapshots: jxb_pcg (Jacobi or none, jax CG semantics) that also copies
  *   the FP64 iterate into snaps[j] (n_dofs doubles each) after every `every`

@@ -188,6 +188,37 @@ __global__ void k_axpy_from_f32(long long n, double a, const float* d, double* x
   if (i < n) x[i] += a * (double)d[i];
 }
 
+// (Re)start of the FP32 iteration from an FP64 residual (reliable update):
+// r32 = s res, z32 = M r32, x32 = 0. On the first start p32 = z32; later the
+// search direction is kept and only rescaled to the new units (p32 *= ratio),
+// so the Krylov recurrence carries on instead of starting over. Partials as
+// k_cg_init: r.z, r.r and r.r again in the ||b||^2 slot (the FP32 right-hand
+// side is the scaled residual).
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_ru_restart(long long n, const double* __restrict__ res,
+                                                                const uint8_t* __restrict__ keep,
+                                                                const float* __restrict__ inv, double s, float ratio,
+                                                                int first, float* x, float* r, float* z, float* p,
+                                                                double* partials) {
+  double rz = 0, rr = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float ri = keep[i] ? (float)(res[i] * s) : 0.f;
+    const float zi = inv[i] * ri;
+    x[i] = 0.f;
+    r[i] = ri;
+    z[i] = zi;
+    p[i] = first ? zi : p[i] * ratio;
+    rz += (double)ri * (double)zi;
+    rr += (double)ri * (double)ri;
+  }
+  double s0 = block_sum_all(rz), s1 = block_sum_all(rr);
+  if (threadIdx.x == 0) {
+    partials[JXB_RED_BLOCKS + blockIdx.x] = s0;
+    partials[2 * JXB_RED_BLOCKS + blockIdx.x] = s1;
+    partials[3 * JXB_RED_BLOCKS + blockIdx.x] = s1;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host helpers
 // ---------------------------------------------------------------------------
@@ -324,6 +355,10 @@ static int get_graph(jxb_plan* plan, cudaStream_t s, int iters, int precond, cud
   return JXB_OK;
 }
 
+template <typename T>
+static int iterate(jxb_plan* plan, cudaStream_t s, long long maxiter, int precond, int check_every,
+                   long long* iters, int* status, double* snaps, long long max_snaps, long long* n_snaps);
+
 // Runs CG on the plan-owned vectors (b given as TB*), solution left in plan x.
 template <typename T, typename TB>
 static int run_cg(jxb_plan* plan, cudaStream_t s, const TB* b, double tol, double atol, long long maxiter,
@@ -339,6 +374,15 @@ static int run_cg(jxb_plan* plan, cudaStream_t s, const TB* b, double tol, doubl
   k_cg_init<T, TB><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, b, plan->d_keep, inv, precond, x, r, z, p, plan->d_red);
   k_cg_init_fin<<<1, JXB_RED_THREADS, 0, s>>>(plan->d_state, plan->d_red, tol, atol, maxiter);
   JXB_CUDA(cudaGetLastError());
+  return iterate<T>(plan, s, maxiter, precond, check_every, iters, status, snaps, max_snaps, n_snaps);
+}
+
+// Launches the captured iteration graph until the device state reports done
+// (the state and the vectors were set up by the caller).
+template <typename T>
+static int iterate(jxb_plan* plan, cudaStream_t s, long long maxiter, int precond, int check_every,
+                   long long* iters, int* status, double* snaps, long long max_snaps, long long* n_snaps) {
+  const double* x = plan->d_x;
   cudaGraphExec_t ge;
   int rc = get_graph<T>(plan, s, check_every, precond, &ge);
   if (rc) return rc;
@@ -504,6 +548,100 @@ extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double*
     stats->seconds = ms * 1e-3;
   }
   if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_refine_solve: non-finite value in inner CG");
+  return JXB_OK;
+}
+
+// FP32 Jacobi-PCG with reliable updates (Sleijpen and van der Vorst, 1996):
+// the iteration runs in FP32 on the residual scaled to unit norm. Each time
+// the FP32 recursive residual has fallen by delta (opts->inner_tol) since the
+// last update, or below tol ||b||, the FP32 iterate is added to the FP64
+// solution, the residual is recomputed in FP64, and the FP32 iteration goes
+// on from it with the same search direction. Unlike restarted refinement the
+// Krylov recurrence is never thrown away, so the iteration count stays close
+// to that of FP64 CG while every K p but one per update is an FP32 apply.
+extern "C" int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
+                             const jxb_solve_opts* opts, jxb_stats* stats) {
+  if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: null argument");
+  if (!plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: plan was created without want_f32");
+  if (!(opts->tol > 0) || !isfinite(opts->tol))
+    return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: tol must be finite and positive");
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+  if (!plan->graph_stream[0]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[0], cudaStreamNonBlocking));
+  cudaStream_t s = plan->graph_stream[0];
+  cudaEvent_t e0, e1, evu;
+  JXB_CUDA(cudaEventCreate(&e0));
+  JXB_CUDA(cudaEventCreate(&e1));
+  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
+  JXB_CUDA(cudaEventRecord(evu, user));
+  JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
+  int rc = ensure_workspace(plan, true);
+  if (rc) return rc;
+  rc = compute_invdiag(plan, s);
+  if (rc) return rc;
+  long long n = plan->n_dofs;
+  double* xb = plan->d_z;   // FP64 solution
+  double* res = plan->d_r;  // FP64 residual at the last update
+  JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaMemsetAsync(xb, 0, n * sizeof(double), s));
+  JXB_CUDA(cudaEventRecord(e0, s));
+  const double delta = opts->inner_tol > 0 ? opts->inner_tol : 1e-2;
+  const int max_updates = opts->max_outer > 0 ? opts->max_outer : 1000;
+  const long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
+  const int every = opts->check_every > 0 ? opts->check_every : 16;
+  long long total_it = 0;
+  int updates = 0, status = JXB_OK;
+  double rn = 0, bn = 0;
+  bool fin = true;
+  rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+  if (rc) return rc;
+  double rn_seg = rn;  // residual norm the FP32 vectors are scaled by
+  while (updates < max_updates && fin && rn > opts->tol * bn && total_it < maxiter) {
+    const float ratio = updates == 0 ? 1.f : (float)(rn_seg / rn);
+    k_ru_restart<<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, res, plan->d_keep, plan->d_invdiag32, 1.0 / rn,
+                                                            ratio, updates == 0, plan->d_x32, plan->d_r32,
+                                                            plan->d_z32, plan->d_p32, plan->d_red);
+    rn_seg = rn;
+    // the FP32 segment stops at the update threshold or at the target, whichever comes first
+    const double seg_tol = fmax(delta, opts->tol * bn / rn);
+    k_cg_init_fin<<<1, JXB_RED_THREADS, 0, s>>>(plan->d_state, plan->d_red, seg_tol, 0.0, maxiter - total_it);
+    JXB_CUDA(cudaGetLastError());
+    long long it = 0;
+    int st = 0;
+    rc = iterate<float>(plan, s, maxiter - total_it, 1, every, &it, &st, nullptr, 0, nullptr);
+    if (rc) return rc;
+    total_it += it;
+    k_axpy_from_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rn_seg, plan->d_x32, xb);
+    JXB_CUDA(cudaGetLastError());
+    rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+    if (rc) return rc;
+    ++updates;
+    if (st == JXB_ERR_NONFINITE) {
+      status = JXB_ERR_NONFINITE;
+      break;
+    }
+    if (!(rn < rn_seg)) break;  // no progress in FP32: stop, the stats report it
+  }
+  JXB_CUDA(cudaEventRecord(e1, s));
+  JXB_CUDA(cudaMemcpyAsync(x, xb, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaEventRecord(evu, s));
+  JXB_CUDA(cudaStreamWaitEvent(user, evu, 0));
+  JXB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(evu);
+  if (stats) {
+    stats->iterations = total_it;
+    stats->outer = updates;
+    stats->residual = rn;
+    stats->b_norm = bn;
+    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
+    stats->finite = fin ? 1 : 0;
+    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
+    stats->seconds = ms * 1e-3;
+  }
+  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_mixed_pcg: non-finite value in FP32 CG");
   return JXB_OK;
 }
 

@@ -253,3 +253,18 @@ class Operator:
         if rc not in (0, 4):
             _lib.check(rc)
         return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+
+    def mixed_pcg(self, b, tol=1e-8, delta=1e-2, maxiter=None, max_updates=1000, check_every=16):
+        """FP32 Jacobi-PCG with reliable FP64 updates every ``delta`` of residual decrease."""
+        if not self.want_f32:
+            raise ValueError("create the Operator with want_f32=True for mixed precision")
+        if not (0 < delta < 1):
+            raise ValueError("delta must lie in (0, 1)")
+        b = self._vec(b)
+        x = self._empty(self.n_dofs)
+        st = _lib.Stats()
+        o = self._opts(tol, 0.0, maxiter, "jacobi", check_every, delta, max_updates)
+        rc = self.lib.jxb_mixed_pcg(self.handle, _stream(), _dptr(b), _dptr(x), ctypes.byref(o), ctypes.byref(st))
+        if rc not in (0, 4):
+            _lib.check(rc)
+        return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}

@@ -32,9 +32,12 @@ class LinearOptions:
     """Linear-solver configuration (solvers/linear.py:76-127) plus the device fields.
 
     ``backend="b200"`` (the only backend here) runs matrix-free CG on the GPU;
-    ``precision`` is ``"fp64"`` (plain) or ``"mixed"`` (FP32 inner solves inside
-    FP64 iterative refinement to ``tol``); ``inner_tol`` is the relative
-    tolerance of each inner solve; ``check_every`` the iterations per captured
+    ``precision`` is ``"fp64"`` (plain) or ``"mixed"`` (FP32 iterations with
+    FP64 corrections to ``tol``). ``refinement`` picks the mixed scheme:
+    ``"reliable"`` (FP32 PCG whose iterate and residual are refreshed in FP64
+    each time the residual has fallen by ``update_delta``, keeping the search
+    direction) or ``"restart"`` (FP64 iterative refinement around FP32 inner
+    solves to ``inner_tol``). ``check_every`` is the iterations per captured
     CUDA graph launch between host convergence checks.
     """
 
@@ -48,6 +51,8 @@ class LinearOptions:
     precision: str = "fp64"
     inner_tol: float = 1e-4
     check_every: int = 16
+    refinement: str = "reliable"
+    update_delta: float = 1e-2
 
     def __post_init__(self):
         if not np.isfinite(self.tol) or self.tol <= 0:
@@ -72,6 +77,10 @@ class LinearOptions:
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {self.precision!r}")
         if not (0 < self.inner_tol < 1):
             raise ValueError("inner_tol must lie in (0, 1)")
+        if self.refinement not in {"reliable", "restart"}:
+            raise ValueError(f"refinement must be 'reliable' or 'restart', got {self.refinement!r}")
+        if not (0 < self.update_delta < 1):
+            raise ValueError("update_delta must lie in (0, 1)")
 
 
 def default_linear(problem) -> LinearOptions:
@@ -162,7 +171,10 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         g[prescribed] = values
         if np.any(values != 0):
             b = F - op.apply(g, masked=False)
-        if linear.precision == "mixed":
+        if linear.precision == "mixed" and linear.refinement == "reliable":
+            xdev, st = op.mixed_pcg(b, tol=linear.tol, delta=linear.update_delta, maxiter=linear.maxiter,
+                                    check_every=linear.check_every)
+        elif linear.precision == "mixed":
             xdev, st = op.refine_solve(b, tol=linear.tol, inner_tol=linear.inner_tol, maxiter=linear.maxiter,
                                        check_every=linear.check_every)
         else:
@@ -187,6 +199,7 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         "outer": int(st["outer"]),
         "seconds": st["seconds"],
         "precision": linear.precision,
+        "refinement": linear.refinement if linear.precision == "mixed" else None,
     }
     if not stats["converged"]:
         warnings.warn(f"linear Galerkin solve did not converge (residual {stats['residual']:.3e}); "

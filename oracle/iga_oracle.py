@@ -603,6 +603,63 @@ def jax_cg(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0):
     return x, k
 
 
+def reliable_cg(matvec, matvec32, b, tol, delta=1e-2, inv_diag=None, maxiter=None):
+    """FP32 Jacobi-PCG with reliable FP64 updates, as the device solver runs it.
+
+    Not part of the reference (its solves are FP64 only): this restates the
+    reliable-update scheme of Sleijpen and van der Vorst (1996), in the form the
+    CUDA path ``jxb_mixed_pcg`` uses, so that its convergence can be checked.
+    The FP32 iteration runs on the residual scaled to unit norm. A segment ends
+    when the FP32 recursive residual has fallen by ``delta`` or below
+    ``tol ||b||``; then x += ||r_seg|| x32, the residual is recomputed in FP64
+    (``matvec``), and the FP32 iteration resumes from it with the search
+    direction kept (rescaled to the new units). Dot products are FP64 sums of
+    FP32 products; alpha and beta are rounded to FP32 as on the device.
+    Returns (x, FP32 iterations, updates).
+    """
+    b = np.asarray(b, dtype=float)
+    if maxiter is None:
+        maxiter = 10 * b.size
+    f32 = np.float32
+    inv32 = (np.ones_like(b) if inv_diag is None else np.asarray(inv_diag)).astype(f32)
+
+    def dot(u, v):
+        return float(np.dot(u.astype(float), v.astype(float)))
+
+    x = np.zeros_like(b)
+    res = b.copy()
+    bn = float(np.linalg.norm(b))
+    rn = bn
+    k = updates = 0
+    p = None
+    rn_seg = rn
+    while rn > tol * bn and k < maxiter:
+        r = (res * (1.0 / rn)).astype(f32)
+        z = inv32 * r
+        p = z.copy() if p is None else p * f32(rn_seg / rn)
+        rn_seg = rn
+        gamma, rr = dot(r, z), dot(r, r)
+        seg2 = max(delta, tol * bn / rn) ** 2 * rr
+        xs = np.zeros_like(r)
+        while rr > seg2 and k < maxiter:
+            Ap = np.asarray(matvec32(p), dtype=f32)
+            alpha = f32(gamma / dot(p, Ap))
+            xs += alpha * p
+            r -= alpha * Ap
+            z = inv32 * r
+            gnew, rr = dot(r, z), dot(r, r)
+            p = z + f32(gnew / gamma) * p
+            gamma = gnew
+            k += 1
+        x = x + rn_seg * xs.astype(float)
+        res = b - matvec(x)
+        rn = float(np.linalg.norm(res))
+        updates += 1
+        if not rn < rn_seg:
+            break
+    return x, k, updates
+
+
 def jacobi_inverse(diagonal):
     """solvers/linear.py:427-431: 1/d where |d| > 0, else 1."""
     diagonal = np.asarray(diagonal)

@@ -132,6 +132,11 @@ def test_linear_options_validation():
     with pytest.raises(ValueError, match="precision"):
         jx.LinearOptions(precision="fp16")
     assert jx.LinearOptions(precision="mixed").precision == "mixed"
+    assert jx.LinearOptions(precision="mixed").refinement == "reliable"
+    with pytest.raises(ValueError, match="refinement"):
+        jx.LinearOptions(precision="mixed", refinement="defect")
+    with pytest.raises(ValueError, match="update_delta"):
+        jx.LinearOptions(precision="mixed", update_delta=1.0)
 
 
 def header_symbols():
