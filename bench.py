@@ -367,8 +367,8 @@ def run_ours(args, rank, world, local_rank):
             rows = {}
             for key, mixed, two in (("learned_fcg_fp64", False, False), ("mixed_learned_fcg", True, False),
                                     ("learned_two_level_fp64", False, True), ("mixed_learned_two_level", True, True)):
-                lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4, two_level=two)  # first call captures the graphs
-                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, inner_tol=1e-4, two_level=two)
+                lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)  # first call captures the graphs
+                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)
                 rows[key] = {"seconds": st_l["seconds"], "iterations": st_l["iterations"],
                              "learned_iterations": st_l["learned_iterations"],
                              "relative_residual": st_l["relative_residual"], "converged": bool(st_l["converged"]),

@@ -232,8 +232,11 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
  *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
  *   Jacobi directions take over after `stall` learned iterations without a new
- *   lowest residual or a non-descent direction. `mode` bit 0: FP32 inner solves
- *   (inner_tol) inside FP64 iterative refinement (plan created with want_f32);
+ *   lowest residual or a non-descent direction. `mode` bit 0: FP32 iterations
+ *   with FP64 corrections (plan created with want_f32): reliable updates each
+ *   time the residual has fallen by inner_tol (default 1e-2), the stored
+ *   directions kept, as jxb_mixed_pcg; with bit 2 also set, restarted FP32
+ *   solves to inner_tol inside FP64 iterative refinement instead;
  *   bit 1: two-level preconditioner z = a n + D^-1 (r - a K n), n the network
  *   output, a = (n.r)/(n^T K n) (one more operator apply per iteration).
  *   stats->outer = iterations that used the network. */

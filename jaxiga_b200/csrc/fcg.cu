@@ -269,6 +269,62 @@ __global__ void k_frestart(FcgState* st) {
   if (st->cg.status == JXB_OK && st->cg.k < st->cg.maxiter && st->cg.rr > st->cg.atol2) st->cg.done = 0;
 }
 
+// Reliable update of the FP32 recurrence (mixed mode): r32 = s res (the FP64
+// residual scaled to unit norm), x32 = 0, and the stored directions and their
+// products rescaled to the new units (P, AP *= ratio; p.Ap *= ratio^2 in the
+// finish kernel), so the A-orthogonalisation carries on across the update.
+__global__ void __launch_bounds__(JXB_RED_THREADS) k_fru_restart(long long n, int m, const double* __restrict__ res,
+                                                                 const uint8_t* __restrict__ keep, double s,
+                                                                 float ratio, int first, float* __restrict__ x,
+                                                                 float* __restrict__ r, float* __restrict__ Pr,
+                                                                 float* __restrict__ APr, double* __restrict__ part) {
+  double acc = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float ri = keep[i] ? (float)(res[i] * s) : 0.f;
+    x[i] = 0.f;
+    r[i] = ri;
+    acc += (double)ri * (double)ri;
+    if (!first)
+      for (int j = 0; j < m; ++j) {
+        Pr[(long long)j * n + i] *= ratio;
+        APr[(long long)j * n + i] *= ratio;
+      }
+  }
+  const double t = block_sum_all(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_fru_fin(FcgState* st, const double* __restrict__ part, double tol, long long maxiter, int m,
+                          int first, double ratio) {
+  const double rr = reduce_partials(part);
+  if (threadIdx.x != 0) return;
+  st->cg.rr = rr;
+  st->cg.bb = rr;
+  st->cg.gamma = 0;
+  st->cg.alpha = st->cg.beta = 0;
+  st->cg.atol2 = tol * tol * rr;
+  st->cg.k = 0;
+  st->cg.maxiter = maxiter;
+  st->cg.status = JXB_OK;
+  st->cg.done = 0;
+  st->bad = 0;
+  if (first) {
+    st->nd = 0;
+    st->m = m;
+  } else {
+    for (int j = 0; j < FCG_MMAX; ++j) st->pAp[j] *= ratio * ratio;
+  }
+  if (!isfinite(rr)) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NONFINITE;
+  } else if (!(rr > st->cg.atol2)) {
+    st->cg.done = 1;
+  } else if (maxiter <= 0) {
+    st->cg.done = 1;
+    st->cg.status = JXB_ERR_NOT_CONVERGED;
+  }
+}
+
 template <typename T>
 __global__ void k_ediff(long long ncp, int vec, const float* __restrict__ e, const float* __restrict__ out,
                         float out_scale, const uint8_t* __restrict__ keep, T* __restrict__ d) {
@@ -475,6 +531,9 @@ int fcg_setup(FcgRun& R, cudaStream_t s) {
   return JXB_OK;
 }
 
+template <typename T>
+int fcg_loop(FcgRun& R, GraphPair& G, cudaStream_t s, long long maxiter, long long* iters, int* status);
+
 // Runs FCG on rhs b (type TB) into the plan's T-typed x. Returns the status
 // (JXB_OK, NOT_CONVERGED, NONFINITE) in *status and the iteration count.
 template <typename T, typename TB>
@@ -488,6 +547,13 @@ int fcg_run(FcgRun& R, GraphPair& G, cudaStream_t s, const TB* b, double tol, do
   k_finit<T, TB><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, b, plan->d_keep, x, r, R.part);
   k_finit_fin<<<1, JXB_RED_THREADS, 0, s>>>(R.d_st, R.part, tol, atol, maxiter, R.m);
   JXB_CUDA(cudaGetLastError());
+  return fcg_loop<T>(R, G, s, maxiter, iters, status);
+}
+
+// Launches the iteration graphs until the device state reports done (state and
+// vectors set up by the caller); learned directions first, Jacobi after a fallback.
+template <typename T>
+int fcg_loop(FcgRun& R, GraphPair& G, cudaStream_t s, long long maxiter, long long* iters, int* status) {
   bool learned = R.cnn != nullptr;
   if (learned && !G.learned) {
     int rc = capture<T>(R, s, true, 1, &G.learned);
@@ -594,6 +660,47 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
     JXB_CUDA(cudaMemcpyAsync(x, plan->d_x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin);
     if (rc) return rc;
+  } else if (!(mode & 4)) {
+    // FP32 FCG with reliable FP64 updates: each time the FP32 residual has
+    // fallen by inner_tol (default 1e-2) or below the target, the FP32 iterate
+    // is added to the FP64 solution and the residual recomputed in FP64; the
+    // stored directions are kept (rescaled), so the recurrence goes on.
+    double* xb = plan->d_z;
+    double* res = plan->d_r;
+    JXB_CUDA(cudaMemsetAsync(xb, 0, n * sizeof(double), s));
+    const double delta = opts->inner_tol > 0 ? opts->inner_tol : 1e-2;
+    const int max_updates = opts->max_outer > 0 ? opts->max_outer : 1000;
+    rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+    if (rc) return rc;
+    double rn_seg = rn;
+    while (outer < max_updates && fin && rn > opts->tol * bn && total < maxiter) {
+      const int first = outer == 0;
+      const double ratio = first ? 1.0 : rn_seg / rn;
+      k_fru_restart<<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.m, res, plan->d_keep, 1.0 / rn, (float)ratio, first,
+                                                               plan->d_x32, plan->d_r32, (float*)R.Pr, (float*)R.APr,
+                                                               R.part);
+      k_fru_fin<<<1, JXB_RED_THREADS, 0, s>>>(R.d_st, R.part, fmax(delta, opts->tol * bn / rn), maxiter - total, R.m,
+                                              first, ratio);
+      JXB_CUDA(cudaGetLastError());
+      rn_seg = rn;
+      long long it = 0;
+      int st = 0;
+      rc = fcg_loop<float>(R, G, s, maxiter - total, &it, &st);
+      if (rc) return rc;
+      total += it;
+      k_axpy_f32<<<nb256(n), 256, 0, s>>>(n, rn_seg, plan->d_x32, xb);
+      JXB_CUDA(cudaGetLastError());
+      rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
+      if (rc) return rc;
+      ++outer;
+      if (st == JXB_ERR_NONFINITE) {
+        status = JXB_ERR_NONFINITE;
+        break;
+      }
+      if (!(rn < rn_seg)) break;  // no progress: stop, the stats report it
+    }
+    JXB_CUDA(cudaEventRecord(e1, s));
+    JXB_CUDA(cudaMemcpyAsync(x, xb, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   } else {
     // FP64 iterative refinement: the FP64 residual, normalised, is the rhs of
     // an FP32 FCG solve to inner_tol; the correction is added in FP64.

@@ -245,16 +245,25 @@ class LearnedPreconditioner:
         return (z * torch.as_tensor(~self.op.prescribed_mask, device=self.dev)).contiguous()
 
     # -- solve -------------------------------------------------------------------
-    def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=1e-4, check_every=16,
-              use_network=True, two_level=False):
+    def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=None, check_every=16,
+              use_network=True, two_level=False, refinement="reliable"):
         """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats).
 
-        ``mixed``: FP32 inner solves to ``inner_tol`` inside FP64 refinement.
+        ``mixed``: the flexible CG runs in FP32 with FP64 corrections. With
+        ``refinement="reliable"`` the FP32 iterate is folded into the FP64
+        solution and the residual recomputed in FP64 each time the residual has
+        fallen by ``inner_tol`` (default 1e-2), keeping the stored directions;
+        with ``"restart"`` each FP32 solve to ``inner_tol`` (default 1e-4) starts
+        afresh inside FP64 iterative refinement.
         ``two_level``: the network output n as a coarse correction with its own
         line search, then one Jacobi step: z = a n + D^-1 (r - a K n).
         ``use_network=False`` runs the same FCG with Jacobi only (the baseline
         the network is measured against).
         """
+        if refinement not in ("reliable", "restart"):
+            raise ValueError(f"refinement must be 'reliable' or 'restart', got {refinement!r}")
+        if inner_tol is None:
+            inner_tol = 1e-2 if refinement == "reliable" else 1e-4
         op = self.op
         b = op._vec(b)
         x = op._empty(op.n_dofs)
@@ -264,7 +273,8 @@ class LearnedPreconditioner:
         rc = self.lib.jxb_fcg_learned(op.handle, self.handle if use_network else None, _s(), _p(b), _p(x),
                                       _p(feats) if feats is not None else None, self.n_feat,
                                       float(self.in_scale), float(self.out_scale), int(stall), int(depth),
-                                      (1 if mixed else 0) | (2 if two_level else 0), ctypes.byref(o), ctypes.byref(st))
+                                      (1 if mixed else 0) | (2 if two_level else 0)
+                                      | (4 if refinement == "restart" else 0), ctypes.byref(o), ctypes.byref(st))
         if rc not in (0, 4):
             _lib.check(rc)
         out = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}

@@ -120,12 +120,12 @@ def main():
     solves["plain_fp64_jacobi_pcg"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth)
     solves["learned_fcg_fp64"] = st
-    x_m, st = lp.solve(F, tol=1e-8, depth=args.depth, mixed=True, inner_tol=1e-4)
+    x_m, st = lp.solve(F, tol=1e-8, depth=args.depth, mixed=True)
     st["relative_difference_to_plain"] = float(torch.linalg.norm(x_m - x_ref) / torch.linalg.norm(x_ref))
     solves["learned_fcg_mixed"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True)
     solves["learned_fcg_two_level"] = st
-    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True, mixed=True, inner_tol=1e-4)
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True, mixed=True)
     solves["learned_fcg_two_level_mixed"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth, use_network=False)
     solves["fcg_jacobi_only"] = st

@@ -216,10 +216,20 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     x_t, st_t = lp.solve(b, tol=1e-8, two_level=True)
     assert st_t["converged"] and st_t["iterations"] < st_ref["iterations"], (st_t, st_ref)
     assert float(torch.linalg.norm(x_t - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
-    # mixed precision: FP32 inner flexible CG inside FP64 refinement
-    x_m, st_m = lp.solve(b, tol=1e-8, mixed=True, inner_tol=1e-4)
+    # mixed precision: FP32 flexible CG with reliable FP64 updates (the stored
+    # directions kept), and restarted FP32 solves inside FP64 refinement
+    x_m, st_m = lp.solve(b, tol=1e-8, mixed=True)
     assert st_m["converged"], st_m
     assert float(torch.linalg.norm(x_m - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
+    x_r, st_r = lp.solve(b, tol=1e-8, mixed=True, refinement="restart")
+    assert st_r["converged"], st_r
+    assert float(torch.linalg.norm(x_r - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
+    # keeping the directions costs fewer iterations than restarting (Jacobi FCG)
+    _, st_jm = lp.solve(b, tol=1e-8, mixed=True, use_network=False)
+    _, st_jr = lp.solve(b, tol=1e-8, mixed=True, use_network=False, refinement="restart")
+    assert st_jm["converged"] and st_jr["converged"]
+    assert st_jm["iterations"] <= 1.15 * st_j["iterations"] + 10, (st_jm, st_j)
+    assert st_jm["iterations"] < st_jr["iterations"], (st_jm, st_jr)
     # checkpoint / resume reproduces the preconditioner
     path = tmp_path / "pc.npz"
     lp.save(path)
