@@ -366,7 +366,9 @@ def run_ours(args, rank, world, local_rank):
             lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
             rows = {}
             for key, mixed, two in (("learned_fcg_fp64", False, False), ("mixed_learned_fcg", True, False),
-                                    ("learned_two_level_fp64", False, True), ("mixed_learned_two_level", True, True)):
+                                    ("learned_two_level_fp64", False, True), ("mixed_learned_two_level", True, True),
+                                    ("learned_additive_fp64", False, "additive"),
+                                    ("mixed_learned_additive", True, "additive")):
                 lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)  # first call captures the graphs
                 x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)
                 rows[key] = {"seconds": st_l["seconds"], "iterations": st_l["iterations"],
@@ -375,6 +377,7 @@ def run_ours(args, rank, world, local_rank):
                              "relative_difference_to_plain": float(torch.linalg.norm(x_l - sol_p) / torch.linalg.norm(sol_p))}
             tts["learned_preconditioner"] = {
                 "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
+                "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
                 "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **rows,
                 **{"speedup_%s_vs_plain" % k: st_p["seconds"] / v["seconds"] for k, v in rows.items()}}
             lp.close()

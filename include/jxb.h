@@ -229,20 +229,28 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  *     flexible CG does not use). e and r are grids [vec][nz][ny][nx]; adds the
  *     parameter gradient and returns the loss.
  *   jxb_cnn_adam: one Adam step with the accumulated gradient times grad_scale.
+ *   jxb_cnn_set_input_pooling: on = 1 pools the input once (2x2x2 average) and
+ *     runs the U-Net on the half-resolution grid, upsampling its output back
+ *     (copying each coarse voxel to its children); forward, backward and the
+ *     losses keep their input-grid shapes. Drops the activation buffers.
  * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
  *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
  *   Jacobi directions take over after `stall` learned iterations without a new
  *   lowest residual or a non-descent direction. `mode` bit 0: FP32 iterations
  *   with FP64 corrections (plan created with want_f32): reliable updates each
  *   time the residual has fallen by inner_tol (default 1e-2), the stored
- *   directions kept, as jxb_mixed_pcg; with bit 2 also set, restarted FP32
- *   solves to inner_tol inside FP64 iterative refinement instead;
+ *   directions kept, as jxb_mixed_pcg, and a fallback to Jacobi lasts for the
+ *   rest of the solve; with bit 2 also set, restarted FP32 solves to inner_tol
+ *   inside FP64 iterative refinement instead;
  *   bit 1: two-level preconditioner z = a n + D^-1 (r - a K n), n the network
- *   output, a = (n.r)/(n^T K n) (one more operator apply per iteration).
+ *   output, a = (n.r)/(n^T K n) (one more operator apply per iteration);
+ *   bit 3 (without bit 1): additive two-level z = n + D^-1 r, the weight of n
+ *   fixed through out_scale (no extra apply).
  *   stats->outer = iterations that used the network. */
 typedef struct jxb_cnn jxb_cnn;
 int jxb_cnn_create(int in_ch, int out_ch, int levels, const int* channels, uint64_t seed, jxb_cnn** out);
 int jxb_cnn_destroy(jxb_cnn* cnn);
+int jxb_cnn_set_input_pooling(jxb_cnn* cnn, int on);
 int jxb_cnn_params(jxb_cnn* cnn, float** params, int64_t* n);
 int jxb_cnn_grads(jxb_cnn* cnn, float** grads, int64_t* n);
 int jxb_cnn_forward(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in, float* out);

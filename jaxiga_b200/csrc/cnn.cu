@@ -16,6 +16,11 @@
 // eight) children of a coarse voxel; upsampling copies a coarse voxel to its
 // children. Activations are [channel][z][y][x], FP32.
 //
+// With input pooling (jxb_cnn_set_input_pooling) the input is pooled once and
+// the U-Net runs on the half-resolution grid; its output is upsampled back.
+// The network then acts on the smooth part of the residual only, at about an
+// eighth of the finest level's cost.
+//
 // Convolutions (forward and data gradient) use one kernel: a CTA computes a
 // 16 x 8 x 4 voxel tile for a block of up to 16 output channels (narrower on
 // small grids, so that the grid still fills the GPU); each thread
@@ -416,6 +421,11 @@ struct jxb_cnn {
   float* arena = nullptr;
   float *A[MAXL] = {}, *S[MAXL] = {}, *P[MAXL] = {}, *U[MAXL] = {}, *M[MAXL] = {}, *D[MAXL] = {}, *GS[MAXL] = {};
   float *B0 = nullptr, *B1 = nullptr, *B2 = nullptr, *OUT = nullptr, *G0 = nullptr, *G1 = nullptr;
+  int pool_in = 0;         // run on the pooled input (half resolution), upsample the output
+  Dims cap_f{0, 0, 0};     // fine grid of the input-pooling buffers
+  float* fine_arena = nullptr;
+  float *INC = nullptr, *OUTF = nullptr, *GOF = nullptr;  // pooled input, fine output, fine output gradient
+  Dims last{0, 0, 0};      // input grid of the last forward pass
   float* wt = nullptr;     // transposed weights scratch
   float* part = nullptr;   // weight-gradient partials
   long long part_cap = 0;
@@ -634,6 +644,53 @@ int backward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   return JXB_OK;
 }
 
+// The public forward/backward: the U-Net on the input grid, or on the pooled
+// input with the output upsampled (input pooling).
+int ensure_fine(jxb_cnn* N, Dims df) {
+  if (df.nx == N->cap_f.nx && df.ny == N->cap_f.ny && df.nz == N->cap_f.nz) return JXB_OK;
+  cudaFree(N->fine_arena);
+  N->fine_arena = nullptr;
+  N->cap_f = {0, 0, 0};
+  if ((long long)64 * df.vox() >= (1ll << 31)) return fail(JXB_ERR_INVALID, "cnn: grid too large (activation indices are 32-bit)");
+  const long long a = ((long long)N->in_ch * half(df).vox() + 63) / 64 * 64, b = (4 * df.vox() + 63) / 64 * 64;
+  JXB_CUDA(cudaMalloc(&N->fine_arena, (a + 2 * b) * sizeof(float)));
+  N->INC = N->fine_arena;
+  N->OUTF = N->INC + a;
+  N->GOF = N->OUTF + b;
+  N->cap_f = df;
+  return JXB_OK;
+}
+
+float* out_buf(jxb_cnn* N) { return N->pool_in ? N->OUTF : N->OUT; }
+float* gout_buf(jxb_cnn* N) { return N->pool_in ? N->GOF : N->G0; }
+
+int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
+  N->last = {0, 0, 0};
+  if (!N->pool_in) {
+    int rc = forward(N, s, d, in);
+    if (!rc) N->last = d;
+    return rc;
+  }
+  int rc = ensure_fine(N, d);
+  if (rc) return rc;
+  const Dims dc = half(d);
+  k_pool<<<nblk(dc.vox() * N->in_ch), 256, 0, s>>>(d, dc, N->in_ch, in, N->INC);
+  if ((rc = forward(N, s, dc, N->INC))) return rc;
+  k_up<<<nblk(d.vox() * 4), 256, 0, s>>>(d, dc, 4, N->OUT, N->OUTF);
+  JXB_CUDA(cudaGetLastError());
+  N->last = d;
+  return JXB_OK;
+}
+
+// backward for the output gradient in gout_buf(N); needs forward_top on the same input
+int backward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
+  if (!N->pool_in) return backward(N, s, d, in);
+  const Dims dc = half(d);
+  k_up_bwd<<<nblk(dc.vox() * 4), 256, 0, s>>>(d, dc, 4, N->GOF, N->G0);
+  JXB_CUDA(cudaGetLastError());
+  return backward(N, s, dc, N->INC);
+}
+
 bool supported_co(int c) { return c == 4 || c == 8 || c == 12 || c == 16 || c == 24 || c == 32 || c == 48 || c == 64; }
 
 }  // namespace
@@ -641,16 +698,16 @@ bool supported_co(int c) { return c == 4 || c == 8 || c == 12 || c == 16 || c ==
 namespace jxb {
 
 int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4) {
-  int rc = forward(N, s, Dims{nx, ny, nz}, in);
+  int rc = forward_top(N, s, Dims{nx, ny, nz}, in);
   if (rc) return rc;
-  if (out4) *out4 = N->OUT;
+  if (out4) *out4 = out_buf(N);
   return JXB_OK;
 }
 
-float* cnn_grad_out(jxb_cnn* N) { return N->G0; }
+float* cnn_grad_out(jxb_cnn* N) { return gout_buf(N); }
 
 int cnn_backward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in) {
-  return backward(N, s, Dims{nx, ny, nz}, in);
+  return backward_top(N, s, Dims{nx, ny, nz}, in);
 }
 
 int cnn_out_channels(const jxb_cnn* N) { return N->out_ch; }
@@ -755,7 +812,21 @@ extern "C" int jxb_cnn_destroy(jxb_cnn* N) {
   cudaFree(N->part);
   cudaFree(N->red);
   cudaFree(N->arena);
+  cudaFree(N->fine_arena);
   delete N;
+  return JXB_OK;
+}
+
+extern "C" int jxb_cnn_set_input_pooling(jxb_cnn* N, int on) {
+  if (!N || (on != 0 && on != 1)) return fail(JXB_ERR_INVALID, "jxb_cnn_set_input_pooling: bad argument");
+  if (N->pool_in != on) {
+    JXB_CUDA(cudaDeviceSynchronize());
+    cudaFree(N->arena);
+    N->arena = nullptr;
+    N->cap = {0, 0, 0};
+    N->last = {0, 0, 0};
+    N->pool_in = on;
+  }
   return JXB_OK;
 }
 
@@ -777,23 +848,24 @@ extern "C" int jxb_cnn_forward(jxb_cnn* N, jxb_stream stream, int nx, int ny, in
   if (!N || !in || !out || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_forward: bad argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
-  int rc = forward(N, s, d, in);
+  int rc = forward_top(N, s, d, in);
   if (rc) return rc;
-  JXB_CUDA(cudaMemcpyAsync(out, N->OUT, (size_t)N->out_ch * d.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaMemcpyAsync(out, out_buf(N), (size_t)N->out_ch * d.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
   return JXB_OK;
 }
 
 extern "C" int jxb_cnn_backward(jxb_cnn* N, jxb_stream stream, int nx, int ny, int nz, const float* in,
                                 const float* gout) {
   if (!N || !in || !gout || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_backward: bad argument");
-  if (N->cap.nx != nx || N->cap.ny != ny || N->cap.nz != nz)
+  if (N->last.nx != nx || N->last.ny != ny || N->last.nz != nz)
     return fail(JXB_ERR_INVALID, "jxb_cnn_backward: no forward pass on these dimensions precedes it");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
   const size_t vb = (size_t)d.vox() * sizeof(float);
-  JXB_CUDA(cudaMemcpyAsync(N->G0, gout, N->out_ch * vb, cudaMemcpyDeviceToDevice, s));
-  JXB_CUDA(cudaMemsetAsync(N->G0 + (size_t)N->out_ch * d.vox(), 0, (4 - N->out_ch) * vb, s));
-  return backward(N, s, d, in);
+  float* g0 = gout_buf(N);
+  JXB_CUDA(cudaMemcpyAsync(g0, gout, N->out_ch * vb, cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaMemsetAsync(g0 + (size_t)N->out_ch * d.vox(), 0, (4 - N->out_ch) * vb, s));
+  return backward_top(N, s, d, in);
 }
 
 extern "C" int jxb_cnn_zero_grad(jxb_cnn* N, jxb_stream stream) {
@@ -807,11 +879,12 @@ extern "C" int jxb_cnn_accumulate(jxb_cnn* N, jxb_stream stream, int nx, int ny,
   if (!N || !in || !target) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate: null argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
-  int rc = forward(N, s, d, in);
+  int rc = forward_top(N, s, d, in);
   if (rc) return rc;
+  float* g0 = gout_buf(N);
   // loss on the first out_ch channels of the (4-channel padded) output
-  k_mse<<<JXB_RED_BLOCKS, 256, 0, s>>>(d.vox(), N->out_ch, N->OUT, target, mask, N->G0, N->red);
-  JXB_CUDA(cudaMemsetAsync(N->G0 + (size_t)N->out_ch * d.vox(), 0, (size_t)(4 - N->out_ch) * d.vox() * sizeof(float), s));
+  k_mse<<<JXB_RED_BLOCKS, 256, 0, s>>>(d.vox(), N->out_ch, out_buf(N), target, mask, g0, N->red);
+  JXB_CUDA(cudaMemsetAsync(g0 + (size_t)N->out_ch * d.vox(), 0, (size_t)(4 - N->out_ch) * d.vox() * sizeof(float), s));
   std::vector<double> h(2 * JXB_RED_BLOCKS);
   JXB_CUDA(cudaMemcpyAsync(h.data(), N->red, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   JXB_CUDA(cudaStreamSynchronize(s));
@@ -821,8 +894,8 @@ extern "C" int jxb_cnn_accumulate(jxb_cnn* N, jxb_stream stream, int nx, int ny,
     m += h[2 * i + 1];
   }
   double denom = m > 0 ? m : 1.0;
-  k_scale<<<nblk((long long)N->out_ch * d.vox()), 256, 0, s>>>((long long)N->out_ch * d.vox(), (float)(1.0 / denom), N->G0);
-  rc = backward(N, s, d, in);
+  k_scale<<<nblk((long long)N->out_ch * d.vox()), 256, 0, s>>>((long long)N->out_ch * d.vox(), (float)(1.0 / denom), g0);
+  rc = backward_top(N, s, d, in);
   if (rc) return rc;
   if (loss) *loss = a / denom;
   return JXB_OK;

@@ -102,6 +102,16 @@ __global__ void __launch_bounds__(JXB_RED_THREADS) k_ftwolevel(long long n, cons
     z[i] = a * z[i] + inv[i] * (r[i] - a * Kz[i]);
 }
 
+// additive two-level preconditioner: z <- z + D^-1 r, the network output z
+// (its weight folded into out_scale) plus one Jacobi step on r
+template <typename T>
+__global__ void k_fadd(long long n, const FcgState* st, const T* __restrict__ inv, const T* __restrict__ r,
+                       T* __restrict__ z) {
+  if (st->cg.done) return;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] += inv[i] * r[i];
+}
+
 // ring slot of stored direction d (0-based since the last restart)
 __device__ __forceinline__ int fcg_slot(long long d, int m) { return (int)(d % m); }
 
@@ -420,6 +430,9 @@ struct FcgRun {
   double out_scale;
   int stall, m, every;
   bool two_level = false;
+  bool additive = false;
+  bool sticky_fallback = false;  // a fallback to Jacobi lasts for the rest of the solve
+  bool net_off = false;
   FcgState *d_st = nullptr, *h_st = nullptr;
   double* part = nullptr;  // (FCG_MMAX + 3) x JXB_RED_BLOCKS
   float* in = nullptr;
@@ -466,6 +479,8 @@ int record_iteration(FcgRun& R, cudaStream_t s, bool learned, int iters) {
         if (rc2) return rc2;
         k_fzr<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, z, r, ppr);
         k_ftwolevel<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, pap, ppr, Ap, r, inv, z);
+      } else if (R.additive) {
+        k_fadd<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, R.d_st, inv, r, z);
       }
     } else {
       k_fjac<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, inv, r, R.d_st, z);
@@ -554,7 +569,7 @@ int fcg_run(FcgRun& R, GraphPair& G, cudaStream_t s, const TB* b, double tol, do
 // vectors set up by the caller); learned directions first, Jacobi after a fallback.
 template <typename T>
 int fcg_loop(FcgRun& R, GraphPair& G, cudaStream_t s, long long maxiter, long long* iters, int* status) {
-  bool learned = R.cnn != nullptr;
+  bool learned = R.cnn != nullptr && !R.net_off;
   if (learned && !G.learned) {
     int rc = capture<T>(R, s, true, 1, &G.learned);
     if (rc) return rc;
@@ -584,6 +599,7 @@ int fcg_loop(FcgRun& R, GraphPair& G, cudaStream_t s, long long maxiter, long lo
       }
       if (h.bad || since >= R.stall) {  // fall back to Jacobi directions
         learned = false;
+        R.net_off = R.sticky_fallback;
         k_frestart<<<1, 1, 0, s>>>(R.d_st);
         JXB_CUDA(cudaGetLastError());
         JXB_CUDA(cudaMemcpyAsync(R.h_st, R.d_st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
@@ -643,6 +659,7 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
   R.m = depth;
   R.every = opts->check_every > 0 ? opts->check_every : 16;
   R.two_level = (mode & 2) != 0;
+  R.additive = (mode & 8) != 0 && !R.two_level;
   GraphPair G;
   rc = mixed ? fcg_setup<float>(R, s) : fcg_setup<double>(R, s);
   if (rc) return rc;
@@ -673,6 +690,7 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
     rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
     if (rc) return rc;
     double rn_seg = rn;
+    R.sticky_fallback = true;  // the segments continue one recurrence
     while (outer < max_updates && fin && rn > opts->tol * bn && total < maxiter) {
       const int first = outer == 0;
       const double ratio = first ? 1.0 : rn_seg / rn;

@@ -60,10 +60,15 @@ class LearnedPreconditioner:
         Static per-control-point input channels, e.g. a normalised log-coefficient.
     channels : sequence of int or None
         Channels per U-Net level (2..6 levels, each in {4,8,12,16,24,32,48,64});
-        None picks :func:`default_channels` for the grid.
+        None picks :func:`default_channels` for the grid the network runs on.
+    pool_input : bool
+        Run the network on the 2x2x2-pooled residual (half resolution) and
+        upsample its output: the network then supplies the smooth part of the
+        correction, the Jacobi term of the additive two-level map the rest, at
+        about an eighth of the finest level's cost.
     """
 
-    def __init__(self, op, features=None, channels=None, seed=0):
+    def __init__(self, op, features=None, channels=None, seed=0, pool_input=False):
         import torch
 
         self.lib = _lib.load()
@@ -79,20 +84,25 @@ class LearnedPreconditioner:
         else:
             self.features = None
         self.n_feat = 0 if self.features is None else self.features.shape[0]
+        self.pool_input = bool(pool_input)
         if channels is None:
-            channels = default_channels(self.grid)
+            g = self.grid
+            channels = default_channels(tuple((n + 1) // 2 for n in g) if self.pool_input else g)
         self.channels = tuple(int(c) for c in channels)
         ch = (ctypes.c_int32 * len(self.channels))(*self.channels)
         h = ctypes.c_void_p()
         _lib.check(self.lib.jxb_cnn_create(self.vec + self.n_feat, self.vec, len(self.channels), ch, int(seed),
                                            ctypes.byref(h)))
         self.handle = h
+        if self.pool_input:
+            _lib.check(self.lib.jxb_cnn_set_input_pooling(h, 1))
         ptr, n = ctypes.c_void_p(), ctypes.c_int64()
         _lib.check(self.lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
         self.params = torch.as_tensor(_DeviceArray(ptr.value, n.value), device=self.dev)
         self.n_params = n.value
         self.in_scale = 1.0
         self.out_scale = 1.0
+        self.additive_weight = 1.0
         self.history = []
 
     def close(self):
@@ -244,6 +254,39 @@ class LearnedPreconditioner:
         z = out.double().t().reshape(-1) * rn * self.out_scale
         return (z * torch.as_tensor(~self.op.prescribed_mask, device=self.dev)).contiguous()
 
+    def fit_additive_weight(self, R, E, n_pairs=64):
+        """Weight a of the network in the additive two-level map z = a n + D^-1 r.
+
+        For a pair (r, e = K^-1 r) the energy-optimal a minimises
+        ||e - a n - D^-1 r||_K: a = (n.r - (K n).(D^-1 r)) / (n^T K n). The pooled
+        estimate sums numerator and denominator over up to ``n_pairs`` pairs,
+        each normalised by its e.r. One operator apply per pair; sets and
+        returns ``additive_weight``.
+        """
+        import torch
+
+        op = self.op
+        inv = op.diag()
+        free = torch.as_tensor(~op.prescribed_mask, device=self.dev)
+        inv = torch.where(free & (inv.abs() > 0), 1.0 / torch.where(inv.abs() > 0, inv, torch.ones_like(inv)),
+                          torch.zeros_like(inv))
+        num = den = 0.0
+        m = min(int(R.shape[0]), int(n_pairs))
+        for j in range(m):
+            r = R[j].t().reshape(-1).double().contiguous()
+            e = E[j].t().reshape(-1).double().contiguous()
+            er = float(e @ r)
+            if not er > 0:
+                continue
+            z = self.forward(r)
+            Kz = op.apply(z)
+            num += (float(z @ r) - float(Kz @ (inv * r))) / er
+            den += float(z @ Kz) / er
+        if not den > 0:
+            raise ValueError("fit_additive_weight: the network output has no energy on these pairs")
+        self.additive_weight = num / den
+        return self.additive_weight
+
     # -- solve -------------------------------------------------------------------
     def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=None, check_every=16,
               use_network=True, two_level=False, refinement="reliable"):
@@ -255,13 +298,21 @@ class LearnedPreconditioner:
         fallen by ``inner_tol`` (default 1e-2), keeping the stored directions;
         with ``"restart"`` each FP32 solve to ``inner_tol`` (default 1e-4) starts
         afresh inside FP64 iterative refinement.
-        ``two_level``: the network output n as a coarse correction with its own
-        line search, then one Jacobi step: z = a n + D^-1 (r - a K n).
+        ``two_level``: ``True`` (or ``"multiplicative"``) takes the network
+        output n as a coarse correction with its own line search, then one
+        Jacobi step: z = a n + D^-1 (r - a K n), one more apply per iteration;
+        ``"additive"`` uses z = a n + D^-1 r with the fixed weight
+        ``additive_weight`` (``fit_additive_weight``) and no extra apply.
         ``use_network=False`` runs the same FCG with Jacobi only (the baseline
         the network is measured against).
         """
         if refinement not in ("reliable", "restart"):
             raise ValueError(f"refinement must be 'reliable' or 'restart', got {refinement!r}")
+        if two_level not in (False, True, "multiplicative", "additive"):
+            raise ValueError(f"two_level must be False, True, 'multiplicative' or 'additive', got {two_level!r}")
+        additive = two_level == "additive"
+        mult = two_level is True or two_level == "multiplicative"
+        out_scale = self.out_scale * (self.additive_weight if additive else 1.0)
         if inner_tol is None:
             inner_tol = 1e-2 if refinement == "reliable" else 1e-4
         op = self.op
@@ -272,8 +323,8 @@ class LearnedPreconditioner:
         feats = self.features
         rc = self.lib.jxb_fcg_learned(op.handle, self.handle if use_network else None, _s(), _p(b), _p(x),
                                       _p(feats) if feats is not None else None, self.n_feat,
-                                      float(self.in_scale), float(self.out_scale), int(stall), int(depth),
-                                      (1 if mixed else 0) | (2 if two_level else 0)
+                                      float(self.in_scale), float(out_scale), int(stall), int(depth),
+                                      (1 if mixed else 0) | (2 if mult else 0) | (8 if additive else 0)
                                       | (4 if refinement == "restart" else 0), ctypes.byref(o), ctypes.byref(st))
         if rc not in (0, 4):
             _lib.check(rc)
@@ -285,13 +336,15 @@ class LearnedPreconditioner:
     def save(self, path):
         np.savez(path, params=self.params.cpu().numpy(), in_scale=self.in_scale, out_scale=self.out_scale,
                  channels=np.asarray(self.channels), vec=self.vec, n_feat=self.n_feat,
-                 history=np.asarray(self.history))
+                 history=np.asarray(self.history), additive_weight=self.additive_weight,
+                 pool_input=int(self.pool_input))
 
     @classmethod
     def from_checkpoint(cls, op, path, features=None):
         """A preconditioner with the network shape, weights and scales stored in ``path``."""
         d = np.load(path)
-        lp = cls(op, features=features, channels=tuple(int(c) for c in d["channels"]))
+        pool = bool(int(d["pool_input"])) if "pool_input" in d.files else False
+        lp = cls(op, features=features, channels=tuple(int(c) for c in d["channels"]), pool_input=pool)
         lp.load(path)
         return lp
 
@@ -299,11 +352,14 @@ class LearnedPreconditioner:
         import torch
 
         d = np.load(path)
-        if tuple(d["channels"]) != self.channels or int(d["vec"]) != self.vec or int(d["n_feat"]) != self.n_feat:
+        pool = bool(int(d["pool_input"])) if "pool_input" in d.files else False
+        if (tuple(d["channels"]) != self.channels or int(d["vec"]) != self.vec or int(d["n_feat"]) != self.n_feat
+                or pool != self.pool_input):
             raise ValueError("checkpoint does not match this network's shape")
         self.params.copy_(torch.as_tensor(d["params"], device=self.dev))
         self.in_scale = float(d["in_scale"])
         self.out_scale = float(d["out_scale"])
+        self.additive_weight = float(d["additive_weight"]) if "additive_weight" in d.files else 1.0
         self.history = list(d["history"])
 
 
@@ -318,18 +374,21 @@ def default_channels(grid):
     return (8, 16, 24, 32, 48, 48)[:levels]
 
 
-def time_network(n=99, channels=None, reps=10, in_ch=2, once=False):
+def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=False):
     """Device time (ms) of the network's forward and backward on an n^3 grid of
     random inputs, CUDA events on the current stream. ``once``: one forward and
     one backward after three warm-up forwards (for a profiler launch list)."""
     import torch
 
     lib = _lib.load()
-    channels = tuple(channels or default_channels((n, n, n)))
+    m = (n + 1) // 2 if pool_input else n
+    channels = tuple(channels or default_channels((m, m, m)))
     h = ctypes.c_void_p()
     _lib.check(lib.jxb_cnn_create(in_ch, 1, len(channels), (ctypes.c_int32 * len(channels))(*channels), 1,
                                   ctypes.byref(h)))
     try:
+        if pool_input:
+            _lib.check(lib.jxb_cnn_set_input_pooling(h, 1))
         x = torch.randn(in_ch, n, n, n, device="cuda")
         out = torch.empty(1, n, n, n, device="cuda")
         g = torch.randn(1, n, n, n, device="cuda")
@@ -353,7 +412,8 @@ def time_network(n=99, channels=None, reps=10, in_ch=2, once=False):
         e2.record()
         torch.cuda.synchronize()
         f = e0.elapsed_time(e1) / reps
-        return {"grid": n, "channels": channels, "forward_ms": f, "backward_ms": e1.elapsed_time(e2) / reps - f}
+        return {"grid": n, "channels": channels, "pool_input": bool(pool_input), "forward_ms": f,
+                "backward_ms": e1.elapsed_time(e2) / reps - f}
     finally:
         lib.jxb_cnn_destroy(h)
 
@@ -366,6 +426,7 @@ if __name__ == "__main__":
     ap.add_argument("--grid", type=int, default=99)
     ap.add_argument("--channels", default=None, help="per-level channels, e.g. 8,16,24,32,48")
     ap.add_argument("--once", action="store_true", help="3 warm-up forwards, then one forward and one backward")
+    ap.add_argument("--pool-input", action="store_true", help="run on the pooled input (half resolution)")
     a = ap.parse_args()
     ch = None if a.channels is None else [int(c) for c in a.channels.split(",")]
-    print(json.dumps(time_network(a.grid, ch, once=a.once)))
+    print(json.dumps(time_network(a.grid, ch, once=a.once, pool_input=a.pool_input)))

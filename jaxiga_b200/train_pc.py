@@ -7,11 +7,13 @@ vector first, then seeded random right-hand sides), one (residual, error)
 pair per iteration, plus ``--random`` pairs (r ~ N(0, I), e = K^-1 r); training minimises the energy norm of the
 preconditioner's error with the network's own forward/backward kernels and
 Adam until the time budget is spent; the checkpoint (weights, scales, loss
-history) is written to ``--out``. Then the workload is solved to 1e-8 by
-plain FP64 Jacobi-PCG, by flexible CG with the network (FP64), by the same
-with FP32 inner solves inside FP64 refinement, and by the flexible CG
-without the network, and one JSON line with the training record and the
-solves is printed.
+history, the fitted weight of the additive two-level map) is written to
+``--out``. ``--pool-input`` trains a network that runs on the pooled
+(half-resolution) residual. Then the workload is solved to 1e-8 by plain
+FP64 Jacobi-PCG, by flexible CG with the network alone, with the
+multiplicative and the additive two-level maps (FP64 and mixed precision),
+and by the flexible CG without the network, and one JSON line with the
+training record and the solves is printed.
 """
 
 from __future__ import annotations
@@ -77,12 +79,13 @@ def main():
     ap.add_argument("--epochs", type=int, default=1000)
     ap.add_argument("--depth", type=int, default=4)
     ap.add_argument("--out", required=True)
+    ap.add_argument("--pool-input", action="store_true", help="network on the pooled (half-resolution) residual")
     ap.add_argument("--seed", type=int, default=20260901)
     args = ap.parse_args()
     t0 = time.time()
     V, op, F, features = build(args.workload, args.span)
     channels = None if args.channels is None else tuple(int(c) for c in args.channels.split(","))
-    lp = LearnedPreconditioner(op, features=features, channels=channels, seed=args.seed)
+    lp = LearnedPreconditioner(op, features=features, channels=channels, seed=args.seed, pool_input=args.pool_input)
     gen = torch.Generator(device=op.device).manual_seed(args.seed)
     Rs, Es, solves_data = [], [], []
     have = 0
@@ -113,6 +116,8 @@ def main():
         lp.train(R, E, epochs=1, lr=lr, batch=4, seed=ep)
         ep += 1
     t_train = time.time() - t1
+    idx = torch.linspace(0, R.shape[0] - 1, min(64, R.shape[0]), device=R.device).long()
+    lp.fit_additive_weight(R[idx], E[idx], n_pairs=64)
     lp.save(args.out)
     del R, E
     solves = {}
@@ -127,6 +132,10 @@ def main():
     solves["learned_fcg_two_level"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level=True, mixed=True)
     solves["learned_fcg_two_level_mixed"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level="additive")
+    solves["learned_fcg_additive"] = st
+    _, st = lp.solve(F, tol=1e-8, depth=args.depth, two_level="additive", mixed=True)
+    solves["learned_fcg_additive_mixed"] = st
     _, st = lp.solve(F, tol=1e-8, depth=args.depth, use_network=False)
     solves["fcg_jacobi_only"] = st
     # network inference time on its own
@@ -143,6 +152,7 @@ def main():
     print(json.dumps({"workload": args.workload, "n_dofs": V.n_dofs, "pairs": int(have), "channels": lp.channels,
                       "solves_for_pairs": solves_data, "data_seconds": t_data, "train_seconds": t_train,
                       "epochs": ep, "loss_first": lp.history[0], "loss_last": lp.history[-1],
+                      "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
                       "params": lp.n_params, "forward_ms": e0.elapsed_time(e1) / 10, "solves": solves,
                       "checkpoint": args.out}))
 

@@ -13,6 +13,9 @@ the way libjxb defines it: a U-Net with L levels and channels c[0..L-1],
                           y = c[l] -> c[l] relu (m_l)
     output:               c[0] -> 4 (linear; the first out_ch channels are used)
 
+With input pooling the input is pooled once, the U-Net runs on the pooled
+grid and its output is upsampled to the input grid.
+
 3x3x3 convolutions use zero padding, tap index k = dx + 3 dy + 9 dz; pooling
 averages the existing children of a coarse voxel (odd sizes round up);
 upsampling copies a coarse voxel to its children. Parameters are one flat
@@ -132,8 +135,11 @@ def up_grad(gf, coarse_shape):
     return out
 
 
-def forward(params, x, in_ch, channels):
+def forward(params, x, in_ch, channels, pool_input=False):
     """Returns (output [4, ...], cache)."""
+    if pool_input:
+        out, cache = forward(params, pool(x), in_ch, channels)
+        return up(out, x.shape[1:]), cache
     L = unpack(np.asarray(params, dtype=np.float64), in_ch, channels)
     n = len(channels)
     relu = lambda v: np.maximum(v, 0.0)  # noqa: E731
@@ -164,8 +170,11 @@ def forward(params, x, in_ch, channels):
     return out, (L, a)
 
 
-def backward(params, x, gout, in_ch, channels):
+def backward(params, x, gout, in_ch, channels, pool_input=False):
     """Flat parameter gradient of sum(gout * forward(x)[:gout.shape[0]])."""
+    if pool_input:
+        xc = pool(x)
+        return backward(params, xc, up_grad(gout, xc.shape[1:]), in_ch, channels)
     out, (L, a) = forward(params, x, in_ch, channels)
     n = len(channels)
     g = np.zeros_like(out)
@@ -207,12 +216,12 @@ def backward(params, x, gout, in_ch, channels):
     return np.concatenate([np.concatenate([gw.reshape(-1), gb]) for gw, gb in grads])
 
 
-def loss_and_grads(params, x, target, mask, in_ch, out_ch, channels):
+def loss_and_grads(params, x, target, mask, in_ch, out_ch, channels, pool_input=False):
     """Masked MSE over the first out_ch outputs and its parameter gradient (flat)."""
-    out, _ = forward(params, x, in_ch, channels)
+    out, _ = forward(params, x, in_ch, channels, pool_input)
     m = np.ones(x.shape[1:]) if mask is None else mask
     diff = out[:out_ch] - target
     denom = m.sum() * out_ch
     loss = float((m * diff**2).sum() / denom)
     g = 2 * m * diff / denom
-    return loss, out, backward(params, x, g, in_ch, channels)
+    return loss, out, backward(params, x, g, in_ch, channels, pool_input)

@@ -29,12 +29,14 @@ def _s():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def _make_net(lib, in_ch, out_ch, channels, seed, rng):
+def _make_net(lib, in_ch, out_ch, channels, seed, rng, pool=False):
     import torch
 
     h = ctypes.c_void_p()
     _lib.check(lib.jxb_cnn_create(in_ch, out_ch, len(channels), (ctypes.c_int32 * len(channels))(*channels), seed,
                                   ctypes.byref(h)))
+    if pool:
+        _lib.check(lib.jxb_cnn_set_input_pooling(h, 1))
     ptr, n = ctypes.c_void_p(), ctypes.c_int64()
     _lib.check(lib.jxb_cnn_params(h, ctypes.byref(ptr), ctypes.byref(n)))
     params = torch.as_tensor(_DeviceArray(ptr.value, n.value), device="cuda")
@@ -50,20 +52,22 @@ def _grads(lib, h):
     return torch.as_tensor(_DeviceArray(gp.value, gn.value), device="cuda").cpu().numpy()
 
 
-@pytest.mark.parametrize("grid,in_ch,out_ch,channels", [
-    ((9, 7, 5), 2, 1, (4, 8, 12)),
-    ((6, 6, 1), 3, 3, (8, 8, 16)),
-    ((19, 18, 17), 2, 1, (8, 16, 24, 32)),
-    ((11, 9, 7), 4, 3, (12, 24)),
-    ((21, 5, 3), 1, 1, (16, 32, 48)),
-    ((66, 64, 40), 2, 1, (8, 16)),  # level 0 with wide channel blocks, level 1 with narrow ones
+@pytest.mark.parametrize("grid,in_ch,out_ch,channels,pool", [
+    ((9, 7, 5), 2, 1, (4, 8, 12), False),
+    ((6, 6, 1), 3, 3, (8, 8, 16), False),
+    ((19, 18, 17), 2, 1, (8, 16, 24, 32), False),
+    ((11, 9, 7), 4, 3, (12, 24), False),
+    ((21, 5, 3), 1, 1, (16, 32, 48), False),
+    ((66, 64, 40), 2, 1, (8, 16), False),  # level 0 with wide channel blocks, level 1 with narrow ones
+    ((19, 18, 17), 2, 1, (8, 16, 24), True),  # input pooling: odd sizes round up
+    ((13, 10, 6), 4, 3, (8, 16), True),
 ])
-def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels):
+def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels, pool):
     import torch
 
     lib = _lib.load()
     rng = np.random.default_rng(3)
-    h, p32 = _make_net(lib, in_ch, out_ch, channels, 5, rng)
+    h, p32 = _make_net(lib, in_ch, out_ch, channels, 5, rng, pool)
     nx, ny, nz = grid
     x = rng.standard_normal((in_ch, nz, ny, nx))
     t = rng.standard_normal((out_ch, nz, ny, nx))
@@ -73,7 +77,7 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
     _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out)))
     x32 = x.astype(np.float32).astype(np.float64)
     loss_ref, out_ref, g_ref = cnn_oracle.loss_and_grads(p32, x32, t.astype(np.float32).astype(np.float64), mask,
-                                                         in_ch, out_ch, channels)
+                                                         in_ch, out_ch, channels, pool)
     o = out.cpu().numpy()
     assert np.abs(o - out_ref[:out_ch]).max() <= 2e-4 * np.abs(out_ref[:out_ch]).max()
     _lib.check(lib.jxb_cnn_zero_grad(h, _s()))
@@ -91,13 +95,14 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
     _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out)))
     _lib.check(lib.jxb_cnn_backward(h, _s(), nx, ny, nz, _p(xd), _p(god)))
     g2 = _grads(lib, h)
-    g2_ref = cnn_oracle.backward(p32, x32, gout.astype(np.float32).astype(np.float64), in_ch, channels)
+    g2_ref = cnn_oracle.backward(p32, x32, gout.astype(np.float32).astype(np.float64), in_ch, channels, pool)
     assert np.abs(g2 - g2_ref).max() <= 2e-3 * np.abs(g2_ref).max()
     lib.jxb_cnn_destroy(h)
 
 
-@pytest.mark.parametrize("op_name,angle", [("poisson", 0), ("elasticity", 0), ("poisson", 1), ("elasticity", 1)])
-def test_energy_loss_gradient_matches_oracle(op_name, angle):
+@pytest.mark.parametrize("op_name,angle,pool", [("poisson", 0, False), ("elasticity", 0, False), ("poisson", 1, False),
+                                               ("elasticity", 1, False), ("poisson", 1, True)])
+def test_energy_loss_gradient_matches_oracle(op_name, angle, pool):
     """Energy-norm losses against the oracle network and the assembled K:
     w d^T K d with d = P_f (e - s N(in)), and w (1 - (z.r)^2 / ((z^T K z)(e.r)))
     with z = P_f s N(in), r = K e."""
@@ -121,7 +126,7 @@ def test_energy_loss_gradient_matches_oracle(op_name, angle):
     nx, ny, nz = V.n_cp
     ncp = V.n_scalar_basis
     in_ch = vec + 1
-    h, p32 = _make_net(lib, in_ch, vec, (4, 8, 12), 7, rng)
+    h, p32 = _make_net(lib, in_ch, vec, (4, 8, 12), 7, rng, pool)
     x = rng.standard_normal((in_ch, nz, ny, nx))
     e = rng.standard_normal((vec, nz, ny, nx)).astype(np.float32).astype(np.float64)
     s, w = 0.7, 0.3
@@ -145,7 +150,7 @@ def test_energy_loss_gradient_matches_oracle(op_name, angle):
                                              ctypes.byref(loss)))
     g = _grads(lib, h)
     x32 = x.astype(np.float32).astype(np.float64)
-    out, _ = cnn_oracle.forward(p32, x32, in_ch, (4, 8, 12))
+    out, _ = cnn_oracle.forward(p32, x32, in_ch, (4, 8, 12), pool)
     if not angle:
         d = to_dof(e - s * out[:vec])
         d[mask] = 0.0
@@ -163,7 +168,7 @@ def test_energy_loss_gradient_matches_oracle(op_name, angle):
         gz = w * 2.0 * a / (bq * c) * (a / bq * Kz - rdof)
         gz[mask] = 0.0
         gout = to_grid(s * gz)
-    g_ref = cnn_oracle.backward(p32, x32, gout, in_ch, (4, 8, 12))
+    g_ref = cnn_oracle.backward(p32, x32, gout, in_ch, (4, 8, 12), pool)
     assert abs(loss.value - loss_ref) <= 1e-4 * abs(loss_ref)
     assert np.abs(g - g_ref).max() <= 2e-3 * np.abs(g_ref).max()
     lib.jxb_cnn_destroy(h)
@@ -230,6 +235,27 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     assert st_jm["converged"] and st_jr["converged"]
     assert st_jm["iterations"] <= 1.15 * st_j["iterations"] + 10, (st_jm, st_j)
     assert st_jm["iterations"] < st_jr["iterations"], (st_jm, st_jr)
+    # additive two-level map with the fitted weight: one apply per iteration
+    a = lp.fit_additive_weight(R, E, n_pairs=32)
+    assert np.isfinite(a) and a > 0
+    x_a, st_a = lp.solve(b, tol=1e-8, two_level="additive")
+    assert st_a["converged"] and st_a["iterations"] < st_ref["iterations"], (st_a, st_ref)
+    assert float(torch.linalg.norm(x_a - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
+    _, st_am = lp.solve(b, tol=1e-8, two_level="additive", mixed=True)
+    assert st_am["converged"], st_am
+    # a network on the pooled residual (half resolution) in the additive map
+    lpp = LearnedPreconditioner(op, features=feat, seed=2, pool_input=True)
+    lpp.in_scale, lpp.out_scale = lp.in_scale, lp.out_scale
+    lpp.train(R, E, epochs=6, lr=3e-3, batch=4)
+    lpp.fit_additive_weight(R, E, n_pairs=32)
+    x_p, st_p = lpp.solve(b, tol=1e-8, two_level="additive", mixed=True)
+    assert st_p["converged"], st_p
+    assert float(torch.linalg.norm(x_p - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
+    lpp.save(tmp_path / "pool.npz")
+    lpq = LearnedPreconditioner.from_checkpoint(op, tmp_path / "pool.npz", features=feat)
+    assert lpq.pool_input and lpq.channels == lpp.channels
+    lpq.close()
+    lpp.close()
     # checkpoint / resume reproduces the preconditioner
     path = tmp_path / "pc.npz"
     lp.save(path)
@@ -237,6 +263,7 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     lp2.load(path)
     r = torch.randn(V.n_dofs, dtype=torch.float64, device="cuda") * torch.as_tensor(~op.prescribed_mask, device="cuda")
     assert torch.equal(lp.forward(r), lp2.forward(r))
+    assert lp2.additive_weight == lp.additive_weight
     lp.close()
     lp2.close()
     op.close()
