@@ -224,15 +224,18 @@ int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* 
  *   jxb_cnn_accumulate_energy: forward, then, with z = P_f out_scale N(in) in DOF
  *     layout (0 on prescribed DOFs) and the plan's operator K, the loss
  *     angle == 0: weight * d^T K d, d = P_f e - z (energy norm of the error);
- *     angle != 0: weight * (1 - (z.r)^2 / ((z^T K z)(e.r))) for the pair r = K e
+ *     angle == 1: weight * (1 - (z.r)^2 / ((z^T K z)(e.r))) for the pair r = K e
  *     (energy-norm angle between z and e: blind to the scale of z, which
- *     flexible CG does not use). e and r are grids [vec][nz][ny][nx]; adds the
- *     parameter gradient and returns the loss.
+ *     flexible CG does not use);
+ *     angle == 2: the same angle for z + D^-1 r, the additive two-level map
+ *     (the network learns what the Jacobi step misses).
+ *     e and r are grids [vec][nz][ny][nx]; adds the parameter gradient and
+ *     returns the loss.
  *   jxb_cnn_adam: one Adam step with the accumulated gradient times grad_scale.
  *   jxb_cnn_set_input_pooling: on = 1 pools the input once (2x2x2 average) and
- *     runs the U-Net on the half-resolution grid, upsampling its output back
- *     (copying each coarse voxel to its children); forward, backward and the
- *     losses keep their input-grid shapes. Drops the activation buffers.
+ *     runs the U-Net on the half-resolution grid, interpolating its output back
+ *     (trilinear); forward, backward and the losses keep their input-grid
+ *     shapes. Drops the activation buffers.
  * jxb_fcg_learned: truncated flexible CG keeping `depth` (1..8) directions,
  *   z = ||r|| out_scale N(in_scale r/||r||, features) (cnn NULL: Jacobi only);
  *   Jacobi directions take over after `stall` learned iterations without a new

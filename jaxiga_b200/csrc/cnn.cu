@@ -17,7 +17,9 @@
 // children. Activations are [channel][z][y][x], FP32.
 //
 // With input pooling (jxb_cnn_set_input_pooling) the input is pooled once and
-// the U-Net runs on the half-resolution grid; its output is upsampled back.
+// the U-Net runs on the half-resolution grid; its output is interpolated back
+// (trilinear: a piecewise-constant correction would carry its block edges into
+// the energy norm).
 // The network then acts on the smooth part of the residual only, at about an
 // eighth of the finest level's cost.
 //
@@ -335,6 +337,84 @@ __global__ void k_up_bwd(Dims f, Dims c, int ch, const float* __restrict__ gf, f
         const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
         if (X < f.nx && Y < f.ny && Z < f.nz) s += src[(Z * f.ny + Y) * f.nx + X];
       }
+  gc[i] = s;
+}
+
+// Linear prolongation along one direction from nc coarse to nf = 2 nc or
+// 2 nc - 1 fine points: fine X = 2c takes coarse c; odd X the mean of its two
+// neighbours (X - 1) / 2 and (X + 1) / 2, or the lower one alone past the end.
+__device__ __forceinline__ void lin_taps(int X, int nc, int* i0, int* i1, float* w0, float* w1) {
+  const int lo = X >> 1;
+  if (!(X & 1)) {
+    *i0 = *i1 = lo;
+    *w0 = 1.f;
+    *w1 = 0.f;
+  } else if (lo + 1 < nc) {
+    *i0 = lo;
+    *i1 = lo + 1;
+    *w0 = *w1 = 0.5f;
+  } else {
+    *i0 = *i1 = lo;
+    *w0 = 1.f;
+    *w1 = 0.f;
+  }
+}
+
+// weight of coarse c in fine X (the adjoint of lin_taps)
+__device__ __forceinline__ float lin_w(int X, int c, int nc) {
+  int i0, i1;
+  float w0, w1;
+  lin_taps(X, nc, &i0, &i1, &w0, &w1);
+  return (i0 == c ? w0 : 0.f) + (i1 == c ? w1 : 0.f);
+}
+
+// trilinear upsampling of the pooled network's output to the input grid
+__global__ void k_up_lin(Dims f, Dims c, int ch, const float* __restrict__ in, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fv = (int)f.vox(), cv = (int)c.vox();
+  if (i >= fv * ch) return;
+  const int k = i / fv, o = i - k * fv;
+  const int X = o % f.nx, Y = (o / f.nx) % f.ny, Z = o / (f.nx * f.ny);
+  int x[2], y[2], z[2];
+  float wx[2], wy[2], wz[2];
+  lin_taps(X, c.nx, &x[0], &x[1], &wx[0], &wx[1]);
+  lin_taps(Y, c.ny, &y[0], &y[1], &wy[0], &wy[1]);
+  lin_taps(Z, c.nz, &z[0], &z[1], &wz[0], &wz[1]);
+  const float* src = in + (long long)k * cv;
+  float s = 0.f;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int d = 0; d < 2; ++d) s += wz[a] * wy[b] * wx[d] * src[(z[a] * c.ny + y[b]) * c.nx + x[d]];
+  out[i] = s;
+}
+
+// adjoint of k_up_lin: each coarse voxel gathers its fine neighbours 2c-1..2c+1 (fixed order)
+__global__ void k_up_lin_bwd(Dims f, Dims c, int ch, const float* __restrict__ gf, float* __restrict__ gc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cv = (int)c.vox(), fv = (int)f.vox();
+  if (i >= cv * ch) return;
+  const int k = i / cv, o = i - k * cv;
+  const int x = o % c.nx, y = (o / c.nx) % c.ny, z = o / (c.nx * c.ny);
+  const float* src = gf + (long long)k * fv;
+  float s = 0.f;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int Z = 2 * z + dz;
+    if (Z < 0 || Z >= f.nz) continue;
+    const float wz = lin_w(Z, z, c.nz);
+    if (wz == 0.f) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int Y = 2 * y + dy;
+      if (Y < 0 || Y >= f.ny) continue;
+      const float wy = lin_w(Y, y, c.ny);
+      if (wy == 0.f) continue;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int X = 2 * x + dx;
+        if (X < 0 || X >= f.nx) continue;
+        const float wx = lin_w(X, x, c.nx);
+        if (wx != 0.f) s += wz * wy * wx * src[(Z * f.ny + Y) * f.nx + X];
+      }
+    }
+  }
   gc[i] = s;
 }
 
@@ -676,7 +756,7 @@ int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
   const Dims dc = half(d);
   k_pool<<<nblk(dc.vox() * N->in_ch), 256, 0, s>>>(d, dc, N->in_ch, in, N->INC);
   if ((rc = forward(N, s, dc, N->INC))) return rc;
-  k_up<<<nblk(d.vox() * 4), 256, 0, s>>>(d, dc, 4, N->OUT, N->OUTF);
+  k_up_lin<<<nblk(d.vox() * 4), 256, 0, s>>>(d, dc, 4, N->OUT, N->OUTF);
   JXB_CUDA(cudaGetLastError());
   N->last = d;
   return JXB_OK;
@@ -686,7 +766,7 @@ int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
 int backward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
   if (!N->pool_in) return backward(N, s, d, in);
   const Dims dc = half(d);
-  k_up_bwd<<<nblk(dc.vox() * 4), 256, 0, s>>>(d, dc, 4, N->GOF, N->G0);
+  k_up_lin_bwd<<<nblk(dc.vox() * 4), 256, 0, s>>>(d, dc, 4, N->GOF, N->G0);
   JXB_CUDA(cudaGetLastError());
   return backward(N, s, dc, N->INC);
 }

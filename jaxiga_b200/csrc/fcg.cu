@@ -371,6 +371,15 @@ __global__ void k_zdof(long long ncp, int vec, const float* __restrict__ out, fl
   z[i] = keep[i] ? (double)out_scale * (double)out[(long long)c * ncp + cp] : 0.0;
 }
 
+// z += D^-1 r (r in grid layout [vec][ncp]; inv is 0 on prescribed DOFs):
+// the additive two-level map whose network part is being trained
+__global__ void k_zadd_jacobi(long long ncp, int vec, const float* __restrict__ r, const double* __restrict__ inv,
+                              double* __restrict__ z) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncp * vec) return;
+  z[i] += inv[i] * (double)r[(long long)(i % vec) * ncp + i / vec];
+}
+
 // partials of z . r and e . r over free DOFs (r, e: grid layout [vec][ncp])
 __global__ void __launch_bounds__(JXB_RED_THREADS) k_angle_dots(long long ncp, int vec, const double* __restrict__ z,
                                                                 const float* __restrict__ r, const float* __restrict__ e,
@@ -783,8 +792,10 @@ extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_strea
   if (cnn_out_channels(cnn) != plan->vec)
     return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: the network's outputs must equal the plan's vec");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (angle < 0 || angle > 2) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: angle must be 0, 1 or 2");
   int rc = ensure_workspace(plan, false);
   if (rc) return rc;
+  if (angle == 2 && (rc = compute_invdiag(plan, s))) return rc;
   const long long ncp = plan->n_scalar;
   const int vec = plan->vec;
   const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
@@ -809,8 +820,10 @@ extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_strea
     value = weight * dkd;
   } else {
     // scale-free: loss = weight (1 - (z.r)^2 / ((z^T K z)(e.r))), z = P_f s N(in), r = K e;
-    // dL/dz = weight 2a/(b c) ((a/b) K z - r), a = z.r, b = z^T K z, c = e.r
+    // dL/dz = weight 2a/(b c) ((a/b) K z - r), a = z.r, b = z^T K z, c = e.r.
+    // angle == 2: z = P_f s N(in) + D^-1 r (the additive two-level map), same dL/dN
     k_zdof<<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, out4, out_scale, plan->d_keep, d);
+    if (angle == 2) k_zadd_jacobi<<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, r, plan->d_invdiag, d);
     if ((rc = launch_bricks<double>(plan, s, MODE_APPLY, d, nullptr, nullptr, 1))) return rc;
     if ((rc = launch_combine<double>(plan, s, Kd, 1, d, plan->d_red, nullptr))) return rc;
     k_angle_dots<<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(ncp, vec, d, r, e, plan->d_keep,

@@ -200,11 +200,13 @@ class LearnedPreconditioner:
     # -- training ----------------------------------------------------------------
     def train(self, R, E, epochs=4, lr=2e-3, batch=4, seed=0, loss="angle", log=None):
         """Adam on the energy-norm angle (or scaled energy norm, or masked-MSE) loss;
-        returns the per-epoch mean losses."""
+        returns the per-epoch mean losses. ``loss="additive"`` takes the angle of
+        the additive two-level map z = n + D^-1 r, so that the network learns
+        what the Jacobi step misses (use ``two_level="additive"`` with it)."""
         import torch
 
-        if loss not in ("angle", "energy", "mse"):
-            raise ValueError("loss must be 'angle', 'energy' or 'mse'")
+        if loss not in ("angle", "additive", "energy", "mse"):
+            raise ValueError("loss must be 'angle', 'additive', 'energy' or 'mse'")
         g = torch.Generator().manual_seed(seed)
         nx, ny, nz = self.grid
         m = R.shape[0]
@@ -222,12 +224,12 @@ class LearnedPreconditioner:
                 for j in idx:
                     inp = self._input(R[j] * self.in_scale)
                     val = ctypes.c_double()
-                    if loss in ("energy", "angle"):
-                        angle = loss == "angle"
+                    if loss in ("energy", "angle", "additive"):
+                        angle = {"energy": 0, "angle": 1, "additive": 2}[loss]
                         _lib.check(self.lib.jxb_cnn_accumulate_energy(
                             self.op.handle, self.handle, _s(), _p(inp), _p(E[j].contiguous()),
                             _p(R[j].contiguous()) if angle else None, float(self.out_scale),
-                            1.0 if angle else float(w[j]), 1 if angle else 0, ctypes.byref(val)))
+                            1.0 if angle else float(w[j]), angle, ctypes.byref(val)))
                     else:
                         tgt = (E[j] / self.out_scale).contiguous()
                         _lib.check(self.lib.jxb_cnn_accumulate(self.handle, _s(), nx, ny, nz, _p(inp), _p(tgt),

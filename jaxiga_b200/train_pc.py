@@ -80,6 +80,8 @@ def main():
     ap.add_argument("--depth", type=int, default=4)
     ap.add_argument("--out", required=True)
     ap.add_argument("--pool-input", action="store_true", help="network on the pooled (half-resolution) residual")
+    ap.add_argument("--loss", choices=["angle", "additive"], default="angle",
+                    help="energy angle of the network's output, or of the additive two-level map n + D^-1 r")
     ap.add_argument("--seed", type=int, default=20260901)
     args = ap.parse_args()
     t0 = time.time()
@@ -113,7 +115,7 @@ def main():
     ep = 0
     while time.time() - t1 < args.seconds and ep < args.epochs:
         lr = args.lr if ep < 4 else args.lr / 3
-        lp.train(R, E, epochs=1, lr=lr, batch=4, seed=ep)
+        lp.train(R, E, epochs=1, lr=lr, batch=4, seed=ep, loss=args.loss)
         ep += 1
     t_train = time.time() - t1
     idx = torch.linspace(0, R.shape[0] - 1, min(64, R.shape[0]), device=R.device).long()
@@ -152,7 +154,7 @@ def main():
     print(json.dumps({"workload": args.workload, "n_dofs": V.n_dofs, "pairs": int(have), "channels": lp.channels,
                       "solves_for_pairs": solves_data, "data_seconds": t_data, "train_seconds": t_train,
                       "epochs": ep, "loss_first": lp.history[0], "loss_last": lp.history[-1],
-                      "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
+                      "pool_input": lp.pool_input, "additive_weight": lp.additive_weight, "loss": args.loss,
                       "params": lp.n_params, "forward_ms": e0.elapsed_time(e1) / 10, "solves": solves,
                       "checkpoint": args.out}))
 

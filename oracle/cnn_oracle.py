@@ -14,7 +14,9 @@ the way libjxb defines it: a U-Net with L levels and channels c[0..L-1],
     output:               c[0] -> 4 (linear; the first out_ch channels are used)
 
 With input pooling the input is pooled once, the U-Net runs on the pooled
-grid and its output is upsampled to the input grid.
+grid and its output is interpolated to the input grid: trilinear, fine point
+X = 2c taking coarse c and odd X the mean of (X - 1) / 2 and (X + 1) / 2 (the
+lower one alone past the end).
 
 3x3x3 convolutions use zero padding, tap index k = dx + 3 dy + 9 dz; pooling
 averages the existing children of a coarse voxel (odd sizes round up);
@@ -135,11 +137,33 @@ def up_grad(gf, coarse_shape):
     return out
 
 
+def lin_matrix(nf, nc):
+    """Linear prolongation along one direction, (nf, nc)."""
+    P = np.zeros((nf, nc))
+    for X in range(nf):
+        lo = X // 2
+        if X % 2 == 0 or lo + 1 >= nc:
+            P[X, lo] = 1.0
+        else:
+            P[X, lo] = P[X, lo + 1] = 0.5
+    return P
+
+
+def up_lin(x, fine_shape):
+    Pz, Py, Px = (lin_matrix(f, c) for f, c in zip(fine_shape, x.shape[1:]))
+    return np.einsum("Zz,Yy,Xx,czyx->cZYX", Pz, Py, Px, x)
+
+
+def up_lin_grad(gf, coarse_shape):
+    Pz, Py, Px = (lin_matrix(f, c) for f, c in zip(gf.shape[1:], coarse_shape))
+    return np.einsum("Zz,Yy,Xx,cZYX->czyx", Pz, Py, Px, gf)
+
+
 def forward(params, x, in_ch, channels, pool_input=False):
     """Returns (output [4, ...], cache)."""
     if pool_input:
         out, cache = forward(params, pool(x), in_ch, channels)
-        return up(out, x.shape[1:]), cache
+        return up_lin(out, x.shape[1:]), cache
     L = unpack(np.asarray(params, dtype=np.float64), in_ch, channels)
     n = len(channels)
     relu = lambda v: np.maximum(v, 0.0)  # noqa: E731
@@ -174,7 +198,7 @@ def backward(params, x, gout, in_ch, channels, pool_input=False):
     """Flat parameter gradient of sum(gout * forward(x)[:gout.shape[0]])."""
     if pool_input:
         xc = pool(x)
-        return backward(params, xc, up_grad(gout, xc.shape[1:]), in_ch, channels)
+        return backward(params, xc, up_lin_grad(gout, xc.shape[1:]), in_ch, channels)
     out, (L, a) = forward(params, x, in_ch, channels)
     n = len(channels)
     g = np.zeros_like(out)

@@ -101,7 +101,8 @@ def test_network_forward_and_gradient_match_oracle(grid, in_ch, out_ch, channels
 
 
 @pytest.mark.parametrize("op_name,angle,pool", [("poisson", 0, False), ("elasticity", 0, False), ("poisson", 1, False),
-                                               ("elasticity", 1, False), ("poisson", 1, True)])
+                                               ("elasticity", 1, False), ("poisson", 1, True), ("poisson", 2, True),
+                                               ("elasticity", 2, False)])
 def test_energy_loss_gradient_matches_oracle(op_name, angle, pool):
     """Energy-norm losses against the oracle network and the assembled K:
     w d^T K d with d = P_f (e - s N(in)), and w (1 - (z.r)^2 / ((z^T K z)(e.r)))
@@ -162,6 +163,10 @@ def test_energy_loss_gradient_matches_oracle(op_name, angle, pool):
         z[mask] = 0.0
         rdof = to_dof(r)
         rdof[mask] = 0.0
+        if angle == 2:  # additive two-level map z = s N + D^-1 r
+            inv = np.zeros(V.n_dofs)
+            inv[A.free] = O.jacobi_inverse(A.diag)
+            z = z + inv * rdof
         Kz = K(z)
         a, bq, c = float(z @ rdof), float(z @ Kz), float(ed_ @ rdof)
         loss_ref = w * (1.0 - a * a / (bq * c))
@@ -246,7 +251,7 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     # a network on the pooled residual (half resolution) in the additive map
     lpp = LearnedPreconditioner(op, features=feat, seed=2, pool_input=True)
     lpp.in_scale, lpp.out_scale = lp.in_scale, lp.out_scale
-    lpp.train(R, E, epochs=6, lr=3e-3, batch=4)
+    lpp.train(R, E, epochs=6, lr=3e-3, batch=4, loss="additive")
     lpp.fit_additive_weight(R, E, n_pairs=32)
     x_p, st_p = lpp.solve(b, tol=1e-8, two_level="additive", mixed=True)
     assert st_p["converged"], st_p
