@@ -257,7 +257,9 @@ class LearnedPreconditioner:
         return (z * torch.as_tensor(~self.op.prescribed_mask, device=self.dev)).contiguous()
 
     def fit_additive_weight(self, R, E, n_pairs=64):
-        """Weight a of the network in the additive two-level map z = a n + D^-1 r.
+        """Weight a of the network in the additive two-level map z = a n + D^-1 r,
+        for a network trained on its own (``loss="angle"``); one trained on the
+        map itself (``loss="additive"``) keeps a = 1.
 
         For a pair (r, e = K^-1 r) the energy-optimal a minimises
         ||e - a n - D^-1 r||_K: a = (n.r - (K n).(D^-1 r)) / (n^T K n). The pooled

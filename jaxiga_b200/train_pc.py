@@ -118,8 +118,11 @@ def main():
         lp.train(R, E, epochs=1, lr=lr, batch=4, seed=ep, loss=args.loss)
         ep += 1
     t_train = time.time() - t1
-    idx = torch.linspace(0, R.shape[0] - 1, min(64, R.shape[0]), device=R.device).long()
-    lp.fit_additive_weight(R[idx], E[idx], n_pairs=64)
+    if args.loss == "additive":
+        lp.additive_weight = 1.0  # trained as n + D^-1 r: the combination is the one learned
+    else:  # trained alone (n ~ e up to scale): the energy-optimal weight of n beside D^-1 r
+        idx = torch.linspace(0, R.shape[0] - 1, min(64, R.shape[0]), device=R.device).long()
+        lp.fit_additive_weight(R[idx], E[idx], n_pairs=64)
     lp.save(args.out)
     del R, E
     solves = {}
