@@ -25,7 +25,9 @@
 //
 // Convolutions (forward and data gradient) use one kernel: a CTA computes a
 // 16 x 8 x 4 voxel tile for a block of up to 16 output channels (narrower on
-// small grids, so that the grid still fills the GPU); each thread
+// small grids, so that the grid still fills the GPU, and on the coarsest
+// grids with the input channels split over CTAs and the partial sums added in
+// a fixed order by a second kernel); each thread
 // owns one (x, y) column of 4 voxels along z, so the three z taps reuse
 // registers and a warp reads consecutive x from shared memory. Input halos
 // and weights are staged in shared memory four input channels at a time.
@@ -62,10 +64,12 @@ static long long n_tiles(Dims d) {
 // out[co] = b[co] + sum_ci sum_k w[co][ci][k] in[ci](v + k)   (+ add[co]) (relu)
 // for co in [co0, co0 + COB), co0 = blockIdx.y * COB. K = 3 (27 taps,
 // k = dx + 3 dy + 9 dz) or 1. beta: out = beta * out + result.
+// Split input channels (small grids): block z sums channels [z cps, (z+1) cps)
+// into its own slab out + z * co_n * vox, bias/add/relu/beta left to k_sum_split.
 template <int K, int COB>
 __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __restrict__ in, const float* __restrict__ w,
                                             const float* __restrict__ bias, const float* __restrict__ add, int relu,
-                                            float beta, float* __restrict__ out) {
+                                            float beta, float* __restrict__ out, int cps, int co_n) {
   constexpr int R = K / 2, HX = CTX + 2 * R, HY = CTY + 2 * R, HZ = CTZ + 2 * R, KK = K * K * K;
   constexpr int HV = HX * HY * HZ;
   __shared__ __align__(16) float tile[CIB * HV];
@@ -75,6 +79,8 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
   const int bx = blockIdx.x % ntx, by = (blockIdx.x / ntx) % nty, bz = blockIdx.x / (ntx * nty);
   const int co0 = blockIdx.y * COB;
   const long long vox = d.vox();
+  const int cb = blockIdx.z * cps, ce = min(ci_n, cb + cps);
+  out += (long long)blockIdx.z * co_n * vox;
   float acc[CTZ][COB];
 #pragma unroll
   for (int c = 0; c < COB; ++c) {
@@ -82,8 +88,8 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
 #pragma unroll
     for (int j = 0; j < CTZ; ++j) acc[j][c] = b0;
   }
-  for (int ci0 = 0; ci0 < ci_n; ci0 += CIB) {
-    const int nc = min(CIB, ci_n - ci0);
+  for (int ci0 = cb; ci0 < ce; ci0 += CIB) {
+    const int nc = min(CIB, ce - ci0);
     for (int i = threadIdx.x; i < nc * HV; i += CT) {
       const int c = i / HV, r = i % HV;
       const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
@@ -145,6 +151,20 @@ __global__ void __launch_bounds__(CT) k_conv(Dims d, int ci_n, const float* __re
       out[idx] = beta != 0.f ? beta * out[idx] + v : v;
     }
   }
+}
+
+// out = relu(bias + sum_z part[z] (+ add)) (beta: out = beta * out + result),
+// the split-channel slabs summed in a fixed order
+__global__ void k_sum_split(long long vox, int co_n, int nsplit, const float* __restrict__ part,
+                            const float* __restrict__ bias, const float* __restrict__ add, int relu, float beta,
+                            float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= vox * co_n) return;
+  float v = bias ? bias[i / vox] : 0.f;
+  for (int z = 0; z < nsplit; ++z) v += part[(long long)z * co_n * vox + i];
+  if (add) v += add[i];
+  if (relu) v = fmaxf(v, 0.f);
+  out[i] = beta != 0.f ? beta * out[i] + v : v;
 }
 
 // Weight (and bias) gradient partials of one voxel tile:
@@ -507,6 +527,8 @@ struct jxb_cnn {
   float *INC = nullptr, *OUTF = nullptr, *GOF = nullptr;  // pooled input, fine output, fine output gradient
   Dims last{0, 0, 0};      // input grid of the last forward pass
   float* wt = nullptr;     // transposed weights scratch
+  float* cpart = nullptr;  // split-channel conv partials
+  long long cpart_cap = 0;
   float* part = nullptr;   // weight-gradient partials
   long long part_cap = 0;
   double* red = nullptr;   // loss partials
@@ -524,8 +546,8 @@ inline int dec_c(const jxb_cnn* N, int l) { return 2 * (N->levels - 1) + 3 + 2 *
 inline int dec_d(const jxb_cnn* N, int l) { return dec_c(N, l) + 1; }
 inline int out_layer(const jxb_cnn* N) { return 4 * N->levels - 1; }
 
-int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in, const float* add, float beta,
-         float* out) {
+int conv(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in, const float* add,
+         float beta, float* out) {
   const float* w = p + L.w_off;
   const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
   const int relu = L.relu ? 1 : 0;
@@ -535,10 +557,39 @@ int conv(cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in
   // (every output still sums its inputs in the same order, so results do not change)
   for (const int c : {12, 8, 4})
     if (tiles * (L.co / cob) < 2 * 148 && c < cob && L.co % c == 0) cob = c;
-  const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob));
+  // still fewer than two CTAs per SM: split the input channels over blocks
+  // (each sums a run of whole CIB groups), then sum the slabs in a fixed order.
+  // The partial buffer only grows; its first sizing happens on the forward pass
+  // that runs before any graph capture.
+  int nsplit = 1, cps = L.ci;
+  const long long ctas = tiles * (L.co / cob);
+  if (ctas < 2 * 148 && L.ci > CIB) {
+    const int groups = (L.ci + CIB - 1) / CIB;
+    const int want = (int)std::min<long long>(groups, (2 * 148 + ctas - 1) / ctas);
+    cps = ((groups + want - 1) / want) * CIB;
+    nsplit = (L.ci + cps - 1) / cps;
+  }
+  float* dst = out;
+  if (nsplit > 1) {
+    const long long need = (long long)nsplit * L.co * d.vox();
+    if (need > N->cpart_cap) {
+      cudaFree(N->cpart);
+      N->cpart = nullptr;
+      N->cpart_cap = 0;
+      JXB_CUDA(cudaMalloc(&N->cpart, need * sizeof(float)));
+      N->cpart_cap = need;
+    }
+    dst = N->cpart;
+  }
+  const dim3 grid((unsigned)tiles, (unsigned)(L.co / cob), (unsigned)nsplit);
 #define JXB_CONV(KS, C)                                                                         \
   if (L.k == KS && cob == C) {                                                                  \
-    k_conv<KS, C><<<grid, CT, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out);                  \
+    if (nsplit == 1) {                                                                          \
+      k_conv<KS, C><<<grid, CT, 0, s>>>(d, L.ci, in, w, b, add, relu, beta, out, L.ci, L.co);   \
+    } else {                                                                                    \
+      k_conv<KS, C><<<grid, CT, 0, s>>>(d, L.ci, in, w, nullptr, nullptr, 0, 0.f, dst, cps, L.co); \
+      k_sum_split<<<nblk(d.vox() * L.co), 256, 0, s>>>(d.vox(), L.co, nsplit, dst, b, add, relu, beta, out); \
+    }                                                                                           \
     JXB_CUDA(cudaGetLastError());                                                               \
     return JXB_OK;                                                                              \
   }
@@ -554,7 +605,7 @@ int conv_dgrad(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* 
   int n = L.co * L.ci * KK;
   k_transpose_w<<<(n + 255) / 256, 256, 0, s>>>(L.co, L.ci, KK, N->p + L.w_off, N->wt);
   Layer T{L.co, L.ci, L.k, false, 0, -1};
-  return conv(s, d, T, N->wt, g, nullptr, beta, gin);
+  return conv(N, s, d, T, N->wt, g, nullptr, beta, gin);
 }
 
 int conv_wgrad(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* in, const float* g) {
@@ -647,23 +698,23 @@ int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   const float* p = N->p;
   const float* x = in;
   for (int l = 0; l < nl - 1; ++l) {
-    if ((rc = conv(s, d[l], N->L[enc_a(l)], p, x, nullptr, 0.f, N->A[l]))) return rc;
-    if ((rc = conv(s, d[l], N->L[enc_b(l)], p, N->A[l], nullptr, 0.f, N->S[l]))) return rc;
+    if ((rc = conv(N, s, d[l], N->L[enc_a(l)], p, x, nullptr, 0.f, N->A[l]))) return rc;
+    if ((rc = conv(N, s, d[l], N->L[enc_b(l)], p, N->A[l], nullptr, 0.f, N->S[l]))) return rc;
     k_pool<<<nblk(d[l + 1].vox() * N->c[l]), 256, 0, s>>>(d[l], d[l + 1], N->c[l], N->S[l], N->P[l + 1]);
     x = N->P[l + 1];
   }
   const Dims db = d[nl - 1];
-  if ((rc = conv(s, db, N->L[bot(N, 0)], p, x, nullptr, 0.f, N->B0))) return rc;
-  if ((rc = conv(s, db, N->L[bot(N, 1)], p, N->B0, nullptr, 0.f, N->B1))) return rc;
-  if ((rc = conv(s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
+  if ((rc = conv(N, s, db, N->L[bot(N, 0)], p, x, nullptr, 0.f, N->B0))) return rc;
+  if ((rc = conv(N, s, db, N->L[bot(N, 1)], p, N->B0, nullptr, 0.f, N->B1))) return rc;
+  if ((rc = conv(N, s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
   const float* y = N->B2;
   for (int l = nl - 2; l >= 0; --l) {
     k_up<<<nblk(d[l].vox() * N->c[l + 1]), 256, 0, s>>>(d[l], d[l + 1], N->c[l + 1], y, N->U[l]);
-    if ((rc = conv(s, d[l], N->L[dec_c(N, l)], p, N->U[l], N->S[l], 0.f, N->M[l]))) return rc;
-    if ((rc = conv(s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
+    if ((rc = conv(N, s, d[l], N->L[dec_c(N, l)], p, N->U[l], N->S[l], 0.f, N->M[l]))) return rc;
+    if ((rc = conv(N, s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
     y = N->D[l];
   }
-  if ((rc = conv(s, d0, N->L[out_layer(N)], p, y, nullptr, 0.f, N->OUT))) return rc;
+  if ((rc = conv(N, s, d0, N->L[out_layer(N)], p, y, nullptr, 0.f, N->OUT))) return rc;
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }
@@ -890,6 +941,7 @@ extern "C" int jxb_cnn_destroy(jxb_cnn* N) {
   cudaFree(N->v);
   cudaFree(N->wt);
   cudaFree(N->part);
+  cudaFree(N->cpart);
   cudaFree(N->red);
   cudaFree(N->arena);
   cudaFree(N->fine_arena);
