@@ -346,13 +346,16 @@ def run_ours(args, rank, world, local_rank):
                                                  "outer": st_m["outer"], "relative_residual": st_m["relative_residual"],
                                                  "converged": bool(st_m["converged"]),
                                                  "relative_difference_to_plain": diff},
-            "speedup_mixed_vs_plain": st_p["seconds"] / st_m["seconds"] if st_m["seconds"] > 0 else None,
+            # a speed-up is reported only for a solve that reached the tolerance
+            "speedup_mixed_vs_plain": (st_p["seconds"] / st_m["seconds"]
+                                       if st_m["seconds"] > 0 and st_m["converged"] else None),
             "mixed_fp32_pcg_reliable_fp64_updates": {"seconds": st_r["seconds"], "iterations": st_r["iterations"],
                                                      "updates": st_r["outer"],
                                                      "relative_residual": st_r["relative_residual"],
                                                      "converged": bool(st_r["converged"]),
                                                      "relative_difference_to_plain": diff_r},
-            "speedup_mixed_reliable_vs_plain": st_p["seconds"] / st_r["seconds"] if st_r["seconds"] > 0 else None,
+            "speedup_mixed_reliable_vs_plain": (st_p["seconds"] / st_r["seconds"]
+                                                if st_r["seconds"] > 0 and st_r["converged"] else None),
             "learned_preconditioner": None,
         }
         ckpt = os.path.join(ROOT, "jaxiga_b200", "checkpoints", f"{args.workload}{span}.npz")
@@ -379,7 +382,8 @@ def run_ours(args, rank, world, local_rank):
                 "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
                 "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
                 "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **rows,
-                **{"speedup_%s_vs_plain" % k: st_p["seconds"] / v["seconds"] for k, v in rows.items()}}
+                **{"speedup_%s_vs_plain" % k: (st_p["seconds"] / v["seconds"] if v["converged"] else None)
+                   for k, v in rows.items()}}
             lp.close()
 
     cpu = None
