@@ -50,6 +50,7 @@ constexpr int CTX = 16, CTY = 8, CTZ = 4;  // voxel tile of the conv kernels
 constexpr int CT = CTX * CTY;              // threads per CTA (one z column of CTZ voxels each)
 constexpr int CIB = 4;                     // input channels staged per pass
 constexpr int MAXL = 6;
+constexpr int MAXC = 64;  // widest supported layer
 
 struct Dims {
   int nx, ny, nz;
@@ -165,6 +166,40 @@ __global__ void k_sum_split(long long vox, int co_n, int nsplit, const float* __
   if (add) v += add[i];
   if (relu) v = fmaxf(v, 0.f);
   out[i] = beta != 0.f ? beta * out[i] + v : v;
+}
+
+// 1x1 convolution, one thread per voxel and a block of COB output channels:
+// out[co](v) = b[co] + sum_ci w[co][ci] in[ci](v) (+ add) (relu), beta as k_conv.
+// The input channels are summed in the order k_conv uses, so results match it;
+// without a halo to stage, reading straight from global memory is coalesced
+// and keeps the kernel at the bandwidth of its reads and writes.
+template <int COB>
+__global__ void __launch_bounds__(256) k_conv1(long long vox, int ci_n, const float* __restrict__ in,
+                                               const float* __restrict__ w, const float* __restrict__ bias,
+                                               const float* __restrict__ add, int relu, float beta,
+                                               float* __restrict__ out) {
+  __shared__ float sw[64 * COB];  // [ci][co], ci_n <= 64
+  const int co0 = blockIdx.y * COB;
+  for (int i = threadIdx.x; i < ci_n * COB; i += blockDim.x) sw[i] = w[(long long)(co0 + i % COB) * ci_n + i / COB];
+  __syncthreads();
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= vox) return;
+  float acc[COB];
+#pragma unroll
+  for (int c = 0; c < COB; ++c) acc[c] = bias ? bias[co0 + c] : 0.f;
+  for (int ci = 0; ci < ci_n; ++ci) {
+    const float a = in[(long long)ci * vox + v];
+#pragma unroll
+    for (int c = 0; c < COB; ++c) acc[c] = fmaf(sw[ci * COB + c], a, acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < COB; ++c) {
+    const long long idx = (long long)(co0 + c) * vox + v;
+    float r = acc[c];
+    if (add) r += add[idx];
+    if (relu) r = fmaxf(r, 0.f);
+    out[idx] = beta != 0.f ? beta * out[idx] + r : r;
+  }
 }
 
 // Weight (and bias) gradient partials of one voxel tile:
@@ -334,13 +369,14 @@ __global__ void k_pool_bwd(Dims f, Dims c, int ch, const float* __restrict__ gc,
   gf[i] = beta != 0.f ? beta * gf[i] + v : v;
 }
 
-__global__ void k_up(Dims f, Dims c, int ch, const float* __restrict__ in, float* __restrict__ out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int fv = (int)f.vox(), cv = (int)c.vox();
-  if (i >= fv * ch) return;
-  const int k = i / fv, o = i - k * fv;
-  const int X = o % f.nx, Y = (o / f.nx) % f.ny, Z = o / (f.nx * f.ny);
-  out[i] = in[(long long)k * cv + ((Z / 2) * c.ny + Y / 2) * c.nx + X / 2];
+// grid (ceil(nx / 128), ny, nz * ch): one thread per fine voxel along x, no divisions
+__global__ void __launch_bounds__(128) k_up(Dims f, Dims c, int ch, const float* __restrict__ in,
+                                           float* __restrict__ out) {
+  const int X = blockIdx.x * 128 + threadIdx.x;
+  if (X >= f.nx) return;
+  const int Y = blockIdx.y, Z = blockIdx.z % f.nz, k = blockIdx.z / f.nz;
+  out[((long long)k * f.nz + Z) * f.ny * f.nx + (long long)Y * f.nx + X] =
+      in[(long long)k * c.vox() + ((long long)(Z >> 1) * c.ny + (Y >> 1)) * c.nx + (X >> 1)];
 }
 
 __global__ void k_up_bwd(Dims f, Dims c, int ch, const float* __restrict__ gf, float* __restrict__ gc) {
@@ -551,21 +587,33 @@ int conv(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* p, con
   const float* w = p + L.w_off;
   const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
   const int relu = L.relu ? 1 : 0;
+  if (L.k == 1 && L.ci <= 64) {
+    const int cob1 = L.co % 16 == 0 ? 16 : (L.co % 8 == 0 ? 8 : 4);
+    const dim3 g1((unsigned)((d.vox() + 255) / 256), (unsigned)(L.co / cob1));
+    if (cob1 == 16) k_conv1<16><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
+    else if (cob1 == 8) k_conv1<8><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
+    else k_conv1<4><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
+    JXB_CUDA(cudaGetLastError());
+    return JXB_OK;
+  }
   const long long tiles = n_tiles(d);
   int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
   // small grids: narrower output-channel blocks until there are two CTAs per SM
   // (every output still sums its inputs in the same order, so results do not change)
   for (const int c : {12, 8, 4})
     if (tiles * (L.co / cob) < 2 * 148 && c < cob && L.co % c == 0) cob = c;
-  // still fewer than two CTAs per SM: split the input channels over blocks
-  // (each sums a run of whole CIB groups), then sum the slabs in a fixed order.
+  // fewer than eight CTAs per SM: split the input channels over blocks (each
+  // sums a run of whole CIB groups), then sum the slabs in a fixed order. A CTA
+  // walks its channel groups one after another, each a staging round trip, so
+  // on the coarse levels the split trades a small slab sum for that latency.
   // The partial buffer only grows; its first sizing happens on the forward pass
   // that runs before any graph capture.
+  constexpr long long SPLIT_CTAS = 8 * 148;
   int nsplit = 1, cps = L.ci;
   const long long ctas = tiles * (L.co / cob);
-  if (ctas < 2 * 148 && L.ci > CIB) {
+  if (ctas < SPLIT_CTAS && L.ci > CIB) {
     const int groups = (L.ci + CIB - 1) / CIB;
-    const int want = (int)std::min<long long>(groups, (2 * 148 + ctas - 1) / ctas);
+    const int want = (int)std::min<long long>(groups, (SPLIT_CTAS + ctas - 1) / ctas);
     cps = ((groups + want - 1) / want) * CIB;
     nsplit = (L.ci + cps - 1) / cps;
   }
@@ -658,6 +706,8 @@ int ensure_bufs(jxb_cnn* N, Dims d0) {
   auto add = [&](float** ptr, long long n) { want.push_back({ptr, (std::max<long long>(n, 1) + 63) / 64 * 64}); };
   long long gmax = (long long)std::max(N->in_ch, 4) * d0.vox();
   if ((long long)64 * d0.vox() >= (1ll << 31)) return fail(JXB_ERR_INVALID, "cnn: grid too large (activation indices are 32-bit)");
+  // the upsampling launch maps y and z * channels onto grid dimensions
+  if (d0.ny > 65535 || (long long)d0.nz * MAXC > 65535) return fail(JXB_ERR_INVALID, "cnn: grid too large in y or z");
   for (int l = 0; l < nl - 1; ++l) {
     add(&N->A[l], N->c[l] * d[l].vox());
     add(&N->S[l], N->c[l] * d[l].vox());
@@ -709,7 +759,8 @@ int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   if ((rc = conv(N, s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
   const float* y = N->B2;
   for (int l = nl - 2; l >= 0; --l) {
-    k_up<<<nblk(d[l].vox() * N->c[l + 1]), 256, 0, s>>>(d[l], d[l + 1], N->c[l + 1], y, N->U[l]);
+    k_up<<<dim3((d[l].nx + 127) / 128, d[l].ny, d[l].nz * N->c[l + 1]), 128, 0, s>>>(d[l], d[l + 1], N->c[l + 1], y,
+                                                                                   N->U[l]);
     if ((rc = conv(N, s, d[l], N->L[dec_c(N, l)], p, N->U[l], N->S[l], 0.f, N->M[l]))) return rc;
     if ((rc = conv(N, s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
     y = N->D[l];
