@@ -173,22 +173,31 @@ __global__ void k_sum_split(long long vox, int co_n, int nsplit, const float* __
 // The input channels are summed in the order k_conv uses, so results match it;
 // without a halo to stage, reading straight from global memory is coalesced
 // and keeps the kernel at the bandwidth of its reads and writes.
-template <int COB>
-__global__ void __launch_bounds__(256) k_conv1(long long vox, int ci_n, const float* __restrict__ in,
+// UP: the input is the coarse grid c and in(v) its upsampled value (the coarse
+// voxel holding v), so the decoder never writes the upsampled activation.
+template <int COB, bool UP>
+__global__ void __launch_bounds__(256) k_conv1(Dims d, Dims c, int ci_n, const float* __restrict__ in,
                                                const float* __restrict__ w, const float* __restrict__ bias,
                                                const float* __restrict__ add, int relu, float beta,
                                                float* __restrict__ out) {
+  const long long vox = d.vox();
   __shared__ float sw[64 * COB];  // [ci][co], ci_n <= 64
   const int co0 = blockIdx.y * COB;
   for (int i = threadIdx.x; i < ci_n * COB; i += blockDim.x) sw[i] = w[(long long)(co0 + i % COB) * ci_n + i / COB];
   __syncthreads();
   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= vox) return;
+  long long src = v, svox = vox;
+  if constexpr (UP) {
+    const int X = (int)(v % d.nx), Y = (int)((v / d.nx) % d.ny), Z = (int)(v / ((long long)d.nx * d.ny));
+    src = ((long long)(Z >> 1) * c.ny + (Y >> 1)) * c.nx + (X >> 1);
+    svox = c.vox();
+  }
   float acc[COB];
 #pragma unroll
   for (int c = 0; c < COB; ++c) acc[c] = bias ? bias[co0 + c] : 0.f;
   for (int ci = 0; ci < ci_n; ++ci) {
-    const float a = in[(long long)ci * vox + v];
+    const float a = in[(long long)ci * svox + src];
 #pragma unroll
     for (int c = 0; c < COB; ++c) acc[c] = fmaf(sw[ci * COB + c], a, acc[c]);
   }
@@ -582,20 +591,27 @@ inline int dec_c(const jxb_cnn* N, int l) { return 2 * (N->levels - 1) + 3 + 2 *
 inline int dec_d(const jxb_cnn* N, int l) { return dec_c(N, l) + 1; }
 inline int out_layer(const jxb_cnn* N) { return 4 * N->levels - 1; }
 
+// up_from: for a 1x1 layer, `in` is on that coarse grid and is read upsampled
 int conv(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in, const float* add,
-         float beta, float* out) {
+         float beta, float* out, const Dims* up_from = nullptr) {
   const float* w = p + L.w_off;
   const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
   const int relu = L.relu ? 1 : 0;
   if (L.k == 1 && L.ci <= 64) {
     const int cob1 = L.co % 16 == 0 ? 16 : (L.co % 8 == 0 ? 8 : 4);
     const dim3 g1((unsigned)((d.vox() + 255) / 256), (unsigned)(L.co / cob1));
-    if (cob1 == 16) k_conv1<16><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
-    else if (cob1 == 8) k_conv1<8><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
-    else k_conv1<4><<<g1, 256, 0, s>>>(d.vox(), L.ci, in, w, b, add, relu, beta, out);
+    const Dims c = up_from ? *up_from : d;
+#define JXB_CONV1(C)                                                                                         \
+  if (cob1 == C) {                                                                                           \
+    if (up_from) k_conv1<C, true><<<g1, 256, 0, s>>>(d, c, L.ci, in, w, b, add, relu, beta, out);            \
+    else k_conv1<C, false><<<g1, 256, 0, s>>>(d, c, L.ci, in, w, b, add, relu, beta, out);                   \
+  }
+    JXB_CONV1(16) JXB_CONV1(8) JXB_CONV1(4)
+#undef JXB_CONV1
     JXB_CUDA(cudaGetLastError());
     return JXB_OK;
   }
+  if (up_from) return fail(JXB_ERR_INVALID, "cnn: upsampled input needs a 1x1 layer with at most 64 inputs");
   const long long tiles = n_tiles(d);
   int cob = L.co <= 16 ? L.co : (L.co % 16 == 0 ? 16 : (L.co % 12 == 0 ? 12 : 8));
   // small grids: narrower output-channel blocks until there are two CTAs per SM
@@ -759,9 +775,8 @@ int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   if ((rc = conv(N, s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
   const float* y = N->B2;
   for (int l = nl - 2; l >= 0; --l) {
-    k_up<<<dim3((d[l].nx + 127) / 128, d[l].ny, d[l].nz * N->c[l + 1]), 128, 0, s>>>(d[l], d[l + 1], N->c[l + 1], y,
-                                                                                   N->U[l]);
-    if ((rc = conv(N, s, d[l], N->L[dec_c(N, l)], p, N->U[l], N->S[l], 0.f, N->M[l]))) return rc;
+    // the 1x1 layer reads y upsampled; U[l] is only materialised by the backward pass
+    if ((rc = conv(N, s, d[l], N->L[dec_c(N, l)], p, y, N->S[l], 0.f, N->M[l], &d[l + 1]))) return rc;
     if ((rc = conv(N, s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
     y = N->D[l];
   }
@@ -790,6 +805,9 @@ int backward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
     k_relu_mask<<<nblk(n), 256, 0, s>>>(n, N->D[l], ga);
     if ((rc = conv_wgrad(N, s, d[l], N->L[dec_d(N, l)], N->M[l], ga))) return rc;
     if ((rc = conv_dgrad(N, s, d[l], N->L[dec_d(N, l)], ga, 0.f, N->GS[l]))) return rc;  // dL/dM_l = dL/ds_l (skip part)
+    const float* yc = l + 1 < nl - 1 ? N->D[l + 1] : N->B2;  // the decoder input below this level
+    k_up<<<dim3((d[l].nx + 127) / 128, d[l].ny, d[l].nz * N->c[l + 1]), 128, 0, s>>>(d[l], d[l + 1], N->c[l + 1], yc,
+                                                                                   N->U[l]);
     if ((rc = conv_wgrad(N, s, d[l], N->L[dec_c(N, l)], N->U[l], N->GS[l]))) return rc;
     if ((rc = conv_dgrad(N, s, d[l], N->L[dec_c(N, l)], N->GS[l], 0.f, gb))) return rc;  // dL/dU_l
     k_up_bwd<<<nblk((long long)N->c[l + 1] * d[l + 1].vox()), 256, 0, s>>>(d[l], d[l + 1], N->c[l + 1], gb, ga);
