@@ -161,6 +161,11 @@ def test_library_reports_errors_without_a_gpu():
     rc = lib.jxb_plan_create(None, ctypes.byref(out))
     assert rc == 1
     assert b"desc" in lib.jxb_last_error()
+    # argument checks come before any device work
+    assert lib.jxb_mixed_pcg(None, None, None, None, None, None) == 1
+    assert b"jxb_mixed_pcg" in lib.jxb_last_error()
+    assert lib.jxb_cnn_set_input_pooling(None, 1) == 1
+    assert b"input_pooling" in lib.jxb_last_error()
 
 
 def test_struct_layouts_match_header(tmp_path):

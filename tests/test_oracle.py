@@ -155,3 +155,37 @@ def test_reliable_update_cg_keeps_the_fp64_iteration_count(tag, vec, op):
     assert updates >= 5  # one per two decades at least
     assert k <= 1.15 * k64 + 10, (k, k64)
     assert np.linalg.norm(A.lift(x) - g[tag + "/u"]) <= 1e-7 * np.linalg.norm(g[tag + "/u"])
+
+
+@pytest.mark.parametrize("fine", [(7, 6, 5), (8, 9, 3), (1, 2, 3)])
+def test_cnn_oracle_trilinear_upsampling(fine):
+    """The pooled network's output interpolation: rows of each 1D prolongation sum
+    to one, a constant stays constant, and the gradient map is its adjoint."""
+    from oracle import cnn_oracle as C
+
+    coarse = C.half(fine)
+    for nf, nc in zip(fine, coarse):
+        P = C.lin_matrix(nf, nc)
+        np.testing.assert_allclose(P.sum(axis=1), 1.0)
+        assert all(P[X, X // 2] == 1.0 for X in range(0, nf, 2))  # even fine points copy their coarse point
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((2,) + coarse)
+    g = rng.standard_normal((2,) + fine)
+    assert abs((C.up_lin(x, fine) * g).sum() - (x * C.up_lin_grad(g, coarse)).sum()) < 1e-12
+    np.testing.assert_allclose(C.up_lin(np.full((1,) + coarse, 3.0), fine), 3.0)
+
+
+def test_cnn_oracle_pooled_forward_is_the_coarse_network_interpolated():
+    from oracle import cnn_oracle as C
+
+    rng = np.random.default_rng(1)
+    ch = (4, 8)
+    n = sum(ci * co * k ** 3 + co for ci, co, k, _ in C.layer_shapes(2, ch))
+    p = rng.uniform(-0.3, 0.3, n)
+    x = rng.standard_normal((2, 7, 6, 5))
+    out, _ = C.forward(p, x, 2, ch, pool_input=True)
+    coarse, _ = C.forward(p, C.pool(x), 2, ch)
+    np.testing.assert_allclose(out, C.up_lin(coarse, x.shape[1:]))
+    g = rng.standard_normal((1, 7, 6, 5))
+    np.testing.assert_allclose(C.backward(p, x, g, 2, ch, pool_input=True),
+                               C.backward(p, C.pool(x), C.up_lin_grad(g, C.half(x.shape[1:])), 2, ch))
