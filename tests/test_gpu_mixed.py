@@ -99,3 +99,14 @@ def test_reliable_update_at_size_keeps_fp64_iteration_count():
     for x in (xr, xf):
         assert float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64)) < 1e-5
     op.close()
+
+
+def test_mixed_solvers_with_a_zero_right_hand_side():
+    """b = 0: no iteration runs, x = 0, and the stats report convergence, as for jxb_pcg."""
+    V, problem, params, op, pres, coef, field = f32_operator("elast3d")
+    b = np.zeros(V.n_dofs)
+    for solve in (op.pcg, op.mixed_pcg, op.refine_solve):
+        x, st = solve(b, tol=1e-10)
+        assert st["iterations"] == 0 and st["converged"] and st["finite"], (solve.__name__, st)
+        assert float(x.abs().max()) == 0.0
+    op.close()
