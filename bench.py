@@ -67,8 +67,25 @@ REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_c
            0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
 
 
+def nvml_handle(pynvml, device):
+    """NVML handle of CUDA device ``device`` (an index into the visible
+    devices), found by PCI bus id: NVML numbers every GPU of the machine and
+    its order need not follow CUDA's or CUDA_VISIBLE_DEVICES."""
+    import torch
+
+    p = torch.cuda.get_device_properties(device)
+    bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+    try:
+        return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+    except Exception:
+        return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+
+
 class ClockSampler:
-    def __init__(self, index, period=0.005):
+    """SM clock and clock-event reasons of one GPU, sampled in a thread; no
+    samples (and clocks reported as unknown) when NVML cannot find the GPU."""
+
+    def __init__(self, device, period=0.005):
         self.samples, self.reasons, self.max_mhz = [], set(), None
         self.period = period
         self.stop_ev = threading.Event()
@@ -77,7 +94,7 @@ class ClockSampler:
 
             pynvml.nvmlInit()
             self.nvml = pynvml
-            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.h = nvml_handle(pynvml, device)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
         except Exception:
             self.nvml = None
@@ -248,9 +265,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    nvml_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]) \
-        if os.environ.get("CUDA_VISIBLE_DEVICES") else local_rank
-    with ClockSampler(nvml_index) as clocks:
+    with ClockSampler(local_rank) as clocks:
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)

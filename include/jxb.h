@@ -101,6 +101,9 @@ typedef struct jxb_solve_opts {
   double inner_tol;             /* relative tolerance of each FP32 inner solve;
                                    jxb_mixed_pcg: residual drop between updates */
   int max_outer;                /* cap on outer FP64 steps / updates */
+  int restarts;                 /* jxb_pcg: true-residual restarts (0..8) when the recursive residual
+                                   met the tolerance but the FP64 true residual did not; they share the
+                                   maxiter budget, as the reference's CPU CG (linear.py:261-321) */
 } jxb_solve_opts;
 
 typedef struct jxb_stats {
@@ -109,7 +112,7 @@ typedef struct jxb_stats {
   double residual;              /* ||b - K x|| over free DOFs, recomputed in FP64 */
   double relative_residual;
   double b_norm;
-  int converged;                /* finite and residual <= tol * ||b|| */
+  int converged;                /* finite and residual <= max(tol * ||b||, atol) */
   int finite;
   double seconds;               /* device time of the solve (CUDA events) */
 } jxb_stats;
@@ -141,8 +144,9 @@ int jxb_apply_f32(jxb_plan* plan, jxb_stream stream, const float* x, float* y);
  *   JXB_ERR_INVALID. This call allocates nothing. Its first call on a device
  *   looks up the array's address (cudaGetSymbolAddress) and should come before
  *   any stream capture. All calls share the array: calls that overlap on the
- *   GPU race and must be ordered on one stream. No counterpart in the
- *   reference, which has no device kernels. */
+ *   GPU race and must be ordered on one stream. The plan's device (current
+ *   when the plan was created) must be current; otherwise JXB_ERR_INVALID.
+ *   No counterpart in the reference, which has no device kernels. */
 int jxb_apply_static(jxb_plan* plan, jxb_stream stream, const double* x, double* y, int masked);
 int jxb_diag(jxb_plan* plan, jxb_stream stream, double* d);
 
@@ -166,6 +170,14 @@ int jxb_qp_weights(jxb_plan* plan, jxb_stream stream, double* w);
  *   src/jaxiga/solvers/linear.py:399-442): stop when ||r||^2 <= max(tol^2 ||b||^2, atol^2).
  *   b is a full-length vector; its prescribed entries are ignored and x is 0
  *   there on return. Stats carry the FP64 true residual (diagnostics.py:8-19).
+ *   With opts->restarts > 0, a solve whose FP64 true residual is still above
+ *   the tolerance when CG stops restarts CG on that residual (tolerance
+ *   min(0.5, 0.5 tol ||b|| / ||r||)) and adds the correction, at most
+ *   `restarts` times, keeping only corrections that lower the true residual;
+ *   stats->outer counts them.
+ *   Every solve below writes x and stats and then returns JXB_ERR_NOT_CONVERGED
+ *   when the true residual misses the tolerance (iteration cap, stagnation),
+ *   JXB_ERR_NONFINITE when a reduction met NaN/Inf, else JXB_OK.
  * jxb_refine_solve: FP64 iterative refinement around FP32 Jacobi-PCG inner solves
  *   (jxb_apply_f32); the outer residual and correction are FP64.
  * jxb_mixed_pcg: FP32 Jacobi-PCG with reliable FP64 updates. The FP32 iterate

@@ -72,6 +72,7 @@ class SolveOpts(ctypes.Structure):
         ("check_every", ctypes.c_int),
         ("inner_tol", ctypes.c_double),
         ("max_outer", ctypes.c_int),
+        ("restarts", ctypes.c_int),
     ]
 
 
@@ -175,3 +176,16 @@ def check(code):
         msg = load().jxb_last_error()
         raise JxbError(code, msg.decode() if msg else "")
     return code
+
+
+NOT_CONVERGED, NONFINITE = 3, 4
+
+
+def check_solve(code, raise_on_nonfinite=False):
+    """Status of a solve entry point. The solves write x and the stats before
+    returning JXB_ERR_NOT_CONVERGED or JXB_ERR_NONFINITE; both are reported
+    through the stats (the reference's diagnostics report a failed solve the
+    same way), so only the other codes raise, and NONFINITE when asked."""
+    if code == NOT_CONVERGED or (code == NONFINITE and not raise_on_nonfinite):
+        return code
+    return check(code)

@@ -149,8 +149,7 @@ class BatchSolver:
         secs = ctypes.c_double()
         rc = self.batch.lib.jxb_batch_pcg(self.batch.handle, _s(), _p(self.b), _p(x), ctypes.byref(o), stats,
                                           ctypes.byref(secs))
-        if rc not in (0, 4):
-            _lib.check(rc)
+        _lib.check_solve(rc)
         off = self.batch.offsets
         xs = [x[off[i]: off[i + 1]] for i in range(n)]
         st = [{k: getattr(stats[i], k) for k, _ in _lib.Stats._fields_} for i in range(n)]

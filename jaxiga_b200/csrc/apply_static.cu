@@ -22,7 +22,11 @@
 //
 // The device address of the array is looked up with cudaGetSymbolAddress on
 // the first call on each device, with that device current; that first call
-// should therefore be made before any stream capture begins.
+// should therefore be made before any stream capture begins. The plan's
+// device (the one current when the plan was created) must be current at
+// every call; a call made with another device current is refused with
+// JXB_ERR_INVALID instead of running the plan's buffers against that
+// device's array.
 #include <mutex>
 
 #include "jxb_internal.cuh"
@@ -62,6 +66,14 @@ extern "C" int jxb_apply_static(jxb_plan* plan, jxb_stream stream, const double*
                      "jxb_apply_static: this plan needs " + std::to_string(need) +
                          " bytes of brick scratch, more than the fixed " +
                          std::to_string((size_t)JXB_STATIC_SCRATCH_BYTES) + "-byte array; use jxb_apply");
+  // The address below belongs to the current device; the plan's buffers to
+  // the device that was current when it was created. Refuse a mismatch.
+  int dev = 0;
+  JXB_CUDA(cudaGetDevice(&dev));
+  if (dev != plan->device)
+    return jxb::fail(JXB_ERR_INVALID, "jxb_apply_static: the plan was created on device " +
+                                          std::to_string(plan->device) + " but device " + std::to_string(dev) +
+                                          " is current; make the plan's device current first");
   double* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;

@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <map>
+#include <set>
+#include <string>
 #include <vector>
 
 #include "jxb_internal.cuh"
@@ -258,8 +260,17 @@ using namespace jxb;
 extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) {
   if (!plans || n < 1 || !out) return fail(JXB_ERR_INVALID, "jxb_batch_create: bad argument");
   *out = nullptr;
+  // Every instance writes its brick partial sums into its own plan's scratch
+  // inside the shared launches, so a plan listed twice would race with itself.
+  // (checked on the pointers alone, before any plan is read)
+  std::set<const jxb_plan*> seen;
   for (int i = 0; i < n; ++i) {
     if (!plans[i]) return fail(JXB_ERR_INVALID, "jxb_batch_create: null plan");
+    if (!seen.insert(plans[i]).second)
+      return fail(JXB_ERR_INVALID, "jxb_batch_create: plan " + std::to_string(i) +
+                                       " appears more than once; create one plan per instance");
+  }
+  for (int i = 0; i < n; ++i) {
     if (plans[i]->dim != 2 || plans[i]->op != JXB_OP_POISSON)
       return fail(JXB_ERR_INVALID, "jxb_batch_create: batches take 2D Poisson plans");
     if (plans[i]->rational != plans[0]->rational)
@@ -273,9 +284,15 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
   for (int i = 0; i < n; ++i) B->off[i + 1] = B->off[i] + plans[i]->n_dofs;
   B->total = B->off[n];
   auto fail_b = [&](int code) {
+    if (B->stream) cudaStreamSynchronize(B->stream);
     free_batch(B);
     return code;
   };
+#define JXB_CUDA_B(call)                                         \
+  do {                                                           \
+    cudaError_t _e = (call);                                     \
+    if (_e != cudaSuccess) return fail_b(cuda_fail(_e, #call)); \
+  } while (0)
   const size_t N = (size_t)B->total;
   cudaError_t e = cudaSuccess;
   auto al = [&](void** p, size_t bytes) {
@@ -315,7 +332,7 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
     f.first = std::max(f.first, P->br.fp[0]);
     f.second = std::max(f.second, P->br.fp[1]);
     // keep mask of this instance into the concatenated mask
-    JXB_CUDA(cudaMemcpyAsync(B->d_keep + B->off[i], P->d_keep, P->n_dofs, cudaMemcpyDeviceToDevice, s));
+    JXB_CUDA_B(cudaMemcpyAsync(B->d_keep + B->off[i], P->d_keep, P->n_dofs, cudaMemcpyDeviceToDevice, s));
   }
   for (auto& kv : work) {
     jxb_batch::Group g;
@@ -329,26 +346,27 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
     });
     g.n_work = (long long)kv.second.size();
     if ((e = cudaMalloc(&g.d_work, g.n_work * sizeof(int2))) != cudaSuccess) return fail_b(cuda_fail(e, "cudaMalloc"));
-    JXB_CUDA(cudaMemcpyAsync(g.d_work, kv.second.data(), g.n_work * sizeof(int2), cudaMemcpyHostToDevice, s));
+    JXB_CUDA_B(cudaMemcpyAsync(g.d_work, kv.second.data(), g.n_work * sizeof(int2), cudaMemcpyHostToDevice, s));
     B->groups.push_back(g);
   }
-  JXB_CUDA(cudaMemcpyAsync(B->d_off, B->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
-  JXB_CUDA(cudaMemcpyAsync(B->d_brs, brs.data(), n * sizeof(Bricks), cudaMemcpyHostToDevice, s));
-  JXB_CUDA(cudaMemcpyAsync(B->d_scratch, scr.data(), n * sizeof(double*), cudaMemcpyHostToDevice, s));
-  JXB_CUDA(cudaMemcpyAsync(B->d_args_p, ap.data(), n * sizeof(BrickArgs<double>), cudaMemcpyHostToDevice, s));
-  JXB_CUDA(cudaMemcpyAsync(B->d_args_x, ax.data(), n * sizeof(BrickArgs<double>), cudaMemcpyHostToDevice, s));
+  JXB_CUDA_B(cudaMemcpyAsync(B->d_off, B->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+  JXB_CUDA_B(cudaMemcpyAsync(B->d_brs, brs.data(), n * sizeof(Bricks), cudaMemcpyHostToDevice, s));
+  JXB_CUDA_B(cudaMemcpyAsync(B->d_scratch, scr.data(), n * sizeof(double*), cudaMemcpyHostToDevice, s));
+  JXB_CUDA_B(cudaMemcpyAsync(B->d_args_p, ap.data(), n * sizeof(BrickArgs<double>), cudaMemcpyHostToDevice, s));
+  JXB_CUDA_B(cudaMemcpyAsync(B->d_args_x, ax.data(), n * sizeof(BrickArgs<double>), cudaMemcpyHostToDevice, s));
   // Jacobi inverse diagonal of every instance, concatenated
   for (int i = 0; i < n; ++i) {
     jxb_plan* P = plans[i];
     int rc = ensure_workspace(P, false);
     if (rc) return fail_b(rc);
     if ((rc = compute_invdiag(P, s))) return fail_b(rc);
-    JXB_CUDA(cudaMemcpyAsync(B->d_inv + B->off[i], P->d_invdiag, P->n_dofs * sizeof(double),
+    JXB_CUDA_B(cudaMemcpyAsync(B->d_inv + B->off[i], P->d_invdiag, P->n_dofs * sizeof(double),
                              cudaMemcpyDeviceToDevice, s));
   }
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail_b(cuda_fail(e, "jxb_batch_create"));
   *out = B;
   return JXB_OK;
+#undef JXB_CUDA_B
 }
 
 extern "C" int jxb_batch_destroy(jxb_batch* B) {
@@ -378,10 +396,9 @@ extern "C" int jxb_batch_pcg(jxb_batch* B, jxb_stream stream, const double* b, d
   if (!B || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_batch_pcg: null argument");
   cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
   cudaStream_t s = B->stream;
-  cudaEvent_t ev, e0, e1;
-  JXB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
+  SolveEvents evs;
+  if (int rc0 = evs.create()) return rc0;
+  cudaEvent_t ev = evs.order, e0 = evs.e0, e1 = evs.e1;
   JXB_CUDA(cudaEventRecord(ev, user));
   JXB_CUDA(cudaStreamWaitEvent(s, ev, 0));
   const int n = B->n;
@@ -443,27 +460,22 @@ extern "C" int jxb_batch_pcg(jxb_batch* B, jxb_stream stream, const double* b, d
   JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   JXB_CUDA(cudaEventRecord(ev, s));
   JXB_CUDA(cudaStreamWaitEvent(user, ev, 0));
-  cudaEventDestroy(ev);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if (seconds) *seconds = ms * 1e-3;
-  int worst = JXB_OK;
+  int nonfinite = -1, unconverged = -1;
   for (int i = 0; i < n; ++i) {
     const double rn = sqrt(h[3 * i]), bn = sqrt(h[3 * i + 1]);
     const bool fin = h[3 * i + 2] == 0 && isfinite(rn);
-    if (stats) {
-      jxb_stats& st = stats[i];
-      st.iterations = B->h_states[i].k;
-      st.outer = 0;
-      st.residual = rn;
-      st.b_norm = bn;
-      st.relative_residual = rn / (bn > 0 ? bn : 1.0);
-      st.finite = fin ? 1 : 0;
-      st.converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
-      st.seconds = ms * 1e-3;
-    }
-    if (B->h_states[i].status == JXB_ERR_NONFINITE) worst = JXB_ERR_NONFINITE;
+    jxb_stats one;
+    const int st = finish_solve("jxb_batch_pcg", &one, B->h_states[i].k, 0, rn, bn, fin, opts->tol, opts->atol, ms,
+                                B->h_states[i].status == JXB_ERR_NONFINITE);
+    if (stats) stats[i] = one;
+    if (st == JXB_ERR_NONFINITE && nonfinite < 0) nonfinite = i;
+    if (st == JXB_ERR_NOT_CONVERGED && unconverged < 0) unconverged = i;
   }
-  if (worst == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_batch_pcg: non-finite value in an instance");
+  if (nonfinite >= 0)
+    return fail(JXB_ERR_NONFINITE, "jxb_batch_pcg: non-finite value in instance " + std::to_string(nonfinite));
+  if (unconverged >= 0)
+    return fail(JXB_ERR_NOT_CONVERGED, "jxb_batch_pcg: instance " + std::to_string(unconverged) +
+                                           " (and maybe others) missed the tolerance; see its stats");
   return JXB_OK;
 }

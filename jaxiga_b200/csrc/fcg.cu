@@ -646,13 +646,13 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
   cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
   if (!plan->graph_stream[1]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[1], cudaStreamNonBlocking));
   cudaStream_t s = plan->graph_stream[1];
-  cudaEvent_t e0, e1, evu;
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
-  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
+  SolveEvents ev;
+  int rc = ev.create();
+  if (rc) return rc;
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1, evu = ev.order;
   JXB_CUDA(cudaEventRecord(evu, user));
   JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
-  int rc = ensure_workspace(plan, mixed != 0);
+  rc = ensure_workspace(plan, mixed != 0);
   if (rc) return rc;
   rc = compute_invdiag(plan, s);
   if (rc) return rc;
@@ -768,21 +768,8 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
   JXB_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
   JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(evu);
-  if (stats) {
-    stats->iterations = total;
-    stats->outer = R.learned_iters;
-    stats->residual = rn;
-    stats->b_norm = bn;
-    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
-    stats->finite = (fin && isfinite(rn)) ? 1 : 0;
-    stats->converged = (stats->finite && rn <= opts->tol * bn) ? 1 : 0;
-    stats->seconds = ms * 1e-3;
-  }
-  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_fcg_learned: non-finite value or breakdown");
-  return JXB_OK;
+  return finish_solve("jxb_fcg_learned", stats, total, R.learned_iters, rn, bn, fin, opts->tol, opts->atol, ms,
+                      status == JXB_ERR_NONFINITE);
 }
 
 extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in,

@@ -9,8 +9,9 @@
 //   * Per-point factors ("geo") are stored element-slot-major in brick order:
 //     slot = ((brick * layers + layer) * elems_per_layer + e_in_layer), and
 //     per slot [factor k][quadrature point q] with q first-direction fastest.
-//     One layer of a brick is therefore one contiguous tile, which the apply
-//     kernel streams into shared memory with a bulk asynchronous copy.
+//     One layer of a brick is therefore one contiguous tile: the apply kernels
+//     prefetch the next layer's tile into L2 (cp.async.bulk.prefetch.L2) and
+//     read it with coalesced loads.
 //   * The brick's footprint partial sums go to a scratch buffer; a combine
 //     pass sums, per control point, the (at most JXB_MAXC per direction)
 //     bricks that cover it, always in the same order.
@@ -79,6 +80,26 @@ struct Material {
   double lam, mu;  // elasticity (effective plane lambda in 2D)
 };
 
+// CUDA events of one solve call (two timing events and one ordering event),
+// destroyed on every return path.
+struct SolveEvents {
+  cudaEvent_t e0 = nullptr, e1 = nullptr, order = nullptr;
+  SolveEvents() = default;
+  SolveEvents(const SolveEvents&) = delete;
+  SolveEvents& operator=(const SolveEvents&) = delete;
+  ~SolveEvents() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (order) cudaEventDestroy(order);
+  }
+  int create() {
+    JXB_CUDA(cudaEventCreate(&e0));
+    JXB_CUDA(cudaEventCreate(&e1));
+    JXB_CUDA(cudaEventCreateWithFlags(&order, cudaEventDisableTiming));
+    return JXB_OK;
+  }
+};
+
 // Solver state for one Krylov loop, resident in device memory.
 struct CgState {
   double gamma;    // r . z
@@ -132,6 +153,7 @@ constexpr int TILE2[N_TILE2][2] = {{32, 8}, {16, 8}, {32, 16}, {64, 4}};
 }  // namespace jxb
 
 struct jxb_plan {
+  int device = 0;  // the CUDA device that was current at creation; its buffers live there
   int dim, vec, p, q, op, rational, order, plane_strain;
   int n_span[3], n_cp[3];
   long long n_elem, n_scalar, n_dofs, n_free, n_qp, nqe;
@@ -162,6 +184,8 @@ struct jxb_plan {
          *d_Ap = nullptr, *d_invdiag = nullptr;
   float *d_x32 = nullptr, *d_r32 = nullptr, *d_z32 = nullptr, *d_p32 = nullptr, *d_Ap32 = nullptr,
         *d_invdiag32 = nullptr;
+  // true-residual restarts of jxb_pcg: accumulated solution and FP64 residual
+  double *d_xacc = nullptr, *d_res = nullptr;
   jxb::CgState* d_state = nullptr;
   jxb::CgState* h_state = nullptr;  // pinned
   bool diag_valid = false;
@@ -205,6 +229,11 @@ int dot(jxb_plan* plan, cudaStream_t s, const double* a, const double* b, double
 // not null; blocks until the norms are on the host
 int true_residual(jxb_plan* plan, cudaStream_t s, const double* b, const double* x, double* res_out, double* rnorm,
                   double* bnorm, bool* finite);
+// Writes the stats of a finished solve and returns its status:
+// JXB_ERR_NONFINITE (nonfinite), JXB_ERR_NOT_CONVERGED (true residual above
+// max(tol ||b||, atol)) or JXB_OK.
+int finish_solve(const char* who, jxb_stats* stats, long long iters, long long outer, double rn, double bn, bool fin,
+                 double tol, double atol, float ms, bool nonfinite);
 
 // cnn.cu (the network of the learned preconditioner)
 int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4);

@@ -13,7 +13,9 @@
 // graph launch. All reductions use a fixed grid and a fixed summation order,
 // so results are bitwise reproducible run to run.
 #include <math.h>
+#include <stdio.h>
 
+#include <string>
 #include <vector>
 
 #include "jxb_internal.cuh"
@@ -412,88 +414,155 @@ static int iterate(jxb_plan* plan, cudaStream_t s, long long maxiter, int precon
 
 using namespace jxb;
 
+namespace jxb {
+
+__global__ void k_add(long long n, const double* a, const double* b, double* out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+
+int finish_solve(const char* who, jxb_stats* stats, long long iters, long long outer, double rn, double bn, bool fin,
+                 double tol, double atol, float ms, bool nonfinite) {
+  // the stopping rule of jax's CG: ||r|| <= max(tol ||b||, atol)
+  const bool conv = fin && isfinite(rn) && rn <= fmax(tol * bn, atol);
+  if (stats) {
+    stats->iterations = iters;
+    stats->outer = outer;
+    stats->residual = rn;
+    stats->b_norm = bn;
+    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
+    stats->finite = (fin && isfinite(rn)) ? 1 : 0;
+    stats->converged = conv ? 1 : 0;
+    stats->seconds = ms * 1e-3;
+  }
+  if (nonfinite) return fail(JXB_ERR_NONFINITE, std::string(who) + ": non-finite value in the Krylov reductions");
+  if (!conv) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s: not converged (true residual %.3e > %.3e after %lld iterations)", who, rn,
+             fmax(tol * bn, atol), iters);
+    return fail(JXB_ERR_NOT_CONVERGED, buf);
+  }
+  return JXB_OK;
+}
+
+// Solve-local stream set-up shared by the entry points: plan stream `slot`
+// created on first use, ordered after the caller's stream.
+static int enter_stream(jxb_plan* plan, int slot, cudaStream_t user, SolveEvents& ev, cudaStream_t* out) {
+  if (!plan->graph_stream[slot])
+    JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[slot], cudaStreamNonBlocking));
+  int rc = ev.create();
+  if (rc) return rc;
+  JXB_CUDA(cudaEventRecord(ev.order, user));
+  JXB_CUDA(cudaStreamWaitEvent(plan->graph_stream[slot], ev.order, 0));
+  *out = plan->graph_stream[slot];
+  return JXB_OK;
+}
+
+// Hands the plan stream's work back to the caller's stream and reads the
+// device time between e0 and e1.
+static int leave_stream(cudaStream_t s, cudaStream_t user, SolveEvents& ev, float* ms) {
+  JXB_CUDA(cudaEventRecord(ev.order, s));
+  JXB_CUDA(cudaStreamWaitEvent(user, ev.order, 0));
+  JXB_CUDA(cudaEventSynchronize(ev.e1));
+  JXB_CUDA(cudaEventElapsedTime(ms, ev.e0, ev.e1));
+  return JXB_OK;
+}
+
+}  // namespace jxb
+
 extern "C" int jxb_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                        const jxb_solve_opts* opts, jxb_stats* stats) {
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_pcg: null argument");
   if (!(opts->tol > 0) || !isfinite(opts->tol)) return fail(JXB_ERR_INVALID, "jxb_pcg: tol must be finite and positive");
-  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
-  cudaStream_t s = plan->graph_stream[0];
-  if (!s) {
-    JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[0], cudaStreamNonBlocking));
-    s = plan->graph_stream[0];
-  }
-  cudaEvent_t e0, e1, evu;
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
-  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
-  JXB_CUDA(cudaEventRecord(evu, user));
-  JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
-  int rc = ensure_workspace(plan, false);
+  if (opts->restarts < 0 || opts->restarts > 8) return fail(JXB_ERR_INVALID, "jxb_pcg: restarts must be in 0..8");
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream), s = nullptr;
+  SolveEvents ev;
+  int rc = enter_stream(plan, 0, user, ev, &s);
   if (rc) return rc;
-  int precond = opts->preconditioner ? 1 : 0;
-  if (precond) {
-    rc = compute_invdiag(plan, s);
-    if (rc) return rc;
-  }
-  long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
-  int every = opts->check_every > 0 ? opts->check_every : 16;
-  JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, plan->n_dofs * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  JXB_CUDA(cudaEventRecord(e0, s));
+  if ((rc = ensure_workspace(plan, false))) return rc;
+  const int precond = opts->preconditioner ? 1 : 0;
+  if (precond && (rc = compute_invdiag(plan, s))) return rc;
+  const long long n = plan->n_dofs;
+  const long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
+  const int every = opts->check_every > 0 ? opts->check_every : 16;
+  JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  JXB_CUDA(cudaEventRecord(ev.e0, s));
   long long iters = 0;
   int status = 0;
-  rc = run_cg<double, double>(plan, s, plan->d_b, opts->tol, opts->atol, maxiter, precond, every, &iters, &status);
-  if (rc) return rc;
-  JXB_CUDA(cudaEventRecord(e1, s));
-  JXB_CUDA(cudaMemcpyAsync(x, plan->d_x, plan->n_dofs * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  double rn, bn;
-  bool fin;
-  rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin);
-  if (rc) return rc;
-  float ms = 0;
-  JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  JXB_CUDA(cudaEventRecord(evu, s));
-  JXB_CUDA(cudaStreamWaitEvent(user, evu, 0));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(evu);
-  if (stats) {
-    stats->iterations = iters;
-    stats->outer = 0;
-    stats->residual = rn;
-    stats->b_norm = bn;
-    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
-    stats->finite = fin ? 1 : 0;
-    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
-    stats->seconds = ms * 1e-3;
+  if ((rc = run_cg<double, double>(plan, s, plan->d_b, opts->tol, opts->atol, maxiter, precond, every, &iters,
+                                   &status)))
+    return rc;
+  double rn = 0, bn = 0;
+  bool fin = true;
+  long long restarts = 0;
+  if (opts->restarts == 0 || status == JXB_ERR_NONFINITE) {
+    JXB_CUDA(cudaEventRecord(ev.e1, s));
+    JXB_CUDA(cudaMemcpyAsync(x, plan->d_x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if ((rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin))) return rc;
+  } else {
+    // True-residual restarts (the correction solves of the reference's CPU
+    // CG, src/jaxiga/solvers/linear.py:261-321): CG's recursive residual
+    // drifts from b - K x on ill-conditioned operators, so the FP64 residual
+    // of the accumulated solution is the right-hand side of another CG solve
+    // whenever it is still above the target; a correction is kept only if it
+    // lowers the true residual, and all solves share the iteration budget.
+    if (!plan->d_xacc) JXB_CUDA(cudaMalloc(&plan->d_xacc, n * sizeof(double)));
+    if (!plan->d_res) JXB_CUDA(cudaMalloc(&plan->d_res, n * sizeof(double)));
+    JXB_CUDA(cudaMemcpyAsync(plan->d_xacc, plan->d_x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if ((rc = true_residual(plan, s, plan->d_b, plan->d_xacc, plan->d_res, &rn, &bn, &fin))) return rc;
+    const double target = fmax(opts->tol * bn, opts->atol);
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    while (restarts < opts->restarts && fin && rn > target && iters < maxiter) {
+      long long it = 0;
+      int st = 0;
+      if ((rc = run_cg<double, double>(plan, s, plan->d_res, fmin(0.5, 0.5 * target / rn), 0.0, maxiter - iters,
+                                       precond, every, &it, &st)))
+        return rc;
+      iters += it;
+      ++restarts;
+      if (st == JXB_ERR_NONFINITE) {
+        status = JXB_ERR_NONFINITE;
+        break;
+      }
+      // candidate in d_z, its residual in d_r (both free once CG has stopped)
+      k_add<<<nb, 256, 0, s>>>(n, plan->d_xacc, plan->d_x, plan->d_z);
+      JXB_CUDA(cudaGetLastError());
+      double rn_new = 0, bn_new = 0;
+      bool fin_new = true;
+      if ((rc = true_residual(plan, s, plan->d_b, plan->d_z, plan->d_r, &rn_new, &bn_new, &fin_new))) return rc;
+      if (!fin_new || !(rn_new < rn)) break;  // stagnation: keep the previous solution
+      JXB_CUDA(cudaMemcpyAsync(plan->d_xacc, plan->d_z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      JXB_CUDA(cudaMemcpyAsync(plan->d_res, plan->d_r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      rn = rn_new;
+    }
+    JXB_CUDA(cudaEventRecord(ev.e1, s));
+    JXB_CUDA(cudaMemcpyAsync(x, plan->d_xacc, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
-  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_pcg: non-finite value in CG reductions");
-  return JXB_OK;
+  float ms = 0;
+  if ((rc = leave_stream(s, user, ev, &ms))) return rc;
+  return finish_solve("jxb_pcg", stats, iters, restarts, rn, bn, fin, opts->tol, opts->atol, ms,
+                      status == JXB_ERR_NONFINITE);
 }
 
 extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                                 const jxb_solve_opts* opts, jxb_stats* stats) {
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_refine_solve: null argument");
   if (!plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_refine_solve: plan was created without want_f32");
-  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
-  if (!plan->graph_stream[0]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[0], cudaStreamNonBlocking));
-  cudaStream_t s = plan->graph_stream[0];
-  cudaEvent_t e0, e1, evu;
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
-  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
-  JXB_CUDA(cudaEventRecord(evu, user));
-  JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
-  int rc = ensure_workspace(plan, true);
+  if (!(opts->tol > 0) || !isfinite(opts->tol))
+    return fail(JXB_ERR_INVALID, "jxb_refine_solve: tol must be finite and positive");
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream), s = nullptr;
+  SolveEvents ev;
+  int rc = enter_stream(plan, 0, user, ev, &s);
   if (rc) return rc;
-  rc = compute_invdiag(plan, s);
-  if (rc) return rc;
+  if ((rc = ensure_workspace(plan, true))) return rc;
+  if ((rc = compute_invdiag(plan, s))) return rc;
   long long n = plan->n_dofs;
   // d_b: rhs, d_r: FP64 residual, d_z: FP64 iterate (d_x/d_r/d_z of the FP64 CG are free here)
   double* xb = plan->d_z;
   double* res = plan->d_r;
   JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   JXB_CUDA(cudaMemsetAsync(xb, 0, n * sizeof(double), s));
-  JXB_CUDA(cudaEventRecord(e0, s));
+  JXB_CUDA(cudaEventRecord(ev.e0, s));
   double inner = opts->inner_tol > 0 ? opts->inner_tol : 1e-4;
   int max_outer = opts->max_outer > 0 ? opts->max_outer : 30;
   long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
@@ -503,23 +572,21 @@ extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double*
   double rn = 0, bn = 0;
   bool fin = true;
   int status = JXB_OK;
-  rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
-  if (rc) return rc;
-  while (outer < max_outer && fin && rn > opts->tol * bn && total_it < maxiter) {
+  if ((rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin))) return rc;
+  const double target = fmax(opts->tol * bn, opts->atol);
+  while (outer < max_outer && fin && rn > target && total_it < maxiter) {
     // normalised residual as the FP32 right-hand side; Ap32 holds it until the
     // CG init kernel has copied it into r32 (iterations overwrite Ap32 later)
     float* rhs32 = plan->d_Ap32;
     k_scale_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, res, 1.0 / rn, rhs32);
     long long it = 0;
     int st = 0;
-    rc = run_cg<float, float>(plan, s, rhs32, inner, 0.0, maxiter - total_it, 1, every, &it, &st);
-    if (rc) return rc;
+    if ((rc = run_cg<float, float>(plan, s, rhs32, inner, 0.0, maxiter - total_it, 1, every, &it, &st))) return rc;
     total_it += it;
     k_axpy_from_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rn, plan->d_x32, xb);
     JXB_CUDA(cudaGetLastError());
     double prev = rn;
-    rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
-    if (rc) return rc;
+    if ((rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin))) return rc;
     ++outer;
     if (st == JXB_ERR_NONFINITE) {
       status = JXB_ERR_NONFINITE;
@@ -527,28 +594,12 @@ extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double*
     }
     if (!(rn < prev)) break;  // stagnation: stop, the stats report it
   }
-  JXB_CUDA(cudaEventRecord(e1, s));
+  JXB_CUDA(cudaEventRecord(ev.e1, s));
   JXB_CUDA(cudaMemcpyAsync(x, xb, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  JXB_CUDA(cudaEventRecord(evu, s));
-  JXB_CUDA(cudaStreamWaitEvent(user, evu, 0));
-  JXB_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
-  JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(evu);
-  if (stats) {
-    stats->iterations = total_it;
-    stats->outer = outer;
-    stats->residual = rn;
-    stats->b_norm = bn;
-    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
-    stats->finite = fin ? 1 : 0;
-    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
-    stats->seconds = ms * 1e-3;
-  }
-  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_refine_solve: non-finite value in inner CG");
-  return JXB_OK;
+  if ((rc = leave_stream(s, user, ev, &ms))) return rc;
+  return finish_solve("jxb_refine_solve", stats, total_it, outer, rn, bn, fin, opts->tol, opts->atol, ms,
+                      status == JXB_ERR_NONFINITE);
 }
 
 // FP32 Jacobi-PCG with reliable updates (Sleijpen and van der Vorst, 1996):
@@ -565,25 +616,18 @@ extern "C" int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b,
   if (!plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: plan was created without want_f32");
   if (!(opts->tol > 0) || !isfinite(opts->tol))
     return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: tol must be finite and positive");
-  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
-  if (!plan->graph_stream[0]) JXB_CUDA(cudaStreamCreateWithFlags(&plan->graph_stream[0], cudaStreamNonBlocking));
-  cudaStream_t s = plan->graph_stream[0];
-  cudaEvent_t e0, e1, evu;
-  JXB_CUDA(cudaEventCreate(&e0));
-  JXB_CUDA(cudaEventCreate(&e1));
-  JXB_CUDA(cudaEventCreateWithFlags(&evu, cudaEventDisableTiming));
-  JXB_CUDA(cudaEventRecord(evu, user));
-  JXB_CUDA(cudaStreamWaitEvent(s, evu, 0));
-  int rc = ensure_workspace(plan, true);
+  cudaStream_t user = reinterpret_cast<cudaStream_t>(stream), s = nullptr;
+  SolveEvents ev;
+  int rc = enter_stream(plan, 0, user, ev, &s);
   if (rc) return rc;
-  rc = compute_invdiag(plan, s);
-  if (rc) return rc;
+  if ((rc = ensure_workspace(plan, true))) return rc;
+  if ((rc = compute_invdiag(plan, s))) return rc;
   long long n = plan->n_dofs;
   double* xb = plan->d_z;   // FP64 solution
   double* res = plan->d_r;  // FP64 residual at the last update
   JXB_CUDA(cudaMemcpyAsync(plan->d_b, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   JXB_CUDA(cudaMemsetAsync(xb, 0, n * sizeof(double), s));
-  JXB_CUDA(cudaEventRecord(e0, s));
+  JXB_CUDA(cudaEventRecord(ev.e0, s));
   const double delta = opts->inner_tol > 0 ? opts->inner_tol : 1e-2;
   const int max_updates = opts->max_outer > 0 ? opts->max_outer : 1000;
   const long long maxiter = opts->maxiter > 0 ? opts->maxiter : 10 * plan->n_free;
@@ -592,28 +636,26 @@ extern "C" int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b,
   int updates = 0, status = JXB_OK;
   double rn = 0, bn = 0;
   bool fin = true;
-  rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
-  if (rc) return rc;
+  if ((rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin))) return rc;
+  const double target = fmax(opts->tol * bn, opts->atol);
   double rn_seg = rn;  // residual norm the FP32 vectors are scaled by
-  while (updates < max_updates && fin && rn > opts->tol * bn && total_it < maxiter) {
+  while (updates < max_updates && fin && rn > target && total_it < maxiter) {
     const float ratio = updates == 0 ? 1.f : (float)(rn_seg / rn);
     k_ru_restart<<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(n, res, plan->d_keep, plan->d_invdiag32, 1.0 / rn,
                                                             ratio, updates == 0, plan->d_x32, plan->d_r32,
                                                             plan->d_z32, plan->d_p32, plan->d_red);
     rn_seg = rn;
     // the FP32 segment stops at the update threshold or at the target, whichever comes first
-    const double seg_tol = fmax(delta, opts->tol * bn / rn);
+    const double seg_tol = fmax(delta, target / rn);
     k_cg_init_fin<<<1, JXB_RED_THREADS, 0, s>>>(plan->d_state, plan->d_red, seg_tol, 0.0, maxiter - total_it);
     JXB_CUDA(cudaGetLastError());
     long long it = 0;
     int st = 0;
-    rc = iterate<float>(plan, s, maxiter - total_it, 1, every, &it, &st, nullptr, 0, nullptr);
-    if (rc) return rc;
+    if ((rc = iterate<float>(plan, s, maxiter - total_it, 1, every, &it, &st, nullptr, 0, nullptr))) return rc;
     total_it += it;
     k_axpy_from_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rn_seg, plan->d_x32, xb);
     JXB_CUDA(cudaGetLastError());
-    rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin);
-    if (rc) return rc;
+    if ((rc = true_residual(plan, s, plan->d_b, xb, res, &rn, &bn, &fin))) return rc;
     ++updates;
     if (st == JXB_ERR_NONFINITE) {
       status = JXB_ERR_NONFINITE;
@@ -621,28 +663,12 @@ extern "C" int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b,
     }
     if (!(rn < rn_seg)) break;  // no progress in FP32: stop, the stats report it
   }
-  JXB_CUDA(cudaEventRecord(e1, s));
+  JXB_CUDA(cudaEventRecord(ev.e1, s));
   JXB_CUDA(cudaMemcpyAsync(x, xb, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  JXB_CUDA(cudaEventRecord(evu, s));
-  JXB_CUDA(cudaStreamWaitEvent(user, evu, 0));
-  JXB_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
-  JXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(evu);
-  if (stats) {
-    stats->iterations = total_it;
-    stats->outer = updates;
-    stats->residual = rn;
-    stats->b_norm = bn;
-    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
-    stats->finite = fin ? 1 : 0;
-    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
-    stats->seconds = ms * 1e-3;
-  }
-  if (status == JXB_ERR_NONFINITE) return fail(JXB_ERR_NONFINITE, "jxb_mixed_pcg: non-finite value in FP32 CG");
-  return JXB_OK;
+  if ((rc = leave_stream(s, user, ev, &ms))) return rc;
+  return finish_solve("jxb_mixed_pcg", stats, total_it, updates, rn, bn, fin, opts->tol, opts->atol, ms,
+                      status == JXB_ERR_NONFINITE);
 }
 
 extern "C" int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host) {
@@ -680,15 +706,6 @@ extern "C" int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double
   if ((rc = true_residual(plan, s, plan->d_b, plan->d_x, nullptr, &rn, &bn, &fin))) return rc;
   JXB_CUDA(cudaStreamSynchronize(s));
   *n_snaps = ns;
-  if (stats) {
-    stats->iterations = iters;
-    stats->outer = 0;
-    stats->residual = rn;
-    stats->b_norm = bn;
-    stats->relative_residual = rn / (bn > 0 ? bn : 1.0);
-    stats->finite = fin ? 1 : 0;
-    stats->converged = (fin && rn <= opts->tol * bn) ? 1 : 0;
-    stats->seconds = 0;
-  }
-  return status == JXB_ERR_NONFINITE ? fail(JXB_ERR_NONFINITE, "jxb_pcg_snapshots: non-finite") : JXB_OK;
+  return finish_solve("jxb_pcg_snapshots", stats, iters, 0, rn, bn, fin, opts->tol, opts->atol, 0.f,
+                      status == JXB_ERR_NONFINITE);
 }

@@ -57,7 +57,7 @@ static void free_plan(jxb_plan* p) {
   void* bufs[] = {p->d_geo, p->d_geo32, p->d_wq, p->d_invW, p->d_cpts, p->d_wgts, p->d_wgts32,
                   p->d_keep, p->d_scratch, p->d_scratch32, p->d_red, p->d_x, p->d_b, p->d_r,
                   p->d_z, p->d_p, p->d_Ap, p->d_invdiag, p->d_x32, p->d_r32, p->d_z32, p->d_p32,
-                  p->d_Ap32, p->d_invdiag32, p->d_state};
+                  p->d_Ap32, p->d_invdiag32, p->d_xacc, p->d_res, p->d_state};
   for (void* b : bufs) cudaFree(b);
   if (p->h_state) cudaFreeHost(p->h_state);
   for (int i = 0; i < 2; ++i) {
@@ -112,7 +112,10 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
   *out = nullptr;
   int rc = validate(desc);
   if (rc) return rc;
+  int device = 0;
+  JXB_CUDA(cudaGetDevice(&device));
   jxb_plan* P = new jxb_plan();
+  P->device = device;
   P->dim = desc->dim;
   P->vec = desc->vec;
   P->p = desc->degree;

@@ -145,8 +145,9 @@ class LearnedPreconditioner:
         o = op._opts(tol, 0.0, maxiter, "jacobi", every, 0.0, 0)
         st = _lib.Stats()
         ns = ctypes.c_int64()
-        _lib.check(self.lib.jxb_pcg_snapshots(op.handle, _s(), _p(b), _p(x), ctypes.byref(o), int(every),
-                                              _p(snaps), int(n_pairs), ctypes.byref(ns), ctypes.byref(st)))
+        _lib.check_solve(self.lib.jxb_pcg_snapshots(op.handle, _s(), _p(b), _p(x), ctypes.byref(o), int(every),
+                                                    _p(snaps), int(n_pairs), ctypes.byref(ns), ctypes.byref(st)),
+                         raise_on_nonfinite=True)
         m = min(ns.value + 1, int(n_pairs))
         R = torch.empty((m, self.vec, self.ncp), dtype=torch.float32, device=self.dev)
         E = torch.empty_like(R)
@@ -330,8 +331,7 @@ class LearnedPreconditioner:
                                       float(self.in_scale), float(out_scale), int(stall), int(depth),
                                       (1 if mixed else 0) | (2 if mult else 0) | (8 if additive else 0)
                                       | (4 if refinement == "restart" else 0), ctypes.byref(o), ctypes.byref(st))
-        if rc not in (0, 4):
-            _lib.check(rc)
+        _lib.check_solve(rc)
         out = {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
         out["learned_iterations"] = out.pop("outer")
         return x, out

@@ -219,7 +219,7 @@ class Operator:
         return r.value
 
     # -- solves ---------------------------------------------------------------
-    def _opts(self, tol, atol, maxiter, preconditioner, check_every, inner_tol, max_outer):
+    def _opts(self, tol, atol, maxiter, preconditioner, check_every, inner_tol, max_outer, restarts=0):
         o = _lib.SolveOpts()
         o.tol = float(tol)
         o.atol = float(atol)
@@ -228,17 +228,23 @@ class Operator:
         o.check_every = int(check_every)
         o.inner_tol = float(inner_tol)
         o.max_outer = int(max_outer)
+        o.restarts = int(restarts)
         return o
 
-    def pcg(self, b, tol=1e-12, atol=0.0, maxiter=None, preconditioner="jacobi", check_every=16, raise_on_nonfinite=False):
-        """Jacobi-PCG from x = 0 (jax CG semantics); returns (x, stats dict)."""
+    def pcg(self, b, tol=1e-12, atol=0.0, maxiter=None, preconditioner="jacobi", check_every=16, restarts=0,
+            raise_on_nonfinite=False):
+        """Jacobi-PCG from x = 0 (jax CG semantics); returns (x, stats dict).
+
+        ``restarts`` > 0: when the FP64 true residual misses the tolerance after
+        CG stopped, restart CG on it (at most that many times, sharing
+        ``maxiter``), as the reference's CPU CG does; stats["outer"] counts them.
+        """
         b = self._vec(b)
         x = self._empty(self.n_dofs)
         st = _lib.Stats()
-        o = self._opts(tol, atol, maxiter, preconditioner, check_every, 0.0, 0)
+        o = self._opts(tol, atol, maxiter, preconditioner, check_every, 0.0, 0, restarts)
         rc = self.lib.jxb_pcg(self.handle, _stream(), _dptr(b), _dptr(x), ctypes.byref(o), ctypes.byref(st))
-        if rc != 0 and (rc != 4 or raise_on_nonfinite):
-            _lib.check(rc)
+        _lib.check_solve(rc, raise_on_nonfinite)
         return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
 
     def refine_solve(self, b, tol=1e-8, inner_tol=1e-4, maxiter=None, max_outer=40, check_every=16):
@@ -250,8 +256,7 @@ class Operator:
         st = _lib.Stats()
         o = self._opts(tol, 0.0, maxiter, "jacobi", check_every, inner_tol, max_outer)
         rc = self.lib.jxb_refine_solve(self.handle, _stream(), _dptr(b), _dptr(x), ctypes.byref(o), ctypes.byref(st))
-        if rc not in (0, 4):
-            _lib.check(rc)
+        _lib.check_solve(rc)
         return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
 
     def mixed_pcg(self, b, tol=1e-8, delta=1e-2, maxiter=None, max_updates=1000, check_every=16):
@@ -265,6 +270,5 @@ class Operator:
         st = _lib.Stats()
         o = self._opts(tol, 0.0, maxiter, "jacobi", check_every, delta, max_updates)
         rc = self.lib.jxb_mixed_pcg(self.handle, _stream(), _dptr(b), _dptr(x), ctypes.byref(o), ctypes.byref(st))
-        if rc not in (0, 4):
-            _lib.check(rc)
+        _lib.check_solve(rc)
         return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}

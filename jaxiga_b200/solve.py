@@ -39,6 +39,18 @@ class LinearOptions:
     direction) or ``"restart"`` (FP64 iterative refinement around FP32 inner
     solves to ``inner_tol``). ``check_every`` is the iterations per captured
     CUDA graph launch between host convergence checks.
+
+    ``restarts``: FP64 CG restarts on the true residual when CG's recursive
+    residual met ``tol`` but b - K u did not (at most this many, sharing
+    ``maxiter``), the correction solves of the reference's CPU CG
+    (solvers/linear.py:261-321).
+
+    ``preconditioner="learned"`` runs flexible CG with the trained network of
+    ``checkpoint`` (see ``jaxiga_b200.learned``), Jacobi as its fallback;
+    ``learned_map`` picks how the network output n enters: ``"network"`` (n
+    alone), ``"multiplicative"`` (n, then a Jacobi step on the remaining
+    residual) or ``"additive"`` (n + D^-1 r). With ``precision="mixed"`` the
+    flexible CG runs in FP32 with FP64 corrections.
     """
 
     method: str = "cg"
@@ -53,6 +65,10 @@ class LinearOptions:
     check_every: int = 16
     refinement: str = "reliable"
     update_delta: float = 1e-2
+    restarts: int = 3
+    checkpoint: str | None = None
+    learned_map: str = "additive"
+    learned_stall: int = 50
 
     def __post_init__(self):
         if not np.isfinite(self.tol) or self.tol <= 0:
@@ -63,8 +79,18 @@ class LinearOptions:
         allowed = {"cg", "bicgstab", "gmres", "dense", "scipy"}
         if self.method not in allowed:
             raise ValueError(f"unknown linear method {self.method!r}; expected one of {allowed}")
-        if self.preconditioner not in {"none", "jacobi"}:
-            raise ValueError(f"unknown preconditioner {self.preconditioner!r}; expected 'none' or 'jacobi'")
+        if self.preconditioner not in {"none", "jacobi", "learned"}:
+            raise ValueError(f"unknown preconditioner {self.preconditioner!r}; expected 'none', 'jacobi' or 'learned'")
+        if self.preconditioner == "learned" and not self.checkpoint:
+            raise ValueError("preconditioner='learned' needs checkpoint=<path of a trained network (.npz)>")
+        if self.learned_map not in {"network", "multiplicative", "additive"}:
+            raise ValueError(f"learned_map must be 'network', 'multiplicative' or 'additive', got {self.learned_map!r}")
+        if (isinstance(self.restarts, (bool, np.bool_)) or not isinstance(self.restarts, (int, np.integer))
+                or not 0 <= self.restarts <= 8):
+            raise ValueError("restarts must be an integer in 0..8")
+        if isinstance(self.learned_stall, (bool, np.bool_)) or not isinstance(self.learned_stall, (int, np.integer)) \
+                or self.learned_stall < 1:
+            raise ValueError("learned_stall must be a positive integer")
         orderings = {"auto", "NATURAL", "MMD_ATA", "MMD_AT_PLUS_A", "COLAMD"}
         if self.superlu_ordering not in orderings:
             raise ValueError(f"unknown SuperLU ordering {self.superlu_ordering!r}; expected one of {orderings}")
@@ -126,29 +152,58 @@ class Solution:
         return g.interpolate(u).cpu().numpy()
 
 
-def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptions | None = None,
-          initial_guess=None, **method_opts):
-    """Solve a linear problem by the Galerkin method on the GPU."""
-    import torch
+# at most this many device operators stay cached per space (each holds the
+# per-point factors of one operator, up to a few GB at the largest sizes)
+OPERATOR_CACHE_SIZE = 2
 
-    if method != "galerkin":
-        raise NotImplementedError(f"method={method!r}: the B200 backend implements 'galerkin' only")
-    if not problem.is_linear:
-        raise NotImplementedError("the B200 backend solves linear problems only")
-    if problem.neumann:
-        raise NotImplementedError("Neumann loads are not applied by the B200 backend")
-    if problem.quadrature is not None and problem.quadrature != problem.space.degree[0] + 1:
-        raise NotImplementedError("the B200 backend uses the default p+1 Gauss rule")
-    if linear is None:
-        linear = default_linear(problem)
-    if linear.method != "cg":
-        raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG")
+
+def _digest(a):
+    """Content key of an array (or None) for the operator cache."""
+    if a is None:
+        return None
+    import hashlib
+
+    a = np.ascontiguousarray(a)
+    return (a.shape, a.dtype.str, hashlib.blake2b(a.view(np.uint8).reshape(-1), digest_size=16).hexdigest())
+
+
+def cached_operator(space, op_name, coef, prescribed_mask=None, coef_qp=None, want_f32=False, plane_strain=False):
+    """The device operator of (space, operator, coefficients, Dirichlet set),
+    built once and reused by later solves on the same space: the per-point
+    factors, the Jacobi diagonal and the captured CG graphs persist across
+    calls. Least recently used operators beyond ``OPERATOR_CACHE_SIZE`` are
+    released."""
+    from collections import OrderedDict
+
+    cache = space._plans.setdefault("operators", OrderedDict())
+    key = (op_name, tuple(float(c) for c in coef), _digest(coef_qp), _digest(prescribed_mask), bool(plane_strain))
+    op = cache.get(key)
+    if op is not None and op.handle is not None and (op.want_f32 or not want_f32):
+        cache.move_to_end(key)
+        return op
+    if op is not None:
+        cache.pop(key).close()
+    op = Operator(space, op_name, coef, prescribed=prescribed_mask, coef_qp=coef_qp, want_f32=want_f32,
+                  plane_strain=plane_strain)
+    cache[key] = op
+    while len(cache) > OPERATOR_CACHE_SIZE:
+        cache.popitem(last=False)[1].close()
+    return op
+
+
+def release_operators(space):
+    """Free the device operators cached on ``space`` by earlier solves."""
+    for op in space._plans.pop("operators", {}).values():
+        op.close()
+
+
+def _problem_operator(problem, params, want_f32):
+    """Dirichlet partition and cached device operator of a linear problem."""
     space = problem.space
     n = space.n_dofs
     prescribed, values = problem.resolve_dirichlet(params)
     mask = np.zeros(n, dtype=bool)
     mask[prescribed] = True
-
     coef, field = problem.operator_coefficients(params)
     coef_qp = None
     if field is not None:
@@ -157,34 +212,95 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         else:
             x = qp_points(space)
             coef_qp = call_points(field, x, flat_params(params, x.shape[0])).reshape(-1)
-    op = Operator(space, problem.op, coef, prescribed=mask, coef_qp=coef_qp,
-                  want_f32=linear.precision == "mixed", plane_strain=getattr(problem, "plane", "stress") == "strain")
-    try:
-        F = torch.zeros(n, dtype=torch.float64, device=op.device)
-        if problem.source is not None:
-            x = qp_points(space)
-            f = call_points(problem.source, x, flat_params(params, x.shape[0]))
-            f = np.broadcast_to(f.reshape(x.shape[0], -1), (x.shape[0], space.vec))
-            F = op.load(np.array(f, dtype=np.float64, copy=True))
-        b = F
-        g = np.zeros(n)
-        g[prescribed] = values
-        if np.any(values != 0):
-            b = F - op.apply(g, masked=False)
-        if linear.precision == "mixed" and linear.refinement == "reliable":
-            xdev, st = op.mixed_pcg(b, tol=linear.tol, delta=linear.update_delta, maxiter=linear.maxiter,
-                                    check_every=linear.check_every)
-        elif linear.precision == "mixed":
-            xdev, st = op.refine_solve(b, tol=linear.tol, inner_tol=linear.inner_tol, maxiter=linear.maxiter,
-                                       check_every=linear.check_every)
-        else:
-            xdev, st = op.pcg(b, tol=linear.tol, maxiter=linear.maxiter, preconditioner=linear.preconditioner,
-                              check_every=linear.check_every)
-        if len(prescribed):
-            xdev[torch.as_tensor(prescribed, device=op.device)] = torch.as_tensor(values, device=op.device)
-        u = xdev.cpu().numpy()
-    finally:
-        op.close()
+    op = cached_operator(space, problem.op, coef, mask, coef_qp, want_f32,
+                         getattr(problem, "plane", "stress") == "strain")
+    return op, prescribed, values
+
+
+def _rhs(problem, params, op, prescribed, values):
+    """b = F - K_fp g on the device (methods/galerkin.py:240-245)."""
+    import torch
+
+    space = problem.space
+    n = space.n_dofs
+    F = torch.zeros(n, dtype=torch.float64, device=op.device)
+    if problem.source is not None:
+        x = qp_points(space)
+        f = call_points(problem.source, x, flat_params(params, x.shape[0]))
+        f = np.broadcast_to(f.reshape(x.shape[0], -1), (x.shape[0], space.vec))
+        F = op.load(np.array(f, dtype=np.float64, copy=True))
+    g = np.zeros(n)
+    g[prescribed] = values
+    if np.any(values != 0):
+        F = F - op.apply(g, masked=False)
+    return F
+
+
+def _check_problem(problem, method):
+    if method != "galerkin":
+        raise NotImplementedError(f"method={method!r}: the B200 backend implements 'galerkin' only")
+    if not problem.is_linear:
+        raise NotImplementedError("the B200 backend solves linear problems only")
+    if problem.neumann:
+        raise NotImplementedError("Neumann loads are not applied by the B200 backend")
+    if problem.quadrature is not None and problem.quadrature != problem.space.degree[0] + 1:
+        raise NotImplementedError("the B200 backend uses the default p+1 Gauss rule")
+
+
+def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptions | None = None,
+          initial_guess=None, features=None, **method_opts):
+    """Solve a linear problem by the Galerkin method on the GPU.
+
+    ``problem`` may also be a list of problems (with ``params`` a list of the
+    same length), or ``params`` a list of parameter dicts for one problem: the
+    B200 form of the reference's ``jax.vmap`` over ``solve``. The instances
+    (2D Poisson, constant a0 per instance, homogeneous Dirichlet data) are then
+    solved together, every CG iteration of all of them in one captured CUDA
+    graph, and a list of Solutions is returned.
+
+    ``features``: static per-control-point input channels of a learned
+    preconditioner (for example a normalised log-permeability), shape
+    (n_features, n_control_points); only read with ``preconditioner="learned"``.
+    """
+    if isinstance(problem, (list, tuple)) or isinstance(params, (list, tuple)):
+        return _solve_batch(problem, params, linear, method)
+    import torch
+
+    _check_problem(problem, method)
+    if linear is None:
+        linear = default_linear(problem)
+    if linear.method != "cg":
+        raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG")
+    space = problem.space
+    n = space.n_dofs
+    op, prescribed, values = _problem_operator(problem, params, linear.precision == "mixed")
+    b = _rhs(problem, params, op, prescribed, values)
+    if linear.preconditioner == "learned":
+        from .learned import LearnedPreconditioner
+
+        lp = LearnedPreconditioner.from_checkpoint(op, linear.checkpoint, features=features)
+        try:
+            two = {"network": False, "multiplicative": "multiplicative", "additive": "additive"}[linear.learned_map]
+            reliable = linear.refinement == "reliable"
+            xdev, st = lp.solve(b, tol=linear.tol, maxiter=linear.maxiter, stall=linear.learned_stall,
+                                mixed=linear.precision == "mixed", two_level=two, refinement=linear.refinement,
+                                inner_tol=linear.update_delta if reliable else linear.inner_tol,
+                                check_every=linear.check_every)
+        finally:
+            lp.close()
+        st["outer"] = st["learned_iterations"]
+    elif linear.precision == "mixed" and linear.refinement == "reliable":
+        xdev, st = op.mixed_pcg(b, tol=linear.tol, delta=linear.update_delta, maxiter=linear.maxiter,
+                                check_every=linear.check_every)
+    elif linear.precision == "mixed":
+        xdev, st = op.refine_solve(b, tol=linear.tol, inner_tol=linear.inner_tol, maxiter=linear.maxiter,
+                                   check_every=linear.check_every)
+    else:
+        xdev, st = op.pcg(b, tol=linear.tol, maxiter=linear.maxiter, preconditioner=linear.preconditioner,
+                          check_every=linear.check_every, restarts=linear.restarts)
+    if len(prescribed):
+        xdev[torch.as_tensor(prescribed, device=op.device)] = torch.as_tensor(values, device=op.device)
+    u = xdev.cpu().numpy()
     stats = {
         "method": "galerkin",
         "linear": linear.method,
@@ -199,12 +315,54 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         "outer": int(st["outer"]),
         "seconds": st["seconds"],
         "precision": linear.precision,
+        "preconditioner": linear.preconditioner,
         "refinement": linear.refinement if linear.precision == "mixed" else None,
     }
     if not stats["converged"]:
         warnings.warn(f"linear Galerkin solve did not converge (residual {stats['residual']:.3e}); "
                       "do not use this result for implicit sensitivities", RuntimeWarning, stacklevel=2)
     return Solution(space=space, u=u, params=params, problem=problem, stats=stats, u_device=xdev)
+
+
+def _solve_batch(problems, params, linear, method):
+    """Many independent instances in one device batch (``BatchSolver``)."""
+    from .batch import BatchSolver
+
+    if isinstance(problems, (list, tuple)):
+        problems = list(problems)
+        params = list(params) if isinstance(params, (list, tuple)) else [params] * len(problems)
+    else:
+        params = list(params)
+        problems = [problems] * len(params)
+    if len(problems) != len(params):
+        raise ValueError(f"{len(problems)} problems but {len(params)} parameter sets")
+    if not problems:
+        return []
+    for pr in problems:
+        _check_problem(pr, method)
+    linear = linear or default_linear(problems[0])
+    if linear.method != "cg" or linear.preconditioner != "jacobi" or linear.precision != "fp64":
+        raise NotImplementedError("batched solves run FP64 Jacobi-PCG")
+    bs = BatchSolver(problems, params)
+    try:
+        xs, sts, secs = bs.solve(tol=linear.tol, maxiter=linear.maxiter, check_every=linear.check_every)
+        out = []
+        for pr, pa, x, st in zip(problems, params, xs, sts):
+            u = x.cpu().numpy().copy()
+            stats = {"method": "galerkin", "linear": "cg", "matrix_free": True,
+                     "n_free": int(pr.space.n_dofs - len(pr.resolve_dirichlet(pa)[0])), "nnz": None,
+                     "residual": st["residual"], "relative_residual": st["relative_residual"],
+                     "converged": bool(st["converged"]), "finite": bool(st["finite"]),
+                     "iterations": int(st["iterations"]), "outer": 0, "seconds": secs, "batched": len(problems),
+                     "precision": "fp64", "preconditioner": "jacobi", "refinement": None}
+            out.append(Solution(space=pr.space, u=u, params=pa, problem=pr, stats=stats, u_device=x.clone()))
+    finally:
+        bs.close()
+    bad = [i for i, so in enumerate(out) if not so.stats["converged"]]
+    if bad:
+        warnings.warn(f"{len(bad)} of {len(out)} batched solves did not converge (first: instance {bad[0]})",
+                      RuntimeWarning, stacklevel=3)
+    return out
 
 
 def _exact_at(exact, x):

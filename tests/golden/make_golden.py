@@ -1,9 +1,10 @@
 """Generate golden fixtures from the reference JAXIGA code.
 
-Run in a container where the reference sources are mounted (read-only) at
-``/root/reference``:
+Run where the reference sources are available (read-only is enough), giving
+the reference checkout's root as an argument or in ``JAXIGA_REFERENCE``:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
+    JAXIGA_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 jax/jaxlib are not installed there, so the reference's setup stage and its
 basis evaluation / element kernels run under the NumPy stand-in in
@@ -41,8 +42,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import _jax_stub  # noqa: E402
 
-REF_SRC = "/root/reference/src"
 SEED = 20260901
+
+
+def reference_src(argv=None):
+    """``src`` directory of the reference checkout named on the command line
+    or by ``JAXIGA_REFERENCE``."""
+    argv = sys.argv[1:] if argv is None else argv
+    root = argv[0] if argv else os.environ.get("JAXIGA_REFERENCE")
+    if not root:
+        raise SystemExit("usage: make_golden.py <reference checkout> (or set JAXIGA_REFERENCE)")
+    src = os.path.join(root, "src")
+    if not os.path.isdir(os.path.join(src, "jaxiga")):
+        raise SystemExit(f"{src} holds no jaxiga package")
+    return src
 
 
 def sha(a):
@@ -51,7 +64,7 @@ def sha(a):
 
 
 def main():
-    m = _jax_stub.load_reference(REF_SRC)
+    m = _jax_stub.load_reference(reference_src())
     prim, fs, P, ev = m["primitives"], m["function_space"], m["pointset"], m["evaluation"]
     prob_mod, lib, lin, common, gal = m["problem"], m["library"], m["linear"], m["_common"], m["galerkin"]
     bern = m["bernstein"]

@@ -193,3 +193,43 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(out[cname]) == ctypes.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert int(out[f"{cname}.{fname}"]) == getattr(cls, fname).offset, f"{cname}.{fname}"
+
+
+def test_batch_rejects_a_plan_listed_twice():
+    """A plan given twice would share its brick scratch inside one launch; the
+    pointers are checked before any plan is read, so a stand-in pointer works."""
+    lib = _lib.load()
+    buf = ctypes.create_string_buffer(64)
+    fake = ctypes.cast(buf, ctypes.c_void_p).value
+    arr = (ctypes.c_void_p * 2)(fake, fake)
+    out = ctypes.c_void_p()
+    assert lib.jxb_batch_create(arr, 2, ctypes.byref(out)) == 1
+    assert b"more than once" in lib.jxb_last_error()
+    assert out.value is None
+
+
+def test_solve_status_codes_map_to_stats():
+    """NOT_CONVERGED and NONFINITE come back with x and stats written: they are
+    reported through the stats, every other code raises."""
+    assert _lib.check_solve(0) == 0
+    assert _lib.check_solve(3) == 3
+    assert _lib.check_solve(4) == 4
+    with pytest.raises(_lib.JxbError):
+        _lib.check_solve(4, raise_on_nonfinite=True)
+    with pytest.raises(_lib.JxbError):
+        _lib.check_solve(1)
+
+
+def test_linear_options_learned_and_restarts():
+    import jaxiga_b200 as jx
+
+    with pytest.raises(ValueError, match="checkpoint"):
+        jx.LinearOptions(preconditioner="learned")
+    o = jx.LinearOptions(preconditioner="learned", checkpoint="net.npz", learned_map="multiplicative")
+    assert o.learned_map == "multiplicative"
+    with pytest.raises(ValueError, match="learned_map"):
+        jx.LinearOptions(preconditioner="learned", checkpoint="net.npz", learned_map="other")
+    for bad in (-1, 9, 1.5, True):
+        with pytest.raises(ValueError, match="restarts"):
+            jx.LinearOptions(restarts=bad)
+    assert jx.LinearOptions().restarts == 3
