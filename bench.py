@@ -11,17 +11,31 @@ free DOFs) of the 3D linear-elasticity workload: unit cube, cubic NURBS,
 CUDA events, barrier + synchronize on both sides). ``e2e`` is the same metric
 through the C ABI with host buffers: pinned host u -> device, apply, device
 y -> pinned host, every step. ``time_to_solution`` gives the solves to a
-1e-8 relative residual: plain FP64 Jacobi-PCG and FP32-inner / FP64-refined,
-and, when jaxiga_b200/checkpoints holds a trained network for the workload
+1e-8 true relative residual: plain FP64 Jacobi-PCG (with the reference CPU
+CG's true-residual restarts), the two mixed-precision schemes and, when
+jaxiga_b200/checkpoints holds a trained network for the workload
 (``python -m jaxiga_b200.train_pc``), flexible CG with the learned
-preconditioner in FP64 and as FP32 inner solves in FP64 refinement.
+preconditioner in every map.
 
-``--impl reference`` times the reference's CPU path for the same metric on a
-bounded sample (SciPy CSR K.u on an assembled 10^3-element instance, the
-matvec inside src/jaxiga/solvers/linear.py:261-321), single-threaded.
+On one GPU the same line also carries, under ``workloads``, the other
+benchmark configurations measured the same way (apply DOF/s, roofline and
+time to solution): Darcy 96^3 with a lognormal random coefficient, the
+clamped Kirchhoff plate 256^2, and 256 uneven quarter-annulus Poisson
+instances solved as one batch.
+
+``cpu_baseline`` times the reference's CPU path on the host cores: SciPy's
+CSR K.u and its Jacobi-CG with true-residual restarts
+(src/jaxiga/solvers/linear.py:261-321, restated in the oracle) on the same
+elasticity workload at 16^3 elements -- the 64^3 assembled operator is
+infeasible on a CPU (its element matrices alone are 77 GB) -- next to the
+GPU's time to solution at that same size.
+
+``--impl reference`` times that CPU path alone for the headline metric: each
+step one SciPy CSR K.u of the 16^3 sample; the line adds its time to solution.
 
 With ``--gpus N > 1`` (torchrun) every rank runs an independent replica of
-the workload (weak scaling; the single-patch apply does not exchange data).
+the headline workload (weak scaling; the single-patch apply does not
+exchange data).
 """
 
 from __future__ import annotations
@@ -41,7 +55,8 @@ sys.path.insert(0, ROOT)
 METRIC = "time-to-1e-8 residual & K·u DOF/s: mixed+learned vs plain FP64 PCG, 1 B200"
 UNIT = "DOF/s"
 N_SPAN = 64
-CPU_SAMPLE_SPAN = 10
+CPU_SAMPLE_SPAN = 16
+TOL = 1e-8
 
 
 def parse():
@@ -52,6 +67,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-solution runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extra", action="store_true", help="skip the Darcy / plate / batch rows")
     ap.add_argument("--span", type=int, default=None, help="elements per direction (default 64, Darcy 96)")
     ap.add_argument("--workload", default="elasticity", choices=["elasticity", "darcy", "plate", "batch"],
                     help="elasticity: 3D elasticity 64^3 (the headline); darcy: 3D Darcy 96^3; plate: Kirchhoff "
@@ -150,20 +166,45 @@ def profile_traffic(workload, span):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's CPU matvec (SciPy CSR) on an assembled sample
+# CPU baseline: the reference's CPU path (SciPy CSR K.u and Jacobi-CG with
+# true-residual restarts) on the elasticity workload at a feasible size
 # ---------------------------------------------------------------------------
+INFEASIBLE = ("64^3 elements assembled on a CPU is infeasible: 262,144 element matrices of 192 x 192 "
+              "(77 GB), a 38.7 GB int32 scatter map and ~1 h of CSR-pattern construction")
+
+
+def host_info():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_count": os.cpu_count(), "cpu_model": model,
+            "threads_env": {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                                           "MKL_NUM_THREADS")},
+            "note": "SciPy's CSR matvec and CG run on one thread (the reference's CPU CG calls them)"}
+
+
 def cpu_sample(span=CPU_SAMPLE_SPAN):
+    """The elasticity workload at ``span``^3 assembled by the oracle, with its
+    load vector (body force plus the interpolated random field)."""
     from jaxiga_b200 import workloads
     from oracle import iga_oracle as O
 
+    t0 = time.perf_counter()
     V, problem, params = workloads.config2(n=span)
     pres, vals = problem.resolve_dirichlet(params)
     S = O.Space(V.knots, V.degree, V.cpts, V.wgts, 3)
-    A = O.Assembled(S, "elasticity", {"E": 1.0, "nu": 0.3}, pres, vals, need_full=False)
-    return V, A
+    fq = O.interpolate_qp(S, params["eta"]) + np.array([0.0, 0.0, -1.0])
+    A = O.Assembled(S, "elasticity", {"E": 1.0, "nu": 0.3}, pres, vals, source_qp=fq, need_full=False)
+    return V, A, time.perf_counter() - t0
 
 
-def time_cpu_matvec(A, n_dofs, seconds=10.0, min_reps=3, max_reps=None):
+def time_cpu_matvec(A, n_dofs, seconds=5.0, min_reps=3):
     x = np.random.default_rng(0).standard_normal(A.K.shape[0])
     A.K @ x
     reps, t0 = 0, time.perf_counter()
@@ -171,24 +212,42 @@ def time_cpu_matvec(A, n_dofs, seconds=10.0, min_reps=3, max_reps=None):
         A.K @ x
         reps += 1
         el = time.perf_counter() - t0
-        if (el >= seconds and reps >= min_reps) or (max_reps and reps >= max_reps):
+        if el >= seconds and reps >= min_reps:
             break
     return n_dofs * reps / el, reps, el
 
 
-def cpu_baseline(seconds=10.0):
-    V, A = cpu_sample()
-    v, reps, el = time_cpu_matvec(A, V.n_dofs, seconds)
+def cpu_time_to_solution(A, runs=3):
+    """Warm median of ``runs`` SciPy Jacobi-CG solves to TOL (the reference's
+    restart logic), with the true relative residual of the last."""
+    from oracle import iga_oracle as O
+
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        u, it = O.scipy_cg(A.K, A.b, TOL)
+        times.append(time.perf_counter() - t0)
+    rel = float(np.linalg.norm(A.b - A.K @ u) / np.linalg.norm(A.b))
+    return {"seconds": float(np.median(times)), "runs": runs, "iterations": int(it), "relative_residual": rel,
+            "converged": rel <= TOL}
+
+
+def cpu_baseline():
+    V, A, setup = cpu_sample()
+    v, reps, el = time_cpu_matvec(A, V.n_dofs)
+    tts = cpu_time_to_solution(A)
     return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"3D elasticity, cubic, {CPU_SAMPLE_SPAN}^3 elements ({V.n_dofs} DOFs, nnz {A.K.nnz}); "
-                      f"SciPy CSR K.u of the assembled operator (reference CPU CG matvec), {reps} reps in {el:.1f} s, "
-                      f"1 thread; assembly excluded"}
+            "sample": f"3D elasticity workload at {CPU_SAMPLE_SPAN}^3 elements ({V.n_dofs} DOFs, nnz {A.K.nnz}); "
+                      f"SciPy CSR K.u of the oracle-assembled operator, {reps} reps in {el:.1f} s, one thread; "
+                      f"assembly ({setup:.1f} s) excluded; {INFEASIBLE}",
+            "span": CPU_SAMPLE_SPAN, "n_dofs": V.n_dofs, "assembly_seconds": setup,
+            "time_to_solution": tts, "host": host_info()}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    V, A = cpu_sample()
+    V, A, setup = cpu_sample()
     x = np.random.default_rng(0).standard_normal(A.K.shape[0])
     for _ in range(args.warmup):
         A.K @ x
@@ -197,14 +256,18 @@ def run_reference(args, rank, world):
         A.K @ x
     el = time.perf_counter() - t0
     value = V.n_dofs * args.steps / el
+    tts = cpu_time_to_solution(A)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"elasticity3d_p3_{CPU_SAMPLE_SPAN}^3 (bounded CPU sample of the 64^3 workload)",
-                   "n_dofs": V.n_dofs, "nnz": int(A.K.nnz), "operator": "assembled CSR (SciPy)"},
+                   "n_dofs": V.n_dofs, "nnz": int(A.K.nnz), "operator": "assembled CSR (SciPy)",
+                   "full_size": INFEASIBLE, "assembly_seconds": setup},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"SciPy CSR K.u, {CPU_SAMPLE_SPAN}^3-element elasticity instance, single thread"},
+                         "sample": f"SciPy CSR K.u, {CPU_SAMPLE_SPAN}^3-element elasticity workload, one thread",
+                         "host": host_info()},
+        "time_to_solution": {"tol": TOL, "scipy_jacobi_cg_true_residual_restarts": tts},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -213,45 +276,201 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
+def build_workload(name, span, dev):
+    """(space, operator, load vector, learned-network features, points per element)."""
     import torch
-    import torch.distributed as dist
 
     import jaxiga_b200 as jx
     from jaxiga_b200 import workloads
     from jaxiga_b200.solve import geometry_operator
 
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    t_setup = time.perf_counter()
-    darcy = args.workload == "darcy"
-    plate = args.workload == "plate"
-    span = args.span or (96 if darcy else 256 if plate else N_SPAN)
-    if plate:
+    if name == "plate":
         V, problem, params = workloads.config5(n=span)
-        pres, vals = problem.resolve_dirichlet(params)
+        pres, _ = problem.resolve_dirichlet(params)
         mask = np.zeros(V.n_dofs, bool)
         mask[pres] = True
         op = jx.Operator(V, "plate", problem.operator_coefficients(params)[0], prescribed=mask, want_f32=True)
-    elif darcy:
+        nqe = 25
+        F = op.load(torch.ones(V.n_elems * nqe, dtype=torch.float64, device=dev))
+        return V, op, F, None, nqe
+    if name == "darcy":
         V, problem, params = workloads.config4(n=span)
-        geo0 = geometry_operator(V)
-        a_qp = torch.exp(geo0.interpolate(params["loga"])[..., 0])
-        pres, vals = problem.resolve_dirichlet(params)
+        a_qp = torch.exp(geometry_operator(V).interpolate(params["loga"])[..., 0])
+        pres, _ = problem.resolve_dirichlet(params)
         mask = np.zeros(V.n_dofs, bool)
         mask[pres] = True
         op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a_qp.cpu().numpy(), want_f32=True)
         del a_qp
+        F = op.load(torch.ones(V.n_elems * 64, dtype=torch.float64, device=dev))
+        loga = params["loga"]
+        return V, op, F, ((loga - loga.mean()) / loga.std())[None, :], 64
+    V, problem, params = workloads.config2(n=span)
+    pres, _ = problem.resolve_dirichlet(params)
+    mask = np.zeros(V.n_dofs, bool)
+    mask[pres] = True
+    op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
+    fq = geometry_operator(V).interpolate(params["eta"])
+    fq[..., 2] -= 1.0
+    F = op.load(fq)
+    return V, op, F, None, 64
+
+
+def workload_tag(name, span):
+    return f"plate2d_p4_{span}^2" if name == "plate" else f"{'darcy3d' if name == 'darcy' else 'elasticity3d'}_p3_{span}^3"
+
+
+def roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span):
+    """Per-kernel device times (CUDA events on the launching stream) and the
+    HBM roofline of the brick kernel: algorithmic bytes = u and y once plus the
+    per-point factors, 8 (2 N_dof + N_qp n_geo)."""
+    n = V.n_dofs
+    ms_bricks, ms_combine = op.profile_apply(x, reps=50)
+    ms_b32, _ = op.profile_apply(x.float(), reps=50, f32=True)
+    ngeo = op.info["ngeo"]
+    alg_bytes = 8 * 2 * n + 8 * n_qp * ngeo
+    alg_bytes32 = 4 * 2 * n + 4 * n_qp * ngeo
+    # n_e vec 2*2*d^2 (p+1)^(d+1) + N_qp c_pt, c_pt = 2 d^4 (elasticity) or 2 d^2 (scalar)
+    if name == "plate":  # 2D, p = 4: x 2.5 for the Hessian channels, 2 * 15 per point
+        flops = int(V.n_elems * 2 * 2 * 4 * 5**3 * 2.5 + n_qp * 2 * 15)
     else:
-        V, problem, params = workloads.config2(n=span)
-        pres, vals = problem.resolve_dirichlet(params)
-        mask = np.zeros(V.n_dofs, bool)
-        mask[pres] = True
-        op = jx.Operator(V, "elasticity", (1.0, 0.3), prescribed=mask, want_f32=True)
+        flops = V.n_elems * V.vec * (2 * 2 * 9 * 4**3 * 4) + n_qp * (2 * 81 if V.vec == 3 else 2 * 9)
+    achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
+    traffic = profile_traffic(name, span)
+    mma = os.environ.get("JXB_BRICK3_MMA", "1") != "0"
+    kernel = ("k_brick2<double,4,5,plate> (brick apply)" if name == "plate" else
+              "k_brick3_mma (FP64 mma.sync brick apply, %s p=3)" % ("poisson" if name == "darcy" else "elasticity")
+              if mma else "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if name == "darcy" else "elasticity"))
+    return {
+        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+        "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"), "kernel": kernel,
+        "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
+        "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
+        "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
+    }
+
+
+def _row(st, ref_x=None, x=None):
+    import torch
+
+    r = {"seconds": st["seconds"], "iterations": int(st["iterations"]),
+         "relative_residual": st["relative_residual"], "converged": bool(st["converged"])}
+    if ref_x is not None and x is not None:
+        r["relative_difference_to_plain"] = float(torch.linalg.norm(x - ref_x) / torch.linalg.norm(ref_x))
+    return r
+
+
+def time_to_solution(name, span, op, F, feats):
+    """Solves to TOL, each run twice and the second reported (the first
+    captures its CUDA graphs); speed-ups only for solves that converged."""
+    tts = {"tol": TOL}
+    for _ in range(2):
+        x_p, st_p = op.pcg(F, tol=TOL, preconditioner="jacobi", check_every=32, maxiter=80000, restarts=3)
+    tts["plain_fp64_jacobi_pcg"] = dict(_row(st_p), restarts=int(st_p["outer"]))
+    t_plain = st_p["seconds"] if st_p["converged"] else None
+    rows = {}
+    if name == "plate":
+        rows["mixed"] = {"not_run": "the FP32 operator cannot resolve the biharmonic plate (condition number "
+                                    "times FP32 rounding > 1): its mixed form keeps the FP64 operator and puts "
+                                    "FP32 only in the preconditioner (the learned rows)"}
+    else:
+        for _ in range(2):
+            x_m, st_m = op.refine_solve(F, tol=TOL, inner_tol=1e-3, check_every=32, maxiter=80000)
+        rows["mixed_fp32_inner_fp64_refinement"] = dict(_row(st_m, x_p, x_m), outer=int(st_m["outer"]))
+        for _ in range(2):
+            x_r, st_r = op.mixed_pcg(F, tol=TOL, delta=1e-2, check_every=32, maxiter=80000)
+        rows["mixed_fp32_pcg_reliable_fp64_updates"] = dict(_row(st_r, x_p, x_r), updates=int(st_r["outer"]))
+    tts.update(rows)
+    tts["learned_preconditioner"] = None
+    ckpt = os.path.join(ROOT, "jaxiga_b200", "checkpoints", f"{name}{span}.npz")
+    if os.path.exists(ckpt):
+        from jaxiga_b200.learned import LearnedPreconditioner
+
+        lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
+        lrows = {}
+        # FP32 operator rows only where the FP32 operator resolves the problem
+        variants = [("learned_fcg_fp64", False, False), ("learned_two_level_fp64", False, True),
+                    ("learned_additive_fp64", False, "additive")]
+        if name != "plate":
+            variants += [("mixed_learned_fcg", True, False), ("mixed_learned_two_level", True, True),
+                         ("mixed_learned_additive", True, "additive")]
+        for key, mixed, two in variants:
+            lp.solve(F, tol=TOL, mixed=mixed, two_level=two)
+            x_l, st_l = lp.solve(F, tol=TOL, mixed=mixed, two_level=two)
+            lrows[key] = dict(_row(st_l, x_p, x_l), learned_iterations=int(st_l["learned_iterations"]))
+        tts["learned_preconditioner"] = {
+            "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
+            "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
+            "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **lrows}
+        rows.update(lrows)
+        lp.close()
+    for k, v in rows.items():
+        if isinstance(v, dict) and "seconds" in v:
+            tts[f"speedup_{k}_vs_plain"] = (t_plain / v["seconds"] if t_plain and v["converged"] else None)
+    best = [(k, v) for k, v in rows.items() if isinstance(v, dict) and v.get("converged")]
+    if best and t_plain:
+        k, v = min(best, key=lambda kv: kv[1]["seconds"])
+        tts["best"] = {"form": k, "seconds": v["seconds"], "speedup_vs_plain": t_plain / v["seconds"],
+                       "target_speedup": 10.0}
+    return tts
+
+
+def measure_workload(name, span, dev, steps, peaks, peak_kind, solve=True):
+    """Apply DOF/s, roofline and time to solution of one extra workload."""
+    import torch
+
+    t0 = time.perf_counter()
+    V, op, F, feats, nqe = build_workload(name, span, dev)
+    setup = time.perf_counter() - t0
+    n_qp = V.n_elems * nqe
+    x = torch.randn(V.n_dofs, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(7))
+    y = torch.empty_like(x)
+    for _ in range(3):
+        op.apply(x, out=y)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        op.apply(x, out=y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    rec = {"workload": workload_tag(name, span), "n_dofs": V.n_dofs, "elements": V.n_elems, "gauss_points": n_qp,
+           "value": V.n_dofs / (ms * 1e-3), "unit": UNIT, "ms_per_apply": ms, "setup_seconds": setup,
+           "roofline": roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span)}
+    if solve:
+        rec["time_to_solution"] = time_to_solution(name, span, op, F, feats)
+    op.close()
+    del F, x, y
+    torch.cuda.empty_cache()
+    return rec
+
+
+def matched_gpu_solve(dev):
+    """GPU time to solution of the CPU baseline's workload (elasticity 16^3)."""
+    V, op, F, _, _ = build_workload("elasticity", CPU_SAMPLE_SPAN, dev)
+    for _ in range(2):
+        _, st = op.pcg(F, tol=TOL, preconditioner="jacobi", check_every=32, restarts=3)
+    for _ in range(2):
+        _, st_r = op.mixed_pcg(F, tol=TOL, delta=1e-2, check_every=32)
+    op.close()
+    return {"span": CPU_SAMPLE_SPAN, "n_dofs": V.n_dofs, "plain_fp64_jacobi_pcg": _row(st),
+            "mixed_fp32_pcg_reliable_fp64_updates": _row(st_r)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    name = args.workload
+    span = args.span or {"darcy": 96, "plate": 256}.get(name, N_SPAN)
+    t_setup = time.perf_counter()
+    V, op, F, feats, nqe = build_workload(name, span, dev)
     setup_s = time.perf_counter() - t_setup
     n = V.n_dofs
-    n_qp = V.n_elems * (25 if plate else 64)
-    vec = V.vec
+    n_qp = V.n_elems * nqe
     gen = torch.Generator(device=dev).manual_seed(1234 + rank)
     x = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
     y = torch.empty_like(x)
@@ -280,34 +499,8 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = world * n * args.steps / (ms_max * 1e-3)
-
-    # per-kernel split for the roofline (CUDA events on the launching stream)
-    ms_bricks, ms_combine = op.profile_apply(x, reps=50)
-    ms_b32, ms_c32 = op.profile_apply(x.float(), reps=50, f32=True)
-    ngeo = op.info["ngeo"]
-    alg_bytes = 8 * 2 * n + 8 * n_qp * ngeo
-    alg_bytes32 = 4 * 2 * n + 4 * n_qp * ngeo
-    # survey formula: n_e vec 2*2*d^2 (p+1)^(d+1) + N_qp c_pt, c_pt = 2 d^4 (elasticity) or 2 d^2 (scalar)
-    if plate:  # 2D, p = 4: 2*2*d^2*(p+1)^(d+1) x 2.5 for the Hessian channels, 2 * 15 per point
-        flops = int(V.n_elems * 2 * 2 * 4 * 5**3 * 2.5 + n_qp * 2 * 15)
-    else:
-        p1, q = 4, 4
-        flops = V.n_elems * vec * (2 * 2 * 9 * p1**3 * q) + n_qp * (2 * 81 if vec == 3 else 2 * 9)
     peaks, peak_kind = measured_peaks()
-    achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
-    traffic = profile_traffic(args.workload, span)
-    roofline = {
-        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-        "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-        "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-        "kernel": ("k_brick2<double,4,5,plate> (brick apply)" if plate else
-                   "k_brick3_mma (FP64 mma.sync brick apply, %s p=3)" % ("poisson" if darcy else "elasticity")
-                   if os.environ.get("JXB_BRICK3_MMA", "1") != "0" else
-                   "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if darcy else "elasticity")),
-        "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
-        "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
-        "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
-    }
+    roofline = roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span)
 
     # e2e through the C ABI with host buffers
     xh = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -334,85 +527,35 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * n * k_e2e / (float(t.item()) * 1e-3)
 
-    tts = None
-    if not args.no_solve:
-        geo = geometry_operator(V)
-        if darcy or plate:
-            F = op.load(torch.ones(n_qp, dtype=torch.float64, device=dev))
-        else:
-            fq = geo.interpolate(params["eta"])
-            fq[..., 2] -= 1.0
-            F = op.load(fq)
-            del fq
-        # each solve runs twice and the second run is reported: the first captures its CUDA graph
-        for _ in range(2):
-            sol_p, st_p = op.pcg(F, tol=1e-8, preconditioner="jacobi", check_every=32, maxiter=40000)
-        for _ in range(2):
-            sol_m, st_m = op.refine_solve(F, tol=1e-8, inner_tol=1e-3, check_every=32, maxiter=80000)
-        diff = float(torch.linalg.norm(sol_m - sol_p) / torch.linalg.norm(sol_p))
-        for _ in range(2):
-            sol_r, st_r = op.mixed_pcg(F, tol=1e-8, delta=1e-2, check_every=32, maxiter=80000)
-        diff_r = float(torch.linalg.norm(sol_r - sol_p) / torch.linalg.norm(sol_p))
-        tts = {
-            "tol": 1e-8,
-            "plain_fp64_jacobi_pcg": {"seconds": st_p["seconds"], "iterations": st_p["iterations"],
-                                      "relative_residual": st_p["relative_residual"], "converged": bool(st_p["converged"])},
-            "mixed_fp32_inner_fp64_refinement": {"seconds": st_m["seconds"], "iterations": st_m["iterations"],
-                                                 "outer": st_m["outer"], "relative_residual": st_m["relative_residual"],
-                                                 "converged": bool(st_m["converged"]),
-                                                 "relative_difference_to_plain": diff},
-            # a speed-up is reported only for a solve that reached the tolerance
-            "speedup_mixed_vs_plain": (st_p["seconds"] / st_m["seconds"]
-                                       if st_m["seconds"] > 0 and st_m["converged"] else None),
-            "mixed_fp32_pcg_reliable_fp64_updates": {"seconds": st_r["seconds"], "iterations": st_r["iterations"],
-                                                     "updates": st_r["outer"],
-                                                     "relative_residual": st_r["relative_residual"],
-                                                     "converged": bool(st_r["converged"]),
-                                                     "relative_difference_to_plain": diff_r},
-            "speedup_mixed_reliable_vs_plain": (st_p["seconds"] / st_r["seconds"]
-                                                if st_r["seconds"] > 0 and st_r["converged"] else None),
-            "learned_preconditioner": None,
-        }
-        ckpt = os.path.join(ROOT, "jaxiga_b200", "checkpoints", f"{args.workload}{span}.npz")
-        if os.path.exists(ckpt):
-            from jaxiga_b200.learned import LearnedPreconditioner
+    tts = None if args.no_solve else time_to_solution(name, span, op, F, feats)
+    ngeo = op.info["ngeo"]
+    op.close()
+    del F, x, y, xd
+    torch.cuda.empty_cache()
 
-            feats = None
-            if darcy:
-                loga = params["loga"]
-                feats = ((loga - loga.mean()) / loga.std())[None, :]
-            lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
-            rows = {}
-            for key, mixed, two in (("learned_fcg_fp64", False, False), ("mixed_learned_fcg", True, False),
-                                    ("learned_two_level_fp64", False, True), ("mixed_learned_two_level", True, True),
-                                    ("learned_additive_fp64", False, "additive"),
-                                    ("mixed_learned_additive", True, "additive")):
-                lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)  # first call captures the graphs
-                x_l, st_l = lp.solve(F, tol=1e-8, mixed=mixed, two_level=two)
-                rows[key] = {"seconds": st_l["seconds"], "iterations": st_l["iterations"],
-                             "learned_iterations": st_l["learned_iterations"],
-                             "relative_residual": st_l["relative_residual"], "converged": bool(st_l["converged"]),
-                             "relative_difference_to_plain": float(torch.linalg.norm(x_l - sol_p) / torch.linalg.norm(sol_p))}
-            tts["learned_preconditioner"] = {
-                "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
-                "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
-                "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **rows,
-                **{"speedup_%s_vs_plain" % k: (st_p["seconds"] / v["seconds"] if v["converged"] else None)
-                   for k, v in rows.items()}}
-            lp.close()
+    extra = None
+    if world == 1 and not args.no_extra and args.span is None and name == "elasticity":
+        extra = {}
+        for w in ("darcy", "plate"):
+            extra[w] = measure_workload(w, {"darcy": 96, "plate": 256}[w], dev, max(args.steps, 20), peaks,
+                                        peak_kind, solve=not args.no_solve)
+        extra["batch"] = batch_record(max(args.steps, 20), rank, world, peaks, peak_kind, solve=not args.no_solve)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline()
+        cpu["gpu_same_size"] = matched_gpu_solve(dev)
+        g = cpu["gpu_same_size"]["plain_fp64_jacobi_pcg"]
+        c = cpu["time_to_solution"]
+        cpu["time_to_solution_ratio_cpu_over_gpu"] = (c["seconds"] / g["seconds"]
+                                                      if g["converged"] and c["converged"] else None)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": (f"plate2d_p4_{span}^2" if plate else
-                                    f"{'darcy3d' if darcy else 'elasticity3d'}_p3_{span}^3"), "n_dofs": n,
-                       "elements": V.n_elems,
+            "config": {"workload": workload_tag(name, span), "n_dofs": n, "elements": V.n_elems,
                        "gauss_points": n_qp, "operator": "matrix-free sum-factorised K.u, FP64, masked",
                        "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),
                        "parallelism": f"replicas x{world}", "setup_seconds": setup_s},
@@ -422,32 +565,27 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roofline,
             "clocks": clocks.summary(),
             "time_to_solution": tts,
+            "workloads": extra,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    op.close()
 
 
-def run_batch(args, rank, world, local_rank):
+def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     """256 uneven 2D Poisson instances (quarter annuli, p in {2,3,4}, 8-128 spans per
-    direction): one batched K.u over all instances per step, then the time to a
-    1e-8 residual of the batched PCG (one captured graph) against the instances
-    solved one after another (the reference loops over its solves)."""
+    direction), sharded over the ranks by cost: one batched K.u over all instances
+    per step, then the time to TOL of the batched PCG (one captured graph) against
+    the instances solved one after another (the reference loops over its solves)."""
     import torch
-    import torch.distributed as dist
 
     from jaxiga_b200 import _lib, workloads
     from jaxiga_b200.batch import BatchSolver
     from jaxiga_b200.dist import max_over_ranks, partition_by_cost
     from jaxiga_b200.solve import geometry_operator
 
-    torch.cuda.set_device(local_rank)
     t0 = time.perf_counter()
-    # source sum_k c_k R_k evaluated at the Gauss points by each space's geometry plan
     problems, params = workloads.config3(
         interpolate=lambda V, c: geometry_operator(V).interpolate(c).cpu().numpy())
-    # independent instances shard without communication: each rank takes a
-    # cost-balanced share (elements x points per element); the whole batch is the unit
     n_all = sum(pr.space.n_dofs for pr in problems)
     costs = [pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems]  # Gauss points
     elems_all = sum(pr.space.n_elems for pr in problems)
@@ -462,35 +600,26 @@ def run_batch(args, rank, world, local_rank):
     y = torch.empty_like(x)
     apply = lambda xx, yy: _lib.check(b.lib.jxb_batch_apply(b.handle, torch.cuda.current_stream().cuda_stream,  # noqa: E731
                                                             xx.data_ptr(), yy.data_ptr()))
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(3):
         apply(x, y)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        e0.record()
-        for _ in range(args.steps):
-            apply(x, y)
-        e1.record()
-        torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
-    value = n_all * args.steps / (ms * 1e-3)
+    e0.record()
+    for _ in range(steps):
+        apply(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    value = n_all * steps / (ms * 1e-3)
     # algorithmic bytes: u and y once, 6 factors per point (rational 2D scalar metric)
     n_qp = sum(pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems)
     alg = 8 * 2 * n + 8 * 6 * n_qp
-    peaks, peak_kind = measured_peaks()
-    achieved = alg / (ms / args.steps * 1e-3) / 1e9
+    achieved = alg / (ms / steps * 1e-3) / 1e9
     # end to end: pinned host x -> device, batched apply, device y -> pinned host
     xh = torch.empty(n, dtype=torch.float64).pin_memory()
     yh = torch.empty(n, dtype=torch.float64).pin_memory()
     xh.copy_(x.cpu())
-    k_e2e = max(10, args.steps // 5)
+    k_e2e = max(10, steps // 5)
     torch.cuda.synchronize()
     e0.record()
     for _ in range(k_e2e):
@@ -501,49 +630,65 @@ def run_batch(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e2e = n_all * k_e2e / (max_over_ranks(e0.elapsed_time(e1), device="cuda") * 1e-3)
     tts = None
-    if not args.no_solve:
-        bs.solve(tol=1e-8)  # captures the graph
-        xs, sts, secs = bs.solve(tol=1e-8)
+    if solve:
+        bs.solve(tol=TOL)  # captures the graph
+        xs, sts, secs = bs.solve(tol=TOL)
         secs = max_over_ranks(secs, device="cuda")
         seq_s, seq_it = 0.0, 0
         for op, bb in zip(bs.ops, torch.split(bs.b, [op.n_dofs for op in bs.ops])):
-            _, st = op.pcg(bb.contiguous(), tol=1e-8, preconditioner="jacobi")
+            _, st = op.pcg(bb.contiguous(), tol=TOL, preconditioner="jacobi")
             seq_s += st["seconds"]
             seq_it += st["iterations"]
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         for op, bb in zip(bs.ops, torch.split(bs.b, [op.n_dofs for op in bs.ops])):
-            op.pcg(bb.contiguous(), tol=1e-8, preconditioner="jacobi")
+            op.pcg(bb.contiguous(), tol=TOL, preconditioner="jacobi")
         torch.cuda.synchronize()
         seq_wall = max_over_ranks(time.perf_counter() - t1, device="cuda")
         seq_s = max_over_ranks(seq_s, device="cuda")
-        tts = {"tol": 1e-8, "batched_pcg_one_graph": {"seconds": secs, "converged": int(sum(s["converged"] for s in sts)),
-                                                       "max_iterations": int(max(s["iterations"] for s in sts))},
+        tts = {"tol": TOL, "batched_pcg_one_graph": {"seconds": secs, "converged": int(sum(s["converged"] for s in sts)),
+                                                      "max_iterations": int(max(s["iterations"] for s in sts))},
                "sequential_pcg_loop": {"device_seconds": seq_s, "wall_seconds": seq_wall, "iterations": seq_it},
                "speedup_batched_vs_sequential_wall": seq_wall / secs if secs > 0 else None}
+    rec = {"workload": "batched_quarter_annuli_256", "instances": len(costs), "n_dofs": n_all,
+           "instances_on_rank0": len(problems), "elements": elems_all, "gauss_points": sum(costs),
+           "degrees": sorted({pr.space.degree[0] for pr in problems}),
+           "tiles": {str(k): v for k, v in bs.tiles.items()},
+           "operator": "batched matrix-free K.u, FP64, masked, one launch per degree group",
+           "parallelism": "instances sharded over %d GPU(s) by cost, no collective" % world,
+           "setup_seconds": setup_s, "value": value, "unit": UNIT, "ms_per_apply": ms / steps,
+           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                   "steps": k_e2e},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": achieved / peaks["hbm_gbs"],
+                        "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+                        "kernel": "k_brick2_batch (batched 2D brick apply) + k_combine_batch",
+                        "algorithmic_bytes_per_launch": alg},
+           "time_to_solution": tts}
+    bs.close()
+    torch.cuda.empty_cache()
+    return rec
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batched workload as the line's own measurement (``--workload batch``)."""
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    with ClockSampler(local_rank) as clk:
+        rec = batch_record(args.steps, rank, world, *measured_peaks(), solve=not args.no_solve)
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched_quarter_annuli_256", "instances": len(costs), "n_dofs": n_all,
-                       "instances_on_rank0": len(problems),
-                       "elements": elems_all, "gauss_points": sum(costs),
-                       "degrees": sorted({pr.space.degree[0] for pr in problems}), "tiles": {str(k): v for k, v in bs.tiles.items()},
-                       "operator": "batched matrix-free K.u, FP64, masked, one launch per degree group",
-                       "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * 6 * n_qp / 1e9),
-                       "parallelism": "instances sharded over %d GPU(s) by cost, no collective" % world,
-                       "setup_seconds": setup_s},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n, "steps": k_e2e},
-            "gpu_launches": 3 * args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                         "traffic": None, "kernel": "k_brick2_batch (batched 2D brick apply) + k_combine_batch",
-                         "algorithmic_bytes_per_launch": alg},
-            "clocks": clk.summary(), "time_to_solution": tts, "cpu_baseline": None,
+            "metric": METRIC, "value": rec["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": rec["ms_per_apply"], "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {k: rec[k] for k in ("workload", "instances", "n_dofs", "instances_on_rank0", "elements",
+                                           "gauss_points", "degrees", "tiles", "operator", "parallelism",
+                                           "setup_seconds")},
+            "e2e": rec["e2e"], "gpu_launches": 3 * args.steps, "roofline": rec["roofline"],
+            "clocks": clk.summary(), "time_to_solution": rec["time_to_solution"], "cpu_baseline": None,
         }
         print(json.dumps(line), flush=True)
-    bs.close()
 
 
 def main():

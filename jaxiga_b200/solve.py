@@ -273,7 +273,13 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG")
     space = problem.space
     n = space.n_dofs
-    op, prescribed, values = _problem_operator(problem, params, linear.precision == "mixed")
+    # The Kirchhoff plate's FP32 operator cannot resolve the biharmonic system:
+    # its condition number (~h^-4) times FP32 rounding exceeds 1, so FP32
+    # iterations diverge. Its mixed form keeps the FP64 operator and FP64
+    # Krylov loop and runs in FP32 only what the preconditioner computes (the
+    # learned network; the Jacobi scaling otherwise).
+    fp32_operator = linear.precision == "mixed" and problem.op != "plate"
+    op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)
     if linear.preconditioner == "learned":
         from .learned import LearnedPreconditioner
@@ -283,16 +289,16 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
             two = {"network": False, "multiplicative": "multiplicative", "additive": "additive"}[linear.learned_map]
             reliable = linear.refinement == "reliable"
             xdev, st = lp.solve(b, tol=linear.tol, maxiter=linear.maxiter, stall=linear.learned_stall,
-                                mixed=linear.precision == "mixed", two_level=two, refinement=linear.refinement,
+                                mixed=fp32_operator, two_level=two, refinement=linear.refinement,
                                 inner_tol=linear.update_delta if reliable else linear.inner_tol,
                                 check_every=linear.check_every)
         finally:
             lp.close()
         st["outer"] = st["learned_iterations"]
-    elif linear.precision == "mixed" and linear.refinement == "reliable":
+    elif fp32_operator and linear.refinement == "reliable":
         xdev, st = op.mixed_pcg(b, tol=linear.tol, delta=linear.update_delta, maxiter=linear.maxiter,
                                 check_every=linear.check_every)
-    elif linear.precision == "mixed":
+    elif fp32_operator:
         xdev, st = op.refine_solve(b, tol=linear.tol, inner_tol=linear.inner_tol, maxiter=linear.maxiter,
                                    check_every=linear.check_every)
     else:
@@ -315,8 +321,9 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         "outer": int(st["outer"]),
         "seconds": st["seconds"],
         "precision": linear.precision,
+        "fp32_operator": fp32_operator,
         "preconditioner": linear.preconditioner,
-        "refinement": linear.refinement if linear.precision == "mixed" else None,
+        "refinement": linear.refinement if fp32_operator else None,
     }
     if not stats["converged"]:
         warnings.warn(f"linear Galerkin solve did not converge (residual {stats['residual']:.3e}); "

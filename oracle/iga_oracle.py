@@ -422,15 +422,22 @@ def element_tangents(op, basis, params, vec=1):
     if op == "elasticity":
         dim = basis["dR"].shape[2]
         C = isotropic(params["E"], params["nu"], dim, params.get("plane", "stress"))
-        B = strain_displacement(basis["dR"])
-        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, C, B, optimize=True)
+        return _btdb(w, strain_displacement(basis["dR"]), C)
     if op == "plate":
         E, nu, t = params["E"], params["nu"], params["t"]
         D = E * t**3 / (12 * (1 - nu**2)) * np.array([[1, nu, 0], [nu, 1, 0], [0, 0, (1 - nu) / 2]])
         d2R = basis["d2R"]
         B = -np.stack([d2R[:, :, 0], d2R[:, :, 2], 2.0 * d2R[:, :, 1]], axis=2)
-        return np.einsum("eq,eqsi,st,eqtj->eij", w, B, D, B, optimize=True)
+        return _btdb(w, B, D)
     raise ValueError(op)
+
+
+def _btdb(w, B, D):
+    """sum_q w_q B_q^T D B_q per element, as one batched matrix product over the
+    stacked (point, strain) rows (the contraction of library.py:125-132, 174-181)."""
+    e, q, ns, n = B.shape
+    DB = np.einsum("st,eqtj->eqsj", D, B) * w[:, :, None, None]
+    return np.matmul(B.reshape(e, q * ns, n).transpose(0, 2, 1), DB.reshape(e, q * ns, n))
 
 
 # --------------------------------------------------------------------------

@@ -1,5 +1,6 @@
-"""bench.py's reference arm runs on the CPU (the reference's SciPy CSR matvec on an
-assembled sample): its JSON line carries the keys the benchmark contract names."""
+"""bench.py's reference arm runs on the CPU (the reference's SciPy CSR matvec and
+Jacobi-CG on an assembled 16^3 sample of the elasticity workload): its JSON line
+carries the keys the benchmark contract names and the CPU time to solution."""
 
 import json
 import os
@@ -21,3 +22,6 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 3
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("port", "reference") and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["host"]["cpu_count"] >= 1
+    tts = d["time_to_solution"]["scipy_jacobi_cg_true_residual_restarts"]
+    assert tts["converged"] and tts["relative_residual"] <= 1e-8 and tts["iterations"] > 0
