@@ -159,6 +159,22 @@ int jxb_diag(jxb_plan* plan, jxb_stream stream, double* d);
  */
 int jxb_qp_coords(jxb_plan* plan, jxb_stream stream, double* x);
 int jxb_interpolate(jxb_plan* plan, jxb_stream stream, const double* coef, int ncomp, double* out);
+/* jxb_interpolate_grad: physical gradients sum_i dR_i/dx(x_q) c_i of a control-point field
+ *   (n_cp_total, ncomp), ncomp 1..3, written as (n_elem, n_q^dim, ncomp, dim)
+ *   -- Solution.grad (src/jaxiga/post/solution.py:50-54) for the H1 and energy
+ *   error norms (src/jaxiga/post/norms.py:59-140). */
+int jxb_interpolate_grad(jxb_plan* plan, jxb_stream stream, const double* coef, int ncomp, double* out);
+/* jxb_eval_points: evaluation at arbitrary points of a PointSet
+ *   (src/jaxiga/space/pointset.py:27-75; evaluate, src/jaxiga/space/evaluation.py:305-467;
+ *   Solution.at/grad, src/jaxiga/post/solution.py:39-54). Point k lies in element
+ *   elems[k] (device int64, reference order) at reference coordinates ref[k]
+ *   (device, (n, dim), in [-1, 1]^dim). Writes, for each non-NULL output:
+ *   val (n, ncomp) and grad (n, ncomp, dim) of the control-point field coef
+ *   (ncomp 1..3; may be NULL when only x/jac are wanted), x (n, dim) physical
+ *   coordinates, jac (n) = |det J| prod(h/2), the factor the reference applies to
+ *   its quadrature weights. Out-of-range element indices give NaN. */
+int jxb_eval_points(jxb_plan* plan, jxb_stream stream, const double* coef, int ncomp, int64_t n,
+                    const int64_t* elems, const double* ref, double* val, double* grad, double* x, double* jac);
 int jxb_load(jxb_plan* plan, jxb_stream stream, const double* f_qp, double* F);
 /* jxb_qp_weights: integration weights w_hat |J| prod(h/2) at every Gauss point,
  *   (n_elem, n_q^dim) -- BasisData.w of src/jaxiga/space/evaluation.py:461-463. */

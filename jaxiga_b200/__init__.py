@@ -22,6 +22,7 @@ from .forms import (ClampedBC, DirichletBC, KirchhoffPlate, LinearElasticity, Ne
                     Problem)
 from .geometry import Patch, primitives
 from .operator import Operator
+from .pointset import PointSet, gauss
 from .solve import LinearOptions, Solution, errornorm, integrate, norm, solve
 from .space import FunctionSpace, bezier_extraction, element_spans, expand_dofs
 
@@ -31,4 +32,5 @@ __all__ = [
     "Patch", "primitives", "FunctionSpace", "expand_dofs", "bezier_extraction", "element_spans",
     "Problem", "DirichletBC", "ClampedBC", "Neumann", "PointField", "Poisson", "LinearElasticity",
     "KirchhoffPlate", "solve", "LinearOptions", "Solution", "errornorm", "norm", "integrate", "Operator",
+    "PointSet", "gauss",
 ]

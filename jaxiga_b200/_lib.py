@@ -102,6 +102,10 @@ SIGNATURES = [
     ("jxb_diag", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_qp_coords", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_interpolate", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("jxb_interpolate_grad", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("jxb_eval_points", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                         ctypes.c_void_p]),
     ("jxb_load", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_qp_weights", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -21,6 +21,8 @@
 
 #include "jxb_internal.cuh"
 
+#define JXB_GRAD_MAXC 3
+
 namespace jxb {
 
 // Bernstein recurrence of src/jaxiga/space/bernstein.py:79-156 at one point.
@@ -455,6 +457,75 @@ __global__ void k_interp(FactorArgs A, const double* __restrict__ coef, int ncom
   for (int c = 0; c < ncomp && c < 8; ++c) out[idx * ncomp + c] = acc[c] / W;
 }
 
+// Physical gradients of sum_a R_a c_a at the Gauss points, reference order,
+// (n_elem, nqe, ncomp, dim): the quotient rule for R = w N / W
+// (evaluation.py:114-121) and the push-forward J^-T (evaluation.py:149-152),
+// applied to the field sums U_c = sum w N c and the geometry sums at once.
+__global__ void k_interp_grad(FactorArgs A, const double* __restrict__ coef, int ncomp, double* out) {
+  const Bricks& br = A.br;
+  const int dim = br.dim, Q = br.q, P1 = br.p + 1;
+  const long long nqe = dim == 2 ? Q * Q : Q * Q * Q;
+  const long long n_elem = (long long)br.n_span[0] * br.n_span[1] * (dim == 3 ? br.n_span[2] : 1);
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_elem * nqe) return;
+  const long long e = idx / nqe;
+  const int q = (int)(idx % nqe);
+  const int sp[3] = {(int)(e % br.n_span[0]), (int)((e / br.n_span[0]) % br.n_span[1]),
+                     (int)(e / ((long long)br.n_span[0] * br.n_span[1]))};
+  const int qq[3] = {q % Q, (q / Q) % Q, dim == 3 ? q / (Q * Q) : 0};
+  const double* nv[3];
+  const double* nd[3];
+  for (int d = 0; d < dim; ++d) {
+    const double* base = A.tab[d] + (size_t)sp[d] * 3 * Q * P1;
+    nv[d] = base + (size_t)qq[d] * P1;
+    nd[d] = base + (size_t)(Q + qq[d]) * P1;
+  }
+  const int f0 = br.first[0][sp[0]], f1 = br.first[1][sp[1]], f2 = dim == 3 ? br.first[2][sp[2]] : 0;
+  double W = 0, Wd[3] = {0, 0, 0}, P[3] = {0, 0, 0}, Pd[3][3] = {}, U[JXB_GRAD_MAXC] = {},
+         Ud[JXB_GRAD_MAXC][3] = {};
+  const int n2 = dim == 3 ? P1 : 1;
+  for (int a2 = 0; a2 < n2; ++a2)
+    for (int a1 = 0; a1 < P1; ++a1)
+      for (int a0 = 0; a0 < P1; ++a0) {
+        const long long cp = (long long)(f0 + a0) +
+                             (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
+        const double z = dim == 3 ? nv[2][a2] : 1.0, dz = dim == 3 ? nd[2][a2] : 0.0;
+        const double w = A.wgts[cp];
+        const double N = w * nv[0][a0] * nv[1][a1] * z;
+        const double dN[3] = {w * nd[0][a0] * nv[1][a1] * z, w * nv[0][a0] * nd[1][a1] * z,
+                              w * nv[0][a0] * nv[1][a1] * dz};
+        W += N;
+        for (int k = 0; k < dim; ++k) Wd[k] += dN[k];
+        for (int i = 0; i < dim; ++i) {
+          const double X = A.cpts[cp * dim + i];
+          P[i] += N * X;
+          for (int k = 0; k < dim; ++k) Pd[i][k] += dN[k] * X;
+        }
+        for (int c = 0; c < ncomp; ++c) {
+          const double v = coef[cp * ncomp + c];
+          U[c] += N * v;
+          for (int k = 0; k < dim; ++k) Ud[c][k] += dN[k] * v;
+        }
+      }
+  const double iW = 1.0 / W;
+  double J[3][3], Ji[3][3];
+  for (int i = 0; i < dim; ++i) {
+    const double x = P[i] * iW;
+    for (int a = 0; a < dim; ++a) J[a][i] = (Pd[i][a] - x * Wd[a]) * iW;  // d x_i / d xi_a
+  }
+  det_inv(dim, J, Ji);
+  for (int c = 0; c < ncomp; ++c) {
+    const double u = U[c] * iW;
+    double ud[3];
+    for (int a = 0; a < dim; ++a) ud[a] = (Ud[c][a] - u * Wd[a]) * iW;  // d u / d xi_a
+    for (int k = 0; k < dim; ++k) {
+      double g = 0;
+      for (int a = 0; a < dim; ++a) g += Ji[k][a] * ud[a];
+      out[(idx * ncomp + c) * dim + k] = g;
+    }
+  }
+}
+
 // Integration weights in reference element order: w = (w / W) * W.
 __global__ void k_qp_weights(Bricks br, const double* __restrict__ wq, const double* __restrict__ invW,
                              double* out) {
@@ -528,11 +599,12 @@ int build_tables(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s) {
     k_tables<<<(total + 127) / 128, 128, 0, s>>>(plan->p, Q, ns, d_ext, d_lo, d_hi, d_nodes,
                                                  plan->d_tab[d], plan->d_tab32[d]);
     JXB_CUDA(cudaGetLastError());
-    JXB_CUDA(cudaStreamSynchronize(s));
-    cudaFree(d_ext);
-    cudaFree(d_lo);
-    cudaFree(d_hi);
+    // kept for evaluation at arbitrary points (jxb_eval_points)
+    plan->d_ext[d] = d_ext;
+    plan->d_lo[d] = d_lo;
+    plan->d_hi[d] = d_hi;
   }
+  JXB_CUDA(cudaStreamSynchronize(s));
   cudaFree(d_nodes);
   return JXB_OK;
 }
@@ -568,6 +640,154 @@ int qp_coords(jxb_plan* plan, cudaStream_t s, double* x) {
   FactorArgs A = make_args(plan);
   long long total = plan->n_elem * plan->nqe;
   k_coords<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(A, x);
+  JXB_CUDA(cudaGetLastError());
+  return JXB_OK;
+}
+
+// Evaluation at arbitrary reference points: point k lies in element
+// elems[k] (reference order, first direction fastest) at ref[k] in [-1, 1]^dim.
+// The extracted 1D basis is formed on the fly from the Bernstein recurrence
+// and the element's extraction rows (evaluation.py:374-386), then the same
+// quotient rule and push-forward as the Gauss-point kernels. Outputs (any may
+// be null): val (n, ncomp), grad (n, ncomp, dim), x (n, dim) and
+// jac = |det J| prod(h/2) (n), the measure the reference multiplies its
+// quadrature weights by (evaluation.py:461-463). A point whose element index
+// is out of range yields NaN.
+struct EvalArgs {
+  Bricks br;
+  const double* ext[3];
+  const double* lo[3];
+  const double* hi[3];
+  const double* cpts;
+  const double* wgts;
+};
+
+__global__ void k_eval_points(EvalArgs A, long long n, const long long* __restrict__ elems,
+                              const double* __restrict__ ref, const double* __restrict__ coef, int ncomp,
+                              double* val, double* grad, double* xout, double* jac) {
+  const Bricks& br = A.br;
+  const int dim = br.dim, P1 = br.p + 1;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const long long n_elem = (long long)br.n_span[0] * br.n_span[1] * (dim == 3 ? br.n_span[2] : 1);
+  const long long e = elems[k];
+  if (e < 0 || e >= n_elem) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int c = 0; c < ncomp; ++c) {
+      if (val) val[k * ncomp + c] = nan;
+      if (grad)
+        for (int d = 0; d < dim; ++d) grad[(k * ncomp + c) * dim + d] = nan;
+    }
+    if (xout)
+      for (int d = 0; d < dim; ++d) xout[k * dim + d] = nan;
+    if (jac) jac[k] = nan;
+    return;
+  }
+  const int sp[3] = {(int)(e % br.n_span[0]), (int)((e / br.n_span[0]) % br.n_span[1]),
+                     (int)(e / ((long long)br.n_span[0] * br.n_span[1]))};
+  double nv[3][JXB_MAXP + 1], nd[3][JXB_MAXP + 1];
+  double meas = 1.0;
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < P1; ++a) {
+      nv[d][a] = d < dim ? 0.0 : 1.0;
+      nd[d][a] = 0.0;
+    }
+  for (int d = 0; d < dim; ++d) {
+    double B[JXB_MAXP + 1], dB[JXB_MAXP + 1], d2B[JXB_MAXP + 1];
+    bernstein_point(ref[k * dim + d], br.p, B, dB, d2B);
+    const double h = A.hi[d][sp[d]] - A.lo[d][sp[d]];
+    const double* C = A.ext[d] + (size_t)sp[d] * P1 * P1;
+    for (int a = 0; a < P1; ++a) {
+      double v = 0, g = 0;
+      for (int j = 0; j < P1; ++j) {
+        v += C[a * P1 + j] * B[j];
+        g += C[a * P1 + j] * dB[j];
+      }
+      nv[d][a] = v;
+      nd[d][a] = g * 2.0 / h;
+    }
+    meas *= h / 2.0;
+  }
+  const int f0 = br.first[0][sp[0]], f1 = br.first[1][sp[1]], f2 = dim == 3 ? br.first[2][sp[2]] : 0;
+  double W = 0, Wd[3] = {0, 0, 0}, P[3] = {0, 0, 0}, Pd[3][3] = {}, U[JXB_GRAD_MAXC] = {},
+         Ud[JXB_GRAD_MAXC][3] = {};
+  const int n2 = dim == 3 ? P1 : 1;
+  for (int a2 = 0; a2 < n2; ++a2)
+    for (int a1 = 0; a1 < P1; ++a1)
+      for (int a0 = 0; a0 < P1; ++a0) {
+        const long long cp = (long long)(f0 + a0) +
+                             (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
+        const double w = A.wgts[cp];
+        const double z = nv[2][a2], dz = nd[2][a2];
+        const double N = w * nv[0][a0] * nv[1][a1] * z;
+        const double dN[3] = {w * nd[0][a0] * nv[1][a1] * z, w * nv[0][a0] * nd[1][a1] * z,
+                              w * nv[0][a0] * nv[1][a1] * dz};
+        W += N;
+        for (int q = 0; q < dim; ++q) Wd[q] += dN[q];
+        for (int i = 0; i < dim; ++i) {
+          const double X = A.cpts[cp * dim + i];
+          P[i] += N * X;
+          for (int q = 0; q < dim; ++q) Pd[i][q] += dN[q] * X;
+        }
+        if (coef)
+          for (int c = 0; c < ncomp; ++c) {
+            const double v = coef[cp * ncomp + c];
+            U[c] += N * v;
+            for (int q = 0; q < dim; ++q) Ud[c][q] += dN[q] * v;
+          }
+      }
+  const double iW = 1.0 / W;
+  double J[3][3], Ji[3][3], x[3];
+  for (int i = 0; i < dim; ++i) {
+    x[i] = P[i] * iW;
+    for (int a = 0; a < dim; ++a) J[a][i] = (Pd[i][a] - x[i] * Wd[a]) * iW;
+  }
+  const double det = det_inv(dim, J, Ji);
+  if (xout)
+    for (int i = 0; i < dim; ++i) xout[k * dim + i] = x[i];
+  if (jac) jac[k] = fabs(det) * meas;
+  if (!coef) return;
+  for (int c = 0; c < ncomp; ++c) {
+    const double u = U[c] * iW;
+    if (val) val[k * ncomp + c] = u;
+    if (grad) {
+      double ud[3];
+      for (int a = 0; a < dim; ++a) ud[a] = (Ud[c][a] - u * Wd[a]) * iW;
+      for (int q = 0; q < dim; ++q) {
+        double g = 0;
+        for (int a = 0; a < dim; ++a) g += Ji[q][a] * ud[a];
+        grad[(k * ncomp + c) * dim + q] = g;
+      }
+    }
+  }
+}
+
+int eval_points(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, long long n,
+                const long long* elems, const double* ref, double* val, double* grad, double* x, double* jac) {
+  if (coef && (ncomp < 1 || ncomp > JXB_GRAD_MAXC))
+    return fail(JXB_ERR_INVALID, "jxb_eval_points: ncomp must be in 1..3");
+  if (n < 0) return fail(JXB_ERR_INVALID, "jxb_eval_points: negative point count");
+  if (n == 0) return JXB_OK;
+  EvalArgs A;
+  A.br = plan->br;
+  for (int d = 0; d < 3; ++d) {
+    A.ext[d] = plan->d_ext[d];
+    A.lo[d] = plan->d_lo[d];
+    A.hi[d] = plan->d_hi[d];
+  }
+  A.cpts = plan->d_cpts;
+  A.wgts = plan->d_wgts;
+  k_eval_points<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(A, n, elems, ref, coef, ncomp, val, grad, x, jac);
+  JXB_CUDA(cudaGetLastError());
+  return JXB_OK;
+}
+
+int interpolate_grad(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out) {
+  if (ncomp < 1 || ncomp > JXB_GRAD_MAXC)
+    return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: ncomp must be in 1..3");
+  FactorArgs A = make_args(plan);
+  long long total = plan->n_elem * plan->nqe;
+  k_interp_grad<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(A, coef, ncomp, out);
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }

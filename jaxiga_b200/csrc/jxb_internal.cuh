@@ -167,6 +167,9 @@ struct jxb_plan {
   int* d_bcp0[3] = {nullptr, nullptr, nullptr};
   int* d_cover[3] = {nullptr, nullptr, nullptr};
   double* d_tab[3] = {nullptr, nullptr, nullptr};
+  double* d_ext[3] = {nullptr, nullptr, nullptr};  // (n_span, p+1, p+1) extraction operators
+  double* d_lo[3] = {nullptr, nullptr, nullptr};   // span bounds
+  double* d_hi[3] = {nullptr, nullptr, nullptr};
   float* d_tab32[3] = {nullptr, nullptr, nullptr};
   double* d_geo = nullptr;    // (slots, ngeo, nqe)
   float* d_geo32 = nullptr;
@@ -204,6 +207,9 @@ int build_tables(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s);
 int build_factors(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s);
 int qp_coords(jxb_plan* plan, cudaStream_t s, double* x);
 int interpolate(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
+int interpolate_grad(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
+int eval_points(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, long long n, const long long* elems,
+                const double* ref, double* val, double* grad, double* x, double* jac);
 int qp_weights(jxb_plan* plan, cudaStream_t s, double* w);
 
 // apply.cu

@@ -52,6 +52,9 @@ static void free_plan(jxb_plan* p) {
     cudaFree(p->d_bcp0[d]);
     cudaFree(p->d_cover[d]);
     cudaFree(p->d_tab[d]);
+    cudaFree(p->d_ext[d]);
+    cudaFree(p->d_lo[d]);
+    cudaFree(p->d_hi[d]);
     cudaFree(p->d_tab32[d]);
   }
   void* bufs[] = {p->d_geo, p->d_geo32, p->d_wq, p->d_invW, p->d_cpts, p->d_wgts, p->d_wgts32,
@@ -349,6 +352,20 @@ extern "C" int jxb_qp_coords(jxb_plan* P, jxb_stream stream, double* x) {
 extern "C" int jxb_interpolate(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, double* out) {
   if (!P || !coef || !out) return fail(JXB_ERR_INVALID, "jxb_interpolate: null argument");
   return interpolate(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, out);
+}
+
+extern "C" int jxb_interpolate_grad(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, double* out) {
+  if (!P || !coef || !out) return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: null argument");
+  return interpolate_grad(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, out);
+}
+
+extern "C" int jxb_eval_points(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, int64_t n,
+                               const int64_t* elems, const double* ref, double* val, double* grad, double* x,
+                               double* jac) {
+  if (!P || (n > 0 && (!elems || !ref))) return fail(JXB_ERR_INVALID, "jxb_eval_points: null argument");
+  if (!coef && (val || grad)) return fail(JXB_ERR_INVALID, "jxb_eval_points: values need a coefficient field");
+  return eval_points(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, n,
+                     reinterpret_cast<const long long*>(elems), ref, val, grad, x, jac);
 }
 
 extern "C" int jxb_qp_weights(jxb_plan* P, jxb_stream stream, double* w) {

@@ -201,6 +201,56 @@ class Operator:
         _lib.check(self.lib.jxb_interpolate(self.handle, _stream(), _dptr(c), ncomp, _dptr(out)))
         return out.view(self.space.n_elems, self.nqe, ncomp)
 
+    def interpolate_grad(self, coef):
+        """Physical gradients of a control-point field at the Gauss points,
+        (n_elem, n_q, ncomp, dim)."""
+        import torch
+
+        c = torch.as_tensor(coef, dtype=torch.float64, device=self.device).contiguous()
+        ncomp = c.numel() // self.space.n_scalar_basis
+        if ncomp * self.space.n_scalar_basis != c.numel():
+            raise ValueError("coefficient field must have n_scalar_basis * ncomp entries")
+        out = self._empty(self.n_qp * ncomp * self.space.dim)
+        _lib.check(self.lib.jxb_interpolate_grad(self.handle, _stream(), _dptr(c), ncomp, _dptr(out)))
+        return out.view(self.space.n_elems, self.nqe, ncomp, self.space.dim)
+
+    def eval_points(self, elems, ref, coef=None, val=True, grad=False, x=False, jac=False):
+        """Evaluate at arbitrary points: element indices (n,) and reference
+        coordinates (n, dim) in [-1, 1]^dim. Returns a dict with the requested
+        "val" (n, ncomp), "grad" (n, ncomp, dim) of the control-point field
+        ``coef``, physical coordinates "x" (n, dim) and "jac" (n) =
+        |det J| prod(h/2)."""
+        import torch
+
+        dim = self.space.dim
+        e = torch.as_tensor(np.asarray(elems, dtype=np.int64), device=self.device).contiguous()
+        r = torch.as_tensor(np.asarray(ref, dtype=np.float64), device=self.device).contiguous()
+        n = e.numel()
+        if r.numel() != n * dim:
+            raise ValueError(f"ref must be ({n}, {dim})")
+        c, ncomp = None, 0
+        if coef is not None:
+            c = torch.as_tensor(coef, dtype=torch.float64, device=self.device).contiguous()
+            ncomp = c.numel() // self.space.n_scalar_basis
+            if ncomp * self.space.n_scalar_basis != c.numel():
+                raise ValueError("coefficient field must have n_scalar_basis * ncomp entries")
+        elif val or grad:
+            raise ValueError("values and gradients need a coefficient field")
+        out = {}
+        if val:
+            out["val"] = self._empty(max(n * ncomp, 1))
+        if grad:
+            out["grad"] = self._empty(max(n * ncomp * dim, 1))
+        if x:
+            out["x"] = self._empty(max(n * dim, 1))
+        if jac:
+            out["jac"] = self._empty(max(n, 1))
+        ptr = lambda k: _dptr(out[k]) if k in out else None  # noqa: E731
+        _lib.check(self.lib.jxb_eval_points(self.handle, _stream(), _dptr(c) if c is not None else None, ncomp, n,
+                                            _dptr(e), _dptr(r), ptr("val"), ptr("grad"), ptr("x"), ptr("jac")))
+        shapes = {"val": (n, ncomp), "grad": (n, ncomp, dim), "x": (n, dim), "jac": (n,)}
+        return {k: v[: int(np.prod(shapes[k]))].view(*shapes[k]) for k, v in out.items()}
+
     def profile_apply(self, x, reps=20, f32=False):
         """Average device ms of one brick launch and one combine launch (CUDA events)."""
         import torch

@@ -132,9 +132,17 @@ def qp_points(space):
     return x
 
 
+def _points(space, ps, coef=None, val=True, grad=False, x=False, jac=False):
+    """Device evaluation on a PointSet, outputs shaped (n_e, n_q, ...) on the host."""
+    g = geometry_operator(space)
+    elems, ref = ps.flat()
+    out = g.eval_points(elems, ref, coef, val=val, grad=grad, x=x, jac=jac)
+    return {k: v.cpu().numpy().reshape(ps.n_elems, ps.n_q, *v.shape[1:]) for k, v in out.items()}
+
+
 @dataclasses.dataclass
 class Solution:
-    """A solved field (post/solution.py:23-50)."""
+    """A solved field (post/solution.py:23-54)."""
 
     space: object
     u: np.ndarray
@@ -143,13 +151,29 @@ class Solution:
     stats: dict = dataclasses.field(default_factory=dict)
     u_device: object = None
 
+    def _coef(self):
+        return self.u_device if self.u_device is not None else self.u
+
     def at(self, ps=None, basis=None):
-        """Values at the interior Gauss points, ``(n_e, n_q, vec)``."""
-        if ps is not None or basis is not None:
-            raise NotImplementedError("the B200 backend evaluates solutions at the interior Gauss set only")
-        g = geometry_operator(self.space)
-        u = self.u_device if self.u_device is not None else self.u
-        return g.interpolate(u).cpu().numpy()
+        """Values on a PointSet (default: the interior p+1 Gauss set), ``(n_e, n_q, vec)``."""
+        if basis is not None:
+            raise NotImplementedError("the B200 backend evaluates on PointSets (jaxiga_b200.pointset), "
+                                      "not on precomputed basis data")
+        if ps is None:
+            return geometry_operator(self.space).interpolate(self._coef()).cpu().numpy()
+        return _points(self.space, ps, self._coef())["val"]
+
+    def __call__(self, ps):
+        return self.at(ps)
+
+    def grad(self, ps=None, basis=None):
+        """Physical gradients on a PointSet, ``(n_e, n_q, vec, dim)``."""
+        if basis is not None:
+            raise NotImplementedError("the B200 backend evaluates on PointSets (jaxiga_b200.pointset), "
+                                      "not on precomputed basis data")
+        if ps is None:
+            return geometry_operator(self.space).interpolate_grad(self._coef()).cpu().numpy()
+        return _points(self.space, ps, self._coef(), val=False, grad=True)["grad"]
 
 
 # at most this many device operators stay cached per space (each holds the
@@ -383,39 +407,95 @@ def _exact_at(exact, x):
     return out.reshape(x.shape[0], -1)
 
 
-def errornorm(sol, exact, norm: str = "L2", exact_grad=None, quad=None, relative: bool = True) -> float:
-    """Relative (default) L2 error against ``exact(x)`` (post/norms.py:59-111)."""
-    if norm != "L2":
-        raise NotImplementedError("the B200 backend computes the L2 error norm")
-    if quad is not None:
-        raise NotImplementedError("the B200 backend uses the default Gauss rule")
-    space = sol.space
+def _quadrature(space, quad, coef=None, grad=False):
+    """Weights, points, and (optionally) values and gradients of a field on the
+    Gauss set with ``quad`` points per direction (default p + 1), flattened over
+    (element, point)."""
+    from .pointset import gauss
+
     g = geometry_operator(space)
-    w = g.qp_weights().reshape(-1).cpu().numpy()
-    uh = sol.at().reshape(-1, space.vec)
-    ue = _exact_at(exact, qp_points(space)).reshape(uh.shape)
-    num = np.sum(w * np.sum((uh - ue) ** 2, -1))
+    if quad is None or all(int(quad) == p + 1 for p in space.degree):
+        out = {"w": g.qp_weights().reshape(-1).cpu().numpy(), "x": qp_points(space)}
+        if coef is not None:
+            out["val"] = g.interpolate(coef).cpu().numpy().reshape(len(out["w"]), -1)
+            if grad:
+                out["grad"] = g.interpolate_grad(coef).cpu().numpy().reshape(len(out["w"]), -1, space.dim)
+        return out
+    ps = gauss(space, quad)
+    r = _points(space, ps, coef, val=coef is not None, grad=grad and coef is not None, x=True, jac=True)
+    out = {"w": (ps.flat_weights() * r["jac"].reshape(-1)), "x": r["x"].reshape(-1, space.dim)}
+    if coef is not None:
+        out["val"] = r["val"].reshape(ps.n_pts, -1)
+        if grad:
+            out["grad"] = r["grad"].reshape(ps.n_pts, -1, space.dim)
+    return out
+
+
+def _strain_voigt(g):
+    """Engineering Voigt strain of displacement gradients (n, dim, dim) (materials.py:91-112)."""
+    if g.shape[-1] == 2:
+        return np.stack([g[:, 0, 0], g[:, 1, 1], g[:, 0, 1] + g[:, 1, 0]], axis=1)
+    return np.stack([g[:, 0, 0], g[:, 1, 1], g[:, 2, 2], g[:, 1, 2] + g[:, 2, 1], g[:, 0, 2] + g[:, 2, 0],
+                     g[:, 0, 1] + g[:, 1, 0]], axis=1)
+
+
+def errornorm(sol, exact, norm: str = "L2", exact_grad=None, quad=None, relative: bool = True) -> float:
+    """Error against an exact solution, relative by default (post/norms.py:59-140).
+
+    ``norm`` is ``"L2"``, ``"H1"`` (the gradient seminorm, needs ``exact_grad``
+    returning (vec, dim) per point) or ``"energy"`` (needs a problem with a
+    constitutive matrix and ``exact_grad`` returning the exact Voigt stress).
+    ``quad`` is the Gauss points per direction (default p + 1).
+    """
+    if norm not in ("L2", "H1", "energy"):
+        raise ValueError(f"unknown norm {norm!r}")
+    if norm in ("H1", "energy") and exact_grad is None:
+        raise ValueError(f"the {norm!r} norm needs exact_grad")
+    space = sol.space
+    Q = _quadrature(space, quad, sol._coef(), grad=norm != "L2")
+    w, x = Q["w"], Q["x"]
+    if norm == "L2":
+        uh = Q["val"]
+        ue = _exact_at(exact, x).reshape(uh.shape)
+        num = np.sum(w * np.sum((uh - ue) ** 2, -1))
+        den = np.sum(w * np.sum(ue**2, -1))
+    elif norm == "H1":
+        gh = Q["grad"]
+        ge = _exact_at(exact_grad, x).reshape(gh.shape)
+        num = np.sum(w * np.sum((gh - ge) ** 2, axis=(-1, -2)))
+        den = np.sum(w * np.sum(ge**2, axis=(-1, -2)))
+    else:
+        problem = sol.problem
+        if problem is None or not hasattr(problem, "C"):
+            raise ValueError(f"the energy norm needs a problem with a constitutive matrix; "
+                             f"{type(problem).__name__} has none")
+        C = problem.C(sol.params)
+        Cinv = np.linalg.inv(C)
+        stress_h = _strain_voigt(Q["grad"]) @ C.T
+        stress_e = _exact_at(exact_grad, x).reshape(stress_h.shape)
+        d = stress_h - stress_e
+        num = np.sum(w * np.einsum("ni,ij,nj->n", d, Cinv, d))
+        den = np.sum(w * np.einsum("ni,ij,nj->n", stress_e, Cinv, stress_e))
     if not relative:
         return float(np.sqrt(num))
-    den = np.sum(w * np.sum(ue**2, -1))
     return float(np.sqrt(num / den))
 
 
 def norm(sol, norm: str = "L2", quad=None) -> float:
-    if norm != "L2":
-        raise NotImplementedError("the B200 backend computes the L2 norm")
-    g = geometry_operator(sol.space)
-    w = g.qp_weights().reshape(-1).cpu().numpy()
-    u = sol.at().reshape(-1, sol.space.vec)
-    return float(np.sqrt(np.sum(w * np.sum(u**2, -1))))
+    """L2 or H1 norm of the solution field (post/norms.py:43-56)."""
+    if norm not in ("L2", "H1"):
+        raise ValueError(f"unknown norm {norm!r}")
+    Q = _quadrature(sol.space, quad, sol._coef(), grad=norm == "H1")
+    s = np.sum(Q["w"] * np.sum(Q["val"] ** 2, -1))
+    if norm == "H1":
+        s += np.sum(Q["w"] * np.sum(Q["grad"] ** 2, axis=(-1, -2)))
+    return float(np.sqrt(s))
 
 
 def integrate(fn, space, quad=None) -> float:
     """Integral of ``fn(x)`` over the patch; ``x`` is (n_points, dim) (post/norms.py:36-40)."""
-    if quad is not None:
-        raise NotImplementedError("the B200 backend uses the default Gauss rule")
-    w = geometry_operator(space).qp_weights().reshape(-1).cpu().numpy()
-    x = qp_points(space)
+    Q = _quadrature(space, quad)
+    w, x = Q["w"], Q["x"]
     try:
         v = np.asarray(fn(x), dtype=float).reshape(x.shape[0], -1)
     except Exception:

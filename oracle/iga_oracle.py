@@ -301,15 +301,21 @@ def dirichlet(space, specs):
 # --------------------------------------------------------------------------
 
 
-def evaluate(space, elems, n_q=None, order=1):
-    """BasisData on the interior Gauss set for ``elems`` (evaluation.py:305-467).
+def evaluate(space, elems, n_q=None, order=1, ref=None, weights=None):
+    """BasisData on the interior Gauss set for ``elems`` (evaluation.py:305-467),
+    or on the reference points ``ref`` (n_q, dim) shared by every element with
+    reference weights ``weights`` (pointset.py:27-75; unit weights if None).
 
     Returns dict with R (n_e,n_q,n_loc), dR (n_e,n_q,dim,n_loc),
     d2R (n_e,n_q,n_d2,n_loc) or None, x (n_e,n_q,dim), w (n_e,n_q).
     """
     dim = space.dim
-    nq = [(p + 1) if n_q is None else int(n_q) for p in space.degree]
-    ref, wq = gauss_rule(nq)
+    if ref is None:
+        nq = [(p + 1) if n_q is None else int(n_q) for p in space.degree]
+        ref, wq = gauss_rule(nq)
+    else:
+        ref = np.asarray(ref, dtype=float).reshape(-1, dim)
+        wq = np.ones(len(ref)) if weights is None else np.asarray(weights, dtype=float)
     B, dB, d2B = bernstein_tensor(ref, space.degree, order=order)
     elems = np.asarray(elems)
     boxes = space.elem_vertex[elems]

@@ -233,3 +233,47 @@ def test_linear_options_learned_and_restarts():
         with pytest.raises(ValueError, match="restarts"):
             jx.LinearOptions(restarts=bad)
     assert jx.LinearOptions().restarts == 3
+
+
+def test_point_set_gauss_rule_matches_oracle_order():
+    import jaxiga_b200 as jx
+    from oracle import iga_oracle as O
+
+    kn = np.linspace(0, 1, 4)[1:-1]
+    V = jx.FunctionSpace(jx.primitives.cuboid([0, 0, 0], [1, 1, 1]).elevate(2).insert_knots(kn, kn, kn))
+    for q in (None, 2, 5):
+        ps = jx.gauss(V, q)
+        pts, wts = O.gauss_rule([(p + 1) if q is None else q for p in V.degree])
+        assert np.array_equal(ps.ref, pts) and np.array_equal(ps.weights, wts)
+        e, r = ps.flat()
+        assert e.shape == (V.n_elems * len(pts),) and r.shape == (V.n_elems * len(pts), 3)
+        assert np.array_equal(e[: len(pts)], np.zeros(len(pts))) and np.array_equal(r[: len(pts)], pts)
+    per_elem = jx.PointSet(elems=[3, 1], ref=np.zeros((2, 4, 3)))
+    assert not per_elem.shared_ref and per_elem.n_pts == 8
+    with pytest.raises(ValueError):
+        jx.PointSet(elems=[0, 1, 2], ref=np.zeros((2, 4, 3)))
+
+
+def test_error_norm_argument_checks_come_first():
+    import jaxiga_b200 as jx
+
+    sol = jx.Solution(space=None, u=None)
+    with pytest.raises(ValueError, match="unknown norm"):
+        jx.errornorm(sol, lambda x: x, "H2")
+    with pytest.raises(ValueError, match="exact_grad"):
+        jx.errornorm(sol, lambda x: x, "H1")
+    with pytest.raises(ValueError, match="unknown norm"):
+        jx.norm(sol, "energy")
+
+
+def test_elasticity_constitutive_matches_oracle():
+    import jaxiga_b200 as jx
+    from oracle import iga_oracle as O
+
+    for dim, plane in ((3, "stress"), (2, "stress"), (2, "strain")):
+        kn = np.linspace(0, 1, 3)[1:-1]
+        patch = (jx.primitives.cuboid([0, 0, 0], [1, 1, 1]).elevate(2).insert_knots(kn, kn, kn) if dim == 3 else
+                 jx.primitives.rectangle(0, 0, 1, 1).elevate(2).insert_knots(kn, kn))
+        V = jx.FunctionSpace(patch, vec=dim)
+        pr = jx.LinearElasticity(V, plane=plane)
+        assert np.allclose(pr.C({"E": 2.0, "nu": 0.25}), O.isotropic(2.0, 0.25, dim, plane), rtol=1e-15, atol=0)
