@@ -18,6 +18,7 @@ Quick start (the reference's README example)::
     sol = jx.solve(problem, params={"a0": 1.0})
 """
 
+from .adjoint import SOLVE_COUNTER, adjoint_solve, parameter_gradients, reset_solve_counter, value_and_grad
 from .forms import (ClampedBC, DirichletBC, KirchhoffPlate, LinearElasticity, Neumann, PointField, Poisson,
                     Problem)
 from .geometry import Patch, primitives
@@ -32,5 +33,6 @@ __all__ = [
     "Patch", "primitives", "FunctionSpace", "expand_dofs", "bezier_extraction", "element_spans",
     "Problem", "DirichletBC", "ClampedBC", "Neumann", "PointField", "Poisson", "LinearElasticity",
     "KirchhoffPlate", "solve", "LinearOptions", "Solution", "errornorm", "norm", "integrate", "Operator",
-    "PointSet", "gauss",
+    "PointSet", "gauss", "value_and_grad", "adjoint_solve", "parameter_gradients", "SOLVE_COUNTER",
+    "reset_solve_counter",
 ]

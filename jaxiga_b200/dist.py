@@ -1,8 +1,8 @@
 """Multi-process plumbing (one process per GPU, torch.distributed).
 
-The single-patch apply does not shard in this build (one patch = one GPU;
-``bench.py --gpus N`` runs N replicas). What does shard is a batch of
-independent instances: ``partition_by_cost`` assigns instances to ranks so
+One patch splits into slabs of element layers with a p-layer exchange
+(``jaxiga_b200.slab``). A batch of independent instances shards without
+communication: ``partition_by_cost`` assigns instances to ranks so
 that the per-rank work (elements, the apply's cost driver) is balanced --
 largest first onto the least-loaded rank, ties to the lowest rank, so every
 rank computes the same assignment without communication. Timings combine as

@@ -305,6 +305,9 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     fp32_operator = linear.precision == "mixed" and problem.op != "plate"
     op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)
+    from .adjoint import SOLVE_COUNTER
+
+    SOLVE_COUNTER["forward"] += 1
     if linear.preconditioner == "learned":
         from .learned import LearnedPreconditioner
 
