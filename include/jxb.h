@@ -175,6 +175,27 @@ int jxb_interpolate_grad(jxb_plan* plan, jxb_stream stream, const double* coef, 
  *   its quadrature weights. Out-of-range element indices give NaN. */
 int jxb_eval_points(jxb_plan* plan, jxb_stream stream, const double* coef, int ncomp, int64_t n,
                     const int64_t* elems, const double* ref, double* val, double* grad, double* x, double* jac);
+/* Neumann loads (tractions / fluxes on boundary sides): the work term
+ * neumann_work of src/jaxiga/methods/_common.py:312-318 on the boundary Gauss
+ * sets of src/jaxiga/space/pointset.py:148-200.
+ * jxb_boundary_points: face f is side sides[f] (2 * direction + end) of element
+ *   elems[f]; its n_q points sit at ref (n_faces * n_q, dim) with reference
+ *   weights wref (n_faces * n_q). Writes physical points x and outward unit
+ *   normals (n_faces * n_q, dim) and surface weights w = wref * surface
+ *   Jacobian * tangential half-widths (src/jaxiga/space/evaluation.py:174-193,
+ *   432-455); any output may be NULL. All arrays are device arrays.
+ * jxb_boundary_load: F[vec*i + c] += sum over faces and points of
+ *   w t[c] R_i for tractions t (n_faces * n_q, vec) at those points. local is
+ *   scratch of n_faces * (p+1)^dim * vec doubles (face-local loads); the
+ *   scatter is deterministic: scalar DOF dofs[k] (k < n_touched) receives the
+ *   local entries contrib[ptr[k] .. ptr[k+1]) (indices face * (p+1)^dim + a,
+ *   a the element-local basis function, first direction fastest), in that order. */
+int jxb_boundary_points(jxb_plan* plan, jxb_stream stream, int64_t n_faces, int n_q, const int64_t* elems,
+                        const int32_t* sides, const double* ref, const double* wref, double* x, double* normal,
+                        double* w);
+int jxb_boundary_load(jxb_plan* plan, jxb_stream stream, int64_t n_faces, int n_q, const int64_t* elems,
+                      const double* ref, const double* w, const double* traction, int64_t n_touched,
+                      const int64_t* dofs, const int64_t* ptr, const int64_t* contrib, double* local, double* F);
 int jxb_load(jxb_plan* plan, jxb_stream stream, const double* f_qp, double* F);
 /* jxb_qp_weights: integration weights w_hat |J| prod(h/2) at every Gauss point,
  *   (n_elem, n_q^dim) -- BasisData.w of src/jaxiga/space/evaluation.py:461-463. */

@@ -782,6 +782,214 @@ int eval_points(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, l
   return JXB_OK;
 }
 
+// Geometry of boundary points: point q of face f lies on side sides[f]
+// (2 * direction + end) of element elems[f] at ref[f, q]. Writes the physical
+// point, the outward unit normal n ~ dxdxi^-1 e_d with the side's sign, and
+// the surface weight wref * |tangent| (2D) or |t0 x t1| (3D) * prod of the
+// tangential half-widths (evaluation.py:174-193, 432-455).
+__device__ void boundary_geometry(const EvalArgs& A, long long e, int side, const double* xi, double* x, double* nrm,
+                                  double* surf, double* nv_out, int P1) {
+  const Bricks& br = A.br;
+  const int dim = br.dim;
+  const int sp[3] = {(int)(e % br.n_span[0]), (int)((e / br.n_span[0]) % br.n_span[1]),
+                     (int)(e / ((long long)br.n_span[0] * br.n_span[1]))};
+  double nv[3][JXB_MAXP + 1], nd[3][JXB_MAXP + 1], half[3] = {1, 1, 1};
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < P1; ++a) {
+      nv[d][a] = d < dim ? 0.0 : 1.0;
+      nd[d][a] = 0.0;
+    }
+  for (int d = 0; d < dim; ++d) {
+    double B[JXB_MAXP + 1], dB[JXB_MAXP + 1], d2B[JXB_MAXP + 1];
+    bernstein_point(xi[d], br.p, B, dB, d2B);
+    const double h = A.hi[d][sp[d]] - A.lo[d][sp[d]];
+    const double* C = A.ext[d] + (size_t)sp[d] * P1 * P1;
+    for (int a = 0; a < P1; ++a) {
+      double v = 0, g = 0;
+      for (int j = 0; j < P1; ++j) {
+        v += C[a * P1 + j] * B[j];
+        g += C[a * P1 + j] * dB[j];
+      }
+      nv[d][a] = v;
+      nd[d][a] = g * 2.0 / h;
+    }
+    half[d] = h / 2.0;
+  }
+  if (nv_out)
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < P1; ++a) nv_out[d * (JXB_MAXP + 1) + a] = nv[d][a];
+  const int f0 = br.first[0][sp[0]], f1 = br.first[1][sp[1]], f2 = dim == 3 ? br.first[2][sp[2]] : 0;
+  double W = 0, Wd[3] = {0, 0, 0}, P[3] = {0, 0, 0}, Pd[3][3] = {};
+  const int n2 = dim == 3 ? P1 : 1;
+  for (int a2 = 0; a2 < n2; ++a2)
+    for (int a1 = 0; a1 < P1; ++a1)
+      for (int a0 = 0; a0 < P1; ++a0) {
+        const long long cp = (long long)(f0 + a0) +
+                             (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
+        const double w = A.wgts[cp];
+        const double N = w * nv[0][a0] * nv[1][a1] * nv[2][a2];
+        const double dN[3] = {w * nd[0][a0] * nv[1][a1] * nv[2][a2], w * nv[0][a0] * nd[1][a1] * nv[2][a2],
+                              w * nv[0][a0] * nv[1][a1] * nd[2][a2]};
+        W += N;
+        for (int q = 0; q < dim; ++q) Wd[q] += dN[q];
+        for (int i = 0; i < dim; ++i) {
+          const double X = A.cpts[cp * dim + i];
+          P[i] += N * X;
+          for (int q = 0; q < dim; ++q) Pd[i][q] += dN[q] * X;
+        }
+      }
+  const double iW = 1.0 / W;
+  double J[3][3] = {}, Ji[3][3];
+  for (int i = 0; i < dim; ++i) {
+    x[i] = P[i] * iW;
+    for (int a = 0; a < dim; ++a) J[a][i] = (Pd[i][a] - x[i] * Wd[a]) * iW;
+  }
+  det_inv(dim, J, Ji);
+  const int dir = side / 2;
+  const double sign = (side % 2) ? 1.0 : -1.0;
+  double len = 0;
+  for (int k = 0; k < dim; ++k) len += Ji[k][dir] * Ji[k][dir];
+  len = sqrt(len);
+  for (int k = 0; k < dim; ++k) nrm[k] = sign * Ji[k][dir] / len;
+  double sj, tang = 1.0;
+  if (dim == 2) {
+    const int t = 1 - dir;
+    sj = sqrt(J[t][0] * J[t][0] + J[t][1] * J[t][1]);
+    tang = half[t];
+  } else {
+    const int t0 = dir == 0 ? 1 : 0, t1 = dir == 2 ? 1 : 2;
+    const double c0 = J[t0][1] * J[t1][2] - J[t0][2] * J[t1][1];
+    const double c1 = J[t0][2] * J[t1][0] - J[t0][0] * J[t1][2];
+    const double c2 = J[t0][0] * J[t1][1] - J[t0][1] * J[t1][0];
+    sj = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    tang = half[t0] * half[t1];
+  }
+  *surf = sj * tang;
+}
+
+__global__ void k_boundary_points(EvalArgs A, long long n_faces, int n_q, const long long* __restrict__ elems,
+                                  const int* __restrict__ sides, const double* __restrict__ ref,
+                                  const double* __restrict__ wref, double* x, double* normal, double* w) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_faces * n_q) return;
+  const int dim = A.br.dim;
+  const long long f = k / n_q;
+  double xx[3], nn[3], surf;
+  boundary_geometry(A, elems[f], sides[f], ref + k * dim, xx, nn, &surf, nullptr, A.br.p + 1);
+  for (int i = 0; i < dim; ++i) {
+    if (x) x[k * dim + i] = xx[i];
+    if (normal) normal[k * dim + i] = nn[i];
+  }
+  if (w) w[k] = wref[k] * surf;
+}
+
+// Face-local loads: local[f, a, c] = sum_q w_q t_q[c] R_a(x_q), one thread per
+// (face, local basis function a), a first-direction-fastest over the element.
+__global__ void k_boundary_local(EvalArgs A, long long n_faces, int n_q, const long long* __restrict__ elems,
+                                 const double* __restrict__ ref, const double* __restrict__ w,
+                                 const double* __restrict__ t, int vec, double* local) {
+  const Bricks& br = A.br;
+  const int dim = br.dim, P1 = br.p + 1;
+  const int n_loc = dim == 3 ? P1 * P1 * P1 : P1 * P1;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_faces * n_loc) return;
+  const long long f = k / n_loc;
+  const int a = (int)(k % n_loc);
+  const int a0 = a % P1, a1 = (a / P1) % P1, a2 = dim == 3 ? a / (P1 * P1) : 0;
+  const long long e = elems[f];
+  const int sp[3] = {(int)(e % br.n_span[0]), (int)((e / br.n_span[0]) % br.n_span[1]),
+                     (int)(e / ((long long)br.n_span[0] * br.n_span[1]))};
+  const int f0 = br.first[0][sp[0]], f1 = br.first[1][sp[1]], f2 = dim == 3 ? br.first[2][sp[2]] : 0;
+  double acc[3] = {0, 0, 0};
+  for (int q = 0; q < n_q; ++q) {
+    const long long pq = f * n_q + q;
+    double nv[3][JXB_MAXP + 1];
+    for (int d = 0; d < 3; ++d)
+      for (int b = 0; b < P1; ++b) nv[d][b] = d < dim ? 0.0 : 1.0;
+    for (int d = 0; d < dim; ++d) {
+      double B[JXB_MAXP + 1], dB[JXB_MAXP + 1], d2B[JXB_MAXP + 1];
+      bernstein_point(ref[pq * dim + d], br.p, B, dB, d2B);
+      const double* C = A.ext[d] + (size_t)sp[d] * P1 * P1;
+      for (int b = 0; b < P1; ++b) {
+        double v = 0;
+        for (int j = 0; j < P1; ++j) v += C[b * P1 + j] * B[j];
+        nv[d][b] = v;
+      }
+    }
+    double W = 0;
+    const int n2 = dim == 3 ? P1 : 1;
+    for (int b2 = 0; b2 < n2; ++b2)
+      for (int b1 = 0; b1 < P1; ++b1)
+        for (int b0 = 0; b0 < P1; ++b0) {
+          const long long cp = (long long)(f0 + b0) +
+                               (long long)br.n_cp[0] * ((f1 + b1) + (long long)br.n_cp[1] * (f2 + b2));
+          W += A.wgts[cp] * nv[0][b0] * nv[1][b1] * nv[2][b2];
+        }
+    const long long cpa = (long long)(f0 + a0) +
+                          (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
+    const double R = A.wgts[cpa] * nv[0][a0] * nv[1][a1] * nv[2][a2] / W;
+    for (int c = 0; c < vec; ++c) acc[c] += w[pq] * t[pq * vec + c] * R;
+  }
+  for (int c = 0; c < vec; ++c) local[k * vec + c] = acc[c];
+}
+
+// F[vec * dof[i] + c] += sum over j in [ptr[i], ptr[i+1]) of local[contrib[j] * vec + c],
+// in the fixed order of contrib (deterministic, no atomics).
+__global__ void k_boundary_gather(long long n_touched, const long long* __restrict__ dof,
+                                  const long long* __restrict__ ptr, const long long* __restrict__ contrib, int vec,
+                                  const double* __restrict__ local, double* F) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_touched) return;
+  for (int c = 0; c < vec; ++c) {
+    double s = 0;
+    for (long long j = ptr[i]; j < ptr[i + 1]; ++j) s += local[contrib[j] * vec + c];
+    F[dof[i] * vec + c] += s;
+  }
+}
+
+static EvalArgs eval_args(jxb_plan* plan) {
+  EvalArgs A;
+  A.br = plan->br;
+  for (int d = 0; d < 3; ++d) {
+    A.ext[d] = plan->d_ext[d];
+    A.lo[d] = plan->d_lo[d];
+    A.hi[d] = plan->d_hi[d];
+  }
+  A.cpts = plan->d_cpts;
+  A.wgts = plan->d_wgts;
+  return A;
+}
+
+int boundary_points(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, const long long* elems,
+                    const int* sides, const double* ref, const double* wref, double* x, double* normal, double* w) {
+  if (n_faces < 0 || n_q < 1) return fail(JXB_ERR_INVALID, "jxb_boundary_points: bad sizes");
+  if (n_faces == 0) return JXB_OK;
+  const long long n = n_faces * n_q;
+  k_boundary_points<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(eval_args(plan), n_faces, n_q, elems, sides, ref,
+                                                                 wref, x, normal, w);
+  JXB_CUDA(cudaGetLastError());
+  return JXB_OK;
+}
+
+int boundary_load(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, const long long* elems,
+                  const double* ref, const double* w, const double* t, long long n_touched, const long long* dof,
+                  const long long* ptr, const long long* contrib, double* local, double* F) {
+  if (n_faces < 0 || n_q < 1 || n_touched < 0) return fail(JXB_ERR_INVALID, "jxb_boundary_load: bad sizes");
+  if (n_faces == 0) return JXB_OK;
+  const int P1 = plan->p + 1;
+  const long long n_loc = plan->dim == 3 ? P1 * P1 * P1 : P1 * P1;
+  const long long n = n_faces * n_loc;
+  k_boundary_local<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(eval_args(plan), n_faces, n_q, elems, ref, w, t,
+                                                                plan->vec, local);
+  JXB_CUDA(cudaGetLastError());
+  if (n_touched > 0) {
+    k_boundary_gather<<<(unsigned)((n_touched + 127) / 128), 128, 0, s>>>(n_touched, dof, ptr, contrib, plan->vec,
+                                                                          local, F);
+    JXB_CUDA(cudaGetLastError());
+  }
+  return JXB_OK;
+}
+
 int interpolate_grad(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out) {
   if (ncomp < 1 || ncomp > JXB_GRAD_MAXC)
     return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: ncomp must be in 1..3");

@@ -210,6 +210,11 @@ int interpolate(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, d
 int interpolate_grad(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
 int eval_points(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, long long n, const long long* elems,
                 const double* ref, double* val, double* grad, double* x, double* jac);
+int boundary_points(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, const long long* elems,
+                    const int* sides, const double* ref, const double* wref, double* x, double* normal, double* w);
+int boundary_load(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, const long long* elems,
+                  const double* ref, const double* w, const double* t, long long n_touched, const long long* dof,
+                  const long long* ptr, const long long* contrib, double* local, double* F);
 int qp_weights(jxb_plan* plan, cudaStream_t s, double* w);
 
 // apply.cu

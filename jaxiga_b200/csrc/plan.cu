@@ -368,6 +368,28 @@ extern "C" int jxb_eval_points(jxb_plan* P, jxb_stream stream, const double* coe
                      reinterpret_cast<const long long*>(elems), ref, val, grad, x, jac);
 }
 
+extern "C" int jxb_boundary_points(jxb_plan* P, jxb_stream stream, int64_t n_faces, int n_q, const int64_t* elems,
+                                   const int32_t* sides, const double* ref, const double* wref, double* x,
+                                   double* normal, double* w) {
+  if (!P || (n_faces > 0 && (!elems || !sides || !ref || (w && !wref))))
+    return fail(JXB_ERR_INVALID, "jxb_boundary_points: null argument");
+  return boundary_points(P, reinterpret_cast<cudaStream_t>(stream), n_faces, n_q,
+                         reinterpret_cast<const long long*>(elems), sides, ref, wref, x, normal, w);
+}
+
+extern "C" int jxb_boundary_load(jxb_plan* P, jxb_stream stream, int64_t n_faces, int n_q, const int64_t* elems,
+                                 const double* ref, const double* w, const double* traction, int64_t n_touched,
+                                 const int64_t* dofs, const int64_t* ptr, const int64_t* contrib, double* local,
+                                 double* F) {
+  if (!P || (n_faces > 0 && (!elems || !ref || !w || !traction || !local || !F)) ||
+      (n_touched > 0 && (!dofs || !ptr || !contrib)))
+    return fail(JXB_ERR_INVALID, "jxb_boundary_load: null argument");
+  return boundary_load(P, reinterpret_cast<cudaStream_t>(stream), n_faces, n_q,
+                       reinterpret_cast<const long long*>(elems), ref, w, traction, n_touched,
+                       reinterpret_cast<const long long*>(dofs), reinterpret_cast<const long long*>(ptr),
+                       reinterpret_cast<const long long*>(contrib), local, F);
+}
+
 extern "C" int jxb_qp_weights(jxb_plan* P, jxb_stream stream, double* w) {
   if (!P || !w) return fail(JXB_ERR_INVALID, "jxb_qp_weights: null argument");
   return qp_weights(P, reinterpret_cast<cudaStream_t>(stream), w);

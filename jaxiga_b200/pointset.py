@@ -21,11 +21,13 @@ from .space import gauss_1d
 
 @dataclasses.dataclass(frozen=True)
 class PointSet:
-    """Evaluation points attached to elements of a function space."""
+    """Evaluation points attached to elements of a function space. ``sides``
+    (boundary sets only) holds each element's side code 2 * direction + end."""
 
     elems: np.ndarray
     ref: np.ndarray
     weights: np.ndarray | None = None
+    sides: np.ndarray | None = None
     tag: str = "interior"
 
     def __post_init__(self):
@@ -86,3 +88,28 @@ def gauss(space, n: int | None = None) -> PointSet:
     p + 1) (pointset.py:115-136)."""
     pts, wts = tensor_rule([(p + 1) if n is None else int(n) for p in space.degree])
     return PointSet(elems=np.arange(space.n_elems), ref=pts, weights=wts, tag="interior")
+
+
+def boundary_gauss(space, bset, n: int | None = None, label: str = "set") -> PointSet:
+    """Gauss rule of dimension dim - 1 on the sides of a boundary set, per
+    element (pointset.py:148-200): the tangential directions carry ``n``
+    (default p + 1) points, the pinned one sits at -1 or +1."""
+    dim = space.dim
+    n_per_dir = [(p + 1) if n is None else int(n) for p in space.degree]
+    sides = np.asarray(bset.sides, dtype=np.int64)
+    rules = {}
+    for code in np.unique(sides):
+        direction, end = divmod(int(code), 2)
+        tangential = [d for d in range(dim) if d != direction]
+        fp, fw = tensor_rule([n_per_dir[d] for d in tangential])
+        pts = np.zeros((len(fp), dim))
+        for k, d in enumerate(tangential):
+            pts[:, d] = fp[:, k]
+        pts[:, direction] = -1.0 if end == 0 else 1.0
+        rules[int(code)] = (pts, fw)
+    n_q = len(next(iter(rules.values()))[0]) if rules else 0
+    ref = np.zeros((len(sides), n_q, dim))
+    wts = np.zeros((len(sides), n_q))
+    for i, code in enumerate(sides):
+        ref[i], wts[i] = rules[int(code)]
+    return PointSet(elems=np.asarray(bset.elems), ref=ref, weights=wts, sides=sides, tag=f"boundary:{label}")

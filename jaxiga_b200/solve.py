@@ -242,7 +242,8 @@ def _problem_operator(problem, params, want_f32):
 
 
 def _rhs(problem, params, op, prescribed, values):
-    """b = F - K_fp g on the device (methods/galerkin.py:240-245)."""
+    """b = F - K_fp g on the device (methods/galerkin.py:240-245), F the source
+    and Neumann loads (methods/_common.py:280-318)."""
     import torch
 
     space = problem.space
@@ -253,6 +254,10 @@ def _rhs(problem, params, op, prescribed, values):
         f = call_points(problem.source, x, flat_params(params, x.shape[0]))
         f = np.broadcast_to(f.reshape(x.shape[0], -1), (x.shape[0], space.vec))
         F = op.load(np.array(f, dtype=np.float64, copy=True))
+    if problem.neumann:
+        from .neumann import neumann_load
+
+        F = neumann_load(op, problem, params, F)
     g = np.zeros(n)
     g[prescribed] = values
     if np.any(values != 0):
@@ -265,8 +270,6 @@ def _check_problem(problem, method):
         raise NotImplementedError(f"method={method!r}: the B200 backend implements 'galerkin' only")
     if not problem.is_linear:
         raise NotImplementedError("the B200 backend solves linear problems only")
-    if problem.neumann:
-        raise NotImplementedError("Neumann loads are not applied by the B200 backend")
     if problem.quadrature is not None and problem.quadrature != problem.space.degree[0] + 1:
         raise NotImplementedError("the B200 backend uses the default p+1 Gauss rule")
 

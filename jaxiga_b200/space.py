@@ -186,6 +186,19 @@ class FunctionSpace:
             ien += (self.first[d][idx[d]][:, None] + local[d][None, :]) * strides[d]
         return ien
 
+    def element_dofs(self, elems) -> np.ndarray:
+        """Scalar DOFs of the given elements only, (len(elems), (p+1)^dim) (function_space.py:326-369)."""
+        elems = np.asarray(elems, dtype=np.int64).reshape(-1)
+        strides = np.array([1, *np.cumprod(self.n_cp[:-1])], dtype=np.int64)
+        local = np.indices([p + 1 for p in self.degree[::-1]]).reshape(self.dim, -1)[::-1]
+        out = np.zeros((len(elems), self.n_local), dtype=np.int64)
+        rest = elems.copy()
+        for d in range(self.dim):
+            idx = rest % self.n_span[d]
+            rest //= self.n_span[d]
+            out += (np.asarray(self.first[d])[idx][:, None] + local[d][None, :]) * strides[d]
+        return out
+
     @cached_property
     def elem_vertex(self) -> np.ndarray:
         idx = self.elem_index

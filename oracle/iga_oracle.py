@@ -369,6 +369,60 @@ def evaluate(space, elems, n_q=None, order=1, ref=None, weights=None):
     return {"R": R, "dR": dR_phys, "d2R": d2R_phys, "x": x, "w": w, "dofs": dofs}
 
 
+def evaluate_boundary(space, elems, sides, ref, wref):
+    """Boundary BasisData (evaluation.py:174-193, 432-455): per face f (side
+    sides[f] = 2 direction + end of element elems[f]) and point q at ref[f, q]
+    with reference weight wref[f, q]: R, x, outward unit normal and
+    w = wref |surface Jacobian| prod of tangential half-widths."""
+    dim = space.dim
+    R, X, N, W = [], [], [], []
+    for f, (e, code) in enumerate(zip(np.asarray(elems), np.asarray(sides))):
+        b = evaluate(space, [e], ref=ref[f], weights=np.ones(len(ref[f])))
+        direction, end = divmod(int(code), 2)
+        lo, hi = space.elem_vertex[e, :dim], space.elem_vertex[e, dim:]
+        # dxdxi[a, i] rows are the parametric tangents, from the (rational) basis
+        C = space.extraction([e])[0]
+        B, dB, _ = bernstein_tensor(ref[f], space.degree, order=1)
+        scale = 2.0 / (hi - lo)
+        Nb = B @ C.T
+        dNb = np.einsum("qdj,ij->qdi", dB, C) * scale[None, :, None]
+        dofs = space.elem_dofs[e]
+        wts = space.wgts[dofs]
+        M, dM = Nb * wts, dNb * wts
+        Wq, dW = M.sum(-1), dM.sum(-1)
+        dR = dM / Wq[:, None, None] - M[:, None, :] * dW[:, :, None] / Wq[:, None, None] ** 2
+        J = np.einsum("qan,ni->qai", dR, space.cpts[dofs])
+        tang = [a for a in range(dim) if a != direction]
+        if dim == 2:
+            sj = np.linalg.norm(J[:, tang[0]], axis=1)
+        else:
+            sj = np.linalg.norm(np.cross(J[:, tang[0]], J[:, tang[1]]), axis=1)
+        e_d = np.zeros(dim)
+        e_d[direction] = 1.0
+        nrm = np.linalg.solve(J, np.broadcast_to(e_d, (len(J), dim))[..., None])[..., 0]
+        nrm = nrm / np.linalg.norm(nrm, axis=1, keepdims=True) * (1.0 if end == 1 else -1.0)
+        half = np.prod([(hi[a] - lo[a]) / 2.0 for a in tang])
+        R.append(b["R"][0])
+        X.append(b["x"][0])
+        N.append(nrm)
+        W.append(wref[f] * sj * half)
+    return {"R": np.stack(R), "x": np.stack(X), "normal": np.stack(N), "w": np.stack(W),
+            "dofs": space.elem_dofs[np.asarray(elems)]}
+
+
+def neumann_load(space, elems, sides, ref, wref, traction):
+    """F_i,c = sum_q w t_c(x, n) R_i on the faces (the negative gradient of
+    neumann_work, methods/_common.py:312-318); traction(x, n) -> (n_pts, vec)."""
+    b = evaluate_boundary(space, elems, sides, ref, wref)
+    nf, nq = b["w"].shape
+    t = np.asarray(traction(b["x"].reshape(-1, space.dim), b["normal"].reshape(-1, space.dim)), dtype=float)
+    t = t.reshape(nf, nq, space.vec)
+    Fe = np.einsum("fq,fqc,fqi->fic", b["w"], t, b["R"]).reshape(nf, -1)
+    F = np.zeros(space.n_dofs)
+    np.add.at(F, space.expand(b["dofs"]), Fe)
+    return F
+
+
 # --------------------------------------------------------------------------
 # Element tangents (forms/library.py, forms/materials.py)
 # --------------------------------------------------------------------------

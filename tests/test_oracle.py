@@ -189,3 +189,35 @@ def test_cnn_oracle_pooled_forward_is_the_coarse_network_interpolated():
     g = rng.standard_normal((1, 7, 6, 5))
     np.testing.assert_allclose(C.backward(p, x, g, 2, ch, pool_input=True),
                                C.backward(p, C.pool(x), C.up_lin_grad(g, C.half(x.shape[1:])), 2, ch))
+
+
+def test_boundary_measures_and_normals_of_the_annulus():
+    """Boundary Gauss sets of the quarter annulus (radii 1 and 4, cubic, refined
+    three times): side lengths 2 pi, pi/2, 3, 3 to 1e-12 and radial outward
+    normals, the known answers of the reference's tests/test_evaluation.py:47-70."""
+    import jaxiga_b200 as jx
+    from jaxiga_b200.pointset import boundary_gauss
+
+    V = jx.FunctionSpace(jx.primitives.quarter_annulus(1.0, 4.0).elevate(3).refine(3))
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, 1)
+    exact = {"outer": 2 * np.pi, "inner": np.pi / 2, "sym_y": 3.0, "sym_x": 3.0}
+    for label, length in exact.items():
+        ps = boundary_gauss(V, V.boundary(label))
+        b = O.evaluate_boundary(S, ps.elems, ps.sides, ps.ref, ps.weights)
+        assert abs(b["w"].sum() - length) < 1e-12 * length, label
+        assert np.abs(np.linalg.norm(b["normal"], axis=-1) - 1.0).max() < 1e-13
+        if label in ("outer", "inner"):
+            r = np.linalg.norm(b["x"], axis=-1)[..., None]
+            sign = 1.0 if label == "outer" else -1.0
+            assert np.abs(b["normal"] - sign * b["x"] / r).max() < 1e-12
+
+
+def test_neumann_load_of_a_constant_flux_sums_to_the_side_length():
+    import jaxiga_b200 as jx
+    from jaxiga_b200.pointset import boundary_gauss
+
+    V = jx.FunctionSpace(jx.primitives.quarter_annulus(1.0, 4.0).elevate(3).refine(3))
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, 1)
+    ps = boundary_gauss(V, V.boundary("outer"))
+    F = O.neumann_load(S, ps.elems, ps.sides, ps.ref, ps.weights, lambda x, n: np.ones((len(x), 1)))
+    assert abs(F.sum() - 2 * np.pi) < 1e-12 * 2 * np.pi  # partition of unity: sum_i int R_i = arc length
