@@ -317,6 +317,44 @@ int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const doubl
                     const float* features, int n_features, float in_scale, double out_scale, int stall,
                     int depth, int mode, const jxb_solve_opts* opts, jxb_stats* stats);
 
+/* ---- geometric multigrid -------------------------------------------------
+ * A V-cycle over nested spline spaces of one patch (the finest first, each
+ * coarser level the same patch with every other interior knot removed), used
+ * as the preconditioner of CG. No counterpart in the reference, whose only
+ * preconditioner is Jacobi (src/jaxiga/solvers/linear.py:419-431).
+ *   jxb_transfer1d: one direction of the prolongation from level l+1 to level l,
+ *     a CSR matrix (HOST arrays) of rows = control points of level l along that
+ *     direction by cols = those of level l+1 (knot insertion); the tensor
+ *     product over the directions maps coarse DOFs to fine ones, the
+ *     restriction is its transpose.
+ *   jxb_mg_create: plans[0..n_levels) of the same operator kind on those
+ *     spaces (each plan listed once, its Dirichlet mask that of its level),
+ *     transfer[3 l + d] for l < n_levels - 1 and d < dim, coarse_inv the dense
+ *     row-major inverse of the coarsest operator on its free DOFs (zero rows and
+ *     columns on prescribed DOFs), n_dofs^2 doubles, host. degree (1..8): the
+ *     Chebyshev-Jacobi smoother's polynomial degree, applied before and after
+ *     each coarse correction; smooth_range (> 1): the ratio lmax / lmin of the
+ *     interval it damps, lmax of D^-1 K estimated at creation by a power
+ *     iteration. The plans must outlive the multigrid object.
+ *   jxb_mg_vcycle: z = V r on the finest level (r, z device, n_dofs).
+ *   jxb_mg_pcg: CG preconditioned by the V-cycle, with the stopping rule, stats
+ *     and return codes of jxb_pcg (opts->preconditioner and restarts unused).
+ *   jxb_mg_info: lmax[l] of D^-1 K per level (the coarsest stays 0). */
+typedef struct jxb_mg jxb_mg;
+typedef struct jxb_transfer1d {
+  int rows, cols;
+  const int32_t* ptr;  /* rows + 1 */
+  const int32_t* idx;  /* column of each entry */
+  const double* val;
+} jxb_transfer1d;
+int jxb_mg_create(jxb_plan* const* plans, int n_levels, const jxb_transfer1d* transfer, const double* coarse_inv,
+                  int degree, double smooth_range, jxb_mg** out);
+int jxb_mg_destroy(jxb_mg* mg);
+int jxb_mg_info(const jxb_mg* mg, double* lmax);
+int jxb_mg_vcycle(jxb_mg* mg, jxb_stream stream, const double* r, double* z);
+int jxb_mg_pcg(jxb_mg* mg, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
+               jxb_stats* stats);
+
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);
 

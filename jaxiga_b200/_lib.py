@@ -89,6 +89,16 @@ class Stats(ctypes.Structure):
     ]
 
 
+class Transfer1d(ctypes.Structure):
+    _fields_ = [
+        ("rows", ctypes.c_int),
+        ("cols", ctypes.c_int),
+        ("ptr", c_int32_p),
+        ("idx", c_int32_p),
+        ("val", c_double_p),
+    ]
+
+
 # (name, argtypes) of every exported entry point, in include/jxb.h order
 SIGNATURES = [
     ("jxb_plan_create", [ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_void_p)]),
@@ -149,6 +159,13 @@ SIGNATURES = [
     ("jxb_fcg_learned", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                          ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_int,
                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    ("jxb_mg_create", [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(Transfer1d), c_double_p,
+                       ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_mg_destroy", [ctypes.c_void_p]),
+    ("jxb_mg_info", [ctypes.c_void_p, c_double_p]),
+    ("jxb_mg_vcycle", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_mg_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                    ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_dot", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
     ("jxb_profile_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                            ctypes.c_int, c_double_p]),

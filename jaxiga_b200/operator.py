@@ -123,6 +123,10 @@ class Operator:
 
     # -- lifetime ------------------------------------------------------------
     def close(self):
+        mg = getattr(self, "_multigrid", None)
+        if mg is not None:  # its V-cycle holds this plan as its finest level
+            mg.close()
+            self._multigrid = None
         if getattr(self, "handle", None) is not None and self.handle.value:
             self.lib.jxb_plan_destroy(self.handle)
             self.handle = None

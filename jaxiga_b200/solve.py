@@ -45,6 +45,11 @@ class LinearOptions:
     ``maxiter``), the correction solves of the reference's CPU CG
     (solvers/linear.py:261-321).
 
+    ``preconditioner="multigrid"`` runs CG preconditioned by a geometric
+    multigrid V-cycle over the patch with every other knot removed level by
+    level (``jaxiga_b200.multigrid``; Chebyshev-Jacobi smoothing of degree
+    ``mg_degree`` on the interval lmax / ``mg_range`` .. lmax, FP64).
+
     ``preconditioner="learned"`` runs flexible CG with the trained network of
     ``checkpoint`` (see ``jaxiga_b200.learned``), Jacobi as its fallback;
     ``learned_map`` picks how the network output n enters: ``"network"`` (n
@@ -66,6 +71,8 @@ class LinearOptions:
     refinement: str = "reliable"
     update_delta: float = 1e-2
     restarts: int = 3
+    mg_degree: int = 3
+    mg_range: float = 20.0
     checkpoint: str | None = None
     learned_map: str = "additive"
     learned_stall: int = 50
@@ -79,8 +86,14 @@ class LinearOptions:
         allowed = {"cg", "bicgstab", "gmres", "dense", "scipy"}
         if self.method not in allowed:
             raise ValueError(f"unknown linear method {self.method!r}; expected one of {allowed}")
-        if self.preconditioner not in {"none", "jacobi", "learned"}:
-            raise ValueError(f"unknown preconditioner {self.preconditioner!r}; expected 'none', 'jacobi' or 'learned'")
+        if self.preconditioner not in {"none", "jacobi", "learned", "multigrid"}:
+            raise ValueError(f"unknown preconditioner {self.preconditioner!r}; expected 'none', 'jacobi', "
+                             f"'learned' or 'multigrid'")
+        if isinstance(self.mg_degree, (bool, np.bool_)) or not isinstance(self.mg_degree, (int, np.integer)) \
+                or not 1 <= self.mg_degree <= 8:
+            raise ValueError("mg_degree must be an integer in 1..8")
+        if not (np.isfinite(self.mg_range) and self.mg_range > 1):
+            raise ValueError("mg_range must be finite and > 1")
         if self.preconditioner == "learned" and not self.checkpoint:
             raise ValueError("preconditioner='learned' needs checkpoint=<path of a trained network (.npz)>")
         if self.learned_map not in {"network", "multiplicative", "additive"}:
@@ -325,6 +338,16 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         finally:
             lp.close()
         st["outer"] = st["learned_iterations"]
+    elif linear.preconditioner == "multigrid":
+        mg = getattr(op, "_multigrid", None)
+        if mg is None or mg.handle is None or (mg.degree, mg.smooth_range) != (linear.mg_degree, linear.mg_range):
+            from .multigrid import Multigrid
+
+            if mg is not None:
+                mg.close()
+            mg = Multigrid(problem, params, degree=linear.mg_degree, smooth_range=linear.mg_range, fine_op=op)
+            op._multigrid = mg
+        xdev, st = mg.solve(b, tol=linear.tol, maxiter=linear.maxiter, check_every=min(linear.check_every, 8))
     elif fp32_operator and linear.refinement == "reliable":
         xdev, st = op.mixed_pcg(b, tol=linear.tol, delta=linear.update_delta, maxiter=linear.maxiter,
                                 check_every=linear.check_every)
