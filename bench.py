@@ -277,7 +277,8 @@ def run_reference(args, rank, world):
 # our arm
 # ---------------------------------------------------------------------------
 def build_workload(name, span, dev):
-    """(space, operator, load vector, learned-network features, points per element)."""
+    """(space, operator, load vector, learned-network features, points per element,
+    (problem, parameters) for the multigrid hierarchy)."""
     import torch
 
     import jaxiga_b200 as jx
@@ -292,18 +293,17 @@ def build_workload(name, span, dev):
         op = jx.Operator(V, "plate", problem.operator_coefficients(params)[0], prescribed=mask, want_f32=True)
         nqe = 25
         F = op.load(torch.ones(V.n_elems * nqe, dtype=torch.float64, device=dev))
-        return V, op, F, None, nqe
+        return V, op, F, None, nqe, (problem, params)
     if name == "darcy":
         V, problem, params = workloads.config4(n=span)
-        a_qp = torch.exp(geometry_operator(V).interpolate(params["loga"])[..., 0])
+        a_qp = torch.exp(geometry_operator(V).interpolate(params["loga"])[..., 0]).cpu().numpy()
         pres, _ = problem.resolve_dirichlet(params)
         mask = np.zeros(V.n_dofs, bool)
         mask[pres] = True
-        op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a_qp.cpu().numpy(), want_f32=True)
-        del a_qp
+        op = jx.Operator(V, "poisson", (1.0,), prescribed=mask, coef_qp=a_qp, want_f32=True)
         F = op.load(torch.ones(V.n_elems * 64, dtype=torch.float64, device=dev))
         loga = params["loga"]
-        return V, op, F, ((loga - loga.mean()) / loga.std())[None, :], 64
+        return V, op, F, ((loga - loga.mean()) / loga.std())[None, :], 64, (problem, {"a0": jx.PointField(a_qp)})
     V, problem, params = workloads.config2(n=span)
     pres, _ = problem.resolve_dirichlet(params)
     mask = np.zeros(V.n_dofs, bool)
@@ -312,7 +312,7 @@ def build_workload(name, span, dev):
     fq = geometry_operator(V).interpolate(params["eta"])
     fq[..., 2] -= 1.0
     F = op.load(fq)
-    return V, op, F, None, 64
+    return V, op, F, None, 64, (problem, params)
 
 
 def workload_tag(name, span):
@@ -360,9 +360,10 @@ def _row(st, ref_x=None, x=None):
     return r
 
 
-def time_to_solution(name, span, op, F, feats):
+def time_to_solution(name, span, op, F, feats, problem_params=None):
     """Solves to TOL, each run twice and the second reported (the first
-    captures its CUDA graphs); speed-ups only for solves that converged."""
+    captures its CUDA graphs); speed-ups only for solves that converged. Set-up
+    (the multigrid hierarchy, a network's weights) is not in the timed solve."""
     tts = {"tol": TOL}
     for _ in range(2):
         x_p, st_p = op.pcg(F, tol=TOL, preconditioner="jacobi", check_every=32, maxiter=80000, restarts=3)
@@ -380,6 +381,17 @@ def time_to_solution(name, span, op, F, feats):
         for _ in range(2):
             x_r, st_r = op.mixed_pcg(F, tol=TOL, delta=1e-2, check_every=32, maxiter=80000)
         rows["mixed_fp32_pcg_reliable_fp64_updates"] = dict(_row(st_r, x_p, x_r), updates=int(st_r["outer"]))
+    if problem_params is not None:
+        from jaxiga_b200.multigrid import Multigrid
+
+        t0 = time.perf_counter()
+        mg = Multigrid(*problem_params, degree=3, smooth_range=20.0, fine_op=op)
+        mg_setup = time.perf_counter() - t0
+        for _ in range(2):
+            x_g, st_g = mg.solve(F, tol=TOL, maxiter=20000)
+        rows["multigrid_fp64_pcg"] = dict(_row(st_g, x_p, x_g), levels=mg.levels, setup_seconds=mg_setup,
+                                          smoother="Chebyshev-Jacobi, degree 3, range 20, before and after")
+        mg.close()
     tts.update(rows)
     tts["learned_preconditioner"] = None
     ckpt = os.path.join(ROOT, "jaxiga_b200", "checkpoints", f"{name}{span}.npz")
@@ -420,7 +432,7 @@ def measure_workload(name, span, dev, steps, peaks, peak_kind, solve=True):
     import torch
 
     t0 = time.perf_counter()
-    V, op, F, feats, nqe = build_workload(name, span, dev)
+    V, op, F, feats, nqe, pp = build_workload(name, span, dev)
     setup = time.perf_counter() - t0
     n_qp = V.n_elems * nqe
     x = torch.randn(V.n_dofs, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(7))
@@ -439,7 +451,7 @@ def measure_workload(name, span, dev, steps, peaks, peak_kind, solve=True):
            "value": V.n_dofs / (ms * 1e-3), "unit": UNIT, "ms_per_apply": ms, "setup_seconds": setup,
            "roofline": roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span)}
     if solve:
-        rec["time_to_solution"] = time_to_solution(name, span, op, F, feats)
+        rec["time_to_solution"] = time_to_solution(name, span, op, F, feats, pp)
     op.close()
     del F, x, y
     torch.cuda.empty_cache()
@@ -448,7 +460,7 @@ def measure_workload(name, span, dev, steps, peaks, peak_kind, solve=True):
 
 def matched_gpu_solve(dev):
     """GPU time to solution of the CPU baseline's workload (elasticity 16^3)."""
-    V, op, F, _, _ = build_workload("elasticity", CPU_SAMPLE_SPAN, dev)
+    V, op, F, _, _, _ = build_workload("elasticity", CPU_SAMPLE_SPAN, dev)
     for _ in range(2):
         _, st = op.pcg(F, tol=TOL, preconditioner="jacobi", check_every=32, restarts=3)
     for _ in range(2):
@@ -467,7 +479,7 @@ def run_ours(args, rank, world, local_rank):
     name = args.workload
     span = args.span or {"darcy": 96, "plate": 256}.get(name, N_SPAN)
     t_setup = time.perf_counter()
-    V, op, F, feats, nqe = build_workload(name, span, dev)
+    V, op, F, feats, nqe, pp = build_workload(name, span, dev)
     setup_s = time.perf_counter() - t_setup
     n = V.n_dofs
     n_qp = V.n_elems * nqe
@@ -527,7 +539,7 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * n * k_e2e / (float(t.item()) * 1e-3)
 
-    tts = None if args.no_solve else time_to_solution(name, span, op, F, feats)
+    tts = None if args.no_solve else time_to_solution(name, span, op, F, feats, pp)
     ngeo = op.info["ngeo"]
     op.close()
     del F, x, y, xd

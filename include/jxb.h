@@ -355,6 +355,24 @@ int jxb_mg_vcycle(jxb_mg* mg, jxb_stream stream, const double* r, double* z);
 int jxb_mg_pcg(jxb_mg* mg, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
                jxb_stats* stats);
 
+/* ---- Jacobi-PCG on an assembled CSR matrix ------------------------------
+ * The device CG of the staggered phase-field solver (DeviceCG,
+ * src/jaxiga/solvers/phase_field.py:305-390): the pattern is set once per
+ * mesh, each solve passes new values and right-hand side.
+ *   jxb_csr_create: n rows, indptr (n + 1, int64) and cols (int32), HOST arrays.
+ *   jxb_csr_matvec: y = A x for values (nnz), x, y device arrays.
+ *   jxb_csr_pcg: Jacobi-PCG with jax CG semantics from the warm start in x
+ *     (r0 = b - A x0, stop when r.r <= max(tol^2 b.b, atol^2) or at maxiter,
+ *     default 10 n); the diagonal of the given values with the reference's
+ *     guard (1/d where |d| > 0, else 1). Stats and return codes as jxb_pcg,
+ *     the residual being |b - A x| over all rows. */
+typedef struct jxb_csr jxb_csr;
+int jxb_csr_create(int64_t n, const int64_t* indptr, const int32_t* cols, jxb_csr** out);
+int jxb_csr_destroy(jxb_csr* csr);
+int jxb_csr_matvec(jxb_csr* csr, jxb_stream stream, const double* values, const double* x, double* y);
+int jxb_csr_pcg(jxb_csr* csr, jxb_stream stream, const double* values, const double* b, double* x,
+                const jxb_solve_opts* opts, jxb_stats* stats);
+
 /* ---- vector helpers used by hosts that drive their own Krylov loop ---- */
 int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const double* b, double* out_host);
 

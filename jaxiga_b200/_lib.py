@@ -166,6 +166,11 @@ SIGNATURES = [
     ("jxb_mg_vcycle", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_mg_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                     ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    ("jxb_csr_create", [ctypes.c_int64, c_int64_p, c_int32_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_csr_destroy", [ctypes.c_void_p]),
+    ("jxb_csr_matvec", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("jxb_csr_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                     ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_dot", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
     ("jxb_profile_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                            ctypes.c_int, c_double_p]),

@@ -634,7 +634,7 @@ def scipy_cg(A, b, tol, maxiter=None, preconditioner="jacobi"):
     return u, total
 
 
-def jax_cg(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0):
+def jax_cg(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0, x0=None):
     """Restatement of jax.scipy.sparse.linalg.cg (jax 0.11.1, ``_cg_solve``).
 
     x0 = 0; stop when r.r <= max(tol^2 b.b, atol^2) (unpreconditioned r when a
@@ -647,7 +647,7 @@ def jax_cg(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0):
     M = (lambda v: v) if inv_diag is None else (lambda v: inv_diag * v)
     bs = b @ b
     atol2 = max(tol**2 * bs, atol**2)
-    x = np.zeros_like(b)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=float)
     r = b - matvec(x)
     z = M(r)
     p = z.copy()

@@ -82,3 +82,17 @@ def with_fields(tag, V, params, interpolate):
 CASES = ["poisson2d", "patch2d", "annulus2d", "elast3d", "darcy3d", "plate2d"]
 OPS = {"poisson2d": "poisson", "patch2d": "poisson", "annulus2d": "poisson", "elast3d": "elasticity",
        "darcy3d": "poisson", "plate2d": "plate"}
+
+
+def make_operator_oracle(tag):
+    """The oracle's assembled free-free operator of a golden case (no per-point fields)."""
+    from oracle import iga_oracle as O
+
+    V, problem, params = build(tag)
+    pres, vals = problem.resolve_dirichlet(params)
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, V.vec)
+    coef, field = problem.operator_coefficients(params)
+    if field is not None:
+        raise ValueError(f"{tag} has a per-point coefficient")
+    names = {"poisson": ("a0",), "elasticity": ("E", "nu"), "plate": ("E", "nu", "t")}[OPS[tag]]
+    return O.Assembled(S, OPS[tag], dict(zip(names, coef)), pres, vals, need_full=False)
