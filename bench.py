@@ -360,6 +360,29 @@ def _row(st, ref_x=None, x=None):
     return r
 
 
+def time_network_of(lp, reps=10):
+    """Device ms of one forward of a preconditioner's network in BF16 inference
+    and in FP32, on a random residual (CUDA events on the current stream)."""
+    import torch
+
+    r = torch.randn(lp.op.n_dofs, dtype=torch.float64, device=lp.dev)
+    out = {}
+    for mode in (True, False):
+        lp.set_inference_bf16(mode)
+        for _ in range(3):
+            lp.forward(r)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            lp.forward(r)
+        e1.record()
+        torch.cuda.synchronize()
+        out["bf16" if mode else "fp32"] = e0.elapsed_time(e1) / reps
+    lp.set_inference_bf16(True)
+    return out
+
+
 def time_to_solution(name, span, op, F, feats, problem_params=None):
     """Solves to TOL, each run twice and the second reported (the first
     captures its CUDA graphs); speed-ups only for solves that converged. Set-up
@@ -398,7 +421,8 @@ def time_to_solution(name, span, op, F, feats, problem_params=None):
     if os.path.exists(ckpt):
         from jaxiga_b200.learned import LearnedPreconditioner
 
-        lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats)
+        # the network's inference runs its <= 32-channel convolutions on the BF16 tensor cores
+        lp = LearnedPreconditioner.from_checkpoint(op, ckpt, features=feats, inference_bf16=True)
         lrows = {}
         # FP32 operator rows only where the FP32 operator resolves the problem
         variants = [("learned_fcg_fp64", False, False), ("learned_two_level_fp64", False, True),
@@ -410,8 +434,22 @@ def time_to_solution(name, span, op, F, feats, problem_params=None):
             lp.solve(F, tol=TOL, mixed=mixed, two_level=two)
             x_l, st_l = lp.solve(F, tol=TOL, mixed=mixed, two_level=two)
             lrows[key] = dict(_row(st_l, x_p, x_l), learned_iterations=int(st_l["learned_iterations"]))
+        # the same additive map with the FP32 network, for comparison
+        lp.set_inference_bf16(False)
+        mixed_add = name != "plate"
+        lp.solve(F, tol=TOL, mixed=mixed_add, two_level="additive")
+        x_l, st_l = lp.solve(F, tol=TOL, mixed=mixed_add, two_level="additive")
+        lrows["learned_additive_fp32_network"] = dict(_row(st_l, x_p, x_l), mixed=mixed_add,
+                                                      learned_iterations=int(st_l["learned_iterations"]))
+        lp.set_inference_bf16(True)
+        try:
+            lrows["network_forward_ms"] = dict(time_network_of(lp, reps=10), grid=list(lp.grid))
+        except Exception as exc:  # timing is informative only
+            lrows["network_forward_ms"] = {"error": str(exc)}
         tts["learned_preconditioner"] = {
             "checkpoint": os.path.relpath(ckpt, ROOT), "channels": list(lp.channels), "params": lp.n_params,
+            "inference": "BF16 tensor-core convolutions (mma.sync m16n8k16, FP32 accumulation) on layers of <= 32 "
+                         "channels, FP32 elsewhere",
             "pool_input": lp.pool_input, "additive_weight": lp.additive_weight,
             "training": "offline, python -m jaxiga_b200.train_pc (not in the timed solve)", **lrows}
         rows.update(lrows)

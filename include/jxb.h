@@ -303,6 +303,12 @@ typedef struct jxb_cnn jxb_cnn;
 int jxb_cnn_create(int in_ch, int out_ch, int levels, const int* channels, uint64_t seed, jxb_cnn** out);
 int jxb_cnn_destroy(jxb_cnn* cnn);
 int jxb_cnn_set_input_pooling(jxb_cnn* cnn, int on);
+/* jxb_cnn_set_inference_bf16: on = 1 makes inference forwards (jxb_cnn_forward and
+ *   the network applications inside jxb_fcg_learned) run every 3x3x3 layer of at
+ *   most 32 input and output channels as a BF16 tensor-core implicit GEMM
+ *   (mma.sync m16n8k16, FP32 accumulation); training forwards stay FP32, and a
+ *   jxb_cnn_backward after a BF16 forward is refused. */
+int jxb_cnn_set_inference_bf16(jxb_cnn* cnn, int on);
 int jxb_cnn_params(jxb_cnn* cnn, float** params, int64_t* n);
 int jxb_cnn_grads(jxb_cnn* cnn, float** grads, int64_t* n);
 int jxb_cnn_forward(jxb_cnn* cnn, jxb_stream stream, int nx, int ny, int nz, const float* in, float* out);

@@ -143,6 +143,7 @@ SIGNATURES = [
                         ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_cnn_destroy", [ctypes.c_void_p]),
     ("jxb_cnn_set_input_pooling", [ctypes.c_void_p, ctypes.c_int]),
+    ("jxb_cnn_set_inference_bf16", [ctypes.c_void_p, ctypes.c_int]),
     ("jxb_cnn_params", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_int64_p]),
     ("jxb_cnn_grads", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_int64_p]),
     ("jxb_cnn_forward", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -34,6 +34,7 @@
 // Weight gradients are per-tile partials (one thread per input channel and
 // tap, the block's output channels in registers) summed over tiles in a
 // fixed order, so training is bitwise reproducible run to run.
+#include <cuda_bf16.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -57,7 +58,7 @@ struct Dims {
   __host__ __device__ long long vox() const { return (long long)nx * ny * nz; }
 };
 
-static Dims half(Dims d) { return {(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2}; }
+static Dims halve(Dims d) { return {(d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2}; }
 static long long n_tiles(Dims d) {
   return (long long)((d.nx + CTX - 1) / CTX) * ((d.ny + CTY - 1) / CTY) * ((d.nz + CTZ - 1) / CTZ);
 }
@@ -543,6 +544,160 @@ __global__ void k_init(long long n, unsigned long long seed, float a, float* p) 
   p[i] = (2.f * u - 1.f) * a;
 }
 
+// ---------------------------------------------------------------------------
+// BF16 tensor-core 3x3x3 convolution for inference (the preconditioner's
+// forward pass), as an implicit GEMM on mma.sync.m16n8k16 (BF16 operands,
+// FP32 accumulation): rows are output voxels, columns output channels, and the
+// reduction runs over K = 27 taps x CINP input channels (tap-major, padded to
+// a multiple of 16 with zeros). A CTA computes an 8 x 8 x 4 voxel tile: its
+// input halo (10 x 10 x 6 voxels) is staged once in shared memory as BF16,
+// channel-last, and the layer's weights as BF16 rows [co][k]; each warp owns
+// MF row fragments of 16 voxels and every output channel. Row strides are
+// padded so that the 32-bit fragment loads are free of bank conflicts
+// (stride / 2 = 4 mod 8 words). The epilogue adds bias and skip input, applies
+// the ReLU and writes FP32 channel-first activations, as the FP32 kernel does.
+// Training keeps the FP32 kernels; this path serves layers of at most 32 input
+// and output channels, the fine levels where the network spends its time.
+namespace mmaconv {
+constexpr int TX = 8, TY = 8, TZ = 4, NV = TX * TY * TZ;  // output tile
+constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2, HV = HX * HY * HZ;
+__host__ __device__ constexpr int cin_stride(int cinp) { return ((cinp / 2) % 8 == 4) ? cinp : cinp + 8; }
+__host__ __device__ constexpr int k_pad(int cinp) { return (27 * cinp + 15) / 16 * 16; }
+__host__ __device__ constexpr int k_stride(int cinp) { return k_pad(cinp) + 8; }
+__host__ __device__ constexpr int frags(int co) { return co <= 16 ? 4 : 2; }  // row fragments per warp
+__host__ __device__ constexpr int warps(int co) { return NV / 16 / frags(co); }
+inline size_t smem(int cinp, int co) {
+  return (size_t)HV * cin_stride(cinp) * 2 + (size_t)co * k_stride(cinp) * 2;
+}
+}  // namespace mmaconv
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// wb[co][k] (row stride k_stride) = bf16(w[co][ci][tap]) with k = tap * CINP + ci, zero padding
+__global__ void k_weights_bf16(int co_n, int ci_n, int cinp, const float* __restrict__ w, __nv_bfloat16* wb) {
+  const int ks = mmaconv::k_stride(cinp);
+  const long long n = (long long)co_n * ks;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int co = (int)(i / ks), k = (int)(i % ks);
+  const int tap = k / cinp, ci = k % cinp;
+  float v = 0.f;
+  if (tap < 27 && ci < ci_n) v = w[((long long)co * ci_n + ci) * 27 + tap];
+  wb[i] = __float2bfloat16_rn(v);
+}
+
+template <int CINP, int CO>
+__global__ void __launch_bounds__(32 * mmaconv::warps(CO))
+    k_conv_mma(Dims d, int ci_n, const float* __restrict__ in, const __nv_bfloat16* __restrict__ wb,
+               const float* __restrict__ bias, const float* __restrict__ add, int relu, float beta,
+               float* __restrict__ out) {
+  using namespace mmaconv;
+  constexpr int CS = cin_stride(CINP), KP = k_pad(CINP), KS = k_stride(CINP), MF = frags(CO), NF = CO / 8;
+  constexpr int NT = 32 * warps(CO);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem_raw);  // [HV][CS]
+  __nv_bfloat16* ws = xs + HV * CS;                                 // [CO][KS]
+  const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+  const int bx = blockIdx.x % ntx, by = (blockIdx.x / ntx) % nty, bz = blockIdx.x / (ntx * nty);
+  const long long vox = d.vox();
+  // stage the halo (channel-last BF16, zero outside the grid and beyond ci_n)
+  for (int i = threadIdx.x; i < CINP * HV; i += NT) {
+    const int c = i / HV, r = i % HV;
+    const int hx = r % HX, hy = (r / HX) % HY, hz = r / (HX * HY);
+    const int gx = bx * TX + hx - 1, gy = by * TY + hy - 1, gz = bz * TZ + hz - 1;
+    float v = 0.f;
+    if (c < ci_n && gx >= 0 && gy >= 0 && gz >= 0 && gx < d.nx && gy < d.ny && gz < d.nz)
+      v = in[(long long)c * vox + ((long long)gz * d.ny + gy) * d.nx + gx];
+    xs[r * CS + c] = __float2bfloat16_rn(v);
+  }
+  // stage the weights, 16-byte rows (KS is a multiple of 8 halves)
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(wb);
+    uint4* dst = reinterpret_cast<uint4*>(ws);
+    for (int i = threadIdx.x; i < CO * KS / 8; i += NT) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  float acc[MF][NF][4];
+#pragma unroll
+  for (int f = 0; f < MF; ++f)
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[f][n][j] = 0.f;
+  // halo index of this lane's two rows in each fragment (tap offset added per k)
+  int hrow[MF][2];
+#pragma unroll
+  for (int f = 0; f < MF; ++f)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int v = (w * MF + f) * 16 + g + 8 * h;
+      const int x = v % TX, y = (v / TX) % TY, z = v / (TX * TY);
+      hrow[f][h] = (z * HY + y) * HX + x;
+    }
+  const uint32_t* xw = reinterpret_cast<const uint32_t*>(xs);
+  const uint32_t* ww = reinterpret_cast<const uint32_t*>(ws);
+#pragma unroll 2
+  for (int kc = 0; kc < KP / 16; ++kc) {
+    // A columns 2t, 2t+1 (and +8): (tap, ci) of each pair
+    int aoff[2];
+    bool aval[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = kc * 16 + 2 * t + 8 * h;
+      const int tap = k / CINP, ci = k % CINP;
+      aval[h] = tap < 27;
+      const int tt = aval[h] ? tap : 0;
+      const int dx = tt % 3, dy = (tt / 3) % 3, dz = tt / 9;
+      aoff[h] = ((dz * HY + dy) * HX + dx) * CS + ci;
+    }
+    uint32_t b[NF][2];
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+      const int row = (n * 8 + g) * KS + kc * 16 + 2 * t;
+      b[n][0] = ww[row >> 1];
+      b[n][1] = ww[(row + 8) >> 1];
+    }
+#pragma unroll
+    for (int f = 0; f < MF; ++f) {
+      const uint32_t a0 = aval[0] ? xw[(hrow[f][0] * CS + aoff[0]) >> 1] : 0u;
+      const uint32_t a1 = aval[0] ? xw[(hrow[f][1] * CS + aoff[0]) >> 1] : 0u;
+      const uint32_t a2 = aval[1] ? xw[(hrow[f][0] * CS + aoff[1]) >> 1] : 0u;
+      const uint32_t a3 = aval[1] ? xw[(hrow[f][1] * CS + aoff[1]) >> 1] : 0u;
+#pragma unroll
+      for (int n = 0; n < NF; ++n) mma_bf16(acc[f][n], a0, a1, a2, a3, b[n][0], b[n][1]);
+    }
+  }
+  // epilogue: rows g, g + 8 of each fragment; columns 2t, 2t + 1 of each n
+#pragma unroll
+  for (int f = 0; f < MF; ++f)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int v = (w * MF + f) * 16 + g + 8 * h;
+      const int x = bx * TX + v % TX, y = by * TY + (v / TX) % TY, z = bz * TZ + v / (TX * TY);
+      if (x >= d.nx || y >= d.ny || z >= d.nz) continue;
+      const long long o = ((long long)z * d.ny + y) * d.nx + x;
+#pragma unroll
+      for (int n = 0; n < NF; ++n)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int co = n * 8 + 2 * t + j;
+          float val = acc[f][n][2 * h + j] + (bias ? bias[co] : 0.f);
+          const long long idx = (long long)co * vox + o;
+          if (add) val += add[idx];
+          if (relu) val = fmaxf(val, 0.f);
+          out[idx] = beta != 0.f ? beta * out[idx] + val : val;
+        }
+    }
+}
+
 struct Layer {
   int ci, co, k;  // kernel size 1 or 3
   bool relu;
@@ -577,6 +732,10 @@ struct jxb_cnn {
   float* part = nullptr;   // weight-gradient partials
   long long part_cap = 0;
   double* red = nullptr;   // loss partials
+  int bf16 = 0;            // inference forwards take the BF16 tensor-core convolution where it applies
+  int last_bf16 = 0;       // the last forward did (its activations cannot be back-propagated)
+  __nv_bfloat16* wbf = nullptr;  // one layer's BF16 weights
+  long long wbf_cap = 0;
 };
 
 namespace {
@@ -716,7 +875,7 @@ int ensure_bufs(jxb_cnn* N, Dims d0) {
   const int nl = N->levels;
   Dims d[MAXL];
   d[0] = d0;
-  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
+  for (int l = 1; l < nl; ++l) d[l] = halve(d[l - 1]);
   // sizes in floats, each rounded up to 64 floats (256 B)
   std::vector<std::pair<float**, long long>> want;
   auto add = [&](float** ptr, long long n) { want.push_back({ptr, (std::max<long long>(n, 1) + 63) / 64 * 64}); };
@@ -754,32 +913,82 @@ int ensure_bufs(jxb_cnn* N, Dims d0) {
   return JXB_OK;
 }
 
-int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
+// The BF16 tensor-core path for a 3x3x3 layer of at most 32 input and output
+// channels (output channels a multiple of 8); 1 when the layer does not
+// qualify (the caller then runs the FP32 kernel), else a status.
+int conv_mma(jxb_cnn* N, cudaStream_t s, Dims d, const Layer& L, const float* p, const float* in, const float* add,
+             float* out) {
+  if (L.k != 3 || L.ci > 32 || L.co > 32 || L.co % 8 != 0) return 1;
+  const int cinp = (L.ci + 7) / 8 * 8;
+  const long long need = (long long)L.co * mmaconv::k_stride(cinp);
+  if (need > N->wbf_cap) {
+    cudaFree(N->wbf);
+    N->wbf = nullptr;
+    N->wbf_cap = 0;
+    // 32 x k_stride(32) halves: sized for the widest qualifying layer at once
+    const long long cap = (long long)32 * mmaconv::k_stride(32);
+    JXB_CUDA(cudaMalloc(&N->wbf, cap * sizeof(__nv_bfloat16)));
+    N->wbf_cap = cap;
+  }
+  k_weights_bf16<<<nblk(need), 256, 0, s>>>(L.co, L.ci, cinp, p + L.w_off, N->wbf);
+  const float* b = L.b_off >= 0 ? p + L.b_off : nullptr;
+  const long long tiles = (long long)((d.nx + 7) / 8) * ((d.ny + 7) / 8) * ((d.nz + 3) / 4);
+#define JXB_MMA(CI, C)                                                                                    \
+  if (cinp == CI && L.co == C) {                                                                          \
+    auto k = k_conv_mma<CI, C>;                                                                           \
+    const size_t sm = mmaconv::smem(CI, C);                                                               \
+    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+    k<<<(unsigned)tiles, 32 * mmaconv::warps(C), sm, s>>>(d, L.ci, in, N->wbf, b, add, L.relu ? 1 : 0, 0.f, out); \
+    JXB_CUDA(cudaGetLastError());                                                                         \
+    return JXB_OK;                                                                                        \
+  }
+  JXB_MMA(8, 8) JXB_MMA(8, 16) JXB_MMA(8, 24) JXB_MMA(8, 32)
+  JXB_MMA(16, 8) JXB_MMA(16, 16) JXB_MMA(16, 24) JXB_MMA(16, 32)
+  JXB_MMA(24, 8) JXB_MMA(24, 16) JXB_MMA(24, 24) JXB_MMA(24, 32)
+  JXB_MMA(32, 8) JXB_MMA(32, 16) JXB_MMA(32, 24) JXB_MMA(32, 32)
+#undef JXB_MMA
+  return 1;
+}
+
+// a forward layer: the BF16 tensor-core convolution when `mma` and the layer qualifies
+int conv_f(jxb_cnn* N, cudaStream_t s, bool mma, Dims d, const Layer& L, const float* p, const float* in,
+           const float* add, float* out) {
+  if (mma) {
+    int rc = conv_mma(N, s, d, L, p, in, add, out);
+    if (rc != 1) return rc;
+  }
+  return conv(N, s, d, L, p, in, add, 0.f, out);
+}
+
+int forward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in, bool infer = false) {
+  const bool mma = infer && N->bf16;
+  N->last_bf16 = mma ? 1 : 0;
   int rc = ensure_bufs(N, d0);
   if (rc) return rc;
   const int nl = N->levels;
   Dims d[MAXL];
   d[0] = d0;
-  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
+  for (int l = 1; l < nl; ++l) d[l] = halve(d[l - 1]);
   const float* p = N->p;
   const float* x = in;
   for (int l = 0; l < nl - 1; ++l) {
-    if ((rc = conv(N, s, d[l], N->L[enc_a(l)], p, x, nullptr, 0.f, N->A[l]))) return rc;
-    if ((rc = conv(N, s, d[l], N->L[enc_b(l)], p, N->A[l], nullptr, 0.f, N->S[l]))) return rc;
+    if ((rc = conv_f(N, s, mma, d[l], N->L[enc_a(l)], p, x, nullptr, N->A[l]))) return rc;
+    if ((rc = conv_f(N, s, mma, d[l], N->L[enc_b(l)], p, N->A[l], nullptr, N->S[l]))) return rc;
     k_pool<<<nblk(d[l + 1].vox() * N->c[l]), 256, 0, s>>>(d[l], d[l + 1], N->c[l], N->S[l], N->P[l + 1]);
     x = N->P[l + 1];
   }
   const Dims db = d[nl - 1];
-  if ((rc = conv(N, s, db, N->L[bot(N, 0)], p, x, nullptr, 0.f, N->B0))) return rc;
-  if ((rc = conv(N, s, db, N->L[bot(N, 1)], p, N->B0, nullptr, 0.f, N->B1))) return rc;
-  if ((rc = conv(N, s, db, N->L[bot(N, 2)], p, N->B1, nullptr, 0.f, N->B2))) return rc;
+  if ((rc = conv_f(N, s, mma, db, N->L[bot(N, 0)], p, x, nullptr, N->B0))) return rc;
+  if ((rc = conv_f(N, s, mma, db, N->L[bot(N, 1)], p, N->B0, nullptr, N->B1))) return rc;
+  if ((rc = conv_f(N, s, mma, db, N->L[bot(N, 2)], p, N->B1, nullptr, N->B2))) return rc;
   const float* y = N->B2;
   for (int l = nl - 2; l >= 0; --l) {
     // the 1x1 layer reads y upsampled; U[l] is only materialised by the backward pass
     if ((rc = conv(N, s, d[l], N->L[dec_c(N, l)], p, y, N->S[l], 0.f, N->M[l], &d[l + 1]))) return rc;
-    if ((rc = conv(N, s, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, 0.f, N->D[l]))) return rc;
+    if ((rc = conv_f(N, s, mma, d[l], N->L[dec_d(N, l)], p, N->M[l], nullptr, N->D[l]))) return rc;
     y = N->D[l];
   }
+  // the output layer (4 channels) stays on the FP32 kernel
   if ((rc = conv(N, s, d0, N->L[out_layer(N)], p, y, nullptr, 0.f, N->OUT))) return rc;
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
@@ -792,7 +1001,7 @@ int backward(jxb_cnn* N, cudaStream_t s, Dims d0, const float* in) {
   const int nl = N->levels;
   Dims d[MAXL];
   d[0] = d0;
-  for (int l = 1; l < nl; ++l) d[l] = half(d[l - 1]);
+  for (int l = 1; l < nl; ++l) d[l] = halve(d[l - 1]);
   float *ga = N->G0, *gb = N->G1;
   int rc;
   // output layer
@@ -852,7 +1061,7 @@ int ensure_fine(jxb_cnn* N, Dims df) {
   N->fine_arena = nullptr;
   N->cap_f = {0, 0, 0};
   if ((long long)64 * df.vox() >= (1ll << 31)) return fail(JXB_ERR_INVALID, "cnn: grid too large (activation indices are 32-bit)");
-  const long long a = ((long long)N->in_ch * half(df).vox() + 63) / 64 * 64, b = (4 * df.vox() + 63) / 64 * 64;
+  const long long a = ((long long)N->in_ch * halve(df).vox() + 63) / 64 * 64, b = (4 * df.vox() + 63) / 64 * 64;
   JXB_CUDA(cudaMalloc(&N->fine_arena, (a + 2 * b) * sizeof(float)));
   N->INC = N->fine_arena;
   N->OUTF = N->INC + a;
@@ -864,18 +1073,18 @@ int ensure_fine(jxb_cnn* N, Dims df) {
 float* out_buf(jxb_cnn* N) { return N->pool_in ? N->OUTF : N->OUT; }
 float* gout_buf(jxb_cnn* N) { return N->pool_in ? N->GOF : N->G0; }
 
-int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
+int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in, bool infer = false) {
   N->last = {0, 0, 0};
   if (!N->pool_in) {
-    int rc = forward(N, s, d, in);
+    int rc = forward(N, s, d, in, infer);
     if (!rc) N->last = d;
     return rc;
   }
   int rc = ensure_fine(N, d);
   if (rc) return rc;
-  const Dims dc = half(d);
+  const Dims dc = halve(d);
   k_pool<<<nblk(dc.vox() * N->in_ch), 256, 0, s>>>(d, dc, N->in_ch, in, N->INC);
-  if ((rc = forward(N, s, dc, N->INC))) return rc;
+  if ((rc = forward(N, s, dc, N->INC, infer))) return rc;
   k_up_lin<<<nblk(d.vox() * 4), 256, 0, s>>>(d, dc, 4, N->OUT, N->OUTF);
   JXB_CUDA(cudaGetLastError());
   N->last = d;
@@ -885,7 +1094,7 @@ int forward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
 // backward for the output gradient in gout_buf(N); needs forward_top on the same input
 int backward_top(jxb_cnn* N, cudaStream_t s, Dims d, const float* in) {
   if (!N->pool_in) return backward(N, s, d, in);
-  const Dims dc = half(d);
+  const Dims dc = halve(d);
   k_up_lin_bwd<<<nblk(dc.vox() * 4), 256, 0, s>>>(d, dc, 4, N->GOF, N->G0);
   JXB_CUDA(cudaGetLastError());
   return backward(N, s, dc, N->INC);
@@ -897,8 +1106,8 @@ bool supported_co(int c) { return c == 4 || c == 8 || c == 12 || c == 16 || c ==
 
 namespace jxb {
 
-int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4) {
-  int rc = forward_top(N, s, Dims{nx, ny, nz}, in);
+int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4, bool infer) {
+  int rc = forward_top(N, s, Dims{nx, ny, nz}, in, infer);
   if (rc) return rc;
   if (out4) *out4 = out_buf(N);
   return JXB_OK;
@@ -1012,9 +1221,16 @@ extern "C" int jxb_cnn_destroy(jxb_cnn* N) {
   cudaFree(N->part);
   cudaFree(N->cpart);
   cudaFree(N->red);
+  cudaFree(N->wbf);
   cudaFree(N->arena);
   cudaFree(N->fine_arena);
   delete N;
+  return JXB_OK;
+}
+
+extern "C" int jxb_cnn_set_inference_bf16(jxb_cnn* N, int on) {
+  if (!N || (on != 0 && on != 1)) return fail(JXB_ERR_INVALID, "jxb_cnn_set_inference_bf16: bad argument");
+  N->bf16 = on;
   return JXB_OK;
 }
 
@@ -1049,7 +1265,7 @@ extern "C" int jxb_cnn_forward(jxb_cnn* N, jxb_stream stream, int nx, int ny, in
   if (!N || !in || !out || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_forward: bad argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
-  int rc = forward_top(N, s, d, in);
+  int rc = forward_top(N, s, d, in, true);
   if (rc) return rc;
   JXB_CUDA(cudaMemcpyAsync(out, out_buf(N), (size_t)N->out_ch * d.vox() * sizeof(float), cudaMemcpyDeviceToDevice, s));
   return JXB_OK;
@@ -1060,6 +1276,9 @@ extern "C" int jxb_cnn_backward(jxb_cnn* N, jxb_stream stream, int nx, int ny, i
   if (!N || !in || !gout || nx < 1 || ny < 1 || nz < 1) return fail(JXB_ERR_INVALID, "jxb_cnn_backward: bad argument");
   if (N->last.nx != nx || N->last.ny != ny || N->last.nz != nz)
     return fail(JXB_ERR_INVALID, "jxb_cnn_backward: no forward pass on these dimensions precedes it");
+  if (N->last_bf16)
+    return fail(JXB_ERR_INVALID, "jxb_cnn_backward: the preceding forward ran in BF16 inference mode; "
+                                 "turn it off (jxb_cnn_set_inference_bf16) before training");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   Dims d{nx, ny, nz};
   const size_t vb = (size_t)d.vox() * sizeof(float);

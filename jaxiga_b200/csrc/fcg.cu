@@ -478,7 +478,7 @@ int record_iteration(FcgRun& R, cudaStream_t s, bool learned, int iters) {
     if (learned) {
       k_fpack<T><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, r, plan->d_keep, R.in_scale, R.d_st, R.in);
       const float* out4 = nullptr;
-      int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, &out4);
+      int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, &out4, true);
       if (rc) return rc;
       k_funpack<T><<<nb256(ncp * vec), 256, 0, s>>>(ncp, vec, out4, plan->d_keep, R.out_scale, R.d_st, z);
       if (R.two_level) {  // K z into Ap (free until the direction's apply), z.Kz and z.r partials
@@ -549,7 +549,7 @@ int fcg_setup(FcgRun& R, cudaStream_t s) {
                                cudaMemcpyDeviceToDevice, s));
     // one forward outside capture sizes the network's activation buffers
     const int nx = plan->n_cp[0], ny = plan->n_cp[1], nz = plan->dim == 3 ? plan->n_cp[2] : 1;
-    int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, nullptr);
+    int rc = cnn_forward(R.cnn, s, nx, ny, nz, R.in, nullptr, true);
     if (rc) return rc;
   }
   return JXB_OK;

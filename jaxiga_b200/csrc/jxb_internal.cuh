@@ -247,7 +247,11 @@ int finish_solve(const char* who, jxb_stats* stats, long long iters, long long o
                  double tol, double atol, float ms, bool nonfinite);
 
 // cnn.cu (the network of the learned preconditioner)
-int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4);
+// infer: an inference forward, which takes the BF16 tensor-core convolutions
+// when the network is set to (jxb_cnn_set_inference_bf16); training forwards
+// pass false
+int cnn_forward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in, const float** out4,
+                bool infer = false);
 float* cnn_grad_out(jxb_cnn* N);  // the 4-channel output-gradient buffer read by cnn_backward
 int cnn_backward(jxb_cnn* N, cudaStream_t s, int nx, int ny, int nz, const float* in);
 int cnn_out_channels(const jxb_cnn* N);

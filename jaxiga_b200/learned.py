@@ -104,6 +104,14 @@ class LearnedPreconditioner:
         self.out_scale = 1.0
         self.additive_weight = 1.0
         self.history = []
+        self.inference_bf16 = False
+
+    def set_inference_bf16(self, on=True):
+        """Run the network's applications in the solver (and ``forward``) with
+        the BF16 tensor-core convolution on its layers of at most 32 channels;
+        training keeps FP32."""
+        _lib.check(self.lib.jxb_cnn_set_inference_bf16(self.handle, 1 if on else 0))
+        self.inference_bf16 = bool(on)
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -344,12 +352,15 @@ class LearnedPreconditioner:
                  pool_input=int(self.pool_input))
 
     @classmethod
-    def from_checkpoint(cls, op, path, features=None):
-        """A preconditioner with the network shape, weights and scales stored in ``path``."""
+    def from_checkpoint(cls, op, path, features=None, inference_bf16=False):
+        """A preconditioner with the network shape, weights and scales stored in
+        ``path``; ``inference_bf16`` as :meth:`set_inference_bf16`."""
         d = np.load(path)
         pool = bool(int(d["pool_input"])) if "pool_input" in d.files else False
         lp = cls(op, features=features, channels=tuple(int(c) for c in d["channels"]), pool_input=pool)
         lp.load(path)
+        if inference_bf16:
+            lp.set_inference_bf16(True)
         return lp
 
     def load(self, path):

@@ -248,6 +248,12 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     assert float(torch.linalg.norm(x_a - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
     _, st_am = lp.solve(b, tol=1e-8, two_level="additive", mixed=True)
     assert st_am["converged"], st_am
+    # the network's inference on the BF16 tensor cores: same answer, about as many iterations
+    lp.set_inference_bf16(True)
+    x_b, st_b = lp.solve(b, tol=1e-8, two_level="additive", mixed=True)
+    assert st_b["converged"] and st_b["iterations"] <= 1.2 * st_am["iterations"] + 3, (st_b, st_am)
+    assert float(torch.linalg.norm(x_b - x_ref) / torch.linalg.norm(x_ref)) < 1e-6
+    lp.set_inference_bf16(False)
     # a network on the pooled residual (half resolution) in the additive map
     lpp = LearnedPreconditioner(op, features=feat, seed=2, pool_input=True)
     lpp.in_scale, lpp.out_scale = lp.in_scale, lp.out_scale
@@ -272,3 +278,34 @@ def test_learned_fcg_solves_and_beats_jacobi_pcg(tmp_path):
     lp.close()
     lp2.close()
     op.close()
+
+
+@pytest.mark.parametrize("grid,in_ch,channels", [((35, 33, 31), 2, (8, 16, 24, 32)), ((20, 19, 1), 1, (8, 16, 24))])
+def test_bf16_inference_forward_tracks_the_fp32_network(grid, in_ch, channels):
+    """The BF16 tensor-core convolutions (BF16 operands, FP32 accumulation) on the
+    layers of <= 32 channels against the FP32 kernels and the FP64 oracle: a
+    BF16 tolerance of 2e-2 relative (8-bit mantissas through a dozen layers)."""
+    import torch
+
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    h, p64 = _make_net(lib, in_ch, 1, channels, 3, rng)
+    nx, ny, nz = grid
+    x = rng.standard_normal((in_ch, nz, ny, nx)).astype(np.float32)
+    xd = torch.as_tensor(x, device="cuda").contiguous()
+    out32 = torch.empty((1, nz, ny, nx), device="cuda")
+    out16 = torch.empty_like(out32)
+    _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out32)))
+    _lib.check(lib.jxb_cnn_set_inference_bf16(h, 1))
+    _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out16)))
+    a, b = out16.cpu().numpy().astype(np.float64), out32.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(a - b) < 2e-2 * np.linalg.norm(b)
+    ref, _ = cnn_oracle.forward(p64, x.astype(np.float64), in_ch, channels, False)
+    assert np.linalg.norm(a.reshape(-1) - ref[0].reshape(-1)) < 2e-2 * np.linalg.norm(ref[0])
+    # a backward after a BF16 forward is refused; the FP32 forward makes it valid again
+    g = torch.ones_like(out32)
+    assert lib.jxb_cnn_backward(h, _s(), nx, ny, nz, _p(xd), _p(g)) == 1
+    _lib.check(lib.jxb_cnn_set_inference_bf16(h, 0))
+    _lib.check(lib.jxb_cnn_forward(h, _s(), nx, ny, nz, _p(xd), _p(out32)))
+    _lib.check(lib.jxb_cnn_backward(h, _s(), nx, ny, nz, _p(xd), _p(g)))
+    lib.jxb_cnn_destroy(h)
