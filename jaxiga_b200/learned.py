@@ -389,10 +389,12 @@ def default_channels(grid):
     return (8, 16, 24, 32, 48, 48)[:levels]
 
 
-def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=False):
+def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=False, bf16=False):
     """Device time (ms) of the network's forward and backward on an n^3 grid of
     random inputs, CUDA events on the current stream. ``once``: one forward and
-    one backward after three warm-up forwards (for a profiler launch list)."""
+    one backward after three warm-up forwards (for a profiler launch list).
+    ``bf16``: forwards on the BF16 tensor-core convolutions (inference); the
+    backward is then left out."""
     import torch
 
     lib = _lib.load()
@@ -404,6 +406,8 @@ def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=F
     try:
         if pool_input:
             _lib.check(lib.jxb_cnn_set_input_pooling(h, 1))
+        if bf16:
+            _lib.check(lib.jxb_cnn_set_inference_bf16(h, 1))
         x = torch.randn(in_ch, n, n, n, device="cuda")
         out = torch.empty(1, n, n, n, device="cuda")
         g = torch.randn(1, n, n, n, device="cuda")
@@ -411,11 +415,12 @@ def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=F
         bwd = lambda: _lib.check(lib.jxb_cnn_backward(h, _s(), n, n, n, _p(x), _p(g)))  # noqa: E731
         for _ in range(3):
             fwd()
-        if not once:  # the first backward sizes its buffers: keep that out of the timed loop
+        if not once and not bf16:  # the first backward sizes its buffers: keep that out of the timed loop
             bwd()
         if once:
             fwd()
-            bwd()
+            if not bf16:
+                bwd()
             torch.cuda.synchronize()
             return None
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -423,14 +428,15 @@ def time_network(n=99, channels=None, reps=10, in_ch=2, once=False, pool_input=F
         for _ in range(reps):
             fwd()
         e1.record()
-        for _ in range(reps):
-            fwd()
-            bwd()
+        if not bf16:
+            for _ in range(reps):
+                fwd()
+                bwd()
         e2.record()
         torch.cuda.synchronize()
         f = e0.elapsed_time(e1) / reps
-        return {"grid": n, "channels": channels, "pool_input": bool(pool_input), "forward_ms": f,
-                "backward_ms": e1.elapsed_time(e2) / reps - f}
+        return {"grid": n, "channels": channels, "pool_input": bool(pool_input), "bf16": bool(bf16),
+                "forward_ms": f, "backward_ms": None if bf16 else e1.elapsed_time(e2) / reps - f}
     finally:
         lib.jxb_cnn_destroy(h)
 
@@ -444,6 +450,7 @@ if __name__ == "__main__":
     ap.add_argument("--channels", default=None, help="per-level channels, e.g. 8,16,24,32,48")
     ap.add_argument("--once", action="store_true", help="3 warm-up forwards, then one forward and one backward")
     ap.add_argument("--pool-input", action="store_true", help="run on the pooled input (half resolution)")
+    ap.add_argument("--bf16", action="store_true", help="forwards on the BF16 tensor-core convolutions")
     a = ap.parse_args()
     ch = None if a.channels is None else [int(c) for c in a.channels.split(",")]
-    print(json.dumps(time_network(a.grid, ch, once=a.once, pool_input=a.pool_input)))
+    print(json.dumps(time_network(a.grid, ch, once=a.once, pool_input=a.pool_input, bf16=a.bf16)))
