@@ -279,3 +279,58 @@ class Multigrid:
             self.close()
         except Exception:
             pass
+
+
+def _workload(name, span):
+    """(problem, params, load) of a benchmark workload for the multigrid timing."""
+    import torch
+
+    from . import workloads
+    from .forms import PointField
+    from .solve import _problem_operator, _rhs, geometry_operator
+
+    if name == "plate":
+        V, problem, params = workloads.config5(n=span)
+    elif name == "darcy":
+        V, problem, params = workloads.config4(n=span)
+        a = torch.exp(geometry_operator(V).interpolate(params["loga"])[..., 0]).cpu().numpy()
+        params = {"a0": PointField(a)}
+    else:
+        V, problem, params = workloads.config2(n=span)
+        fq = geometry_operator(V).interpolate(params["eta"]).cpu().numpy()
+        fq[..., 2] -= 1.0
+        params = dict(params, f=PointField(fq))
+    op, prescribed, values = _problem_operator(problem, params, False)
+    return problem, params, op, _rhs(problem, params, op, prescribed, values)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser(description="multigrid-preconditioned CG against Jacobi-PCG on a workload")
+    ap.add_argument("--workload", choices=["plate", "elasticity", "darcy"], default="plate")
+    ap.add_argument("--span", type=int, default=256)
+    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--range", type=float, default=20.0)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--once", action="store_true", help="one multigrid solve only (for a profiler launch list)")
+    a = ap.parse_args()
+    problem, params, op, b = _workload(a.workload, a.span)
+    t0 = time.perf_counter()
+    mg = Multigrid(problem, params, degree=a.degree, smooth_range=a.range, fine_op=op)
+    setup = time.perf_counter() - t0
+    mg.solve(b, tol=a.tol)  # captures the graph
+    if a.once:
+        mg.close()
+        raise SystemExit(0)
+    _, st = mg.solve(b, tol=a.tol)
+    op.pcg(b, tol=a.tol, restarts=3, maxiter=80000, check_every=32)
+    _, sj = op.pcg(b, tol=a.tol, restarts=3, maxiter=80000, check_every=32)
+    print(json.dumps({"workload": a.workload, "span": a.span, "levels": mg.levels, "degree": a.degree,
+                      "range": a.range, "setup_seconds": setup, "lmax": mg.lmax,
+                      "multigrid_pcg": {k: st[k] for k in ("iterations", "seconds", "relative_residual", "converged")},
+                      "jacobi_pcg": {k: sj[k] for k in ("iterations", "seconds", "relative_residual", "converged")},
+                      "speedup": sj["seconds"] / st["seconds"] if st["converged"] and sj["converged"] else None}))
+    mg.close()
