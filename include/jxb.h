@@ -232,6 +232,15 @@ int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double*
 int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                   const jxb_solve_opts* opts, jxb_stats* stats);
 
+/* jxb_bicgstab: BiCGSTAB (van der Vorst) on the same masked operator, the
+ *   reference's method="bicgstab" (jax.scipy.sparse.linalg.bicgstab,
+ *   src/jaxiga/solvers/linear.py:152-171, 399-411): from x = 0, Jacobi (or no)
+ *   right preconditioning, stop when r.r <= max(tol^2 b.b, atol^2) or at maxiter;
+ *   a breakdown (rho, alpha or omega zero) returns JXB_ERR_NONFINITE. Stats and
+ *   return codes as jxb_pcg. */
+int jxb_bicgstab(jxb_plan* plan, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
+                 jxb_stats* stats);
+
 /* jxb_pcg_snapshots: jxb_pcg (Jacobi or none, jax CG semantics) that also copies
  *   the FP64 iterate into snaps[j] (n_dofs doubles each) after every `every`
  *   iterations, up to max_snaps; *n_snaps receives the number written. With the

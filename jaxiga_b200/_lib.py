@@ -130,6 +130,8 @@ SIGNATURES = [
                           ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_mixed_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
+    ("jxb_bicgstab", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                      ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats)]),
     ("jxb_pcg_snapshots", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                            ctypes.POINTER(SolveOpts), ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
                            c_int64_p, ctypes.POINTER(Stats)]),

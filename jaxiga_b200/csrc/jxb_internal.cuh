@@ -152,6 +152,8 @@ constexpr int TILE2[N_TILE2][2] = {{32, 8}, {16, 8}, {32, 16}, {64, 4}};
 
 }  // namespace jxb
 
+struct jxb_krylov_ws;  // BiCGSTAB workspace (krylov.cu)
+
 struct jxb_plan {
   int device = 0;  // the CUDA device that was current at creation; its buffers live there
   int dim, vec, p, q, op, rational, order, plane_strain;
@@ -189,6 +191,7 @@ struct jxb_plan {
         *d_invdiag32 = nullptr;
   // true-residual restarts of jxb_pcg: accumulated solution and FP64 residual
   double *d_xacc = nullptr, *d_res = nullptr;
+  jxb_krylov_ws* krylov = nullptr;  // allocated by the first jxb_bicgstab
   jxb::CgState* d_state = nullptr;
   jxb::CgState* h_state = nullptr;  // pinned
   bool diag_valid = false;
@@ -245,6 +248,9 @@ int true_residual(jxb_plan* plan, cudaStream_t s, const double* b, const double*
 // max(tol ||b||, atol)) or JXB_OK.
 int finish_solve(const char* who, jxb_stats* stats, long long iters, long long outer, double rn, double bn, bool fin,
                  double tol, double atol, float ms, bool nonfinite);
+
+// krylov.cu
+void free_krylov(jxb_plan* plan);
 
 // cnn.cu (the network of the learned preconditioner)
 // infer: an inference forward, which takes the BF16 tensor-core convolutions

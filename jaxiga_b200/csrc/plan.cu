@@ -47,6 +47,7 @@ static int upload(T** d, const T* h, size_t n, cudaStream_t s) {
 
 static void free_plan(jxb_plan* p) {
   if (!p) return;
+  free_krylov(p);
   for (int d = 0; d < 3; ++d) {
     cudaFree(p->d_first[d]);
     cudaFree(p->d_bcp0[d]);

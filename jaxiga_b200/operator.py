@@ -301,6 +301,16 @@ class Operator:
         _lib.check_solve(rc, raise_on_nonfinite)
         return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
 
+    def bicgstab(self, b, tol=1e-12, atol=0.0, maxiter=None, preconditioner="jacobi", check_every=16):
+        """BiCGSTAB from x = 0 (jax semantics, Jacobi right preconditioning); returns (x, stats dict)."""
+        b = self._vec(b)
+        x = self._empty(self.n_dofs)
+        st = _lib.Stats()
+        o = self._opts(tol, atol, maxiter, preconditioner, check_every, 0.0, 0)
+        rc = self.lib.jxb_bicgstab(self.handle, _stream(), _dptr(b), _dptr(x), ctypes.byref(o), ctypes.byref(st))
+        _lib.check_solve(rc)
+        return x, {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+
     def refine_solve(self, b, tol=1e-8, inner_tol=1e-4, maxiter=None, max_outer=40, check_every=16):
         """FP64 iterative refinement around FP32 Jacobi-PCG inner solves."""
         if not self.want_f32:

@@ -309,8 +309,10 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     _check_problem(problem, method)
     if linear is None:
         linear = default_linear(problem)
-    if linear.method != "cg":
-        raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG")
+    if linear.method not in ("cg", "bicgstab"):
+        raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG and BiCGSTAB")
+    if linear.method == "bicgstab" and (linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none")):
+        raise NotImplementedError("BiCGSTAB runs in FP64 with the Jacobi preconditioner (or none)")
     space = problem.space
     n = space.n_dofs
     # The Kirchhoff plate's FP32 operator cannot resolve the biharmonic system:
@@ -338,6 +340,10 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         finally:
             lp.close()
         st["outer"] = st["learned_iterations"]
+    elif linear.method == "bicgstab":
+        xdev, st = op.bicgstab(b, tol=linear.tol, maxiter=linear.maxiter, preconditioner=linear.preconditioner,
+                               check_every=linear.check_every)
+        st["outer"] = 0
     elif linear.preconditioner == "multigrid":
         mg = getattr(op, "_multigrid", None)
         if mg is None or mg.handle is None or (mg.degree, mg.smooth_range) != (linear.mg_degree, linear.mg_range):

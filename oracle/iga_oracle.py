@@ -670,6 +670,46 @@ def jax_cg(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0, x0=None):
     return x, k
 
 
+def bicgstab(matvec, b, tol, maxiter=None, inv_diag=None, atol=0.0):
+    """BiCGSTAB (van der Vorst, 1992) with right preconditioning M, in the
+    stopping semantics of jax.scipy.sparse.linalg.bicgstab (the reference's
+    method="bicgstab", solvers/linear.py:152-171): x0 = 0, stop when r.r <=
+    max(tol^2 b.b, atol^2), or when s.s already is (x then takes the half step).
+    Returns (x, iterations)."""
+    b = np.asarray(b, dtype=float)
+    maxiter = 10 * b.size if maxiter is None else maxiter
+    M = (lambda v: v) if inv_diag is None else (lambda v: inv_diag * v)
+    atol2 = max(tol**2 * (b @ b), atol**2)
+    x = np.zeros_like(b)
+    r = b.copy()
+    rhat = r.copy()
+    rho = alpha = omega = 1.0
+    p = np.zeros_like(b)
+    v = np.zeros_like(b)
+    k = 0
+    while r @ r > atol2 and k < maxiter:
+        rho_new = rhat @ r
+        beta = (rho_new / rho) * (alpha / omega)
+        rho = rho_new
+        p = r + beta * (p - omega * v)
+        ph = M(p)
+        v = matvec(ph)
+        alpha = rho / (rhat @ v)
+        s = r - alpha * v
+        if s @ s <= atol2:
+            x = x + alpha * ph
+            r = s
+            k += 1
+            break
+        sh = M(s)
+        t = matvec(sh)
+        omega = (t @ s) / (t @ t)
+        x = x + alpha * ph + omega * sh
+        r = s - omega * t
+        k += 1
+    return x, k
+
+
 def reliable_cg(matvec, matvec32, b, tol, delta=1e-2, inv_diag=None, maxiter=None):
     """FP32 Jacobi-PCG with reliable FP64 updates, as the device solver runs it.
 
