@@ -159,3 +159,37 @@ class BatchSolver:
         self.batch.close()
         for op in self.ops:
             op.close()
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    import torch
+
+    from . import workloads
+    from .solve import geometry_operator
+
+    ap = argparse.ArgumentParser(description="batched K.u over the quarter-annulus instances (fixed 16 x 8 tiles)")
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    problems, params = workloads.config3(n_instances=a.instances,
+                                         interpolate=lambda V, c: geometry_operator(V).interpolate(c).cpu().numpy())
+    bs = BatchSolver(problems, params, tiles={2: (16, 8), 3: (16, 8), 4: (16, 8)})
+    b = bs.batch
+    x = torch.randn(b.total, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        _lib.check(b.lib.jxb_batch_apply(b.handle, _s(), _p(x), _p(y)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        _lib.check(b.lib.jxb_batch_apply(b.handle, _s(), _p(x), _p(y)))
+    e1.record()
+    torch.cuda.synchronize()
+    n_qp = sum(pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems)
+    ms = e0.elapsed_time(e1) / a.reps
+    print(json.dumps({"instances": a.instances, "n_dofs": int(b.total), "gauss_points": n_qp, "ms_per_apply": ms,
+                      "algorithmic_gbs": (16 * b.total + 48 * n_qp) / (ms * 1e-3) / 1e9}))
+    bs.close()
