@@ -102,8 +102,10 @@ class DeviceCG:
         import torch
 
         y = torch.empty(self.n, dtype=torch.float64, device=self.device)
-        _lib.check(self.lib.jxb_csr_matvec(self.handle, _stream(), _dptr(self._dev(data, self.nnz)),
-                                           _dptr(self._dev(x, self.n)), _dptr(y)))
+        # the device copies must stay referenced until the kernel has run: a
+        # temporary freed after _dptr would hand its memory to the next one
+        d, xv = self._dev(data, self.nnz), self._dev(x, self.n)
+        _lib.check(self.lib.jxb_csr_matvec(self.handle, _stream(), _dptr(d), _dptr(xv), _dptr(y)))
         return y
 
     def relative_residual(self, data, b, x):

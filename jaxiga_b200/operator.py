@@ -269,7 +269,8 @@ class Operator:
 
     def dot(self, a, b):
         r = ctypes.c_double()
-        _lib.check(self.lib.jxb_dot(self.handle, _stream(), _dptr(self._vec(a)), _dptr(self._vec(b)), ctypes.byref(r)))
+        a, b = self._vec(a), self._vec(b)  # referenced until the call returns (it synchronises)
+        _lib.check(self.lib.jxb_dot(self.handle, _stream(), _dptr(a), _dptr(b), ctypes.byref(r)))
         return r.value
 
     # -- solves ---------------------------------------------------------------

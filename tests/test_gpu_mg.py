@@ -81,7 +81,7 @@ def test_multigrid_pcg_on_the_plate():
 
 
 def test_multigrid_pcg_on_a_rational_patch_with_neumann_loads():
-    V = jx.FunctionSpace(jx.primitives.quarter_annulus(1.0, 4.0).elevate(4).refine(3), vec=2)
+    V = jx.FunctionSpace(jx.primitives.quarter_annulus(1.0, 4.0).elevate(4).refine(5), vec=2)
     pr = jx.LinearElasticity(V, plane="stress",
                              dirichlet=[jx.DirichletBC(0.0, where="sym_y", component=1),
                                         jx.DirichletBC(0.0, where="sym_x", component=0)],

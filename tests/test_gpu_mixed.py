@@ -40,7 +40,10 @@ def test_mixed_solve_matches_reference(tag, refinement):
     sol = jx.solve(problem, params=params,
                    linear=jx.LinearOptions(tol=1e-12, precision="mixed", refinement=refinement))
     assert sol.stats["converged"] and sol.stats["relative_residual"] <= 1e-12
-    assert sol.stats["refinement"] == refinement and sol.stats["outer"] >= 1
+    if tag == "plate2d":  # the plate's mixed form keeps the FP64 operator (FP32 cannot resolve it at size)
+        assert sol.stats["fp32_operator"] is False and sol.stats["refinement"] is None
+    else:
+        assert sol.stats["refinement"] == refinement and sol.stats["outer"] >= 1
     # as close to the reference's solution as FP64 CG at the same tolerance
     err, err64 = rel_l2(sol.u, g[f"{tag}/u"]), rel_l2(plain.u, g[f"{tag}/u"])
     assert err < max(1e-9, 10 * err64), (err, err64)
