@@ -336,10 +336,17 @@ def roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span):
         flops = V.n_elems * V.vec * (2 * 2 * 9 * 4**3 * 4) + n_qp * (2 * 81 if V.vec == 3 else 2 * 9)
     achieved = alg_bytes / (ms_bricks * 1e-3) / 1e9
     traffic = profile_traffic(name, span)
-    mma = os.environ.get("JXB_BRICK3_MMA", "1") != "0"
-    kernel = ("k_brick2<double,4,5,plate> (brick apply)" if name == "plate" else
-              "k_brick3_mma (FP64 mma.sync brick apply, %s p=3)" % ("poisson" if name == "darcy" else "elasticity")
-              if mma else "k_brick3<double,3,4,%s> (brick apply)" % ("poisson" if name == "darcy" else "elasticity"))
+    variant = os.environ.get("JXB_BRICK3_MMA", "")
+    opn = "poisson" if name == "darcy" else "elasticity"
+    if name == "plate":
+        kernel = "k_brick2<double,4,5,plate> (brick apply)"
+    elif variant == "0":
+        kernel = "k_brick3<double,3,4,%s> (FMA brick apply)" % opn
+    elif variant in ("1", "2"):
+        kernel = "k_brick3_mma (FP64 mma.sync brick apply, stages through shared memory, %s p=3)" % opn
+    else:
+        kernel = ("k_brick3_rf (FP64 mma.sync brick apply, register fragments%s, %s p=3)"
+                  % (", factor tiles by bulk copy" if variant == "5" or (not variant and opn == "elasticity") else "", opn))
     return {
         "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",

@@ -555,17 +555,25 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
 
 #include "brick2d.cuh"
 #include "brick3_mma.cuh"
+#include "brick3_rf.cuh"
 
-// The FP64 tensor-core brick kernel runs the degree-3 scalar and elasticity
-// applies. The environment variable JXB_BRICK3_MMA selects the variant: 0 =
-// the FMA kernel (to compare), 2 = the scalar MMA kernel built for one CTA per
-// SM, anything else = the default (scalar: two CTAs per SM; elasticity: one).
+// The FP64 tensor-core brick kernels run the degree-3 scalar and elasticity
+// applies. The environment variable JXB_BRICK3_MMA selects the variant, to
+// compare them: 0 = the FMA kernel, 1 = the staged MMA kernel (stage hand-offs
+// through shared memory) built for one CTA per SM, 2 = the staged kernel at
+// its default occupancy (scalar: two CTAs per SM; elasticity: one), 3 = the
+// register-fragment kernel built for one CTA per SM, 4 = the register-fragment
+// kernel at its default occupancy (scalar: two CTAs per SM; elasticity: one)
+// reading the factors from L2, 5 = the same kernel with the factor tiles copied
+// into shared memory one element ahead. The default is 4 for the scalar
+// operator and 5 for elasticity, the faster of the two on each (B200: Darcy
+// 96^3 0.69 / 0.71 ms, elasticity 64^3 0.635 / 0.629 ms).
+template <int OPK>
 static int brick3_mma_mode() {
   static const int mode = [] {
     const char* e = getenv("JXB_BRICK3_MMA");
-    if (e && e[0] == '0') return 0;
-    if (e && e[0] == '2') return 1;
-    return 2;
+    if (e && e[0] >= '0' && e[0] <= '5' && e[1] == 0) return e[0] - '0';
+    return OPK == OPK_ELAST ? 5 : 4;
   }();
   return mode;
 }
@@ -677,7 +685,21 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
     } else {
       if constexpr (sizeof(T) == 8 && P == 3 && (OPK == OPK_SCALAR || OPK == OPK_ELAST) && !RAT &&
                     MODE == MODE_APPLY) {
-        if (const int mode = brick3_mma_mode()) {
+        int mode = brick3_mma_mode<OPK>();
+        // a brick whose footprint leaves no room for the factor tiles reads them from L2
+        if (mode == 5 && smem3_rf<OPK, true>(br) > 227 * 1024) mode = 4;
+        if (mode >= 3) {
+          const size_t sm = mode == 5 ? smem3_rf<OPK, true>(br) : smem3_rf<OPK, false>(br);
+          if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory");
+          constexpr int MB = OPK == OPK_SCALAR ? 2 : 1;
+          auto k = mode == 5 ? k_brick3_rf<OPK, MB, true> : mode == 4 ? k_brick3_rf<OPK, MB, false>
+                                                                       : k_brick3_rf<OPK, 1, false>;
+          JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          k<<<(unsigned)br.n_bricks, brf::NT, sm, s>>>(A);
+          JXB_CUDA(cudaGetLastError());
+          return JXB_OK;
+        }
+        if (mode) {
           const size_t sm = smem3_mma<OPK>(br);
           if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "3D brick does not fit in shared memory");
           // elasticity needs the registers of the one-CTA-per-SM build

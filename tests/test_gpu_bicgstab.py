@@ -27,7 +27,10 @@ def test_bicgstab_matches_oracle(tag):
     x, st = op.bicgstab(bf, tol=1e-10)
     x_o, k_o = O.bicgstab(lambda v: A.K @ v, b, 1e-10, inv_diag=O.jacobi_inverse(A.diag))
     assert st["converged"] and st["relative_residual"] <= 1.01e-10
-    assert abs(st["iterations"] - k_o) <= max(2, 0.05 * k_o), (st["iterations"], k_o)
+    # BiCGSTAB's residual history is erratic, so its iteration count moves more
+    # with the summation order of K.v (matrix-free bricks against a CSR product)
+    # than CG's does
+    assert abs(st["iterations"] - k_o) <= max(2, 0.15 * k_o), (st["iterations"], k_o)
     assert np.linalg.norm(x.cpu().numpy()[A.free] - x_o) < 1e-7 * np.linalg.norm(x_o)
     op.close()
 
