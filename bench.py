@@ -56,6 +56,7 @@ METRIC = "time-to-1e-8 residual & K·u DOF/s: mixed+learned vs plain FP64 PCG, 1
 UNIT = "DOF/s"
 N_SPAN = 64
 CPU_SAMPLE_SPAN = 16
+CPU_SAMPLE_SPAN_LARGE = 24  # the reference arm also times the CPU solve here (about 80 s of assembly and CG)
 TOL = 1e-8
 
 
@@ -257,6 +258,11 @@ def run_reference(args, rank, world):
     el = time.perf_counter() - t0
     value = V.n_dofs * args.steps / el
     tts = cpu_time_to_solution(A)
+    # the larger matched size: one solve (assembly about a minute on one core)
+    V24, A24, setup24 = cpu_sample(CPU_SAMPLE_SPAN_LARGE)
+    tts24 = dict(cpu_time_to_solution(A24, runs=1), span=CPU_SAMPLE_SPAN_LARGE, n_dofs=V24.n_dofs,
+                 nnz=int(A24.K.nnz), assembly_seconds=setup24)
+    del A24
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
@@ -267,7 +273,8 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": f"SciPy CSR K.u, {CPU_SAMPLE_SPAN}^3-element elasticity workload, one thread",
                          "host": host_info()},
-        "time_to_solution": {"tol": TOL, "scipy_jacobi_cg_true_residual_restarts": tts},
+        "time_to_solution": {"tol": TOL, "scipy_jacobi_cg_true_residual_restarts": tts,
+                             "scipy_jacobi_cg_true_residual_restarts_24": tts24},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -503,15 +510,15 @@ def measure_workload(name, span, dev, steps, peaks, peak_kind, solve=True):
     return rec
 
 
-def matched_gpu_solve(dev):
-    """GPU time to solution of the CPU baseline's workload (elasticity 16^3)."""
-    V, op, F, _, _, _ = build_workload("elasticity", CPU_SAMPLE_SPAN, dev)
+def matched_gpu_solve(dev, span=CPU_SAMPLE_SPAN):
+    """GPU time to solution of the CPU baseline's workload (elasticity span^3)."""
+    V, op, F, _, _, _ = build_workload("elasticity", span, dev)
     for _ in range(2):
         _, st = op.pcg(F, tol=TOL, preconditioner="jacobi", check_every=32, restarts=3)
     for _ in range(2):
         _, st_r = op.mixed_pcg(F, tol=TOL, delta=1e-2, check_every=32)
     op.close()
-    return {"span": CPU_SAMPLE_SPAN, "n_dofs": V.n_dofs, "plain_fp64_jacobi_pcg": _row(st),
+    return {"span": span, "n_dofs": V.n_dofs, "plain_fp64_jacobi_pcg": _row(st),
             "mixed_fp32_pcg_reliable_fp64_updates": _row(st_r)}
 
 
@@ -602,6 +609,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline()
         cpu["gpu_same_size"] = matched_gpu_solve(dev)
+        cpu["gpu_same_size_24"] = matched_gpu_solve(dev, CPU_SAMPLE_SPAN_LARGE)
         g = cpu["gpu_same_size"]["plain_fp64_jacobi_pcg"]
         c = cpu["time_to_solution"]
         cpu["time_to_solution_ratio_cpu_over_gpu"] = (c["seconds"] / g["seconds"]
@@ -649,24 +657,36 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     mine = partition_by_cost(costs, world)[rank]
     problems = [problems[i] for i in mine]
     params = [params[i] for i in mine]
-    bs = BatchSolver(problems, params, tiles="auto")
+    bs = BatchSolver(problems, params)  # rows of 32 elements: one persistent launch over every degree
     setup_s = time.perf_counter() - t0
     b = bs.batch
     n = b.total
     x = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1234 + rank))
     y = torch.empty_like(x)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def time_apply(bb, k):
+        run = lambda: _lib.check(bb.lib.jxb_batch_apply(bb.handle, torch.cuda.current_stream().cuda_stream,  # noqa: E731
+                                                        x.data_ptr(), y.data_ptr()))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(k):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), device="cuda")
+
     apply = lambda xx, yy: _lib.check(b.lib.jxb_batch_apply(b.handle, torch.cuda.current_stream().cuda_stream,  # noqa: E731
                                                             xx.data_ptr(), yy.data_ptr()))
-    for _ in range(3):
-        apply(x, y)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        apply(x, y)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    ms = time_apply(b, steps)
+    # the per-degree-group launches with autotuned tiles, for comparison
+    bs_t = BatchSolver(problems, params, tiles="auto")
+    ms_groups = time_apply(bs_t.batch, steps) / steps
+    groups = {"tiles": {str(k): v for k, v in bs_t.tiles.items()}, "brick_launches": bs_t.batch.brick_launches,
+              "persistent": bs_t.batch.persistent, "ms_per_apply": ms_groups}
+    bs_t.close()
     value = n_all * steps / (ms * 1e-3)
     # algorithmic bytes: u and y once, 6 factors per point (rational 2D scalar metric)
     n_qp = sum(pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems)
@@ -710,8 +730,11 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     rec = {"workload": "batched_quarter_annuli_256", "instances": len(costs), "n_dofs": n_all,
            "instances_on_rank0": len(problems), "elements": elems_all, "gauss_points": sum(costs),
            "degrees": sorted({pr.space.degree[0] for pr in problems}),
-           "tiles": {str(k): v for k, v in bs.tiles.items()},
-           "operator": "batched matrix-free K.u, FP64, masked, one launch per degree group",
+           "tiles": "rows of 32 elements, 1-8 rows per brick by patch size",
+           "operator": "batched matrix-free K.u, FP64, masked, " + (
+               "one persistent launch over the bricks of every degree" if b.persistent else
+               "%d launches (one per degree group)" % b.brick_launches),
+           "per_degree_group_launches_autotuned": groups,
            "parallelism": "instances sharded over %d GPU(s) by cost, no collective" % world,
            "setup_seconds": setup_s, "value": value, "unit": UNIT, "ms_per_apply": ms / steps,
            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
@@ -719,7 +742,8 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": achieved / peaks["hbm_gbs"],
                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
-                        "kernel": "k_brick2_batch (batched 2D brick apply) + k_combine_batch",
+                        "kernel": ("k_brick2_persist (persistent batched 2D brick apply)" if b.persistent else
+                                   "k_brick2_batch (batched 2D brick apply)") + " + k_combine_batch",
                         "algorithmic_bytes_per_launch": alg},
            "time_to_solution": tts}
     bs.close()

@@ -78,8 +78,9 @@ typedef struct jxb_desc {
   const double* coef_qp;        /* optional (n_elem, n_quad^dim) per-point a0 (PointField); NULL = coef[0] */
   const uint8_t* prescribed;    /* optional (n_dofs,) 1 = Dirichlet DOF; NULL = none */
   int want_f32;                 /* also keep FP32 copies of the point factors (mixed precision) */
-  int tile[2];                  /* 2D scalar operator: brick shape (elements per row, rows); {0,0} = default.
-                                   Supported: {32,8} {16,8} {32,16} {64,4} (picked by the batch autotuner) */
+  int tile[2];                  /* 2D brick shape (elements per row, rows); {0,0} = default (32 per row, up
+                                   to 8 rows, fewer when the patch is small). Rows: 1..64; elements per
+                                   row: 32, or 16 / 64 for the scalar operator (the batch autotuner picks) */
 } jxb_desc;
 
 typedef struct jxb_info {
@@ -261,6 +262,10 @@ typedef struct jxb_batch jxb_batch;
 int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out);
 int jxb_batch_destroy(jxb_batch* batch);
 int jxb_batch_size(const jxb_batch* batch, int64_t* total_dofs, int64_t* offsets /* n+1 or NULL */);
+/* How a batched K.u runs: *persistent = 1 when one persistent launch walks the
+ * bricks of every instance and degree (every plan has rows of 32 elements and
+ * JXB_BATCH_PERSIST is not "0"), else 0; *brick_launches = brick launches per K.u. */
+int jxb_batch_info(const jxb_batch* batch, int* persistent, int* brick_launches);
 int jxb_batch_apply(jxb_batch* batch, jxb_stream stream, const double* x, double* y);
 int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
                   jxb_stats* stats, double* seconds);

@@ -138,6 +138,7 @@ SIGNATURES = [
     ("jxb_batch_create", [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_batch_destroy", [ctypes.c_void_p]),
     ("jxb_batch_size", [ctypes.c_void_p, c_int64_p, c_int64_p]),
+    ("jxb_batch_info", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("jxb_batch_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_batch_pcg", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.POINTER(SolveOpts), ctypes.POINTER(Stats), c_double_p]),

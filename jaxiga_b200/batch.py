@@ -21,7 +21,7 @@ from .forms import PointField, call_points, flat_params
 from .operator import Operator
 from .solve import qp_points
 
-TILES = [(32, 8), (16, 8), (32, 16), (64, 4)]
+TILES = [(32, 8), (16, 8), (32, 16), (64, 4), (32, 2), (16, 2), (32, 1), (64, 1)]
 
 
 def _s():
@@ -55,6 +55,10 @@ class _Batch:
         _lib.check(self.lib.jxb_batch_size(h, ctypes.byref(total), offs))
         self.total = total.value
         self.offsets = np.array(offs[:], dtype=np.int64)
+        pers, launches = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.lib.jxb_batch_info(h, ctypes.byref(pers), ctypes.byref(launches)))
+        self.persistent = bool(pers.value)  # one persistent launch over every degree
+        self.brick_launches = launches.value
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -170,13 +174,20 @@ if __name__ == "__main__":
     from . import workloads
     from .solve import geometry_operator
 
-    ap = argparse.ArgumentParser(description="batched K.u over the quarter-annulus instances (fixed 16 x 8 tiles)")
+    ap = argparse.ArgumentParser(description="batched K.u over the quarter-annulus instances")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--tiles", default="default",
+                    help="'default' (rows of 32 elements: one persistent launch over every degree) or WxH for "
+                         "every degree (e.g. 16x8: one launch per degree group)")
     a = ap.parse_args()
     problems, params = workloads.config3(n_instances=a.instances,
                                          interpolate=lambda V, c: geometry_operator(V).interpolate(c).cpu().numpy())
-    bs = BatchSolver(problems, params, tiles={2: (16, 8), 3: (16, 8), 4: (16, 8)})
+    tiles = None
+    if a.tiles != "default":
+        w, h = (int(v) for v in a.tiles.split("x"))
+        tiles = {p: (w, h) for p in (1, 2, 3, 4, 5)}
+    bs = BatchSolver(problems, params, tiles=tiles)
     b = bs.batch
     x = torch.randn(b.total, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
@@ -190,6 +201,7 @@ if __name__ == "__main__":
     torch.cuda.synchronize()
     n_qp = sum(pr.space.n_elems * (pr.space.degree[0] + 1) ** 2 for pr in problems)
     ms = e0.elapsed_time(e1) / a.reps
-    print(json.dumps({"instances": a.instances, "n_dofs": int(b.total), "gauss_points": n_qp, "ms_per_apply": ms,
-                      "algorithmic_gbs": (16 * b.total + 48 * n_qp) / (ms * 1e-3) / 1e9}))
+    print(json.dumps({"instances": a.instances, "tiles": a.tiles, "persistent": b.persistent,
+                      "brick_launches": b.brick_launches, "n_dofs": int(b.total), "gauss_points": n_qp,
+                      "ms_per_apply": ms, "algorithmic_gbs": (16 * b.total + 48 * n_qp) / (ms * 1e-3) / 1e9}))
     bs.close()

@@ -26,6 +26,8 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 #include "jxb_internal.cuh"
 
 namespace jxb {
@@ -659,8 +661,9 @@ static size_t smem3(const Bricks& br) {
 }
 
 int tile2_variant(int tx, int ty) {
+  if (ty < 1 || ty > TILE2_MAX_ROWS) return -1;
   for (int v = 0; v < N_TILE2; ++v)
-    if (TILE2[v][0] == tx && TILE2[v][1] == ty) return v;
+    if (TILE2X[v] == tx) return v;
   return -1;
 }
 
@@ -728,10 +731,10 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
     }
 #define JXB_TILE2(V_)                                                                                   \
   if (v == V_) {                                                                                        \
-    constexpr int TXv = TILE2[V_][0], TYv = TILE2[V_][1];                                               \
+    constexpr int TXv = TILE2X[V_];                                                                     \
     size_t sm = smem2<T, P, Q, OPK, RAT, MODE>(br, TXv);                                                \
     if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "2D brick does not fit in shared memory");        \
-    auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv, TYv>;                                               \
+    auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv>;                                                    \
     if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
     k<<<(unsigned)br.n_bricks, TXv * Q, sm, s>>>(A);                                                    \
   }
@@ -739,7 +742,6 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
     if constexpr (OPK == OPK_SCALAR) {
       JXB_TILE2(1)
       JXB_TILE2(2)
-      JXB_TILE2(3)
     }
 #undef JXB_TILE2
   }
@@ -833,10 +835,10 @@ static int launch_batch_p(int variant, const BrickArgs<double>* d_args, const in
   br.fp[1] = fp1;
 #define JXB_BTILE(V_)                                                                                   \
   if (variant == V_) {                                                                                  \
-    constexpr int TXv = TILE2[V_][0], TYv = TILE2[V_][1];                                               \
+    constexpr int TXv = TILE2X[V_];                                                                     \
     size_t sm = smem2<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY>(br, TXv);                              \
     if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");   \
-    auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv, TYv>;                       \
+    auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv>;                            \
     if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
     k<<<(unsigned)n_work, TXv * Q, sm, s>>>(d_args, d_work, d_states);                                  \
     JXB_CUDA(cudaGetLastError());                                                                       \
@@ -845,9 +847,55 @@ static int launch_batch_p(int variant, const BrickArgs<double>* d_args, const in
   JXB_BTILE(0)
   JXB_BTILE(1)
   JXB_BTILE(2)
-  JXB_BTILE(3)
 #undef JXB_BTILE
   return fail(JXB_ERR_INVALID, "unknown tile variant");
+}
+
+// Shared memory of a degree-p 2D scalar apply brick with rows of tx elements
+// and footprint fp0 x fp1 (runtime degree).
+size_t smem2_scalar_apply(int p, bool rational, int tx, int fp0, int fp1) {
+  Bricks br{};
+  br.fp[0] = fp0;
+  br.fp[1] = fp1;
+#define JXB_SM(P_)                                                                                    \
+  case P_:                                                                                            \
+    return rational ? smem2<double, P_, P_ + 1, OPK_SCALAR, true, MODE_APPLY>(br, tx)                 \
+                    : smem2<double, P_, P_ + 1, OPK_SCALAR, false, MODE_APPLY>(br, tx);
+  switch (p) {
+    JXB_SM(1)
+    JXB_SM(2)
+    JXB_SM(3)
+    JXB_SM(4)
+    JXB_SM(5)
+    default:
+      return 0;
+  }
+#undef JXB_SM
+}
+
+// The persistent batched apply (k_brick2_persist): its launch shape for a
+// batch whose largest brick needs `smem` bytes, and the launch itself.
+int persist2_grid(bool rational, size_t smem, int* grid) {
+  auto k = rational ? k_brick2_persist<double, OPK_SCALAR, true, MODE_APPLY>
+                    : k_brick2_persist<double, OPK_SCALAR, false, MODE_APPLY>;
+  if (smem > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");
+  JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  JXB_CUDA(cudaGetDevice(&dev));
+  JXB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  JXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PERSIST_THREADS, smem));
+  *grid = std::max(1, sms * std::max(1, per_sm));
+  return JXB_OK;
+}
+
+int launch_bricks2_persist(bool rational, const BrickArgs<double>* d_args, const int4* d_work, int n_work,
+                           unsigned* d_next, int grid, size_t smem, const CgState* d_states, cudaStream_t s) {
+  if (n_work <= 0) return JXB_OK;
+  auto k = rational ? k_brick2_persist<double, OPK_SCALAR, true, MODE_APPLY>
+                    : k_brick2_persist<double, OPK_SCALAR, false, MODE_APPLY>;
+  k<<<(unsigned)std::min(grid, n_work), PERSIST_THREADS, smem, s>>>(d_args, d_work, n_work, d_next, d_states);
+  JXB_CUDA(cudaGetLastError());
+  return JXB_OK;
 }
 
 int launch_bricks2_batch(int p, bool rational, int variant, const BrickArgs<double>* d_args, const int2* d_work,

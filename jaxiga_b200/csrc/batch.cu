@@ -5,8 +5,11 @@
 //
 // The instances' DOF vectors are concatenated. One CG iteration of the whole
 // batch is:
-//   * one batched brick launch per degree group -- each CTA reads its
-//     instance's arguments and brick index from a work list;
+//   * one persistent brick launch: a fixed grid of CTAs takes (instance,
+//     brick, degree) items of every degree off one work list (when every
+//     instance has rows of 32 elements, the default; otherwise one launch per
+//     degree group, each CTA reading its instance's arguments and brick index
+//     from the group's work list);
 //   * one combine launch with one CTA per instance (its p.Ap reduction stays
 //     inside the CTA, so it is deterministic);
 //   * two vector kernels with one CTA per instance (x/r/z update with r.z and
@@ -15,6 +18,7 @@
 // iterations are captured in one CUDA graph; the host reads the instances'
 // 64-byte states after each graph launch and stops when all are done.
 #include <math.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <map>
@@ -44,6 +48,13 @@ struct jxb_batch {
     int2* d_work = nullptr;
   };
   std::vector<Group> groups;
+  // the persistent path: one work list over all degrees
+  bool persist = false;
+  int4* d_pwork = nullptr;
+  int n_pwork = 0;
+  unsigned* d_next = nullptr;  // self-resetting work counter
+  int pgrid = 0;
+  size_t psmem = 0;
   jxb::BrickArgs<double>* d_args_p = nullptr;  // x = p (the CG direction)
   jxb::BrickArgs<double>* d_args_x = nullptr;  // x = x (true residual)
   cudaGraphExec_t graph = nullptr;
@@ -231,7 +242,13 @@ __global__ void __launch_bounds__(256) k_bres(const long long* __restrict__ off,
 
 int batch_apply(jxb_batch* B, cudaStream_t s, const BrickArgs<double>* d_args, double* y, const double* dot_with,
                 double* dot_out, const CgState* states) {
+  if (B->persist) {
+    int rc = launch_bricks2_persist(B->rational, d_args, B->d_pwork, B->n_pwork, B->d_next, B->pgrid, B->psmem,
+                                    states, s);
+    if (rc) return rc;
+  }
   for (auto& g : B->groups) {
+    if (B->persist) break;
     int rc = launch_bricks2_batch(g.p, B->rational, g.variant, d_args, g.d_work, g.n_work, g.fp0, g.fp1, states, s);
     if (rc) return rc;
   }
@@ -246,6 +263,8 @@ void free_batch(jxb_batch* B) {
                   B->d_gnew, B->d_rrnew, B->d_part, B->d_states, B->d_brs, B->d_scratch, B->d_args_p, B->d_args_x};
   for (void* p : bufs) cudaFree(p);
   for (auto& g : B->groups) cudaFree(g.d_work);
+  cudaFree(B->d_pwork);
+  cudaFree(B->d_next);
   if (B->h_states) cudaFreeHost(B->h_states);
   if (B->graph) cudaGraphExecDestroy(B->graph);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -349,6 +368,35 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
     JXB_CUDA_B(cudaMemcpyAsync(g.d_work, kv.second.data(), g.n_work * sizeof(int2), cudaMemcpyHostToDevice, s));
     B->groups.push_back(g);
   }
+  // The persistent path, unless JXB_BATCH_PERSIST=0 or an instance has rows of
+  // other than 32 elements: highest degree first, then the largest instances.
+  {
+    const char* env = getenv("JXB_BATCH_PERSIST");
+    bool ok = !(env && env[0] == '0');
+    for (int i = 0; i < n && ok; ++i) ok = plans[i]->br.te[0] == PERSIST2_TX && plans[i]->p >= 1 && plans[i]->p <= 5;
+    if (ok) {
+      std::vector<int4> items;
+      for (int i = 0; i < n; ++i) {
+        const jxb_plan* P = plans[i];
+        B->psmem = std::max(B->psmem, smem2_scalar_apply(P->p, B->rational, PERSIST2_TX, P->br.fp[0], P->br.fp[1]));
+        for (long long b = 0; b < P->br.n_bricks; ++b) items.push_back(make_int4(i, (int)b, P->p, 0));
+      }
+      std::stable_sort(items.begin(), items.end(), [&](int4 a, int4 b) {
+        if (a.z != b.z) return a.z > b.z;
+        return plans[a.x]->n_elem > plans[b.x]->n_elem;
+      });
+      if (items.size() > (size_t)0x7fffffff) return fail_b(fail(JXB_ERR_INVALID, "jxb_batch_create: too many bricks"));
+      B->n_pwork = (int)items.size();
+      int rc = persist2_grid(B->rational, B->psmem, &B->pgrid);
+      if (rc) return fail_b(rc);
+      if ((e = cudaMalloc(&B->d_pwork, items.size() * sizeof(int4))) != cudaSuccess)
+        return fail_b(cuda_fail(e, "cudaMalloc"));
+      if ((e = cudaMalloc(&B->d_next, sizeof(unsigned))) != cudaSuccess) return fail_b(cuda_fail(e, "cudaMalloc"));
+      JXB_CUDA_B(cudaMemsetAsync(B->d_next, 0, sizeof(unsigned), s));
+      JXB_CUDA_B(cudaMemcpyAsync(B->d_pwork, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+      B->persist = true;
+    }
+  }
   JXB_CUDA_B(cudaMemcpyAsync(B->d_off, B->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
   JXB_CUDA_B(cudaMemcpyAsync(B->d_brs, brs.data(), n * sizeof(Bricks), cudaMemcpyHostToDevice, s));
   JXB_CUDA_B(cudaMemcpyAsync(B->d_scratch, scr.data(), n * sizeof(double*), cudaMemcpyHostToDevice, s));
@@ -381,6 +429,13 @@ extern "C" int jxb_batch_size(const jxb_batch* B, int64_t* total_dofs, int64_t* 
   *total_dofs = B->total;
   if (offsets)
     for (int i = 0; i <= B->n; ++i) offsets[i] = B->off[i];
+  return JXB_OK;
+}
+
+extern "C" int jxb_batch_info(const jxb_batch* B, int* persistent, int* brick_launches) {
+  if (!B || !persistent || !brick_launches) return fail(JXB_ERR_INVALID, "jxb_batch_info: null argument");
+  *persistent = B->persist ? 1 : 0;
+  *brick_launches = B->persist ? 1 : (int)B->groups.size();
   return JXB_OK;
 }
 

@@ -1,11 +1,13 @@
 // 2D brick kernel (included by apply.cu): TX elements per row, TY rows per brick,
 // Q threads per element; x contraction through shared memory, y in registers.
+// TX is a template parameter (it sets the thread count and the shared-memory
+// layout); TY is the plan's br.te[1], so small problems can take short bricks
+// and still fill the GPU.
 #pragma once
 
 // The body of one brick (element rows [by*TY, +TY) x columns [bx*TX, +TX)).
-// TX / TY are template parameters so that the autotuner can pick them per
-// degree; the host brick decomposition of the plan must use the same shape.
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+// The host brick decomposition of the plan must use the same TX.
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
 __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long long b) {
   constexpr int P1 = P + 1, PP = P1 * P1;
   constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
@@ -20,6 +22,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   if (A.state && A.state->done) return;
   const Bricks& br = A.br;
   const int fp0 = br.fp[0], fp1 = br.fp[1];
+  const int TY = br.te[1];
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T* stx = reinterpret_cast<T*>(smem_raw);   // [TX][3][Q][P1]
@@ -29,15 +32,18 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   T* acc = stage + NE * VEC * PP;            // [VEC][fp1][fp0]
   int* soff = reinterpret_cast<int*>(acc + VEC * fp0 * fp1);
 
-  const int tid = threadIdx.x;
+  // The CTA may be wider than NT threads (the persistent batched kernel runs
+  // every degree in one CTA shape): cooperative loops stride by the CTA size,
+  // and threads past NT own no element.
+  const int tid = threadIdx.x, NTH = blockDim.x;
   const int bx = (int)(b % br.nb[0]);
   const int by = (int)(b / br.nb[0]);
   const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by];
   const int el = tid / Q, t = tid % Q;
   const int ex = bx * TX + el;
-  const bool evalid = ex < br.n_span[0];
+  const bool evalid = el < TX && ex < br.n_span[0];
 
-  for (int i = tid; i < TX * 3 * Q * P1; i += NT) {
+  for (int i = tid; i < TX * 3 * Q * P1; i += NTH) {
     int e = i / (3 * Q * P1), r = i % (3 * Q * P1);
     int sp = min(bx * TX + e, br.n_span[0] - 1);
     stx[i] = A.tab[0][(size_t)sp * 3 * Q * P1 + r];
@@ -47,7 +53,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
     soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
   }
   const int accn = VEC * fp0 * fp1;
-  for (int i = tid; i < accn; i += NT) acc[i] = T(0);
+  for (int i = tid; i < accn; i += NTH) acc[i] = T(0);
   const long long slot_base = b * (long long)TY * NE;
   const int nlayers = min(TY, br.n_span[1] - by * TY);
   const T* nx_v = stx + el * 3 * Q * P1;
@@ -56,7 +62,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
     const int ey = by * TY + ly_;
     const int fy = br.first[1][ey];
     const int offy = fy - cp0y;
-    for (int i = tid; i < 3 * Q * P1; i += NT) sty[i] = A.tab[1][(size_t)ey * 3 * Q * P1 + i];
+    for (int i = tid; i < 3 * Q * P1; i += NTH) sty[i] = A.tab[1][(size_t)ey * 3 * Q * P1 + i];
     __syncthreads();
     const long long slot = slot_base + (long long)ly_ * NE + el;
     const int fx = evalid ? br.first[0][ex] : 0;
@@ -314,7 +320,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
     // gather the row into the brick footprint
     {
       const int nfoot = VEC * fp0 * P1;
-      for (int i = tid; i < nfoot; i += NT) {
+      for (int i = tid; i < nfoot; i += NTH) {
         const int jx = i % fp0;
         const int jyl = (i / fp0) % P1;
         const int c = i / (fp0 * P1);
@@ -331,18 +337,18 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
     __syncthreads();
   }
   T* out = A.scratch + (size_t)b * accn;
-  for (int i = tid; i < accn; i += NT) out[i] = acc[i];
+  for (int i = tid; i < accn; i += NTH) out[i] = acc[i];
 }
 
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
 __global__ void __launch_bounds__(TX* Q) k_brick2(BrickArgs<T> A) {
-  brick2_body<T, P, Q, OPK, RAT, MODE, TX, TY>(A, blockIdx.x);
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX>(A, blockIdx.x);
 }
 
 // Many instances in one launch: block i processes brick work[i].y of instance
 // work[i].x, whose arguments are args[work[i].x]; instances already converged
 // (states[inst].done) are skipped.
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int TY>
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
 __global__ void __launch_bounds__(TX* Q)
     k_brick2_batch(const BrickArgs<T>* __restrict__ args, const int2* __restrict__ work,
                    const CgState* __restrict__ states) {
@@ -351,6 +357,47 @@ __global__ void __launch_bounds__(TX* Q)
   if (states && states[w.x].done) return;
   if (threadIdx.x == 0) sA = args[w.x];
   __syncthreads();
-  brick2_body<T, P, Q, OPK, RAT, MODE, TX, TY>(sA, w.y);
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX>(sA, w.y);
 }
 
+
+// Persistent batched 2D apply. A fixed grid of CTAs takes (instance, brick,
+// degree) items off one work list holding the bricks of every instance of every
+// degree (sorted by the host: highest degree and largest instance first), so
+// one launch covers the whole batch and short instances fill the gaps left by
+// long ones. Every instance uses rows of 32 elements; the CTA has 32 x (p_max
+// + 1) threads and a degree-p item runs on the first 32 (p + 1) of them.
+// The work counter resets itself: each CTA fetches until it draws an index past
+// the list, so a launch performs exactly n_work + gridDim.x increments and
+// atomicInc wraps the counter back to 0 on the last one.
+constexpr int PERSIST_TX = PERSIST2_TX;
+constexpr int PERSIST_THREADS = PERSIST_TX * 6;  // degrees 1..5
+
+template <typename T, int OPK, bool RAT, int MODE>
+__global__ void __launch_bounds__(PERSIST_THREADS)
+    k_brick2_persist(const BrickArgs<T>* __restrict__ args, const int4* __restrict__ work, int n_work,
+                     unsigned* __restrict__ next, const CgState* __restrict__ states) {
+  __shared__ BrickArgs<T> sA;
+  __shared__ int4 item;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned i = atomicInc(next, (unsigned)n_work + gridDim.x - 1u);
+      item = i < (unsigned)n_work ? work[i] : make_int4(-1, 0, 0, 0);
+      if (item.x >= 0) sA = args[item.x];
+    }
+    __syncthreads();
+    const int4 it = item;
+    if (it.x < 0) break;
+    if (!(states && states[it.x].done)) {
+      switch (it.z) {
+        case 1: brick2_body<T, 1, 2, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        case 2: brick2_body<T, 2, 3, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        case 3: brick2_body<T, 3, 4, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        case 4: brick2_body<T, 4, 5, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        case 5: brick2_body<T, 5, 6, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        default: break;
+      }
+    }
+    __syncthreads();  // item and sA are rewritten by the next fetch
+  }
+}

@@ -26,7 +26,7 @@
 
 #define JXB_MAXP 5
 #define JXB_MAXQ 6
-#define JXB_MAXC 3          // bricks covering one control point, per direction
+#define JXB_MAXC 8          // bricks covering one control point, per direction (p + 1 for one-row 2D bricks)
 #define JXB_RED_BLOCKS 296  // fixed grid of every deterministic reduction (2 x 148 SMs)
 #define JXB_RED_THREADS 256
 
@@ -146,9 +146,14 @@ struct BrickArgs {
   double lam, mu;
 };
 
-// 2D brick shapes (elements per row TX, rows per brick TY) the autotuner may pick.
-constexpr int N_TILE2 = 4;
-constexpr int TILE2[N_TILE2][2] = {{32, 8}, {16, 8}, {32, 16}, {64, 4}};
+// 2D brick widths (elements per row TX) the kernels are built for: 32 for every
+// operator, 16 and 64 for the scalar one. The rows per brick TY are a runtime
+// value in [1, TILE2_MAX_ROWS].
+constexpr int N_TILE2 = 3;
+constexpr int TILE2X[N_TILE2] = {32, 16, 64};
+constexpr int TILE2_MAX_ROWS = 64;
+// Row width of every instance of a batch that the persistent batched kernel runs.
+constexpr int PERSIST2_TX = 32;
 
 }  // namespace jxb
 
@@ -232,6 +237,10 @@ int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* do
 int tile2_variant(int tx, int ty);
 template <typename T>
 BrickArgs<T> make_brick_args(jxb_plan* plan, const T* x, const CgState* state, int masked);
+size_t smem2_scalar_apply(int p, bool rational, int tx, int fp0, int fp1);
+int persist2_grid(bool rational, size_t smem, int* grid);
+int launch_bricks2_persist(bool rational, const BrickArgs<double>* d_args, const int4* d_work, int n_work,
+                           unsigned* d_next, int grid, size_t smem, const CgState* d_states, cudaStream_t s);
 int launch_bricks2_batch(int p, bool rational, int variant, const BrickArgs<double>* d_args, const int2* d_work,
                          long long n_work, int fp0, int fp1, const CgState* d_states, cudaStream_t s);
 

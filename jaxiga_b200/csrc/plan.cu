@@ -165,12 +165,20 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
   br.q = P->q;
   host_brick_shape(P->dim, P->p, br.te);
   if (P->dim == 2 && (desc->tile[0] > 0 || desc->tile[1] > 0)) {
-    if (tile2_variant(desc->tile[0], desc->tile[1]) < 0 || P->op != JXB_OP_POISSON) {
+    const int v = tile2_variant(desc->tile[0], desc->tile[1]);
+    if (v < 0 || (v != 0 && P->op != JXB_OP_POISSON)) {
       delete P;
-      return fail(JXB_ERR_INVALID, "tile: unsupported 2D brick shape (scalar operator only)");
+      return fail(JXB_ERR_INVALID,
+                  "tile: unsupported 2D brick shape (rows of 32 elements, or 16 / 64 for the scalar operator; "
+                  "1 to 64 rows per brick)");
     }
     br.te[0] = desc->tile[0];
     br.te[1] = desc->tile[1];
+  } else if (P->dim == 2) {
+    // rows of 32 elements, and the most rows per brick (up to 8) that still
+    // give every SM of a B200 four bricks
+    const long long nbx = (P->n_span[0] + br.te[0] - 1) / br.te[0];
+    while (br.te[1] > 1 && nbx * ((P->n_span[1] + br.te[1] - 1) / br.te[1]) < 4 * 148) br.te[1] /= 2;
   }
   std::vector<int> cover_h[3], bcp0_h[3];
   long long nb_total = 1;

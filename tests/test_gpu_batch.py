@@ -79,3 +79,62 @@ def test_autotuner_picks_a_supported_tile_per_degree():
     for p, tile in best.items():
         assert tile in batch.TILES
         assert timings[(p, tile)] == min(timings[(p, t)] for t in batch.TILES)
+
+
+CHILD = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, {root!r})
+sys.path.insert(0, {tests!r})
+from test_gpu_batch import small_batch
+from jaxiga_b200 import batch, _lib
+problems, params = small_batch(12)
+bs = batch.BatchSolver(problems, params)
+assert not bs.batch.persistent
+x = torch.from_numpy(np.load({xin!r})).cuda()
+y = torch.empty_like(x)
+_lib.check(bs.batch.lib.jxb_batch_apply(bs.batch.handle, torch.cuda.current_stream().cuda_stream, x.data_ptr(),
+                                        y.data_ptr()))
+np.save({out!r}, y.cpu().numpy())
+"""
+
+
+def test_persistent_launch_equals_the_per_degree_launches(tmp_path):
+    """With default tiles (rows of 32 elements) one persistent launch walks the
+    bricks of every instance and degree; with JXB_BATCH_PERSIST=0 (a child
+    process) the same bricks run as one launch per degree group. Same bricks,
+    same per-brick arithmetic: the two K.u agree to rounding, and a second
+    persistent apply (the work counter has reset itself) repeats the first."""
+    import os
+    import subprocess
+    import sys
+
+    import torch
+
+    from jaxiga_b200 import _lib
+
+    problems, params = small_batch(12)
+    assert len({pr.space.degree[0] for pr in problems}) > 1
+    bs = batch.BatchSolver(problems, params)
+    assert bs.batch.persistent and bs.batch.brick_launches == 1
+    x = torch.randn(bs.batch.total, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    ys = []
+    for _ in range(2):
+        y = torch.empty_like(x)
+        _lib.check(bs.batch.lib.jxb_batch_apply(bs.batch.handle, torch.cuda.current_stream().cuda_stream,
+                                                x.data_ptr(), y.data_ptr()))
+        ys.append(y.cpu().numpy())
+    assert np.array_equal(ys[0], ys[1])
+    xin, out = str(tmp_path / "x.npy"), str(tmp_path / "y.npy")
+    np.save(xin, x.cpu().numpy())
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, JXB_BATCH_PERSIST="0")
+    subprocess.run([sys.executable, "-c", CHILD.format(root=root, tests=os.path.join(root, "tests"), xin=xin, out=out)],
+                   env=env, check=True, cwd=root, timeout=600)
+    y_groups = np.load(out)
+    assert np.abs(ys[0] - y_groups).max() <= 1e-14 * np.abs(y_groups).max()
+    # and each instance's block equals its own operator's K.u
+    for i, op in enumerate(bs.ops):
+        lo, hi = bs.batch.offsets[i], bs.batch.offsets[i + 1]
+        yi = op.apply(x[lo:hi].contiguous()).cpu().numpy()
+        assert np.abs(ys[0][lo:hi] - yi).max() <= 1e-13 * max(np.abs(yi).max(), 1e-300)
+    bs.close()

@@ -1,8 +1,11 @@
-"""The degree-3 3D apply exists as an FP64 tensor-core kernel (the default) and
-as the FMA kernel (JXB_BRICK3_MMA=0, read once per process). Both must give the
-same K.v: the FMA result is computed in a child process and compared with the
-tensor-core result of this process to 1e-13 relative (the two sum in different
-orders)."""
+"""The degree-3 3D apply exists in several kernels, selected by JXB_BRICK3_MMA
+(read once per process): 0 = the FMA kernel, 2 = the FP64 tensor-core kernel
+with stage hand-offs through shared memory, 4 = the register-fragment
+tensor-core kernel reading the factor tiles from L2, 5 = the same with the tiles
+copied into shared memory by the bulk-copy engine (the default is 4 for the
+scalar operator, 5 for elasticity). All must give the same K.v: each variant's
+result is computed in a child process and compared with the default kernel's
+result of this process to 1e-13 relative (they sum in different orders)."""
 
 import os
 import subprocess
@@ -44,15 +47,16 @@ def case(kind):
     return V, op, x
 
 
+@pytest.mark.parametrize("variant", ["0", "2", "4", "5"])
 @pytest.mark.parametrize("kind", ["poisson", "elasticity"])
-def test_tensor_core_and_fma_kernels_agree(kind, tmp_path):
+def test_kernel_variants_agree(kind, variant, tmp_path):
     V, op, x = case(kind)
     y_mma = op.apply(x).cpu().numpy()
     out = str(tmp_path / "y.npy")
-    env = dict(os.environ, JXB_BRICK3_MMA="0")
+    env = dict(os.environ, JXB_BRICK3_MMA=variant)
     subprocess.run([sys.executable, "-c", CHILD.format(root=ROOT, kind=kind, out=out)], env=env, check=True,
                    cwd=ROOT, timeout=600)
-    y_fma = np.load(out)
-    assert np.abs(y_mma - y_fma).max() <= 1e-13 * np.abs(y_fma).max()
+    y_var = np.load(out)
+    assert np.abs(y_mma - y_var).max() <= 1e-13 * np.abs(y_var).max()
     assert not np.array_equal(y_mma, np.zeros_like(y_mma))
     op.close()

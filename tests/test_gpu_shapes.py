@@ -95,3 +95,26 @@ def test_poisson_load_and_interpolation_match_oracle(p):
     A = O.Assembled(S, "poisson", {"a0": 1.0}, np.zeros(0, dtype=int), np.zeros(0), source_qp=fq[..., 0], need_full=False)
     assert np.abs(F - A.F).max() < 1e-13 * np.abs(A.F).max()
     dev.close()
+
+
+@pytest.mark.parametrize("op", ["poisson", "elasticity", "plate"])
+def test_brick_rows_leave_the_operator_unchanged(op):
+    """2D bricks of 1 to 64 element rows (a runtime choice; small patches get
+    short bricks by default) give the same K.v and diag K, also for the load."""
+    vec = 2 if op == "elasticity" else 1
+    V = jx.FunctionSpace(patch(2, 3, 23, "graded", rational=True), vec=vec)
+    side = V.side_indices("u0")
+    mask = np.zeros(V.n_dofs, bool)
+    mask[np.unique(jx.expand_dofs(side, vec))] = True
+    coef = {"poisson": (1.3,), "elasticity": (2.0, 0.27), "plate": (2.0, 0.27, 0.1)}[op]
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(V.n_dofs)
+    ref = jx.Operator(V, op, coef, prescribed=mask)
+    y0, d0 = ref.apply(x).cpu().numpy(), ref.diag().cpu().numpy()
+    for tile in [(32, 1), (32, 3), (32, 8), (32, 64)]:
+        dev = jx.Operator(V, op, coef, prescribed=mask, tile=tile)
+        y, d = dev.apply(x).cpu().numpy(), dev.diag().cpu().numpy()
+        assert np.abs(y - y0).max() <= 1e-12 * np.abs(y0).max(), tile
+        assert np.abs(d - d0).max() <= 1e-12 * np.abs(d0).max(), tile
+        dev.close()
+    ref.close()
