@@ -730,7 +730,7 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     rec = {"workload": "batched_quarter_annuli_256", "instances": len(costs), "n_dofs": n_all,
            "instances_on_rank0": len(problems), "elements": elems_all, "gauss_points": sum(costs),
            "degrees": sorted({pr.space.degree[0] for pr in problems}),
-           "tiles": "rows of 32 elements, 1-8 rows per brick by patch size",
+           "tiles": "32 x 8 elements per brick for every degree",
            "operator": "batched matrix-free K.u, FP64, masked, " + (
                "one persistent launch over the bricks of every degree" if b.persistent else
                "%d launches (one per degree group)" % b.brick_launches),

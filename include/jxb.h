@@ -53,7 +53,9 @@ enum jxb_status {
 enum jxb_operator {
   JXB_OP_POISSON = 0,     /* -div(a grad u) = f   (library.py:40-65)      */
   JXB_OP_ELASTICITY = 1,  /* small-strain isotropic (library.py:146-203) */
-  JXB_OP_PLATE = 2        /* Kirchhoff plate, biharmonic (library.py:68-143) */
+  JXB_OP_PLATE = 2,       /* Kirchhoff plate, biharmonic (library.py:68-143) */
+  JXB_OP_HYPERELASTIC = 3 /* compressible neo-Hookean, Newton tangent at a state (library.py:206-225);
+                             coef = {mu, lambda}; jxb_hyper_state sets the state */
 };
 
 /* Everything a plan needs; arrays are HOST pointers, copied at creation. */
@@ -249,6 +251,26 @@ int jxb_bicgstab(jxb_plan* plan, jxb_stream stream, const double* b, double* x, 
 int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                       const jxb_solve_opts* opts, int every, double* snaps, int64_t max_snaps,
                       int64_t* n_snaps, jxb_stats* stats);
+
+/* ---- nonlinear elasticity (compressible neo-Hookean) ----------------------
+ * W(F) = mu/2 (tr F^T F - d) - mu ln J + lambda/2 (ln J)^2, F = I + grad u
+ * (src/jaxiga/forms/library.py:206-225); the reference differentiates W with jax.
+ * For a JXB_OP_HYPERELASTIC plan:
+ *   jxb_hyper_state    evaluates F at every Gauss point of the displacement u
+ *                      (all n_dofs, Dirichlet values included) and stores the
+ *                      tangent state (F^-T, mu - lambda ln J) and the first
+ *                      Piola-Kirchhoff flux P(F); *energy (host, may be NULL)
+ *                      receives the stored energy sum_q w_q W(F_q), summed in a
+ *                      fixed order. Until it is called the state is u = 0.
+ *   jxb_hyper_residual r = int P(F) : grad v over all DOFs (the internal
+ *                      forces of the residual, methods/_common.py:280-309 with
+ *                      the energy's gradient in place of jax.grad).
+ *   jxb_apply / jxb_diag / jxb_pcg act with the tangent
+ *     dP = mu dF + (mu - lambda ln J) F^-T dF^T F^-T + lambda (F^-T : dF) F^-T
+ *   at the stored state (tangent_matvec at u, methods/galerkin.py:207-218).
+ * A state with J <= 0 gives non-finite values, as the reference's log does. */
+int jxb_hyper_state(jxb_plan* plan, jxb_stream stream, const double* u, double* energy);
+int jxb_hyper_residual(jxb_plan* plan, jxb_stream stream, double* r);
 
 /* ---- batches of independent problems -------------------------------------
  * The B200 form of the reference's vmap-over-params batching

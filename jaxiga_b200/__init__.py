@@ -20,9 +20,10 @@ Quick start (the reference's README example)::
 
 from .adjoint import SOLVE_COUNTER, adjoint_solve, parameter_gradients, reset_solve_counter, value_and_grad
 from .csr import CSRPattern, DeviceCG
-from .forms import (ClampedBC, DirichletBC, KirchhoffPlate, LinearElasticity, Neumann, PointField, Poisson,
-                    Problem)
+from .forms import (ClampedBC, DirichletBC, Hyperelasticity, KirchhoffPlate, LinearElasticity, Neumann, PointField,
+                    Poisson, Problem)
 from .geometry import Patch, primitives
+from .newton import history_list
 from .operator import Operator
 from .pointset import PointSet, gauss
 from .solve import LinearOptions, Solution, errornorm, integrate, norm, solve
@@ -35,5 +36,5 @@ __all__ = [
     "Problem", "DirichletBC", "ClampedBC", "Neumann", "PointField", "Poisson", "LinearElasticity",
     "KirchhoffPlate", "solve", "LinearOptions", "Solution", "errornorm", "norm", "integrate", "Operator",
     "PointSet", "gauss", "value_and_grad", "adjoint_solve", "parameter_gradients", "SOLVE_COUNTER",
-    "reset_solve_counter", "DeviceCG", "CSRPattern",
+    "reset_solve_counter", "DeviceCG", "CSRPattern", "Hyperelasticity", "history_list",
 ]

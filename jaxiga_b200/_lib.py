@@ -14,7 +14,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libjxb.so")
 
-OP_POISSON, OP_ELASTICITY, OP_PLATE = 0, 1, 2
+OP_POISSON, OP_ELASTICITY, OP_PLATE, OP_HYPERELASTIC = 0, 1, 2, 3
 
 STATUS = {0: "OK", 1: "invalid argument", 2: "CUDA error", 3: "not converged", 4: "non-finite", 5: "out of memory"}
 
@@ -137,6 +137,8 @@ SIGNATURES = [
                            c_int64_p, ctypes.POINTER(Stats)]),
     ("jxb_batch_create", [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_batch_destroy", [ctypes.c_void_p]),
+    ("jxb_hyper_state", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("jxb_hyper_residual", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_batch_size", [ctypes.c_void_p, c_int64_p, c_int64_p]),
     ("jxb_batch_info", [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("jxb_batch_apply", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

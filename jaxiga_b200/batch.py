@@ -125,7 +125,9 @@ class BatchSolver:
         self.tune = None
         if tiles == "auto":
             tiles, self.tune = autotune_tiles(self.problems, self.params)
-        self.tiles = tiles or {}
+        # default: rows of 32 elements, 8 rows per brick for every degree (the
+        # shape the persistent launch over all degrees runs)
+        self.tiles = tiles or {p: (32, 8) for p in (1, 2, 3, 4, 5)}
         self.ops = []
         loads = []
         for pr, pa in zip(self.problems, self.params):

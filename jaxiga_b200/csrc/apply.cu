@@ -32,7 +32,13 @@
 
 namespace jxb {
 
-enum OpKind { OPK_SCALAR = 0, OPK_ELAST = 1, OPK_PLATE = 2 };
+enum OpKind { OPK_SCALAR = 0, OPK_ELAST = 1, OPK_PLATE = 2, OPK_HYPER = 3 };
+
+// operators with one displacement component per direction
+template <int OPK>
+constexpr bool vec_op() {
+  return OPK == OPK_ELAST || OPK == OPK_HYPER;
+}
 
 // ---------------------------------------------------------------------------
 // compile-time shapes
@@ -59,20 +65,54 @@ struct BrickShape<2, P> {
 // which measured 19 % and 6 % faster than 2 CTAs at p = 3.
 template <typename T, int P, int OPK>
 constexpr int brick3_min_blocks() {
-  return (sizeof(T) == 4 && P <= 3) ? (OPK == OPK_ELAST ? 3 : 4) : BrickShape<3, P>::MINB;
+  return OPK == OPK_HYPER ? 1 : (sizeof(T) == 4 && P <= 3) ? (OPK == OPK_ELAST ? 3 : 4) : BrickShape<3, P>::MINB;
 }
 
+// Factors per Gauss point. The hyperelastic operator stores the elasticity
+// geometry (J^-1, w|J|[, 1/W, grad W / W]) and then its state: F^-T (row major),
+// mu - lambda ln J, and the flux w P(F) J^-T of the residual (row major).
 template <int OPK, bool RAT, int DIM>
 struct GeoCount {
-  static constexpr int value =
-      OPK == OPK_SCALAR ? (RAT ? (DIM + 1) * (DIM + 2) / 2 : DIM * (DIM + 1) / 2)
-      : OPK == OPK_ELAST ? (DIM * DIM + 1 + (RAT ? DIM + 1 : 0))
-                         : (RAT ? 21 : 15);
+  static constexpr int elast = DIM * DIM + 1 + (RAT ? DIM + 1 : 0);
+  static constexpr int value = OPK == OPK_SCALAR ? (RAT ? (DIM + 1) * (DIM + 2) / 2 : DIM * (DIM + 1) / 2)
+                               : OPK == OPK_ELAST ? elast
+                               : OPK == OPK_HYPER ? elast + 2 * DIM * DIM + 1
+                                                  : (RAT ? 21 : 15);
 };
+
+// om times the neo-Hookean first Piola-Kirchhoff increment at a stored state
+// (M = F^-T, c = mu - lambda ln J):
+// dP = mu dF + c F^-T dF^T F^-T + lambda (F^-T : dF) F^-T.
+template <typename T, int D>
+__device__ __forceinline__ void hyper_dP(const T (&M)[D][D], T c, T lam, T mu, T om, const T (&dF)[D][D],
+                                         T (&S)[D][D]) {
+  T t1[D][D];  // F^-T dF^T
+  T tr = 0;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int b = 0; b < D; ++b) {
+      T v = 0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) v += M[i][a] * dF[b][a];
+      t1[i][b] = v;
+      tr += M[i][b] * dF[i][b];
+    }
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      T v = 0;
+#pragma unroll
+      for (int b = 0; b < D; ++b) v += t1[i][b] * M[b][k];
+      S[i][k] = om * (mu * dF[i][k] + c * v + lam * tr * M[i][k]);
+    }
+}
 
 int host_geo_count(int op, int rational, int dim) {
   if (op == JXB_OP_POISSON) return rational ? (dim + 1) * (dim + 2) / 2 : dim * (dim + 1) / 2;
   if (op == JXB_OP_ELASTICITY) return dim * dim + 1 + (rational ? dim + 1 : 0);
+  if (op == JXB_OP_HYPERELASTIC) return dim * dim + 1 + (rational ? dim + 1 : 0) + 2 * dim * dim + 1;
   return rational ? 21 : 15;
 }
 
@@ -115,8 +155,9 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
   constexpr int P1 = P + 1, PP = P1 * P1, PPP = PP * P1;
   constexpr int TX = BrickShape<3, P>::TX, TY = BrickShape<3, P>::TY, CZ = BrickShape<3, P>::CZ;
   constexpr int NE = TX * TY, QQ = Q * Q, NQE = Q * Q * Q, NT = NE * QQ;
-  constexpr int VEC = OPK == OPK_ELAST ? 3 : 1;
+  constexpr int VEC = vec_op<OPK>() ? 3 : 1;
   constexpr int NG = GeoCount<OPK, RAT, 3>::value;
+  constexpr int E0 = GeoCount<OPK_ELAST, RAT, 3>::elast;  // hyperelastic: start of the state
   constexpr bool HASV = RAT || MODE == MODE_LOAD;  // value channel
   constexpr int SX = S::SX, SY1 = S::SY1, SYC = S::SYC, SP = S::SP, SST = S::SST;
 
@@ -322,7 +363,7 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
               g[0][1][q2] = m[2] * v + m[5] * gx + m[7] * gy + m[8] * gz;
               g[0][2][q2] = m[3] * v + m[6] * gx + m[8] * gy + m[9] * gz;
             }
-          } else if constexpr (OPK == OPK_ELAST) {
+          } else if constexpr (OPK == OPK_ELAST || OPK == OPK_HYPER) {
             T Ji[3][3];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
@@ -351,11 +392,21 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
             }
             const T tr = Gx[0][0] + Gx[1][1] + Gx[2][2];
             const T lam = (T)A.lam, mu = (T)A.mu;
+            T Sh[3][3];  // hyperelastic: om dP at the stored state
+            if constexpr (OPK == OPK_HYPER) {
+              T M[3][3];
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) M[i][k] = __ldg(G + (E0 + i * 3 + k) * NQE + qo);
+              hyper_dP<T, 3>(M, __ldg(G + (E0 + 9) * NQE + qo), lam, mu, om, Gx, Sh);
+            }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
               T Sr[3];
 #pragma unroll
-              for (int k = 0; k < 3; ++k) Sr[k] = om * (mu * (Gx[c][k] + Gx[k][c]) + (c == k ? lam * tr : T(0)));
+              for (int k = 0; k < 3; ++k)
+                Sr[k] = OPK == OPK_HYPER ? Sh[c][k] : om * (mu * (Gx[c][k] + Gx[k][c]) + (c == k ? lam * tr : T(0)));
               T F[3];
 #pragma unroll
               for (int a = 0; a < 3; ++a) F[a] = Sr[0] * Ji[0][a] + Sr[1] * Ji[1][a] + Sr[2] * Ji[2][a];
@@ -385,9 +436,37 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
           }
         }
       }
+    } else if constexpr (MODE == MODE_RESID) {  // hyperelastic: the stored flux w P J^-T
+      if (evalid) {
+        const T* G = A.geo + (size_t)slot * NG * NQE + t;
+#pragma unroll
+        for (int q2 = 0; q2 < Q; ++q2) {
+          const int qo = QQ * q2;
+          T iW = 1, gW[3] = {0, 0, 0};
+          if constexpr (RAT) {
+            iW = G[10 * NQE + qo];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) gW[a] = G[(11 + a) * NQE + qo];
+          }
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) {
+            T F[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) F[a] = G[(E0 + 10 + c * 3 + a) * NQE + qo];
+            if constexpr (RAT) {
+              g[c][3][q2] = -(F[0] * gW[0] + F[1] * gW[1] + F[2] * gW[2]) * iW;
+#pragma unroll
+              for (int a = 0; a < 3; ++a) g[c][a][q2] = F[a] * iW;
+            } else {
+#pragma unroll
+              for (int a = 0; a < 3; ++a) g[c][a][q2] = F[a];
+            }
+          }
+        }
+      }
     }
 
-    if constexpr (MODE == MODE_APPLY || MODE == MODE_LOAD) {
+    if constexpr (MODE == MODE_APPLY || MODE == MODE_LOAD || MODE == MODE_RESID) {
       // ---------------- backward contractions, one component at a time ------
 #pragma unroll
       for (int c = 0; c < VEC; ++c) {
@@ -509,8 +588,19 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
 #pragma unroll
               for (int k = 0; k < 3; ++k) gx[k] = Ji[k][0] * gp[0] + Ji[k][1] * gp[1] + Ji[k][2] * gp[2];
               const T n2 = gx[0] * gx[0] + gx[1] * gx[1] + gx[2] * gx[2];
+              if constexpr (OPK == OPK_HYPER) {
+                // mu |g|^2 + (c + lambda) (F^-T_c . g)^2 at the stored state
+                const T ch = G[(E0 + 9) * NQE] + (T)A.lam;
 #pragma unroll
-              for (int c = 0; c < VEC; ++c) d[c] += om * ((T)(A.lam + A.mu) * gx[c] * gx[c] + (T)A.mu * n2);
+                for (int c = 0; c < VEC; ++c) {
+                  const T mg = G[(E0 + c * 3) * NQE] * gx[0] + G[(E0 + c * 3 + 1) * NQE] * gx[1] +
+                               G[(E0 + c * 3 + 2) * NQE] * gx[2];
+                  d[c] += om * ((T)A.mu * n2 + ch * mg * mg);
+                }
+              } else {
+#pragma unroll
+                for (int c = 0; c < VEC; ++c) d[c] += om * ((T)(A.lam + A.mu) * gx[c] * gx[c] + (T)A.mu * n2);
+              }
             }
           }
           T wsq = 1;
@@ -653,7 +743,7 @@ static size_t smem3(const Bricks& br) {
   constexpr int P1 = P + 1;
   constexpr int TX = BrickShape<3, P>::TX, TY = BrickShape<3, P>::TY;
   constexpr int NE = TX * TY;
-  constexpr int VEC = OPK == OPK_ELAST ? 3 : 1;
+  constexpr int VEC = vec_op<OPK>() ? 3 : 1;
   size_t n = (size_t)(TX + TY + 1) * 2 * Q * P1 + (size_t)NE * 2 * Q * S::SX + (size_t)NE * 3 * S::SYC +
              (size_t)NE * VEC * S::SST + (size_t)VEC * br.fp[0] * br.fp[1] * br.fp[2] +
              (MODE == MODE_APPLY ? (size_t)P1 * br.fp[0] * br.fp[1] * VEC : 0);
@@ -670,7 +760,7 @@ int tile2_variant(int tx, int ty) {
 template <typename T, int P, int Q, int OPK, bool RAT, int MODE>
 static size_t smem2(const Bricks& br, const int TX) {
   constexpr int P1 = P + 1, PP = P1 * P1;
-  constexpr int VEC = OPK == OPK_ELAST ? 2 : 1;
+  constexpr int VEC = vec_op<OPK>() ? 2 : 1;
   constexpr int NK = OPK == OPK_PLATE ? 3 : 2;
   constexpr int SX = P1 + 1;
   size_t n = (size_t)TX * 3 * Q * P1 + 3 * Q * P1 + TX * NK * Q * SX + TX * VEC * PP +
@@ -751,8 +841,29 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
 
 template <typename T, int MODE>
 static int dispatch(jxb_plan* plan, const BrickArgs<T>& A, cudaStream_t s) {
-  int opk = plan->op == JXB_OP_POISSON ? OPK_SCALAR : plan->op == JXB_OP_ELASTICITY ? OPK_ELAST : OPK_PLATE;
   bool rat = plan->rational != 0;
+  if (plan->op == JXB_OP_HYPERELASTIC) {  // FP64, degrees 1..4
+    if constexpr (sizeof(T) == 8) {
+#define JXB_HCASE(P_) \
+  case P_:            \
+    return rat ? launch_one<T, P_, OPK_HYPER, true, MODE>(A, s) : launch_one<T, P_, OPK_HYPER, false, MODE>(A, s);
+      switch (plan->p) {
+        JXB_HCASE(1)
+        JXB_HCASE(2)
+        JXB_HCASE(3)
+        JXB_HCASE(4)
+        default:
+          return fail(JXB_ERR_INVALID, "the hyperelastic operator takes degrees 1..4");
+      }
+#undef JXB_HCASE
+    } else {
+      return fail(JXB_ERR_INVALID, "the hyperelastic operator has no FP32 copy");
+    }
+  }
+  if constexpr (MODE == MODE_RESID) {
+    return fail(JXB_ERR_INVALID, "the residual mode belongs to the hyperelastic operator");
+  } else {
+  int opk = plan->op == JXB_OP_POISSON ? OPK_SCALAR : plan->op == JXB_OP_ELASTICITY ? OPK_ELAST : OPK_PLATE;
 #define JXB_CASE(P_)                                                                         \
   case P_:                                                                                  \
     if (opk == OPK_SCALAR) return rat ? launch_one<T, P_, OPK_SCALAR, true, MODE>(A, s)     \
@@ -771,6 +882,7 @@ static int dispatch(jxb_plan* plan, const BrickArgs<T>& A, cudaStream_t s) {
       return fail(JXB_ERR_INVALID, "degree must be in 1..5");
   }
 #undef JXB_CASE
+  }
 }
 
 template <typename T>
@@ -807,6 +919,7 @@ int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const do
   if constexpr (!F32) {
     if (mode == MODE_LOAD) return dispatch<T, MODE_LOAD>(plan, A, s);
     if (mode == MODE_DIAG) return dispatch<T, MODE_DIAG>(plan, A, s);
+    if (mode == MODE_RESID) return dispatch<T, MODE_RESID>(plan, A, s);
   }
   return fail(JXB_ERR_INVALID, "unsupported brick mode");
 }
@@ -879,7 +992,9 @@ int persist2_grid(bool rational, size_t smem, int* grid) {
   auto k = rational ? k_brick2_persist<double, OPK_SCALAR, true, MODE_APPLY>
                     : k_brick2_persist<double, OPK_SCALAR, false, MODE_APPLY>;
   if (smem > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");
-  JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the attribute is per kernel, shared by every batch: allow the largest size,
+  // each launch passes its own
+  JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   int dev = 0, sms = 0, per_sm = 0;
   JXB_CUDA(cudaGetDevice(&dev));
   JXB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

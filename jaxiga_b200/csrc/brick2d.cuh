@@ -11,8 +11,9 @@ template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
 __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long long b) {
   constexpr int P1 = P + 1, PP = P1 * P1;
   constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
-  constexpr int VEC = OPK == OPK_ELAST ? 2 : 1;
+  constexpr int VEC = vec_op<OPK>() ? 2 : 1;
   constexpr int NG = GeoCount<OPK, RAT, 2>::value;
+  constexpr int E0 = GeoCount<OPK_ELAST, RAT, 2>::elast;  // hyperelastic: start of the state
   constexpr bool HASV = RAT || MODE == MODE_LOAD;
   constexpr bool HESS = OPK == OPK_PLATE;
   constexpr int NK = HESS ? 3 : 2;      // 1D table kinds used
@@ -184,10 +185,15 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
               for (int k = 0; k < 2; ++k) Gx[c][k] = Ji[k][0] * gp[c][0] + Ji[k][1] * gp[c][1];
             T tr = Gx[0][0] + Gx[1][1];
             T lam = (T)A.lam, mu = (T)A.mu;
+            T Sh[2][2];  // hyperelastic: om dP at the stored state
+            if constexpr (OPK == OPK_HYPER) {
+              const T M[2][2] = {{G[E0 * NQE + q], G[(E0 + 1) * NQE + q]}, {G[(E0 + 2) * NQE + q], G[(E0 + 3) * NQE + q]}};
+              hyper_dP<T, 2>(M, G[(E0 + 4) * NQE + q], lam, mu, om, Gx, Sh);
+            }
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-              T S0 = om * (mu * (Gx[c][0] + Gx[0][c]) + (c == 0 ? lam * tr : T(0)));
-              T S1 = om * (mu * (Gx[c][1] + Gx[1][c]) + (c == 1 ? lam * tr : T(0)));
+              T S0 = OPK == OPK_HYPER ? Sh[c][0] : om * (mu * (Gx[c][0] + Gx[0][c]) + (c == 0 ? lam * tr : T(0)));
+              T S1 = OPK == OPK_HYPER ? Sh[c][1] : om * (mu * (Gx[c][1] + Gx[1][c]) + (c == 1 ? lam * tr : T(0)));
               T F0 = S0 * Ji[0][0] + S1 * Ji[1][0];
               T F1 = S0 * Ji[0][1] + S1 * Ji[1][1];
               if constexpr (RAT) {
@@ -218,9 +224,37 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
           }
         }
       }
+    } else if constexpr (MODE == MODE_RESID) {  // hyperelastic: the stored flux w P J^-T
+      if (evalid) {
+        const T* G = A.geo + (size_t)slot * NG * NQE;
+#pragma unroll
+        for (int q1 = 0; q1 < Q; ++q1) {
+          const int q = t + Q * q1;
+          T iW = 1, gW[2] = {0, 0};
+          if constexpr (RAT) {
+            iW = G[5 * NQE + q];
+            gW[0] = G[6 * NQE + q];
+            gW[1] = G[7 * NQE + q];
+          }
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) {
+            const T F0 = G[(E0 + 5 + 2 * c) * NQE + q], F1 = G[(E0 + 6 + 2 * c) * NQE + q];
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) g[c][k][q1] = T(0);
+            if constexpr (RAT) {
+              g[c][0][q1] = -(F0 * gW[0] + F1 * gW[1]) * iW;
+              g[c][1][q1] = F0 * iW;
+              g[c][2][q1] = F1 * iW;
+            } else {
+              g[c][1][q1] = F0;
+              g[c][2][q1] = F1;
+            }
+          }
+        }
+      }
     }
 
-    if constexpr (MODE == MODE_APPLY || MODE == MODE_LOAD) {
+    if constexpr (MODE == MODE_APPLY || MODE == MODE_LOAD || MODE == MODE_RESID) {
 #pragma unroll
       for (int c = 0; c < VEC; ++c) {
         if (evalid) {  // Y^T: q0 = t -> bufX[k][q0][i1]
@@ -302,8 +336,18 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
               }
               T gx[2] = {Ji[0][0] * gp[0] + Ji[0][1] * gp[1], Ji[1][0] * gp[0] + Ji[1][1] * gp[1]};
               T n2 = gx[0] * gx[0] + gx[1] * gx[1];
+              if constexpr (OPK == OPK_HYPER) {
+                // mu |g|^2 + (c + lambda) (F^-T_c . g)^2 at the stored state
+                const T ch = G[(E0 + 4) * NQE] + (T)A.lam;
 #pragma unroll
-              for (int c = 0; c < VEC; ++c) d[c] += om * ((T)(A.lam + A.mu) * gx[c] * gx[c] + (T)A.mu * n2);
+                for (int c = 0; c < VEC; ++c) {
+                  const T mg = G[(E0 + 2 * c) * NQE] * gx[0] + G[(E0 + 2 * c + 1) * NQE] * gx[1];
+                  d[c] += om * ((T)A.mu * n2 + ch * mg * mg);
+                }
+              } else {
+#pragma unroll
+                for (int c = 0; c < VEC; ++c) d[c] += om * ((T)(A.lam + A.mu) * gx[c] * gx[c] + (T)A.mu * n2);
+              }
             }
           }
           T wsq = 1;
@@ -379,15 +423,22 @@ __global__ void __launch_bounds__(PERSIST_THREADS)
                      unsigned* __restrict__ next, const CgState* __restrict__ states) {
   __shared__ BrickArgs<T> sA;
   __shared__ int4 item;
+  static_assert(sizeof(BrickArgs<T>) % 8 == 0, "BrickArgs copy in 8-byte words");
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned i = atomicInc(next, (unsigned)n_work + gridDim.x - 1u);
       item = i < (unsigned)n_work ? work[i] : make_int4(-1, 0, 0, 0);
-      if (item.x >= 0) sA = args[item.x];
     }
     __syncthreads();
     const int4 it = item;
     if (it.x < 0) break;
+    // the instance's arguments, copied by the whole CTA
+    {
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(args + it.x);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sA);
+      for (int w = threadIdx.x; w < (int)(sizeof(BrickArgs<T>) / 8); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
     if (!(states && states[it.x].done)) {
       switch (it.z) {
         case 1: brick2_body<T, 1, 2, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;

@@ -327,7 +327,7 @@ __global__ void k_factors(FactorArgs A) {
         M[r][c] = a0 * om * s;
       }
     store_sym(g, nqe, nc, M, off);
-  } else if (A.op == JXB_OP_ELASTICITY) {
+  } else if (A.op == JXB_OP_ELASTICITY || A.op == JXB_OP_HYPERELASTIC) {
     int k = 0;
     for (int i = 0; i < dim; ++i)
       for (int a = 0; a < dim; ++a) g[nqe * (k++)] = Ji[i][a];
@@ -335,6 +335,12 @@ __global__ void k_factors(FactorArgs A) {
     if (A.rational) {
       g[nqe * (k++)] = iW;
       for (int a = 0; a < dim; ++a) g[nqe * (k++)] = S.Wd[a] * iW;
+    }
+    if (A.op == JXB_OP_HYPERELASTIC) {  // the state of u = 0: F^-T = I, mu - lambda ln J = mu, no flux
+      for (int i = 0; i < dim; ++i)
+        for (int a = 0; a < dim; ++a) g[nqe * (k++)] = i == a ? 1.0 : 0.0;
+      g[nqe * (k++)] = A.coef[0];
+      for (int i = 0; i < dim * dim; ++i) g[nqe * (k++)] = 0.0;
     }
   } else {  // plate (2D): channels (v, v0, v1, v00, v01, v11)
     double E = A.coef[0], nu = A.coef[1], t = A.coef[2];
@@ -986,6 +992,138 @@ int boundary_load(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, co
     k_boundary_gather<<<(unsigned)((n_touched + 127) / 128), 128, 0, s>>>(n_touched, dof, ptr, contrib, plan->vec,
                                                                           local, F);
     JXB_CUDA(cudaGetLastError());
+  }
+  return JXB_OK;
+}
+
+// Neo-Hookean state at every (element slot, Gauss point) for the displacement
+// u (interleaved (n_cp, dim)): F = I + grad u, J = det F, and written after the
+// elasticity geometry of the point: F^-T, c = mu - lambda ln J and the flux
+// w P J^-T, P = mu (F - F^-T) + lambda ln J F^-T the gradient of the stored
+// energy W = mu/2 (tr F^T F - d) - mu ln J + lambda/2 (ln J)^2
+// (src/jaxiga/forms/library.py:206-225). Each block adds its points' w W into
+// partials[blockIdx.x] in a fixed order (grid JXB_RED_BLOCKS, grid-stride).
+__global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double* __restrict__ u,
+                                                     double* __restrict__ partials) {
+  const Bricks& br = A.br;
+  const int dim = br.dim, Q = br.q, P1 = br.p + 1;
+  const long long nqe = dim == 2 ? Q * Q : Q * Q * Q;
+  const double mu = A.coef[0], lam = A.coef[1];
+  const int e0 = dim * dim + 1 + (A.rational ? dim + 1 : 0);
+  double wsum = 0.0;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < br.slots * nqe;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long slot = idx / nqe;
+    const int q = (int)(idx % nqe);
+    int ex, ey, ez;
+    bool valid;
+    elem_of_slot(br, slot, ex, ey, ez, valid);
+    if (!valid) continue;
+    const int sp[3] = {ex, ey, ez};
+    const int qq[3] = {q % Q, (q / Q) % Q, dim == 3 ? q / (Q * Q) : 0};
+    const double* nv[3];
+    const double* nd[3];
+    for (int d = 0; d < dim; ++d) {
+      const double* base = A.tab[d] + (size_t)sp[d] * 3 * Q * P1;
+      nv[d] = base + (size_t)qq[d] * P1;
+      nd[d] = base + (size_t)(Q + qq[d]) * P1;
+    }
+    const int f0 = br.first[0][ex], f1 = br.first[1][ey], f2 = dim == 3 ? br.first[2][ez] : 0;
+    double W = 0, Wd[3] = {0, 0, 0}, Px[3] = {0, 0, 0}, Pd[3][3] = {}, U[3] = {0, 0, 0}, Ud[3][3] = {};
+    const int n2 = dim == 3 ? P1 : 1;
+    for (int a2 = 0; a2 < n2; ++a2)
+      for (int a1 = 0; a1 < P1; ++a1)
+        for (int a0 = 0; a0 < P1; ++a0) {
+          const long long cp = (long long)(f0 + a0) +
+                               (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
+          const double z = dim == 3 ? nv[2][a2] : 1.0, dz = dim == 3 ? nd[2][a2] : 0.0;
+          const double w = A.wgts[cp];
+          const double N = w * nv[0][a0] * nv[1][a1] * z;
+          const double dN[3] = {w * nd[0][a0] * nv[1][a1] * z, w * nv[0][a0] * nd[1][a1] * z,
+                                w * nv[0][a0] * nv[1][a1] * dz};
+          W += N;
+          for (int k = 0; k < dim; ++k) Wd[k] += dN[k];
+          for (int i = 0; i < dim; ++i) {
+            const double X = A.cpts[cp * dim + i];
+            Px[i] += N * X;
+            for (int k = 0; k < dim; ++k) Pd[i][k] += dN[k] * X;
+            const double v = u[cp * dim + i];
+            U[i] += N * v;
+            for (int k = 0; k < dim; ++k) Ud[i][k] += dN[k] * v;
+          }
+        }
+    const double iW = 1.0 / W;
+    double J[3][3], Ji[3][3];
+    for (int i = 0; i < dim; ++i) {
+      const double x = Px[i] * iW;
+      for (int a = 0; a < dim; ++a) J[a][i] = (Pd[i][a] - x * Wd[a]) * iW;  // d x_i / d xi_a
+    }
+    const double det = det_inv(dim, J, Ji);
+    double jac = 1.0, wh = 1.0;
+    for (int d = 0; d < dim; ++d) {
+      jac *= (A.span_hi[d][sp[d]] - A.span_lo[d][sp[d]]) / 2.0;
+      wh *= A.gw[qq[d]];
+    }
+    const double om = wh * fabs(det) * jac;
+    // F = I + du_i / dx_k
+    double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int i = 0; i < dim; ++i) {
+      const double ui = U[i] * iW;
+      double ud[3];
+      for (int a = 0; a < dim; ++a) ud[a] = (Ud[i][a] - ui * Wd[a]) * iW;
+      for (int k = 0; k < dim; ++k) {
+        double gk = 0;
+        for (int a = 0; a < dim; ++a) gk += Ji[k][a] * ud[a];
+        F[i][k] += gk;
+      }
+    }
+    double Fi[3][3];
+    const double Jd = det_inv(dim, F, Fi);  // Fi = F^-1
+    const double lnJ = log(Jd);             // J <= 0: not finite, as the reference's log
+    double I1 = 0;
+    for (int i = 0; i < dim; ++i)
+      for (int k = 0; k < dim; ++k) I1 += F[i][k] * F[i][k];
+    wsum += om * (0.5 * mu * (I1 - dim) - mu * lnJ + 0.5 * lam * lnJ * lnJ);
+    double* g = A.geo + (size_t)slot * A.ngeo * nqe + q;
+    int k = e0;
+    for (int i = 0; i < dim; ++i)
+      for (int a = 0; a < dim; ++a) g[nqe * (k++)] = Fi[a][i];  // F^-T
+    g[nqe * (k++)] = mu - lam * lnJ;
+    for (int i = 0; i < dim; ++i)
+      for (int a = 0; a < dim; ++a) {  // w P J^-T, P_ik = mu (F_ik - F^-T_ik) + lambda ln J F^-T_ik
+        double f = 0;
+        for (int kk = 0; kk < dim; ++kk) {
+          const double Pik = mu * (F[i][kk] - Fi[kk][i]) + lam * lnJ * Fi[kk][i];
+          f += Pik * Ji[kk][a];
+        }
+        g[nqe * (k++)] = om * f;
+      }
+  }
+  // fixed-order block sum
+  __shared__ double part[8];
+  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = wsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += part[i];
+    partials[blockIdx.x] = t;
+  }
+}
+
+int hyper_state(jxb_plan* plan, cudaStream_t s, const double* u, double* energy) {
+  if (plan->op != JXB_OP_HYPERELASTIC) return fail(JXB_ERR_INVALID, "jxb_hyper_state: not a hyperelastic plan");
+  FactorArgs A = make_args(plan);
+  k_hyper_state<<<JXB_RED_BLOCKS, 256, 0, s>>>(A, u, plan->d_red);
+  JXB_CUDA(cudaGetLastError());
+  plan->diag_valid = false;  // the Jacobi diagonal follows the state
+  if (energy) {
+    double h[JXB_RED_BLOCKS];
+    JXB_CUDA(cudaMemcpyAsync(h, plan->d_red, sizeof h, cudaMemcpyDeviceToHost, s));
+    JXB_CUDA(cudaStreamSynchronize(s));
+    double e = 0;
+    for (int i = 0; i < JXB_RED_BLOCKS; ++i) e += h[i];
+    *energy = e;
   }
   return JXB_OK;
 }

@@ -216,6 +216,7 @@ int build_factors(jxb_plan* plan, const jxb_desc* desc, cudaStream_t s);
 int qp_coords(jxb_plan* plan, cudaStream_t s, double* x);
 int interpolate(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
 int interpolate_grad(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, double* out);
+int hyper_state(jxb_plan* plan, cudaStream_t s, const double* u, double* energy);
 int eval_points(jxb_plan* plan, cudaStream_t s, const double* coef, int ncomp, long long n, const long long* elems,
                 const double* ref, double* val, double* grad, double* x, double* jac);
 int boundary_points(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, const long long* elems,
@@ -226,7 +227,7 @@ int boundary_load(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, co
 int qp_weights(jxb_plan* plan, cudaStream_t s, double* w);
 
 // apply.cu
-enum Mode { MODE_APPLY = 0, MODE_LOAD = 1, MODE_DIAG = 2 };
+enum Mode { MODE_APPLY = 0, MODE_LOAD = 1, MODE_DIAG = 2, MODE_RESID = 3 };
 template <typename T>
 int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const double* f_qp,
                   const CgState* state, int masked);

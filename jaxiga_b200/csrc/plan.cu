@@ -84,6 +84,11 @@ static int validate(const jxb_desc* d) {
   } else if (d->op == JXB_OP_PLATE) {
     if (d->dim != 2 || d->vec != 1) return fail(JXB_ERR_INVALID, "plate needs dim == 2 and vec == 1");
     if (d->degree < 2) return fail(JXB_ERR_INVALID, "plate needs degree >= 2 (C1 continuity)");
+  } else if (d->op == JXB_OP_HYPERELASTIC) {
+    if (d->vec != d->dim) return fail(JXB_ERR_INVALID, "the hyperelastic operator needs vec == dim");
+    if (d->degree > 4) return fail(JXB_ERR_INVALID, "the hyperelastic operator takes degrees 1..4");
+    if (d->want_f32) return fail(JXB_ERR_INVALID, "the hyperelastic operator has no FP32 copy");
+    if (!(d->coef[0] > 0) || !(d->coef[1] >= 0)) return fail(JXB_ERR_INVALID, "hyperelastic coef = {mu > 0, lambda >= 0}");
   } else {
     return fail(JXB_ERR_INVALID, "unknown operator");
   }
@@ -153,6 +158,9 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
       P->mat.lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     else
       P->mat.lam = E * nu / (1.0 - nu * nu);
+  } else if (P->op == JXB_OP_HYPERELASTIC) {
+    P->mat.mu = desc->coef[0];
+    P->mat.lam = desc->coef[1];
   } else {
     P->mat.lam = P->mat.mu = 0.0;
   }
@@ -176,9 +184,10 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
     br.te[1] = desc->tile[1];
   } else if (P->dim == 2) {
     // rows of 32 elements, and the most rows per brick (up to 8) that still
-    // give every SM of a B200 four bricks
+    // give every SM of a B200 one brick (shorter bricks cost more per element:
+    // each loads its tables and writes a footprint of p more rows)
     const long long nbx = (P->n_span[0] + br.te[0] - 1) / br.te[0];
-    while (br.te[1] > 1 && nbx * ((P->n_span[1] + br.te[1] - 1) / br.te[1]) < 4 * 148) br.te[1] /= 2;
+    while (br.te[1] > 1 && nbx * ((P->n_span[1] + br.te[1] - 1) / br.te[1]) < 148) br.te[1] /= 2;
   }
   std::vector<int> cover_h[3], bcp0_h[3];
   long long nb_total = 1;
@@ -343,6 +352,20 @@ extern "C" int jxb_diag(jxb_plan* P, jxb_stream stream, double* d) {
   int rc = launch_bricks<double>(P, s, MODE_DIAG, nullptr, nullptr, nullptr, 1);
   if (rc) return rc;
   return launch_combine<double>(P, s, d, 1, nullptr, nullptr, nullptr);
+}
+
+extern "C" int jxb_hyper_state(jxb_plan* P, jxb_stream stream, const double* u, double* energy) {
+  if (!P || !u) return fail(JXB_ERR_INVALID, "jxb_hyper_state: null argument");
+  return hyper_state(P, reinterpret_cast<cudaStream_t>(stream), u, energy);
+}
+
+extern "C" int jxb_hyper_residual(jxb_plan* P, jxb_stream stream, double* r) {
+  if (!P || !r) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: null argument");
+  if (P->op != JXB_OP_HYPERELASTIC) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: not a hyperelastic plan");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int rc = launch_bricks<double>(P, s, MODE_RESID, nullptr, nullptr, nullptr, 0);
+  if (rc) return rc;
+  return launch_combine<double>(P, s, r, 0, nullptr, nullptr, nullptr);
 }
 
 extern "C" int jxb_load(jxb_plan* P, jxb_stream stream, const double* f_qp, double* F) {

@@ -35,15 +35,18 @@ class Operator:
     Parameters
     ----------
     space : FunctionSpace
-    op : {"poisson", "elasticity", "plate"}
-    coef : sequence of up to 4 floats -- a0 | (E, nu) | (E, nu, t)
+    op : {"poisson", "elasticity", "plate", "hyperelastic"}
+    coef : sequence of up to 4 floats -- a0 | (E, nu) | (E, nu, t) | (mu, lambda)
+        ("hyperelastic": the compressible neo-Hookean tangent at the state set by
+        ``state(u)``, u = 0 until then)
     prescribed : optional bool/uint8 array (n_dofs,), True on Dirichlet DOFs
     coef_qp : optional (n_elem, n_q^dim) per-point a0 for Poisson
     want_f32 : keep FP32 copies of the factors for mixed precision
     plane_strain : 2D elasticity flavour
     """
 
-    OPS = {"poisson": _lib.OP_POISSON, "elasticity": _lib.OP_ELASTICITY, "plate": _lib.OP_PLATE}
+    OPS = {"poisson": _lib.OP_POISSON, "elasticity": _lib.OP_ELASTICITY, "plate": _lib.OP_PLATE,
+           "hyperelastic": _lib.OP_HYPERELASTIC}
 
     def __init__(self, space, op="poisson", coef=(1.0,), prescribed=None, coef_qp=None,
                  want_f32=False, plane_strain=False, vec=None, tile=None):
@@ -172,6 +175,27 @@ class Operator:
         d = self._empty(self.n_dofs)
         _lib.check(self.lib.jxb_diag(self.handle, _stream(), _dptr(d)))
         return d
+
+    def state(self, u, energy=False):
+        """Hyperelastic plans: set the state to the displacement ``u`` (all DOFs,
+        Dirichlet values included) for the tangent and the residual; with
+        ``energy`` return the stored energy sum_q w_q W(F_q) (host float)."""
+        if self.op != "hyperelastic":
+            raise ValueError("state() belongs to the hyperelastic operator")
+        uv = self._vec(u)  # referenced until the launch is queued on the stream
+        e = ctypes.c_double()
+        _lib.check(self.lib.jxb_hyper_state(self.handle, _stream(), _dptr(uv),
+                                            ctypes.byref(e) if energy else None))
+        return e.value if energy else None
+
+    def residual(self):
+        """Hyperelastic plans: the internal forces int P(F) : grad v at the
+        current state, over all DOFs (device tensor)."""
+        if self.op != "hyperelastic":
+            raise ValueError("residual() belongs to the hyperelastic operator")
+        r = self._empty(self.n_dofs)
+        _lib.check(self.lib.jxb_hyper_residual(self.handle, _stream(), _dptr(r)))
+        return r
 
     def load(self, f_qp):
         """F = sum_q w f R (full length) for source values at the Gauss points."""

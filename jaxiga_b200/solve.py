@@ -282,7 +282,7 @@ def _check_problem(problem, method):
     if method != "galerkin":
         raise NotImplementedError(f"method={method!r}: the B200 backend implements 'galerkin' only")
     if not problem.is_linear:
-        raise NotImplementedError("the B200 backend solves linear problems only")
+        raise NotImplementedError("the B200 backend solves linear problems and the neo-Hookean Hyperelasticity form")
     if problem.quadrature is not None and problem.quadrature != problem.space.degree[0] + 1:
         raise NotImplementedError("the B200 backend uses the default p+1 Gauss rule")
 
@@ -306,6 +306,21 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
         return _solve_batch(problem, params, linear, method)
     import torch
 
+    if not problem.is_linear and method == "galerkin" and getattr(problem, "op", None) == "hyperelastic":
+        # Newton on the device (methods/galerkin.py:337-354, solvers/newton.py)
+        from .newton import newton_solve
+
+        if problem.quadrature is not None and problem.quadrature != problem.space.degree[0] + 1:
+            raise NotImplementedError("the B200 backend uses the default p+1 Gauss rule")
+        if linear is None:
+            linear = default_linear(problem)
+        if linear.method != "cg" or linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none"):
+            raise NotImplementedError("Newton steps run FP64 CG with the Jacobi preconditioner (or none)")
+        opts = {k: method_opts[k] for k in ("tol", "max_steps", "line_search") if k in method_opts}
+        unknown = set(method_opts) - set(opts)
+        if unknown:
+            raise TypeError(f"unknown Newton options {sorted(unknown)}")
+        return newton_solve(problem, params, linear, initial_guess=initial_guess, **opts)
     _check_problem(problem, method)
     if linear is None:
         linear = default_linear(problem)
