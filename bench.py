@@ -657,7 +657,7 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     mine = partition_by_cost(costs, world)[rank]
     problems = [problems[i] for i in mine]
     params = [params[i] for i in mine]
-    bs = BatchSolver(problems, params)  # rows of 32 elements: one persistent launch over every degree
+    bs = BatchSolver(problems, params)  # 16 x 8 bricks, one launch per degree group
     setup_s = time.perf_counter() - t0
     b = bs.batch
     n = b.total
@@ -681,10 +681,14 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     apply = lambda xx, yy: _lib.check(b.lib.jxb_batch_apply(b.handle, torch.cuda.current_stream().cuda_stream,  # noqa: E731
                                                             xx.data_ptr(), yy.data_ptr()))
     ms = time_apply(b, steps)
-    # the per-degree-group launches with autotuned tiles, for comparison
-    bs_t = BatchSolver(problems, params, tiles="auto")
+    # the persistent launch over every degree (32 x 8 bricks), for comparison
+    os.environ["JXB_BATCH_PERSIST"] = "1"
+    try:
+        bs_t = BatchSolver(problems, params, tiles={p: (32, 8) for p in (1, 2, 3, 4, 5)})
+    finally:
+        os.environ.pop("JXB_BATCH_PERSIST", None)
     ms_groups = time_apply(bs_t.batch, steps) / steps
-    groups = {"tiles": {str(k): v for k, v in bs_t.tiles.items()}, "brick_launches": bs_t.batch.brick_launches,
+    groups = {"tiles": "32 x 8", "brick_launches": bs_t.batch.brick_launches,
               "persistent": bs_t.batch.persistent, "ms_per_apply": ms_groups}
     bs_t.close()
     value = n_all * steps / (ms * 1e-3)
@@ -730,11 +734,11 @@ def batch_record(steps, rank, world, peaks, peak_kind, solve=True):
     rec = {"workload": "batched_quarter_annuli_256", "instances": len(costs), "n_dofs": n_all,
            "instances_on_rank0": len(problems), "elements": elems_all, "gauss_points": sum(costs),
            "degrees": sorted({pr.space.degree[0] for pr in problems}),
-           "tiles": "32 x 8 elements per brick for every degree",
+           "tiles": "16 x 8 elements per brick for every degree",
            "operator": "batched matrix-free K.u, FP64, masked, " + (
                "one persistent launch over the bricks of every degree" if b.persistent else
                "%d launches (one per degree group)" % b.brick_launches),
-           "per_degree_group_launches_autotuned": groups,
+           "persistent_launch_over_every_degree": groups,
            "parallelism": "instances sharded over %d GPU(s) by cost, no collective" % world,
            "setup_seconds": setup_s, "value": value, "unit": UNIT, "ms_per_apply": ms / steps,
            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,

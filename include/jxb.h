@@ -272,6 +272,19 @@ int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double
 int jxb_hyper_state(jxb_plan* plan, jxb_stream stream, const double* u, double* energy);
 int jxb_hyper_residual(jxb_plan* plan, jxb_stream stream, double* r);
 
+/* ---- several conforming patches (multipatch spaces) ----------------------
+ * A composite plan over n patch plans of one operator (created without
+ * Dirichlet masks), glued by local_to_global[i] (patch i's n_cp entries: the
+ * global scalar index of each control point, src/jaxiga/geometry/multipatch.py
+ * compute_topology). Its K.u is sum_p S_p^T K_p S_p x (S_p the gather of patch
+ * p's DOFs), the patch copies of every global DOF summed in a fixed order;
+ * prescribed (n_global_scalar * vec, or NULL) marks Dirichlet DOFs. It works
+ * with jxb_apply, jxb_diag, jxb_load (f_qp: the patches' points in patch order),
+ * jxb_dot, jxb_pcg and jxb_plan_destroy (which leaves the patch plans alone;
+ * destroy them after the composite); the other entry points reject it. */
+int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_to_global, int64_t n_global_scalar,
+                  const uint8_t* prescribed, jxb_plan** out);
+
 /* ---- batches of independent problems -------------------------------------
  * The B200 form of the reference's vmap-over-params batching
  * (tests/test_advanced.py:338-356; host SciPy solves run once per member,
@@ -285,8 +298,8 @@ int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out);
 int jxb_batch_destroy(jxb_batch* batch);
 int jxb_batch_size(const jxb_batch* batch, int64_t* total_dofs, int64_t* offsets /* n+1 or NULL */);
 /* How a batched K.u runs: *persistent = 1 when one persistent launch walks the
- * bricks of every instance and degree (every plan has rows of 32 elements and
- * JXB_BATCH_PERSIST is not "0"), else 0; *brick_launches = brick launches per K.u. */
+ * bricks of every instance and degree (JXB_BATCH_PERSIST=1 and every plan has rows
+ * of 32 elements), else 0; *brick_launches = brick launches per K.u. */
 int jxb_batch_info(const jxb_batch* batch, int* persistent, int* brick_launches);
 int jxb_batch_apply(jxb_batch* batch, jxb_stream stream, const double* x, double* y);
 int jxb_batch_pcg(jxb_batch* batch, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,

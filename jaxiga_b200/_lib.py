@@ -137,6 +137,8 @@ SIGNATURES = [
                            c_int64_p, ctypes.POINTER(Stats)]),
     ("jxb_batch_create", [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_batch_destroy", [ctypes.c_void_p]),
+    ("jxb_mp_create", [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                       ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_hyper_state", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("jxb_hyper_residual", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_batch_size", [ctypes.c_void_p, c_int64_p, c_int64_p]),

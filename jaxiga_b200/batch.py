@@ -125,9 +125,10 @@ class BatchSolver:
         self.tune = None
         if tiles == "auto":
             tiles, self.tune = autotune_tiles(self.problems, self.params)
-        # default: rows of 32 elements, 8 rows per brick for every degree (the
-        # shape the persistent launch over all degrees runs)
-        self.tiles = tiles or {p: (32, 8) for p in (1, 2, 3, 4, 5)}
+        # default: 16 x 8 element bricks for every degree (the autotuner's pick on
+        # the 256-annuli batch); JXB_BATCH_PERSIST=1 with 32-wide tiles runs the
+        # persistent launch instead
+        self.tiles = tiles or {p: (16, 8) for p in (1, 2, 3, 4, 5)}
         self.ops = []
         loads = []
         for pr, pa in zip(self.problems, self.params):

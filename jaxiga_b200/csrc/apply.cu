@@ -888,6 +888,12 @@ static int dispatch(jxb_plan* plan, const BrickArgs<T>& A, cudaStream_t s) {
 template <typename T>
 int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const double* f_qp,
                   const CgState* state, int masked) {
+  if (plan->mp) {  // composite multipatch plan: gather, then every patch's bricks
+    if constexpr (sizeof(T) == 8)
+      return mp_bricks(plan, s, mode, x, f_qp, state);
+    else
+      return fail(JXB_ERR_INVALID, "multipatch plans have no FP32 copy");
+  }
   BrickArgs<T> A;
   A.br = plan->br;
   constexpr bool F32 = sizeof(T) == 4;
@@ -927,6 +933,12 @@ int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const do
 template <typename T>
 int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* dot_with,
                    double* partials, const CgState* state) {
+  if (plan->mp) {  // composite: the fixed-order sum of the patches' copies of every DOF
+    if constexpr (sizeof(T) == 8)
+      return mp_combine(plan, s, y, masked, dot_with, partials, state);
+    else
+      return fail(JXB_ERR_INVALID, "multipatch plans have no FP32 copy");
+  }
   const T* scratch;
   if constexpr (sizeof(T) == 4)
     scratch = plan->d_scratch32;
@@ -991,10 +1003,13 @@ size_t smem2_scalar_apply(int p, bool rational, int tx, int fp0, int fp1) {
 int persist2_grid(bool rational, size_t smem, int* grid) {
   auto k = rational ? k_brick2_persist<double, OPK_SCALAR, true, MODE_APPLY>
                     : k_brick2_persist<double, OPK_SCALAR, false, MODE_APPLY>;
-  if (smem > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");
-  // the attribute is per kernel, shared by every batch: allow the largest size,
-  // each launch passes its own
-  JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  // the attribute is per kernel, shared by every batch: allow the largest size
+  // (227 KB less the kernel's static shared memory), each launch passes its own
+  cudaFuncAttributes fa;
+  JXB_CUDA(cudaFuncGetAttributes(&fa, k));
+  const int max_dyn = 227 * 1024 - (int)fa.sharedSizeBytes;
+  if (smem > (size_t)max_dyn) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");
+  JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
   int dev = 0, sms = 0, per_sm = 0;
   JXB_CUDA(cudaGetDevice(&dev));
   JXB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -5,11 +5,10 @@
 //
 // The instances' DOF vectors are concatenated. One CG iteration of the whole
 // batch is:
-//   * one persistent brick launch: a fixed grid of CTAs takes (instance,
-//     brick, degree) items of every degree off one work list (when every
-//     instance has rows of 32 elements, the default; otherwise one launch per
-//     degree group, each CTA reading its instance's arguments and brick index
-//     from the group's work list);
+//   * one brick launch per degree group, each CTA reading its instance's
+//     arguments and brick index from the group's work list (or, with
+//     JXB_BATCH_PERSIST=1 and rows of 32 elements, one persistent launch whose
+//     CTAs take (instance, brick, degree) items of every degree off one list);
 //   * one combine launch with one CTA per instance (its p.Ap reduction stays
 //     inside the CTA, so it is deterministic);
 //   * two vector kernels with one CTA per instance (x/r/z update with r.z and
@@ -290,6 +289,7 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
                                        " appears more than once; create one plan per instance");
   }
   for (int i = 0; i < n; ++i) {
+    if (plans[i]->mp) return fail(JXB_ERR_INVALID, "jxb_batch_create: not available on a multipatch plan");
     if (plans[i]->dim != 2 || plans[i]->op != JXB_OP_POISSON)
       return fail(JXB_ERR_INVALID, "jxb_batch_create: batches take 2D Poisson plans");
     if (plans[i]->rational != plans[0]->rational)
@@ -368,11 +368,14 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
     JXB_CUDA_B(cudaMemcpyAsync(g.d_work, kv.second.data(), g.n_work * sizeof(int2), cudaMemcpyHostToDevice, s));
     B->groups.push_back(g);
   }
-  // The persistent path, unless JXB_BATCH_PERSIST=0 or an instance has rows of
-  // other than 32 elements: highest degree first, then the largest instances.
+  // The persistent path on request (JXB_BATCH_PERSIST=1) when every instance has
+  // rows of 32 elements: highest degree first, then the largest instances. It is
+  // not the default: each of its CTAs reserves the shared memory of the largest
+  // degree, which caps the resident CTAs per SM, and on the 256-annuli batch it
+  // measured 0.93 ms per K.u against 0.48 ms for the per-degree launches.
   {
     const char* env = getenv("JXB_BATCH_PERSIST");
-    bool ok = !(env && env[0] == '0');
+    bool ok = env && env[0] == '1';
     for (int i = 0; i < n && ok; ++i) ok = plans[i]->br.te[0] == PERSIST2_TX && plans[i]->p >= 1 && plans[i]->p <= 5;
     if (ok) {
       std::vector<int4> items;

@@ -6,8 +6,9 @@
 #pragma once
 
 // The body of one brick (element rows [by*TY, +TY) x columns [bx*TX, +TX)).
-// The host brick decomposition of the plan must use the same TX.
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
+// The host brick decomposition of the plan must use the same TX. WIDE: the CTA
+// may have more than TX * Q threads (the persistent batched kernel).
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, bool WIDE = false>
 __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long long b) {
   constexpr int P1 = P + 1, PP = P1 * P1;
   constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
@@ -33,16 +34,16 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   T* acc = stage + NE * VEC * PP;            // [VEC][fp1][fp0]
   int* soff = reinterpret_cast<int*>(acc + VEC * fp0 * fp1);
 
-  // The CTA may be wider than NT threads (the persistent batched kernel runs
+  // A WIDE CTA may have more than NT threads (the persistent batched kernel runs
   // every degree in one CTA shape): cooperative loops stride by the CTA size,
   // and threads past NT own no element.
-  const int tid = threadIdx.x, NTH = blockDim.x;
+  const int tid = threadIdx.x, NTH = WIDE ? (int)blockDim.x : NT;
   const int bx = (int)(b % br.nb[0]);
   const int by = (int)(b / br.nb[0]);
   const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by];
   const int el = tid / Q, t = tid % Q;
   const int ex = bx * TX + el;
-  const bool evalid = el < TX && ex < br.n_span[0];
+  const bool evalid = (!WIDE || el < TX) && ex < br.n_span[0];
 
   for (int i = tid; i < TX * 3 * Q * P1; i += NTH) {
     int e = i / (3 * Q * P1), r = i % (3 * Q * P1);
@@ -441,11 +442,11 @@ __global__ void __launch_bounds__(PERSIST_THREADS)
     __syncthreads();
     if (!(states && states[it.x].done)) {
       switch (it.z) {
-        case 1: brick2_body<T, 1, 2, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
-        case 2: brick2_body<T, 2, 3, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
-        case 3: brick2_body<T, 3, 4, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
-        case 4: brick2_body<T, 4, 5, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
-        case 5: brick2_body<T, 5, 6, OPK, RAT, MODE, PERSIST_TX>(sA, it.y); break;
+        case 1: brick2_body<T, 1, 2, OPK, RAT, MODE, PERSIST_TX, true>(sA, it.y); break;
+        case 2: brick2_body<T, 2, 3, OPK, RAT, MODE, PERSIST_TX, true>(sA, it.y); break;
+        case 3: brick2_body<T, 3, 4, OPK, RAT, MODE, PERSIST_TX, true>(sA, it.y); break;
+        case 4: brick2_body<T, 4, 5, OPK, RAT, MODE, PERSIST_TX, true>(sA, it.y); break;
+        case 5: brick2_body<T, 5, 6, OPK, RAT, MODE, PERSIST_TX, true>(sA, it.y); break;
         default: break;
       }
     }

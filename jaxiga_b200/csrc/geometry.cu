@@ -1001,8 +1001,11 @@ int boundary_load(jxb_plan* plan, cudaStream_t s, long long n_faces, int n_q, co
 // elasticity geometry of the point: F^-T, c = mu - lambda ln J and the flux
 // w P J^-T, P = mu (F - F^-T) + lambda ln J F^-T the gradient of the stored
 // energy W = mu/2 (tr F^T F - d) - mu ln J + lambda/2 (ln J)^2
-// (src/jaxiga/forms/library.py:206-225). Each block adds its points' w W into
-// partials[blockIdx.x] in a fixed order (grid JXB_RED_BLOCKS, grid-stride).
+// (src/jaxiga/forms/library.py:206-225). J^-1, w|J| and the rational factors
+// 1/W, grad W / W are read from the point's stored geometry (k_factors), the
+// displacement gradient is summed from the tables. Each block adds its points'
+// w W into partials[blockIdx.x] in a fixed order (grid JXB_RED_BLOCKS,
+// grid-stride).
 __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double* __restrict__ u,
                                                      double* __restrict__ partials) {
   const Bricks& br = A.br;
@@ -1019,6 +1022,16 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
     bool valid;
     elem_of_slot(br, slot, ex, ey, ez, valid);
     if (!valid) continue;
+    double* g = A.geo + (size_t)slot * A.ngeo * nqe + q;
+    double Ji[3][3];
+    for (int i = 0; i < dim; ++i)
+      for (int a = 0; a < dim; ++a) Ji[i][a] = g[nqe * (i * dim + a)];
+    const double om = g[nqe * (dim * dim)];
+    double iW = 1.0, gW[3] = {0, 0, 0};
+    if (A.rational) {
+      iW = g[nqe * (dim * dim + 1)];
+      for (int a = 0; a < dim; ++a) gW[a] = g[nqe * (dim * dim + 2 + a)];
+    }
     const int sp[3] = {ex, ey, ez};
     const int qq[3] = {q % Q, (q / Q) % Q, dim == 3 ? q / (Q * Q) : 0};
     const double* nv[3];
@@ -1029,7 +1042,7 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
       nd[d] = base + (size_t)(Q + qq[d]) * P1;
     }
     const int f0 = br.first[0][ex], f1 = br.first[1][ey], f2 = dim == 3 ? br.first[2][ez] : 0;
-    double W = 0, Wd[3] = {0, 0, 0}, Px[3] = {0, 0, 0}, Pd[3][3] = {}, U[3] = {0, 0, 0}, Ud[3][3] = {};
+    double U[3] = {0, 0, 0}, Ud[3][3] = {};
     const int n2 = dim == 3 ? P1 : 1;
     for (int a2 = 0; a2 < n2; ++a2)
       for (int a1 = 0; a1 < P1; ++a1)
@@ -1037,40 +1050,22 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
           const long long cp = (long long)(f0 + a0) +
                                (long long)br.n_cp[0] * ((f1 + a1) + (long long)br.n_cp[1] * (f2 + a2));
           const double z = dim == 3 ? nv[2][a2] : 1.0, dz = dim == 3 ? nd[2][a2] : 0.0;
-          const double w = A.wgts[cp];
+          const double w = A.rational ? A.wgts[cp] : 1.0;
           const double N = w * nv[0][a0] * nv[1][a1] * z;
           const double dN[3] = {w * nd[0][a0] * nv[1][a1] * z, w * nv[0][a0] * nd[1][a1] * z,
                                 w * nv[0][a0] * nv[1][a1] * dz};
-          W += N;
-          for (int k = 0; k < dim; ++k) Wd[k] += dN[k];
           for (int i = 0; i < dim; ++i) {
-            const double X = A.cpts[cp * dim + i];
-            Px[i] += N * X;
-            for (int k = 0; k < dim; ++k) Pd[i][k] += dN[k] * X;
             const double v = u[cp * dim + i];
             U[i] += N * v;
             for (int k = 0; k < dim; ++k) Ud[i][k] += dN[k] * v;
           }
         }
-    const double iW = 1.0 / W;
-    double J[3][3], Ji[3][3];
-    for (int i = 0; i < dim; ++i) {
-      const double x = Px[i] * iW;
-      for (int a = 0; a < dim; ++a) J[a][i] = (Pd[i][a] - x * Wd[a]) * iW;  // d x_i / d xi_a
-    }
-    const double det = det_inv(dim, J, Ji);
-    double jac = 1.0, wh = 1.0;
-    for (int d = 0; d < dim; ++d) {
-      jac *= (A.span_hi[d][sp[d]] - A.span_lo[d][sp[d]]) / 2.0;
-      wh *= A.gw[qq[d]];
-    }
-    const double om = wh * fabs(det) * jac;
-    // F = I + du_i / dx_k
+    // F = I + du_i / dx_k, du_i / dxi_a = (Ud - u W_a) / W
     double F[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int i = 0; i < dim; ++i) {
       const double ui = U[i] * iW;
       double ud[3];
-      for (int a = 0; a < dim; ++a) ud[a] = (Ud[i][a] - ui * Wd[a]) * iW;
+      for (int a = 0; a < dim; ++a) ud[a] = Ud[i][a] * iW - ui * gW[a];
       for (int k = 0; k < dim; ++k) {
         double gk = 0;
         for (int a = 0; a < dim; ++a) gk += Ji[k][a] * ud[a];
@@ -1084,7 +1079,6 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
     for (int i = 0; i < dim; ++i)
       for (int k = 0; k < dim; ++k) I1 += F[i][k] * F[i][k];
     wsum += om * (0.5 * mu * (I1 - dim) - mu * lnJ + 0.5 * lam * lnJ * lnJ);
-    double* g = A.geo + (size_t)slot * A.ngeo * nqe + q;
     int k = e0;
     for (int i = 0; i < dim; ++i)
       for (int a = 0; a < dim; ++a) g[nqe * (k++)] = Fi[a][i];  // F^-T

@@ -158,6 +158,7 @@ constexpr int PERSIST2_TX = 32;
 }  // namespace jxb
 
 struct jxb_krylov_ws;  // BiCGSTAB workspace (krylov.cu)
+struct jxb_mp_data;    // composite multipatch plan (mp.cu)
 
 struct jxb_plan {
   int device = 0;  // the CUDA device that was current at creation; its buffers live there
@@ -206,6 +207,7 @@ struct jxb_plan {
   int graph_precond[2] = {-1, -1};
   cudaStream_t graph_stream[2] = {nullptr, nullptr};
   size_t scratch_elems = 0;
+  jxb_mp_data* mp = nullptr;  // set on a composite plan over several patch plans
 };
 
 namespace jxb {
@@ -238,6 +240,12 @@ int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* do
 int tile2_variant(int tx, int ty);
 template <typename T>
 BrickArgs<T> make_brick_args(jxb_plan* plan, const T* x, const CgState* state, int masked);
+// mp.cu: the composite plan's hooks in launch_bricks / launch_combine
+int mp_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const double* f_qp, const CgState* state);
+int mp_combine(jxb_plan* plan, cudaStream_t s, double* y, int masked, const double* dot_with, double* partials,
+               const CgState* state);
+void free_mp(jxb_plan* plan);
+
 size_t smem2_scalar_apply(int p, bool rational, int tx, int fp0, int fp1);
 int persist2_grid(bool rational, size_t smem, int* grid);
 int launch_bricks2_persist(bool rational, const BrickArgs<double>* d_args, const int4* d_work, int n_work,

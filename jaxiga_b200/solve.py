@@ -131,7 +131,12 @@ def geometry_operator(space) -> Operator:
     """Cached evaluation plan of a space (coordinates, weights, interpolation)."""
     op = space._plans.get("geometry")
     if op is None:
-        op = Operator(space, "poisson", (1.0,), vec=1)
+        from .multipatch import MultiPatchGeometry, MultiPatchSpace
+
+        if isinstance(space, MultiPatchSpace):
+            op = MultiPatchGeometry(space)
+        else:
+            op = Operator(space, "poisson", (1.0,), vec=1)
         space._plans["geometry"] = op
     return op
 
@@ -220,8 +225,11 @@ def cached_operator(space, op_name, coef, prescribed_mask=None, coef_qp=None, wa
         return op
     if op is not None:
         cache.pop(key).close()
-    op = Operator(space, op_name, coef, prescribed=prescribed_mask, coef_qp=coef_qp, want_f32=want_f32,
-                  plane_strain=plane_strain)
+    from .multipatch import MultiPatchOperator, MultiPatchSpace
+
+    cls = MultiPatchOperator if isinstance(space, MultiPatchSpace) else Operator
+    op = cls(space, op_name, coef, prescribed=prescribed_mask, coef_qp=coef_qp, want_f32=want_f32,
+             plane_strain=plane_strain)
     cache[key] = op
     while len(cache) > OPERATOR_CACHE_SIZE:
         cache.popitem(last=False)[1].close()
@@ -336,6 +344,13 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     # Krylov loop and runs in FP32 only what the preconditioner computes (the
     # learned network; the Jacobi scaling otherwise).
     fp32_operator = linear.precision == "mixed" and problem.op != "plate"
+    from .multipatch import MultiPatchSpace
+
+    if isinstance(space, MultiPatchSpace):
+        if linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none") or linear.method != "cg":
+            raise NotImplementedError("multipatch spaces solve with FP64 Jacobi-PCG")
+        if problem.neumann:
+            raise NotImplementedError("Neumann loads on multipatch spaces are not supported")
     op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)
     from .adjoint import SOLVE_COUNTER

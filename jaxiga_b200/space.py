@@ -120,15 +120,23 @@ class FunctionSpace:
     """Global NURBS basis over one patch (function_space.py:182-274, 372-454).
 
     ``FunctionSpace(patch, vec=1)``; a one-element list of patches is also
-    accepted. Multipatch spaces are outside this build.
+    accepted; a list of several conforming patches gives a ``MultiPatchSpace``.
     """
+
+    def __new__(cls, patches=None, vec: int = 1):
+        # several patches: a conforming multipatch space (multipatch.py)
+        if isinstance(patches, (list, tuple)) and len(patches) > 1:
+            from .multipatch import MultiPatchSpace
+
+            return MultiPatchSpace(patches, vec=vec)
+        return super().__new__(cls)
 
     def __init__(self, patches, vec: int = 1):
         from .geometry import Patch
 
         if isinstance(patches, (list, tuple)):
             if len(patches) != 1:
-                raise NotImplementedError("the B200 backend supports single-patch spaces only")
+                raise ValueError("internal error: a multipatch list reached the single-patch space")
             patches = patches[0]
         if not isinstance(patches, Patch):
             raise TypeError("FunctionSpace expects a Patch")

@@ -88,7 +88,7 @@ sys.path.insert(0, {tests!r})
 from test_gpu_batch import small_batch
 from jaxiga_b200 import batch, _lib
 problems, params = small_batch(12)
-bs = batch.BatchSolver(problems, params)
+bs = batch.BatchSolver(problems, params, tiles={{p: (32, 8) for p in (1, 2, 3, 4, 5)}})
 assert not bs.batch.persistent
 x = torch.from_numpy(np.load({xin!r})).cuda()
 y = torch.empty_like(x)
@@ -98,12 +98,12 @@ np.save({out!r}, y.cpu().numpy())
 """
 
 
-def test_persistent_launch_equals_the_per_degree_launches(tmp_path):
-    """With default tiles (rows of 32 elements) one persistent launch walks the
-    bricks of every instance and degree; with JXB_BATCH_PERSIST=0 (a child
-    process) the same bricks run as one launch per degree group. Same bricks,
-    same per-brick arithmetic: the two K.u agree to rounding, and a second
-    persistent apply (the work counter has reset itself) repeats the first."""
+def test_persistent_launch_equals_the_per_degree_launches(tmp_path, monkeypatch):
+    """With JXB_BATCH_PERSIST=1 and rows of 32 elements one persistent launch
+    walks the bricks of every instance and degree; without it (a child process)
+    the same bricks run as one launch per degree group. Same bricks, same
+    per-brick arithmetic: the two K.u agree to rounding, and a second persistent
+    apply (the work counter has reset itself) repeats the first."""
     import os
     import subprocess
     import sys
@@ -114,7 +114,9 @@ def test_persistent_launch_equals_the_per_degree_launches(tmp_path):
 
     problems, params = small_batch(12)
     assert len({pr.space.degree[0] for pr in problems}) > 1
-    bs = batch.BatchSolver(problems, params)
+    tiles = {p: (32, 8) for p in (1, 2, 3, 4, 5)}
+    monkeypatch.setenv("JXB_BATCH_PERSIST", "1")
+    bs = batch.BatchSolver(problems, params, tiles=tiles)
     assert bs.batch.persistent and bs.batch.brick_launches == 1
     x = torch.randn(bs.batch.total, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
     ys = []
@@ -124,10 +126,14 @@ def test_persistent_launch_equals_the_per_degree_launches(tmp_path):
                                                 x.data_ptr(), y.data_ptr()))
         ys.append(y.cpu().numpy())
     assert np.array_equal(ys[0], ys[1])
+    # the persistent batch also solves: every instance converges
+    xs, stats, _ = bs.solve(tol=1e-10)
+    assert all(st["converged"] for st in stats)
     xin, out = str(tmp_path / "x.npy"), str(tmp_path / "y.npy")
     np.save(xin, x.cpu().numpy())
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    env = dict(os.environ, JXB_BATCH_PERSIST="0")
+    env = dict(os.environ)
+    env.pop("JXB_BATCH_PERSIST", None)
     subprocess.run([sys.executable, "-c", CHILD.format(root=root, tests=os.path.join(root, "tests"), xin=xin, out=out)],
                    env=env, check=True, cwd=root, timeout=600)
     y_groups = np.load(out)
