@@ -49,7 +49,7 @@ template <int P>
 struct BrickShape<3, P> {
   static constexpr int TX = P <= 4 ? 4 : 3;
   static constexpr int TY = TX;
-  static constexpr int CZ = 8;
+  static constexpr int CZ = 8;  // element layers per brick at most (the plan may take fewer)
   static constexpr int MINB = P <= 3 ? 2 : 1;  // resident CTAs per SM the kernel is built for
 };
 template <int P>
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
     k_brick3(BrickArgs<T> A) {
   using S = Strides3<P, Q>;
   constexpr int P1 = P + 1, PP = P1 * P1, PPP = PP * P1;
-  constexpr int TX = BrickShape<3, P>::TX, TY = BrickShape<3, P>::TY, CZ = BrickShape<3, P>::CZ;
+  constexpr int TX = BrickShape<3, P>::TX, TY = BrickShape<3, P>::TY;
   constexpr int NE = TX * TY, QQ = Q * Q, NQE = Q * Q * Q, NT = NE * QQ;
   constexpr int VEC = vec_op<OPK>() ? 3 : 1;
   constexpr int NG = GeoCount<OPK, RAT, 3>::value;
@@ -189,8 +189,9 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
   const int ex = bx * TX + exl, ey = by * TY + eyl;
   const bool evalid = ex < br.n_span[0] && ey < br.n_span[1];
 
-  const long long slot_base = b * (long long)CZ * NE;
-  const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
+  const int cz = br.te[2];  // element layers per brick (<= CZ): fewer for small patches
+  const long long slot_base = b * (long long)cz * NE;
+  const int nlayers = min(cz, br.n_span[2] - bz * cz);
   constexpr unsigned TILE_BYTES = NE * NG * NQE * sizeof(T);
   if constexpr (MODE == MODE_APPLY) {
     if (tid == 0) prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, TILE_BYTES);
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(BrickShape<3, P>::TX* BrickShape<3, P>::TY* Q*
   const long long nxy = (long long)br.n_cp[0] * br.n_cp[1];
 
   for (int lz = 0; lz < nlayers; ++lz) {
-    const int ez = bz * CZ + lz;
+    const int ez = bz * cz + lz;
     const int fz = br.first[2][ez];
     const int offz = fz - cp0z;
     const long long slot = slot_base + (long long)lz * NE + el;

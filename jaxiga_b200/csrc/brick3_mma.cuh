@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
   const int exl = w % TX, eyl = w / TX;
   const int ex = bx * TX + exl, ey = by * TY + eyl;
   const bool evalid = ex < br.n_span[0] && ey < br.n_span[1];
-  const long long slot_base = b * (long long)CZ * NE;
-  const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
+  const int cz = br.te[2];  // element layers per brick (<= CZ): fewer for small patches
+  const long long slot_base = b * (long long)cz * NE;
+  const int nlayers = min(cz, br.n_span[2] - bz * cz);
   if (tid < TX) {
     const int e = bx * TX + tid;
     soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
@@ -140,9 +141,9 @@ __global__ void __launch_bounds__(bm::NT, MINB) k_brick3_mma(BrickArgs<double> A
     const int qoff = 16 * (g & 3) + 8 * hh + 2 * t;
     if (lane == 0) prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
     double un[VEC][2];
-    load_in(bz * CZ, un);
+    load_in(bz * cz, un);
     for (int lz = 0; lz < nlayers; ++lz) {
-      const int ez = bz * CZ + lz;
+      const int ez = bz * cz + lz;
       const int offz = br.first[2][ez] - cp0z;
       const long long slot = slot_base + (long long)lz * NE + w;
       if (lane == 0 && lz + 1 < nlayers) prefetch_l2(A.geo + (size_t)(slot + NE) * NG * NQE, NG * NQE * sizeof(double));

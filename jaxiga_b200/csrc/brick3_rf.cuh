@@ -124,8 +124,9 @@ __global__ void __launch_bounds__(brf::NT, MINB) k_brick3_rf(BrickArgs<double> A
   const int exl = w % TX, eyl = w / TX;
   const int ex = bx * TX + exl, ey = by * TY + eyl;
   const bool evalid = ex < br.n_span[0] && ey < br.n_span[1];
-  const long long slot_base = b * (long long)CZ * NE;
-  const int nlayers = min(CZ, br.n_span[2] - bz * CZ);
+  const int cz = br.te[2];  // element layers per brick (<= CZ): fewer for small patches
+  const long long slot_base = b * (long long)cz * NE;
+  const int nlayers = min(cz, br.n_span[2] - bz * cz);
   if (tid < TX) {
     const int e = bx * TX + tid;
     soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(brf::NT, MINB) k_brick3_rf(BrickArgs<double> A
   // the brick's z tables (values and first derivatives, the first 32 of a span's 48)
   for (int i = tid; i < nlayers * ZT; i += NT) {
     const int lz = i / ZT, r = i - lz * ZT;
-    ztab[i] = A.tab[2][(size_t)(bz * CZ + lz) * 3 * Q * P1 + r];
+    ztab[i] = A.tab[2][(size_t)(bz * cz + lz) * 3 * Q * P1 + r];
   }
   double* cf = colf + w * VEC * fp2 * CF;
   for (int i = lane; i < VEC * fp2 * CF; i += 32) cf[i] = 0.0;
@@ -200,9 +201,9 @@ __global__ void __launch_bounds__(brf::NT, MINB) k_brick3_rf(BrickArgs<double> A
         prefetch_l2(A.geo + (size_t)(slot_base + w) * NG * NQE, NG * NQE * sizeof(double));
     }
     double un[VEC][2];
-    load_in(bz * CZ, un);
+    load_in(bz * cz, un);
     for (int lz = 0; lz < nlayers; ++lz) {
-      const int ez = bz * CZ + lz;
+      const int ez = bz * cz + lz;
       const int offz = br.first[2][ez] - cp0z;
       const long long slot = slot_base + (long long)lz * NE + w;
       if (!STAGE && lane == 0 && lz + 1 < nlayers)

@@ -183,6 +183,13 @@ extern "C" int jxb_plan_create(const jxb_desc* desc, jxb_plan** out) {
     }
     br.te[0] = desc->tile[0];
     br.te[1] = desc->tile[1];
+  } else if (P->dim == 3) {
+    // the most element layers per brick (up to 8) that still give every SM of a
+    // B200 two bricks: the coarse levels of a multigrid hierarchy and other small
+    // patches otherwise leave most SMs idle
+    const long long nbxy = (long long)((P->n_span[0] + br.te[0] - 1) / br.te[0]) *
+                           ((P->n_span[1] + br.te[1] - 1) / br.te[1]);
+    while (br.te[2] > 1 && nbxy * ((P->n_span[2] + br.te[2] - 1) / br.te[2]) < 2 * 148) br.te[2] /= 2;
   } else if (P->dim == 2) {
     // rows of 32 elements, and the most rows per brick (up to 8) that still
     // give every SM of a B200 one brick (shorter bricks cost more per element:

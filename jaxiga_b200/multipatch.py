@@ -304,6 +304,17 @@ class MultiPatchSpace:
     def elem_dofs(self) -> np.ndarray:
         return np.concatenate([self.topology.local_to_global[i][s.elem_dofs] for i, s in enumerate(self.spaces)])
 
+    def element_dofs(self, elems) -> np.ndarray:
+        """Global scalar DOFs of the given (global) elements, (len(elems), (p+1)^dim)."""
+        elems = np.asarray(elems, dtype=np.int64).reshape(-1)
+        patch = np.searchsorted(self.elem_offsets, elems, side="right") - 1
+        out = np.zeros((len(elems), self.n_local), dtype=np.int64)
+        for i, s in enumerate(self.spaces):
+            sel = patch == i
+            if sel.any():
+                out[sel] = self.topology.local_to_global[i][s.element_dofs(elems[sel] - self.elem_offsets[i])]
+        return out
+
     def elem_dofs_vec(self):
         from .space import expand_dofs
 
@@ -464,5 +475,85 @@ class MultiPatchGeometry:
 
         return torch.cat([o.interpolate_grad(self._local(coef, i)) for i, o in enumerate(self.ops)])
 
-    def eval_points(self, *args, **kwargs):
-        raise NotImplementedError("point sets on multipatch spaces: evaluate patch by patch (space.spaces[i])")
+    def eval_points(self, elems, ref, coef=None, val=True, grad=False, x=False, jac=False):
+        """Evaluation at (global element, reference point) pairs, patch by patch,
+        outputs in the order of the pairs."""
+        import torch
+
+        elems = np.asarray(elems, dtype=np.int64).reshape(-1)
+        ref = np.asarray(ref, dtype=float).reshape(len(elems), -1)
+        off = self.space.elem_offsets
+        patch = np.searchsorted(off, elems, side="right") - 1
+        out = {}
+        for i, o in enumerate(self.ops):
+            sel = np.flatnonzero(patch == i)
+            if len(sel) == 0:
+                continue
+            c = None if coef is None else self._local(coef, i)
+            r = o.eval_points(elems[sel] - off[i], ref[sel], c, val=val, grad=grad, x=x, jac=jac)
+            idx = torch.as_tensor(sel, device=o.device)
+            for k, v in r.items():
+                if k not in out:
+                    out[k] = torch.empty((len(elems),) + tuple(v.shape[1:]), dtype=v.dtype, device=v.device)
+                out[k][idx] = v
+        return out
+
+
+def neumann_load_multipatch(op, problem, params, F):
+    """Neumann loads on a multipatch space: each condition's boundary faces split
+    by patch, integrated with the patch's plan (``jxb_boundary_load``), and the
+    patch vectors added into the global one through the numbering on the host,
+    patch after patch (a fixed order)."""
+    import torch
+
+    from .neumann import _call_traction, boundary_points, resolve_set
+    from .pointset import boundary_gauss
+
+    space = problem.space
+    vec = space.vec
+    off = space.elem_offsets
+    total = np.zeros(space.n_dofs)
+    for bc in problem.neumann:
+        bset = resolve_set(space, bc.where)
+        patch = np.searchsorted(off, bset.elems, side="right") - 1
+        for i, (sub, pop) in enumerate(zip(space.spaces, op.patch_ops)):
+            sel = patch == i
+            if not sel.any():
+                continue
+            e = bset.elems[sel] - off[i]
+            local = BoundarySet(e, bset.sides[sel], np.unique(sub.element_dofs(e)))
+            ps = boundary_gauss(sub, local, problem.quadrature)
+            if ps.n_elems == 0:
+                continue
+            x, nrm, w, (de, ref) = boundary_points(pop, ps)
+            t = _call_traction(bc.value, x.cpu().numpy(), nrm.cpu().numpy(), params, vec)
+            Fi = _patch_boundary_load(pop, sub, ps, de, ref, w, t)
+            g = space.topology.local_to_global[i]
+            gd = (g[:, None] * vec + np.arange(vec)[None, :]).reshape(-1)
+            total[gd] += Fi.cpu().numpy()
+    return F + torch.as_tensor(total, device=F.device)
+
+
+def _patch_boundary_load(pop, sub, ps, de, ref, w, t):
+    """The load of given traction values t at a patch's boundary Gauss points."""
+    import torch
+
+    from . import _lib
+    from .neumann import _dptr, _stream
+
+    vec = sub.vec
+    dev = pop.device
+    ed = sub.element_dofs(ps.elems).reshape(-1)
+    order = np.argsort(ed, kind="stable")
+    dofs, starts = np.unique(ed[order], return_index=True)
+    ptr = np.append(starts, len(order)).astype(np.int64)
+    d_dofs = torch.as_tensor(dofs.astype(np.int64), device=dev)
+    d_ptr = torch.as_tensor(ptr, device=dev)
+    d_contrib = torch.as_tensor(order.astype(np.int64), device=dev)
+    tt = torch.as_tensor(np.ascontiguousarray(t), device=dev)
+    local = torch.empty(ps.n_elems * sub.n_local * vec, dtype=torch.float64, device=dev)
+    Fi = torch.zeros(sub.n_dofs, dtype=torch.float64, device=dev)
+    _lib.check(pop.lib.jxb_boundary_load(pop.handle, _stream(), ps.n_elems, ps.n_q, _dptr(de), _dptr(ref), _dptr(w),
+                                         _dptr(tt), len(dofs), _dptr(d_dofs), _dptr(d_ptr), _dptr(d_contrib),
+                                         _dptr(local), _dptr(Fi)))
+    return Fi

@@ -112,6 +112,10 @@ def neumann_load(op, problem, params, F=None):
     space = problem.space
     vec = space.vec
     F = torch.zeros(space.n_dofs, dtype=torch.float64, device=op.device) if F is None else F
+    if hasattr(op, "patch_ops"):  # multipatch: patch by patch through the numbering
+        from .multipatch import neumann_load_multipatch
+
+        return neumann_load_multipatch(op, problem, params, F)
     for bc in problem.neumann:
         bset = resolve_set(space, bc.where)
         ps = boundary_gauss(space, bset, problem.quadrature)

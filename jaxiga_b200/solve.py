@@ -349,8 +349,7 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     if isinstance(space, MultiPatchSpace):
         if linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none") or linear.method != "cg":
             raise NotImplementedError("multipatch spaces solve with FP64 Jacobi-PCG")
-        if problem.neumann:
-            raise NotImplementedError("Neumann loads on multipatch spaces are not supported")
+
     op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)
     from .adjoint import SOLVE_COUNTER

@@ -92,3 +92,30 @@ def test_a_glued_space_reproduces_a_linear_field_across_the_interface():
                                                            where=lambda X: np.ones(len(X), bool))]),
                    params={"a0": 1.0})
     assert jx.errornorm(sol, lambda x: exact(x.T), "L2") < 1e-10
+
+
+def test_neumann_load_on_a_glued_space_matches_the_single_patch():
+    """A traction on the far side of two glued squares equals the traction on
+    the same side of one rectangle covering both, with identical knots (the
+    rectangle's discretization is the two patches' union)."""
+    import torch
+
+    left, right = rect(0, 0, 1, 1).elevate(2).refine(2), rect(1, 0, 2, 1).elevate(2).refine(2)
+    V = jx.FunctionSpace([left, right], vec=2)
+    trac = [jx.Neumann(lambda x, n, p: np.stack([np.full(len(x), 1.5), x[:, 1] ** 2], axis=1), where="right"),
+            jx.Neumann(lambda x, n, p: np.stack([0.5 * x[:, 0], np.full(len(x), -1.0)], axis=1), where="top")]
+    problem = jx.LinearElasticity(V, plane="strain", dirichlet=[jx.DirichletBC([0.0, 0.0], where="left")],
+                                  neumann=trac)
+    sol = jx.solve(problem, params={"E": 10.0, "nu": 0.3}, linear=jx.LinearOptions(tol=1e-13))
+    assert sol.stats["converged"]
+    # one patch over [0, 2] x [0, 1] with the union's knots
+    # 8 elements along x, the interface x = 1 (parameter 0.5) only C0 (multiplicity p = 2) as in the glued space
+    kn = np.concatenate([np.linspace(0, 0.5, 5)[1:-1], [0.5, 0.5], 0.5 + np.linspace(0, 0.5, 5)[1:-1]])
+    one = rect(0, 0, 2, 1).elevate(2).insert_knots(kn, np.linspace(0, 1, 5)[1:-1])
+    W = jx.FunctionSpace(one, vec=2)
+    p1 = jx.LinearElasticity(W, plane="strain", dirichlet=[jx.DirichletBC([0.0, 0.0], where="left")], neumann=trac)
+    s1 = jx.solve(p1, params={"E": 10.0, "nu": 0.3}, linear=jx.LinearOptions(tol=1e-13))
+    # compare at the Gauss points of both (same physical elements, patch order differs): use norms
+    assert abs(jx.norm(sol, "L2") - jx.norm(s1, "L2")) <= 1e-9 * jx.norm(s1, "L2")
+    assert abs(jx.norm(sol, "H1") - jx.norm(s1, "H1")) <= 1e-9 * jx.norm(s1, "H1")
+    del torch
