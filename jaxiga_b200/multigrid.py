@@ -94,6 +94,10 @@ def coarsen(space):
     exact = bool(np.abs(back_grid.reshape(-1, h.shape[1]) - h).max() <= 1e-10 * max(1.0, np.abs(h).max()))
     w = hc[:, -1]
     cp = hc[:, :-1] / w[:, None]
+    if np.all(patch.weights == 1.0):
+        # a polynomial patch stays polynomial: the fit reproduces unit weights only
+        # to rounding, and exact ones keep the coarse plans on the polynomial kernels
+        w = np.ones_like(w)
     coarse = Patch.create(kcs, p, cp, w, labels=patch.labels)
     return FunctionSpace(coarse, vec=space.vec), Ps, exact
 

@@ -59,7 +59,9 @@ class LinearOptions:
     """
 
     method: str = "cg"
-    matrix_free: bool = True
+    # the device path is always matrix-free; the flag keeps the reference's
+    # validation (a direct method cannot be matrix-free)
+    matrix_free: bool = False
     preconditioner: str = "jacobi"
     tol: float = 1e-10
     maxiter: int | None = None
@@ -332,8 +334,15 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     _check_problem(problem, method)
     if linear is None:
         linear = default_linear(problem)
-    if linear.method not in ("cg", "bicgstab"):
-        raise NotImplementedError(f"linear method {linear.method!r}: the B200 backend runs CG and BiCGSTAB")
+    requested = linear.method
+    if linear.method in ("scipy", "dense", "gmres"):
+        # Every supported operator is symmetric positive definite, so the device
+        # CG reaches the same solution: the direct methods ("scipy": SuperLU,
+        # "dense": LU, exact to rounding) run it to 1e-12 or the given tol if
+        # tighter, GMRES to the given tol. stats["linear"] says "cg" and
+        # stats["requested_method"] what was asked.
+        tol = min(linear.tol, 1e-12) if linear.method in ("scipy", "dense") else linear.tol
+        linear = dataclasses.replace(linear, method="cg", matrix_free=True, tol=tol)
     if linear.method == "bicgstab" and (linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none")):
         raise NotImplementedError("BiCGSTAB runs in FP64 with the Jacobi preconditioner (or none)")
     space = problem.space
@@ -398,6 +407,7 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     stats = {
         "method": "galerkin",
         "linear": linear.method,
+        "requested_method": requested,
         "matrix_free": True,
         "n_free": int(n - len(prescribed)),
         "nnz": None,

@@ -36,8 +36,12 @@ def test_bicgstab_matches_oracle(tag):
 
 
 def test_backends_agree():
+    """tests/test_galerkin.py:71-79: every LinearOptions method gives one solution
+    (the direct ones and GMRES run the device CG, the operators being SPD)."""
     V, problem, params = build("poisson2d")
     a = jx.solve(problem, params=params, linear=jx.LinearOptions(method="cg", tol=1e-12))
-    b = jx.solve(problem, params=params, linear=jx.LinearOptions(method="bicgstab", tol=1e-12))
-    assert a.stats["converged"] and b.stats["converged"]
-    assert np.linalg.norm(a.u - b.u) <= 1e-7 * np.linalg.norm(a.u)
+    assert a.stats["converged"]
+    for m in ("bicgstab", "scipy", "dense", "gmres"):
+        b = jx.solve(problem, params=params, linear=jx.LinearOptions(method=m, tol=1e-12))
+        assert b.stats["converged"] and b.stats["requested_method"] == m
+        assert np.linalg.norm(a.u - b.u) <= 1e-7 * np.linalg.norm(a.u)

@@ -278,3 +278,13 @@ def test_elasticity_constitutive_matches_oracle():
         V = jx.FunctionSpace(patch, vec=dim)
         pr = jx.LinearElasticity(V, plane=plane)
         assert np.allclose(pr.C({"E": 2.0, "nu": 0.25}), O.isotropic(2.0, 0.25, dim, plane), rtol=1e-15, atol=0)
+
+
+def test_direct_and_gmres_methods_are_accepted_like_the_reference():
+    """LinearOptions(method="scipy") is the reference's default direct solve;
+    the drop-in accepts it (and "dense", "gmres") and runs the device CG."""
+    for m in ("scipy", "dense", "gmres", "cg", "bicgstab"):
+        o = jx.LinearOptions(method=m)
+        assert o.method == m and not o.matrix_free
+    with pytest.raises(ValueError):
+        jx.LinearOptions(method="dense", matrix_free=True)
