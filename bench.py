@@ -168,13 +168,24 @@ def profile_traffic(workload, span):
 
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's CPU path (SciPy CSR K.u and Jacobi-CG with
-# true-residual restarts) on the elasticity workload at a feasible size
+# true-residual restarts) on the host cores. K.u is timed on a bounded sample
+# of the 64^3 elasticity operator itself (whole rows of its assembled matrix);
+# the solves run at the sizes whose full assembly a CPU can hold.
 # ---------------------------------------------------------------------------
 INFEASIBLE = ("64^3 elements assembled on a CPU is infeasible: 262,144 element matrices of 192 x 192 "
               "(77 GB), a 38.7 GB int32 scatter map and ~1 h of CSR-pattern construction")
+CPU_ROW_BOX = (64, 32, 4)  # elements per direction of the element box whose rows K.u is timed on
+CPU_FLUSH_BYTES = 512 << 20  # read between timed CPU steps so the sample starts outside the caches
 
 
-def host_info():
+def cpu_threads():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return max(1, os.cpu_count() or 1)
+
+
+def host_info(threads):
     model = None
     try:
         with open("/proc/cpuinfo") as f:
@@ -184,13 +195,138 @@ def host_info():
                     break
     except OSError:
         pass
-    return {"cpu_count": os.cpu_count(), "cpu_model": model,
+    return {"cpu_count": os.cpu_count(), "cpu_model": model, "threads_used": threads,
             "threads_env": {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
                                                            "MKL_NUM_THREADS")},
-            "note": "SciPy's CSR matvec and CG run on one thread (the reference's CPU CG calls them)"}
+            "note": "SciPy's CSR matvec runs on row blocks in a thread pool (it releases the GIL); "
+                    "the CG's vector updates and BLAS dots run on one thread"}
 
 
-def cpu_sample(span=CPU_SAMPLE_SPAN):
+class ThreadedCSR:
+    """A SciPy CSR matrix whose K.u runs as row blocks of about equal nonzero
+    count on a thread pool. It offers what the reference's CPU CG uses of its
+    operator (shape, dtype, diagonal(), the product), so the SciPy solver runs
+    on it unchanged."""
+
+    def __init__(self, K, threads):
+        import scipy.sparse.linalg as spla
+        from concurrent.futures import ThreadPoolExecutor
+
+        self.K = K
+        self.shape, self.dtype = K.shape, K.dtype
+        self.threads = threads
+        cuts = np.searchsorted(K.indptr, np.linspace(0, K.nnz, threads + 1)).clip(0, K.shape[0])
+        cuts[0], cuts[-1] = 0, K.shape[0]
+        self.blocks = [(int(a), int(b), K[int(a):int(b)]) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+        self.pool = ThreadPoolExecutor(threads)
+        self.op = spla.LinearOperator(K.shape, matvec=self.matvec, dtype=K.dtype)
+        self.op.diagonal = K.diagonal
+
+    def matvec(self, x):
+        x = np.asarray(x).ravel()
+        y = np.empty(self.shape[0])
+
+        def run(blk):
+            a, b, B = blk
+            y[a:b] = B @ x
+
+        list(self.pool.map(run, self.blocks))
+        return y
+
+    def __matmul__(self, x):
+        return self.matvec(x)
+
+    def flush(self, buf):
+        """Read ``buf`` across the pool (evicts the sample from the caches)."""
+        parts = np.array_split(buf, self.threads)
+        list(self.pool.map(np.sum, parts))
+
+    def close(self):
+        self.pool.shutdown()
+
+
+def cpu_row_sample(span=N_SPAN, box=CPU_ROW_BOX):
+    """Whole rows of the elasticity workload's free-free operator K_ff at
+    ``span``^3 elements, for the free DOFs of every control point whose support
+    lies inside an element box of ``box`` elements (the full width in x, centred
+    in y and z). Only the box's element tangents are formed (oracle restatement of
+    src/jaxiga/forms/library.py:174-181) and scattered into those rows
+    (src/jaxiga/methods/galerkin.py:122-148), so each row is exactly the full
+    operator's row; columns index the free DOFs.
+
+    Returns (space, CSR rows (n_rows x n_free), row DOFs, set-up seconds)."""
+    import scipy.sparse as sps
+
+    from jaxiga_b200 import workloads
+    from oracle import iga_oracle as O
+
+    t0 = time.perf_counter()
+    V, problem, params = workloads.config2(n=span)
+    pres, _ = problem.resolve_dirichlet(params)
+    S = O.Space(V.knots, V.degree, V.cpts, V.wgts, 3)
+    n_dofs, ncp = S.n_dofs, S.n_cp
+    free_index = np.full(n_dofs, -1, dtype=np.int64)
+    free = np.setdiff1d(np.arange(n_dofs), pres)
+    free_index[free] = np.arange(len(free))
+    lo = [(S.n_span[d] - box[d]) // 2 for d in range(3)]
+    hi = [lo[d] + box[d] for d in range(3)]
+    inside = np.all([(S.elem_idx[d] >= lo[d]) & (S.elem_idx[d] < hi[d]) for d in range(3)], axis=0)
+    elems = np.nonzero(inside)[0]
+    # control points whose support (elements first..first+p per direction) is inside the box
+    cp_ok = []
+    for d in range(3):
+        first = S.spans[d][2]
+        ok = np.zeros(ncp[d], bool)
+        for i in range(ncp[d]):
+            sup = np.nonzero((first <= i) & (first + S.degree[d] >= i))[0]
+            ok[i] = len(sup) > 0 and sup.min() >= lo[d] and sup.max() < hi[d]
+        cp_ok.append(ok)
+    idx = np.arange(S.n_scalar)
+    ijk = (idx % ncp[0], (idx // ncp[0]) % ncp[1], idx // (ncp[0] * ncp[1]))
+    cp_sel = cp_ok[0][ijk[0]] & cp_ok[1][ijk[1]] & cp_ok[2][ijk[2]]
+    row_dofs = np.nonzero(np.repeat(cp_sel, 3) & (free_index >= 0))[0]
+    row_index = np.full(n_dofs, -1, dtype=np.int64)
+    row_index[row_dofs] = np.arange(len(row_dofs))
+    gd_all = S.expand(S.elem_dofs)
+    K = None
+    for c0 in range(0, len(elems), 2048):
+        el = elems[c0:c0 + 2048]
+        Ke = O.element_tangents("elasticity", O.evaluate(S, el), {"E": 1.0, "nu": 0.3}, 3)
+        gd = gd_all[el]
+        e_i, r_i = np.nonzero(row_index[gd] >= 0)
+        cols = free_index[gd[e_i]]
+        vals = Ke[e_i, r_i]
+        keep = cols >= 0
+        rows = np.broadcast_to(row_index[gd[e_i, r_i]][:, None], cols.shape)
+        part = sps.csr_matrix((vals[keep], (rows[keep], cols[keep])), shape=(len(row_dofs), len(free)))
+        K = part if K is None else K + part
+    K.sum_duplicates()
+    K.sort_indices()
+    return V, K, row_dofs, time.perf_counter() - t0
+
+
+def time_cpu_rows(K, threads, steps, warmup=1):
+    """Seconds of each of ``steps`` threaded K.u products of the row sample, the
+    caches flushed (a 512 MB read) before each; the flush is outside the timing."""
+    from threadpoolctl import threadpool_limits
+
+    op = ThreadedCSR(K, threads)
+    x = np.random.default_rng(0).standard_normal(K.shape[1])
+    buf = np.ones(CPU_FLUSH_BYTES // 8)
+    times = []
+    with threadpool_limits(1):  # idle BLAS threads would spin against the pool's
+        for _ in range(max(warmup, 1)):
+            op @ x
+        for _ in range(steps):
+            op.flush(buf)
+            t0 = time.perf_counter()
+            op @ x
+            times.append(time.perf_counter() - t0)
+    op.close()
+    return np.asarray(times)
+
+
+def cpu_sample(span):
     """The elasticity workload at ``span``^3 assembled by the oracle, with its
     load vector (body force plus the interpolated random field)."""
     from jaxiga_b200 import workloads
@@ -205,76 +341,84 @@ def cpu_sample(span=CPU_SAMPLE_SPAN):
     return V, A, time.perf_counter() - t0
 
 
-def time_cpu_matvec(A, n_dofs, seconds=5.0, min_reps=3):
-    x = np.random.default_rng(0).standard_normal(A.K.shape[0])
-    A.K @ x
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        A.K @ x
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds and reps >= min_reps:
-            break
-    return n_dofs * reps / el, reps, el
-
-
-def cpu_time_to_solution(A, runs=3):
+def cpu_time_to_solution(A, threads, runs=3):
     """Warm median of ``runs`` SciPy Jacobi-CG solves to TOL (the reference's
-    restart logic), with the true relative residual of the last."""
+    restart logic, src/jaxiga/solvers/linear.py:261-321, restated in the oracle)
+    on the threaded operator, with the true relative residual of the last."""
+    from threadpoolctl import threadpool_limits
+
     from oracle import iga_oracle as O
 
+    op = ThreadedCSR(A.K, threads)
     times = []
-    for _ in range(runs):
-        t0 = time.perf_counter()
-        u, it = O.scipy_cg(A.K, A.b, TOL)
-        times.append(time.perf_counter() - t0)
+    with threadpool_limits(1):  # the CG's BLAS dots stay on one thread, so its threads do not spin
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            u, it = O.scipy_cg(op.op, A.b, TOL)
+            times.append(time.perf_counter() - t0)
     rel = float(np.linalg.norm(A.b - A.K @ u) / np.linalg.norm(A.b))
+    op.close()
     return {"seconds": float(np.median(times)), "runs": runs, "iterations": int(it), "relative_residual": rel,
-            "converged": rel <= TOL}
+            "converged": rel <= TOL, "threads": threads}
 
 
-def cpu_baseline():
-    V, A, setup = cpu_sample()
-    v, reps, el = time_cpu_matvec(A, V.n_dofs)
-    tts = cpu_time_to_solution(A)
-    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"3D elasticity workload at {CPU_SAMPLE_SPAN}^3 elements ({V.n_dofs} DOFs, nnz {A.K.nnz}); "
-                      f"SciPy CSR K.u of the oracle-assembled operator, {reps} reps in {el:.1f} s, one thread; "
-                      f"assembly ({setup:.1f} s) excluded; {INFEASIBLE}",
-            "span": CPU_SAMPLE_SPAN, "n_dofs": V.n_dofs, "assembly_seconds": setup,
-            "time_to_solution": tts, "host": host_info()}
+def cpu_solves(threads, spans=(CPU_SAMPLE_SPAN,), runs=3):
+    out = {}
+    for s in spans:
+        V, A, setup = cpu_sample(s)
+        out[f"elasticity3d_p3_{s}^3"] = dict(cpu_time_to_solution(A, threads, runs=runs if s == spans[0] else 1),
+                                            span=s, n_dofs=V.n_dofs, nnz=int(A.K.nnz), assembly_seconds=setup)
+        del A
+    return out
+
+
+def cpu_kv_record(steps, warmup):
+    """The K.u row sample of the 64^3 workload timed on the host's threads."""
+    threads = cpu_threads()
+    V, K, rows, setup = cpu_row_sample()
+    t = time_cpu_rows(K, threads, steps, warmup)
+    value = len(rows) / float(np.mean(t))
+    sample = (f"{len(rows)} whole rows ({K.nnz} nonzeros, {K.data.nbytes + K.indices.nbytes >> 20} MB) of the "
+              f"64^3 elasticity operator K_ff, assembled by the oracle from the element tangents of a "
+              f"{CPU_ROW_BOX[0]} x {CPU_ROW_BOX[1]} x {CPU_ROW_BOX[2]} element box (set-up {setup:.1f} s, "
+              f"excluded); one step = one SciPy CSR product of those rows on {threads} threads, caches "
+              f"flushed before each; DOF/s = rows per second; {INFEASIBLE}")
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+            "rows": len(rows), "nnz": int(K.nnz), "setup_seconds": setup, "steps": len(t),
+            "ms_per_step": float(np.mean(t)) * 1e3, "host": host_info(threads)}
+
+
+def cpu_baseline(steps=20):
+    rec = cpu_kv_record(steps, 1)
+    rec["time_to_solution"] = cpu_solves(rec["cores"])
+    return rec
+
+
+def headline_config(name, span, V, n_qp, ngeo, world):
+    return {"workload": workload_tag(name, span), "n_dofs": V.n_dofs, "elements": V.n_elems,
+            "gauss_points": n_qp,
+            "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    V, A, setup = cpu_sample()
-    x = np.random.default_rng(0).standard_normal(A.K.shape[0])
-    for _ in range(args.warmup):
-        A.K @ x
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        A.K @ x
-    el = time.perf_counter() - t0
-    value = V.n_dofs * args.steps / el
-    tts = cpu_time_to_solution(A)
-    # the larger matched size: one solve (assembly about a minute on one core)
-    V24, A24, setup24 = cpu_sample(CPU_SAMPLE_SPAN_LARGE)
-    tts24 = dict(cpu_time_to_solution(A24, runs=1), span=CPU_SAMPLE_SPAN_LARGE, n_dofs=V24.n_dofs,
-                 nnz=int(A24.K.nnz), assembly_seconds=setup24)
-    del A24
+    from jaxiga_b200 import workloads
+
+    rec = cpu_kv_record(args.steps, args.warmup)
+    value = rec["value"]
+    V, _, _ = workloads.config2(n=N_SPAN)
+    solves = cpu_solves(rec["cores"], spans=(CPU_SAMPLE_SPAN, CPU_SAMPLE_SPAN_LARGE))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"elasticity3d_p3_{CPU_SAMPLE_SPAN}^3 (bounded CPU sample of the 64^3 workload)",
-                   "n_dofs": V.n_dofs, "nnz": int(A.K.nnz), "operator": "assembled CSR (SciPy)",
-                   "full_size": INFEASIBLE, "assembly_seconds": setup},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"SciPy CSR K.u, {CPU_SAMPLE_SPAN}^3-element elasticity workload, one thread",
-                         "host": host_info()},
-        "time_to_solution": {"tol": TOL, "scipy_jacobi_cg_true_residual_restarts": tts,
-                             "scipy_jacobi_cg_true_residual_restarts_24": tts24},
+        "config": headline_config("elasticity", N_SPAN, V, V.n_elems * 64, 10, world),
+        "operator": "assembled CSR rows (SciPy), the reference's CPU path",
+        "cpu_baseline": rec,
+        "time_to_solution": {"tol": TOL, "scipy_jacobi_cg_true_residual_restarts": solves,
+                             "full_size": INFEASIBLE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -611,7 +755,7 @@ def run_ours(args, rank, world, local_rank):
         cpu["gpu_same_size"] = matched_gpu_solve(dev)
         cpu["gpu_same_size_24"] = matched_gpu_solve(dev, CPU_SAMPLE_SPAN_LARGE)
         g = cpu["gpu_same_size"]["plain_fp64_jacobi_pcg"]
-        c = cpu["time_to_solution"]
+        c = cpu["time_to_solution"][f"elasticity3d_p3_{CPU_SAMPLE_SPAN}^3"]
         cpu["time_to_solution_ratio_cpu_over_gpu"] = (c["seconds"] / g["seconds"]
                                                       if g["converged"] and c["converged"] else None)
 
@@ -620,10 +764,9 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_tag(name, span), "n_dofs": n, "elements": V.n_elems,
-                       "gauss_points": n_qp, "operator": "matrix-free sum-factorised K.u, FP64, masked",
-                       "l2": "inputs larger than L2 (per-point factors %.2f GB per step)" % (8 * n_qp * ngeo / 1e9),
-                       "parallelism": f"replicas x{world}", "setup_seconds": setup_s},
+            "config": headline_config(name, span, V, n_qp, ngeo, world),
+            "operator": "matrix-free sum-factorised K.u, FP64, masked",
+            "setup_seconds": setup_s,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                     "steps": k_e2e},
             "gpu_launches": 2 * args.steps,
