@@ -689,44 +689,33 @@ __device__ __forceinline__ double block_sum(double v) {
   return s;  // valid in thread 0
 }
 
-template <typename T>
+// One thread per control point, every component; the grid-stride mapping of
+// control points to threads is the same in both launch shapes. With `partials`
+// the grid is the fixed JXB_RED_BLOCKS of the deterministic reductions (the
+// per-block p.y partials); without, it covers every control point once.
+template <typename T, int VEC, int DIM>
 __global__ void __launch_bounds__(JXB_RED_THREADS)
     k_combine(Bricks br, const T* __restrict__ scratch, const uint8_t* __restrict__ keep, int masked,
               T* __restrict__ y, const T* __restrict__ dot_with, double* __restrict__ partials,
               const CgState* state) {
   if (state && state->done) return;
-  const int vec = br.vec, dim = br.dim;
-  const long long n_scalar = (long long)br.n_cp[0] * br.n_cp[1] * (dim == 3 ? br.n_cp[2] : 1);
+  const long long n_scalar = (long long)br.n_cp[0] * br.n_cp[1] * (DIM == 3 ? br.n_cp[2] : 1);
   double part = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_scalar;
        i += (long long)gridDim.x * blockDim.x) {
-    int ix = (int)(i % br.n_cp[0]);
-    int iy = (int)((i / br.n_cp[0]) % br.n_cp[1]);
-    int iz = dim == 3 ? (int)(i / ((long long)br.n_cp[0] * br.n_cp[1])) : 0;
-    const int* cx = br.cover[0] + 2 * JXB_MAXC * ix;
-    const int* cy = br.cover[1] + 2 * JXB_MAXC * iy;
-    const int* cz = dim == 3 ? br.cover[2] + 2 * JXB_MAXC * iz : nullptr;
-    for (int c = 0; c < vec; ++c) {
-      T s = 0;
-      for (int kz = 0; kz < (dim == 3 ? JXB_MAXC : 1); ++kz) {
-        int bz = dim == 3 ? cz[2 * kz] : 0, oz = dim == 3 ? cz[2 * kz + 1] : 0;
-        if (bz < 0) break;
-        for (int ky = 0; ky < JXB_MAXC; ++ky) {
-          int by = cy[2 * ky], oy = cy[2 * ky + 1];
-          if (by < 0) break;
-          for (int kx = 0; kx < JXB_MAXC; ++kx) {
-            int bx = cx[2 * kx], ox = cx[2 * kx + 1];
-            if (bx < 0) break;
-            long long brick = bx + (long long)br.nb[0] * (by + (long long)br.nb[1] * bz);
-            long long off = ((brick * vec + c) * (dim == 3 ? br.fp[2] : 1) + oz) * br.fp[1];
-            s += scratch[(off + oy) * br.fp[0] + ox];
-          }
-        }
-      }
-      long long dof = i * vec + c;
-      if (masked && !keep[dof]) s = T(0);
-      y[dof] = s;
-      if (dot_with) part += (double)dot_with[dof] * (double)s;
+    // n_scalar < 2^31 (checked by the launcher): 32-bit index arithmetic
+    const unsigned ii = (unsigned)i, n0 = (unsigned)br.n_cp[0], n1 = (unsigned)br.n_cp[1];
+    const unsigned ix = ii % n0, iyz = ii / n0;
+    const unsigned iy = iyz % n1, iz = DIM == 3 ? iyz / n1 : 0;
+    T s[VEC];
+    combine_point<T, VEC, DIM>(br, scratch, (int)ix, (int)iy, (int)iz, s);
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      const long long dof = i * VEC + c;
+      T v = s[c];
+      if (masked && !keep[dof]) v = T(0);
+      y[dof] = v;
+      if (dot_with) part += (double)dot_with[dof] * (double)v;
     }
   }
   if (partials) {
@@ -945,8 +934,27 @@ int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* do
     scratch = plan->d_scratch32;
   else
     scratch = plan->d_scratch;
-  k_combine<T><<<JXB_RED_BLOCKS, JXB_RED_THREADS, 0, s>>>(plan->br, scratch, plan->d_keep, masked, y,
-                                                           dot_with, partials, state);
+  if (plan->n_scalar >= (1LL << 31)) return fail(JXB_ERR_INVALID, "combine: more than 2^31 control points");
+  unsigned grid = JXB_RED_BLOCKS;
+  if (!partials) {
+    const long long g = (plan->n_scalar + JXB_RED_THREADS - 1) / JXB_RED_THREADS;
+    grid = (unsigned)std::max(1LL, std::min(g, 148LL * 64));
+  }
+  const Bricks& br = plan->br;
+#define JXB_COMBINE(V, D)                                                                                     \
+  k_combine<T, V, D><<<grid, JXB_RED_THREADS, 0, s>>>(br, scratch, plan->d_keep, masked, y, dot_with, partials, \
+                                                      state)
+  if (br.dim == 3 && br.vec == 1)
+    JXB_COMBINE(1, 3);
+  else if (br.dim == 3 && br.vec == 3)
+    JXB_COMBINE(3, 3);
+  else if (br.dim == 2 && br.vec == 1)
+    JXB_COMBINE(1, 2);
+  else if (br.dim == 2 && br.vec == 2)
+    JXB_COMBINE(2, 2);
+  else
+    return fail(JXB_ERR_INVALID, "combine: unsupported (dimension, components)");
+#undef JXB_COMBINE
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }

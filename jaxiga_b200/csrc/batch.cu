@@ -82,11 +82,16 @@ __device__ double block_sum_b(double v) {
   return r;
 }
 
-// y = combine of instance blockIdx.x (2D), optional p.y into dot_out[inst]
-__global__ void __launch_bounds__(256) k_combine_batch(const Bricks* __restrict__ brs, double* const* __restrict__ scratch,
-                                                       const long long* __restrict__ off, const uint8_t* __restrict__ keep,
-                                                       double* __restrict__ y, const double* __restrict__ dot_with,
-                                                       double* __restrict__ dot_out, const CgState* __restrict__ states) {
+// y = combine of instance blockIdx.x (2D), optional p.y into dot_out[inst]. The
+// CTA is large (one CTA serves a whole instance, up to ~17k control points)
+// and issues the loads of all covering bricks of a control point together.
+constexpr int BATCH_COMBINE_THREADS = 512;
+
+__global__ void __launch_bounds__(BATCH_COMBINE_THREADS)
+    k_combine_batch(const Bricks* __restrict__ brs, double* const* __restrict__ scratch,
+                    const long long* __restrict__ off, const uint8_t* __restrict__ keep, double* __restrict__ y,
+                    const double* __restrict__ dot_with, double* __restrict__ dot_out,
+                    const CgState* __restrict__ states) {
   const int inst = blockIdx.x;
   if (states && states[inst].done) return;
   const Bricks& br = brs[inst];
@@ -96,19 +101,9 @@ __global__ void __launch_bounds__(256) k_combine_batch(const Bricks* __restrict_
   double part = 0;
   for (long long i = threadIdx.x; i < n_scalar; i += blockDim.x) {
     const int ix = (int)(i % br.n_cp[0]), iy = (int)(i / br.n_cp[0]);
-    const int* cx = br.cover[0] + 2 * JXB_MAXC * ix;
-    const int* cy = br.cover[1] + 2 * JXB_MAXC * iy;
-    double s = 0;
-    for (int ky = 0; ky < JXB_MAXC; ++ky) {
-      const int by = cy[2 * ky], oy = cy[2 * ky + 1];
-      if (by < 0) break;
-      for (int kx = 0; kx < JXB_MAXC; ++kx) {
-        const int bx = cx[2 * kx], ox = cx[2 * kx + 1];
-        if (bx < 0) break;
-        const long long brick = bx + (long long)br.nb[0] * by;
-        s += sc[(brick * br.fp[1] + oy) * br.fp[0] + ox];
-      }
-    }
+    double sv[1];
+    combine_point<double, 1, 2>(br, sc, ix, iy, 0, sv);
+    double s = sv[0];
     const long long dof = o + i;
     if (!keep[dof]) s = 0;
     y[dof] = s;
@@ -251,7 +246,7 @@ int batch_apply(jxb_batch* B, cudaStream_t s, const BrickArgs<double>* d_args, d
     int rc = launch_bricks2_batch(g.p, B->rational, g.variant, d_args, g.d_work, g.n_work, g.fp0, g.fp1, states, s);
     if (rc) return rc;
   }
-  k_combine_batch<<<B->n, 256, 0, s>>>(B->d_brs, B->d_scratch, B->d_off, B->d_keep, y, dot_with, dot_out, states);
+  k_combine_batch<<<B->n, BATCH_COMBINE_THREADS, 0, s>>>(B->d_brs, B->d_scratch, B->d_off, B->d_keep, y, dot_with, dot_out, states);
   JXB_CUDA(cudaGetLastError());
   return JXB_OK;
 }

@@ -44,6 +44,23 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   const int el = tid / Q, t = tid % Q;
   const int ex = bx * TX + el;
   const bool evalid = (!WIDE || el < TX) && ex < br.n_span[0];
+  const long long slot_base = b * (long long)TY * NE;
+  const int nlayers = min(TY, br.n_span[1] - by * TY);
+
+  // The factors of one row of the brick are one contiguous tile (TX elements x
+  // NG x NQE values; TX is a multiple of 16, so the tile is 16-byte aligned and
+  // sized). The bulk-copy engine brings the first two rows into L2 before the
+  // tables are staged, and every later row two rows ahead, so the point
+  // operator's loads hit L2.
+  constexpr bool GEO = MODE != MODE_LOAD;
+  constexpr unsigned ROW_BYTES = (unsigned)(NE * NG * NQE * sizeof(T));
+  static_assert(ROW_BYTES % 16 == 0, "row tile of whole 16-byte units");
+  if constexpr (GEO) {
+    if (tid == 0) {
+      prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, ROW_BYTES);
+      if (nlayers > 1) prefetch_l2(A.geo + (size_t)(slot_base + NE) * NG * NQE, ROW_BYTES);
+    }
+  }
 
   for (int i = tid; i < TX * 3 * Q * P1; i += NTH) {
     int e = i / (3 * Q * P1), r = i % (3 * Q * P1);
@@ -56,11 +73,13 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   }
   const int accn = VEC * fp0 * fp1;
   for (int i = tid; i < accn; i += NTH) acc[i] = T(0);
-  const long long slot_base = b * (long long)TY * NE;
-  const int nlayers = min(TY, br.n_span[1] - by * TY);
   const T* nx_v = stx + el * 3 * Q * P1;
 
   for (int ly_ = 0; ly_ < nlayers; ++ly_) {
+    if constexpr (GEO) {
+      if (tid == 0 && ly_ + 2 < nlayers)
+        prefetch_l2(A.geo + (size_t)(slot_base + (long long)(ly_ + 2) * NE) * NG * NQE, ROW_BYTES);
+    }
     const int ey = by * TY + ly_;
     const int fy = br.first[1][ey];
     const int offy = fy - cp0y;

@@ -155,6 +155,114 @@ constexpr int TILE2_MAX_ROWS = 64;
 // Row width of every instance of a batch that the persistent batched kernel runs.
 constexpr int PERSIST2_TX = 32;
 
+// ---------------------------------------------------------------------------
+// The combine's sum at one control point: y_i = the sum, over the bricks whose
+// footprint holds control point i, of their footprint values -- bricks taken
+// in the fixed order (z, then y, then x, each in cover-list order), so the
+// result is bitwise reproducible.
+//
+// The cover table lists per direction and control point up to JXB_MAXC
+// (brick, offset) pairs, -1 after the last. Every 3D brick shape and every 2D
+// brick of at least p rows puts a control point in at most 2 bricks per
+// direction; those points read their 2 x 2 (x 2) bricks with all loads issued
+// together, for every component at once. Longer lists (short 2D bricks of high
+// degree) take the loop over the tables.
+// ---------------------------------------------------------------------------
+struct Cover2 {
+  int b[2], o[2];
+  int n;
+  bool longer;
+};
+
+__device__ __forceinline__ void cover2(const int* __restrict__ c, Cover2& C) {
+  C.b[0] = c[0];
+  C.o[0] = c[1];
+  C.b[1] = c[2];
+  C.o[1] = c[3];
+  C.n = (C.b[0] >= 0) + (C.b[1] >= 0);
+  C.longer = c[4] >= 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T cover_sum_long(const Bricks& br, const T* __restrict__ sc, int ix, int iy, int iz) {
+  const int dim = br.dim;
+  const long long fpz = dim == 3 ? br.fp[2] : 1;
+  const int* cx = br.cover[0] + 2 * JXB_MAXC * ix;
+  const int* cy = br.cover[1] + 2 * JXB_MAXC * iy;
+  const int* cz = dim == 3 ? br.cover[2] + 2 * JXB_MAXC * iz : nullptr;
+  T s = 0;
+  for (int kz = 0; kz < (dim == 3 ? JXB_MAXC : 1); ++kz) {
+    const int bz = dim == 3 ? cz[2 * kz] : 0, oz = dim == 3 ? cz[2 * kz + 1] : 0;
+    if (bz < 0) break;
+    for (int ky = 0; ky < JXB_MAXC; ++ky) {
+      const int by = cy[2 * ky], oy = cy[2 * ky + 1];
+      if (by < 0) break;
+      for (int kx = 0; kx < JXB_MAXC; ++kx) {
+        const int bx = cx[2 * kx], ox = cx[2 * kx + 1];
+        if (bx < 0) break;
+        const long long brick = bx + (long long)br.nb[0] * (by + (long long)br.nb[1] * bz);
+        s += sc[((brick * br.vec * fpz + oz) * br.fp[1] + oy) * br.fp[0] + ox];
+      }
+    }
+  }
+  return s;
+}
+
+// s[c] = the combine's sum for component c of control point (ix, iy, iz).
+// VEC = br.vec and DIM = br.dim.
+template <typename T, int VEC, int DIM>
+__device__ __forceinline__ void combine_point(const Bricks& br, const T* __restrict__ scratch, int ix, int iy, int iz,
+                                              T (&s)[VEC]) {
+  const long long layer = (long long)br.fp[0] * br.fp[1];
+  const long long comp = (DIM == 3 ? br.fp[2] : 1) * layer;  // one component of one brick's footprint
+  const long long S = VEC * comp;                            // one brick's footprint
+  Cover2 cx, cy, cz;
+  cover2(br.cover[0] + 2 * JXB_MAXC * ix, cx);
+  cover2(br.cover[1] + 2 * JXB_MAXC * iy, cy);
+  if constexpr (DIM == 3) {
+    cover2(br.cover[2] + 2 * JXB_MAXC * iz, cz);
+  } else {
+    cz.b[0] = 0, cz.o[0] = 0, cz.b[1] = -1, cz.o[1] = 0, cz.n = 1, cz.longer = false;
+  }
+  if (cx.longer || cy.longer || cz.longer) {
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) s[c] = cover_sum_long<T>(br, scratch + c * comp, ix, iy, iz);
+    return;
+  }
+  constexpr int KZ = DIM == 3 ? 2 : 1;
+  long long X[2], Y[2], Z[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    X[k] = cx.b[k] * S + cx.o[k];
+    Y[k] = (long long)cy.b[k] * br.nb[0] * S + (long long)cy.o[k] * br.fp[0];
+    Z[k] = (long long)cz.b[k] * br.nb[0] * br.nb[1] * S + cz.o[k] * layer;
+  }
+  T v[VEC][KZ * 4];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c)
+#pragma unroll
+    for (int kz = 0; kz < KZ; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 2; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 2; ++kx) {
+          const bool ok = kz < cz.n && ky < cy.n && kx < cx.n;
+          v[c][(kz * 2 + ky) * 2 + kx] = ok ? __ldg(scratch + c * comp + Z[kz] + Y[ky] + X[kx]) : T(0);
+        }
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    T a = 0;
+#pragma unroll
+    for (int kz = 0; kz < KZ; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 2; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 2; ++kx)
+          if (kz < cz.n && ky < cy.n && kx < cx.n) a += v[c][(kz * 2 + ky) * 2 + kx];
+    s[c] = a;
+  }
+}
+
 }  // namespace jxb
 
 struct jxb_krylov_ws;  // BiCGSTAB workspace (krylov.cu)
