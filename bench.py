@@ -58,6 +58,12 @@ N_SPAN = 64
 CPU_SAMPLE_SPAN = 16
 CPU_SAMPLE_SPAN_LARGE = 24  # the reference arm also times the CPU solve here (about 80 s of assembly and CG)
 TOL = 1e-8
+# Chebyshev smoother (degree, range) of the multigrid rows, per workload: the
+# fastest of degrees {2, 3, 4} x ranges {10, 20, 40} in a sweep of
+# `python -m jaxiga_b200.multigrid` on a B200 (elasticity 64^3: 0.221 s at
+# (3, 40) against 0.238 s at the library default (3, 20); Darcy 96^3: 0.085 s
+# at (2, 20) against 0.092 s)
+MG_SMOOTHER = {"elasticity": (3, 40.0), "darcy": (2, 20.0), "plate": (3, 20.0)}
 
 
 def parse():
@@ -565,13 +571,14 @@ def time_to_solution(name, span, op, F, feats, problem_params=None):
     if problem_params is not None:
         from jaxiga_b200.multigrid import Multigrid
 
+        deg, rng = MG_SMOOTHER.get(name, (3, 20.0))
         t0 = time.perf_counter()
-        mg = Multigrid(*problem_params, degree=3, smooth_range=20.0, fine_op=op)
+        mg = Multigrid(*problem_params, degree=deg, smooth_range=rng, fine_op=op)
         mg_setup = time.perf_counter() - t0
         for _ in range(2):
             x_g, st_g = mg.solve(F, tol=TOL, maxiter=20000)
         rows["multigrid_fp64_pcg"] = dict(_row(st_g, x_p, x_g), levels=mg.levels, setup_seconds=mg_setup,
-                                          smoother="Chebyshev-Jacobi, degree 3, range 20, before and after")
+                                          smoother=f"Chebyshev-Jacobi, degree {deg}, range {rng:g}, before and after")
         mg.close()
     tts.update(rows)
     tts["learned_preconditioner"] = None
@@ -666,6 +673,60 @@ def matched_gpu_solve(dev, span=CPU_SAMPLE_SPAN):
             "mixed_fp32_pcg_reliable_fp64_updates": _row(st_r)}
 
 
+def time_e2e(op, x, n, steps, stream, barrier, world, dev):
+    """DOF/s of K.u with host input and output (see run_ours), max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    xh = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    yh = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    for h in xh:
+        h.copy_(x.cpu())
+    xd = [torch.empty_like(x) for _ in range(2)]
+    yd = [torch.empty_like(x) for _ in range(2)]
+    s_in, s_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    ev_in = [torch.cuda.Event() for _ in range(2)]     # input j on the device
+    ev_used = [torch.cuda.Event() for _ in range(2)]   # apply j has read xd[j] and written yd[j]
+    ev_out = [torch.cuda.Event() for _ in range(2)]    # result j back on the host
+    k_e2e = max(10, steps // 5)
+
+    def step(k):
+        j = k % 2
+        with torch.cuda.stream(s_in):
+            if k >= 2:
+                s_in.wait_event(ev_used[j])
+            xd[j].copy_(xh[j], non_blocking=True)
+            ev_in[j].record(s_in)
+        stream.wait_event(ev_in[j])
+        if k >= 2:
+            stream.wait_event(ev_out[j])
+        op.apply(xd[j], out=yd[j])
+        ev_used[j].record(stream)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(ev_used[j])
+            yh[j].copy_(yd[j], non_blocking=True)
+            ev_out[j].record(s_out)
+
+    for k in range(4):
+        step(k)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s_in.wait_event(e0)
+    for k in range(k_e2e):
+        step(k)
+    stream.wait_event(ev_out[(k_e2e - 1) % 2])
+    stream.wait_event(ev_out[k_e2e % 2])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return world * n * k_e2e / (float(t.item()) * 1e-3), k_e2e
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -710,35 +771,17 @@ def run_ours(args, rank, world, local_rank):
     peaks, peak_kind = measured_peaks()
     roofline = roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span)
 
-    # e2e through the C ABI with host buffers
-    xh = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    xh.copy_(x.cpu())
-    yh = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    xd = torch.empty_like(x)
-    k_e2e = max(10, args.steps // 5)
-    for _ in range(3):
-        xd.copy_(xh, non_blocking=True)
-        op.apply(xd, out=y)
-        yh.copy_(y, non_blocking=True)
-    torch.cuda.synchronize()
-    barrier()
-    e0.record(stream)
-    for _ in range(k_e2e):
-        xd.copy_(xh, non_blocking=True)
-        op.apply(xd, out=y)
-        yh.copy_(y, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * k_e2e / (float(t.item()) * 1e-3)
-
+    # e2e through the C ABI with host buffers: every step copies its input from
+    # pinned host memory to the device, applies K and copies the result back to
+    # pinned host memory. The copies run on their own streams, two buffers each
+    # way, so step k's input copy and step k-1's result copy overlap step k-1's
+    # and step k's applies (stream order keeps every buffer's copy, apply and
+    # read-back in sequence).
+    e2e_value, k_e2e = time_e2e(op, x, n, args.steps, stream, barrier, world, dev)
     tts = None if args.no_solve else time_to_solution(name, span, op, F, feats, pp)
     ngeo = op.info["ngeo"]
     op.close()
-    del F, x, y, xd
+    del F, x, y
     torch.cuda.empty_cache()
 
     extra = None
@@ -768,7 +811,8 @@ def run_ours(args, rank, world, local_rank):
             "operator": "matrix-free sum-factorised K.u, FP64, masked",
             "setup_seconds": setup_s,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-                    "steps": k_e2e},
+                    "steps": k_e2e, "copies": "pinned host buffers, copy streams overlapping the applies "
+                                              "(two buffers each way)"},
             "gpu_launches": 2 * args.steps,
             "roofline": roofline,
             "clocks": clocks.summary(),

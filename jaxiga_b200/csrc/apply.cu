@@ -748,15 +748,20 @@ int tile2_variant(int tx, int ty) {
 }
 
 template <typename T, int P, int Q, int OPK, bool RAT, int MODE>
-static size_t smem2(const Bricks& br, const int TX) {
+static size_t smem2(const Bricks& br, const int TX, const int RG = 1) {
   constexpr int P1 = P + 1, PP = P1 * P1;
   constexpr int VEC = vec_op<OPK>() ? 2 : 1;
   constexpr int NK = OPK == OPK_PLATE ? 3 : 2;
   constexpr int SX = P1 + 1;
-  size_t n = (size_t)TX * 3 * Q * P1 + 3 * Q * P1 + TX * NK * Q * SX + TX * VEC * PP +
-             (size_t)VEC * br.fp[0] * br.fp[1];
+  const size_t group = 3 * Q * P1 + (size_t)TX * NK * Q * SX + TX * VEC * PP + (size_t)VEC * br.fp[0] * br.fp[1];
+  size_t n = (size_t)TX * 3 * Q * P1 + RG * group;
   return n * sizeof(T) + TX * sizeof(int) + 64;
 }
+
+// Row groups of the 2D brick kernels: 2 when the brick has two rows or more and
+// the doubled stage buffers fit in shared memory, else 1.
+constexpr int RG2 = 2;
+static int brick2_rg(size_t smem_rg2, int rows) { return rows >= 2 && smem_rg2 <= 227 * 1024 ? RG2 : 1; }
 
 template <typename T, int P, int OPK, bool RAT, int MODE>
 static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
@@ -812,11 +817,18 @@ static int launch_one(const BrickArgs<T>& A, cudaStream_t s) {
 #define JXB_TILE2(V_)                                                                                   \
   if (v == V_) {                                                                                        \
     constexpr int TXv = TILE2X[V_];                                                                     \
-    size_t sm = smem2<T, P, Q, OPK, RAT, MODE>(br, TXv);                                                \
-    if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "2D brick does not fit in shared memory");        \
-    auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv>;                                                    \
-    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-    k<<<(unsigned)br.n_bricks, TXv * Q, sm, s>>>(A);                                                    \
+    const size_t sm2 = smem2<T, P, Q, OPK, RAT, MODE>(br, TXv, RG2);                                    \
+    if (brick2_rg(sm2, br.te[1]) == RG2) {                                                              \
+      auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv, RG2>;                                             \
+      if (sm2 > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2)); \
+      k<<<(unsigned)br.n_bricks, brick2_threads(TXv, Q, RG2), sm2, s>>>(A);                             \
+    } else {                                                                                            \
+      size_t sm = smem2<T, P, Q, OPK, RAT, MODE>(br, TXv);                                              \
+      if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "2D brick does not fit in shared memory");      \
+      auto k = k_brick2<T, P, Q, OPK, RAT, MODE, TXv, 1>;                                               \
+      if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+      k<<<(unsigned)br.n_bricks, TXv * Q, sm, s>>>(A);                                                  \
+    }                                                                                                   \
   }
     JXB_TILE2(0)
     if constexpr (OPK == OPK_SCALAR) {
@@ -970,11 +982,18 @@ static int launch_batch_p(int variant, const BrickArgs<double>* d_args, const in
 #define JXB_BTILE(V_)                                                                                   \
   if (variant == V_) {                                                                                  \
     constexpr int TXv = TILE2X[V_];                                                                     \
-    size_t sm = smem2<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY>(br, TXv);                              \
-    if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory");   \
-    auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv>;                            \
-    if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-    k<<<(unsigned)n_work, TXv * Q, sm, s>>>(d_args, d_work, d_states);                                  \
+    const size_t sm2 = smem2<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY>(br, TXv, RG2);                  \
+    if (brick2_rg(sm2, 2) == RG2) {  /* TY is per instance: a one-row brick leaves group 1 idle */     \
+      auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv, RG2>;                     \
+      if (sm2 > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2)); \
+      k<<<(unsigned)n_work, brick2_threads(TXv, Q, RG2), sm2, s>>>(d_args, d_work, d_states);          \
+    } else {                                                                                            \
+      size_t sm = smem2<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY>(br, TXv);                            \
+      if (sm > 227 * 1024) return fail(JXB_ERR_INVALID, "batched brick does not fit in shared memory"); \
+      auto k = k_brick2_batch<double, P, Q, OPK_SCALAR, RAT, MODE_APPLY, TXv, 1>;                       \
+      if (sm > 48 * 1024) JXB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+      k<<<(unsigned)n_work, TXv * Q, sm, s>>>(d_args, d_work, d_states);                                \
+    }                                                                                                   \
     JXB_CUDA(cudaGetLastError());                                                                       \
     return JXB_OK;                                                                                      \
   }

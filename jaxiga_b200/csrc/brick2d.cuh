@@ -5,10 +5,21 @@
 // and still fill the GPU.
 #pragma once
 
+// Threads of a 2D brick CTA: RG row groups of TX * Q threads, each rounded up
+// to whole warps when RG > 1 (a group synchronises on its own named barrier).
+constexpr int brick2_group_threads(int tx, int q, int rg) { return rg == 1 ? tx * q : (tx * q + 31) / 32 * 32; }
+constexpr int brick2_threads(int tx, int q, int rg) { return rg * brick2_group_threads(tx, q, rg); }
+
 // The body of one brick (element rows [by*TY, +TY) x columns [bx*TX, +TX)).
 // The host brick decomposition of the plan must use the same TX. WIDE: the CTA
-// may have more than TX * Q threads (the persistent batched kernel).
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, bool WIDE = false>
+// may have more than TX * Q threads (the persistent batched kernel). RG: row
+// groups working on the brick's rows concurrently (group g takes rows g, g +
+// RG, ...), each with its own stage buffers and its own copy of the brick
+// footprint; the copies are summed in a fixed order at the end, so the result
+// is bitwise reproducible. More rows in flight per CTA hide the latency of the
+// stage hand-offs, which bounds this kernel when a brick's rows run one after
+// another.
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, bool WIDE = false, int RG = 1>
 __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long long b) {
   constexpr int P1 = P + 1, PP = P1 * P1;
   constexpr int NE = TX, NQE = Q * Q, NT = NE * Q;
@@ -20,46 +31,66 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
   constexpr int NK = HESS ? 3 : 2;      // 1D table kinds used
   constexpr int NCH = HESS ? 6 : 3;     // channels (v, g0, g1[, h00, h01, h11])
   constexpr int SX = P1 + 1;            // padded q0 stride
+  constexpr int NTP = brick2_group_threads(TX, Q, RG);
+  static_assert(RG == 1 || !WIDE, "row groups take the CTA's own thread count");
 
   if (A.state && A.state->done) return;
   const Bricks& br = A.br;
   const int fp0 = br.fp[0], fp1 = br.fp[1];
   const int TY = br.te[1];
 
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T* stx = reinterpret_cast<T*>(smem_raw);   // [TX][3][Q][P1]
-  T* sty = stx + TX * 3 * Q * P1;            // [3][Q][P1]
-  T* bufX = sty + 3 * Q * P1;                // [NE][NK][Q][SX]
-  T* stage = bufX + NE * NK * Q * SX;        // [NE][VEC][PP]
-  T* acc = stage + NE * VEC * PP;            // [VEC][fp1][fp0]
-  int* soff = reinterpret_cast<int*>(acc + VEC * fp0 * fp1);
-
   // A WIDE CTA may have more than NT threads (the persistent batched kernel runs
   // every degree in one CTA shape): cooperative loops stride by the CTA size,
   // and threads past NT own no element.
-  const int tid = threadIdx.x, NTH = WIDE ? (int)blockDim.x : NT;
+  const int tid = threadIdx.x, NTH = WIDE ? (int)blockDim.x : RG * NTP;
+  const int rg = RG == 1 ? 0 : tid / NTP;   // this thread's row group
+  const int tg = RG == 1 ? tid : tid % NTP;  // its thread index in the group
+  const int NTG = RG == 1 ? NTH : NTP;       // the group's thread count (cooperative strides)
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int accn = VEC * fp0 * fp1;
+  const int gsz = 3 * Q * P1 + NE * NK * Q * SX + NE * VEC * PP + accn;  // one group's buffers
+  T* stx = reinterpret_cast<T*>(smem_raw);   // [TX][3][Q][P1], shared by the groups
+  T* sty = stx + TX * 3 * Q * P1 + rg * gsz; // [3][Q][P1]
+  T* bufX = sty + 3 * Q * P1;                // [NE][NK][Q][SX]
+  T* stage = bufX + NE * NK * Q * SX;        // [NE][VEC][PP]
+  T* acc = stage + NE * VEC * PP;            // [VEC][fp1][fp0]
+  int* soff = reinterpret_cast<int*>(stx + TX * 3 * Q * P1 + RG * gsz);
+  // a barrier of this thread's row group
+  auto gsync = [&]() {
+    if constexpr (RG == 1)
+      __syncthreads();
+    else
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + rg), "r"(NTP) : "memory");
+  };
+
   const int bx = (int)(b % br.nb[0]);
   const int by = (int)(b / br.nb[0]);
   const int cp0x = br.bcp0[0][bx], cp0y = br.bcp0[1][by];
-  const int el = tid / Q, t = tid % Q;
+  const int el = tg / Q, t = tg % Q;
   const int ex = bx * TX + el;
-  const bool evalid = (!WIDE || el < TX) && ex < br.n_span[0];
+  const bool evalid = (!(WIDE || RG > 1) || el < TX) && ex < br.n_span[0];
   const long long slot_base = b * (long long)TY * NE;
   const int nlayers = min(TY, br.n_span[1] - by * TY);
 
   // The factors of one row of the brick are one contiguous tile (TX elements x
   // NG x NQE values; TX is a multiple of 16, so the tile is 16-byte aligned and
-  // sized). The bulk-copy engine brings the first two rows into L2 before the
-  // tables are staged, and every later row two rows ahead, so the point
-  // operator's loads hit L2.
-  constexpr bool GEO = MODE != MODE_LOAD;
+  // sized). When tiles are small (a few KB, as in batches of small instances,
+  // where the kernel waits on latency) the bulk-copy engine brings the first
+  // rows into L2 at the start and each row group's next row while it works on
+  // the current one. Large tiles are not prefetched: with rows in flight on
+  // every SM a prefetch runs tens of MB ahead of its use and is evicted before
+  // the demand loads arrive (measured on a B200, plate 256^2, rows of 96 KB:
+  // 274-280 MB read from DRAM against 198 MB without the prefetch, and 4-10 %
+  // slower).
   constexpr unsigned ROW_BYTES = (unsigned)(NE * NG * NQE * sizeof(T));
   static_assert(ROW_BYTES % 16 == 0, "row tile of whole 16-byte units");
+  constexpr bool GEO = MODE != MODE_LOAD && ROW_BYTES <= 32768;
+  auto prefetch_row = [&](int ly) {
+    prefetch_l2(A.geo + (size_t)(slot_base + (long long)ly * NE) * NG * NQE, ROW_BYTES);
+  };
   if constexpr (GEO) {
-    if (tid == 0) {
-      prefetch_l2(A.geo + (size_t)slot_base * NG * NQE, ROW_BYTES);
-      if (nlayers > 1) prefetch_l2(A.geo + (size_t)(slot_base + NE) * NG * NQE, ROW_BYTES);
-    }
+    if (tid < RG && tid < nlayers) prefetch_row(tid);
   }
 
   for (int i = tid; i < TX * 3 * Q * P1; i += NTH) {
@@ -71,22 +102,25 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
     int e = bx * TX + tid;
     soff[tid] = e < br.n_span[0] ? br.first[0][e] - cp0x : -100000;
   }
-  const int accn = VEC * fp0 * fp1;
-  for (int i = tid; i < accn; i += NTH) acc[i] = T(0);
+  for (int i = tg; i < accn; i += NTG) acc[i] = T(0);
+  if constexpr (RG > 1) __syncthreads();  // stx and soff, staged by every group, before the groups part
   const T* nx_v = stx + el * 3 * Q * P1;
 
-  for (int ly_ = 0; ly_ < nlayers; ++ly_) {
+  for (int ly_ = rg; ly_ < nlayers; ly_ += RG) {
     if constexpr (GEO) {
-      if (tid == 0 && ly_ + 2 < nlayers)
-        prefetch_l2(A.geo + (size_t)(slot_base + (long long)(ly_ + 2) * NE) * NG * NQE, ROW_BYTES);
+      if (tg == 0 && ly_ + RG < nlayers) prefetch_row(ly_ + RG);
     }
     const int ey = by * TY + ly_;
     const int fy = br.first[1][ey];
     const int offy = fy - cp0y;
-    for (int i = tid; i < 3 * Q * P1; i += NTH) sty[i] = A.tab[1][(size_t)ey * 3 * Q * P1 + i];
-    __syncthreads();
+    for (int i = tg; i < 3 * Q * P1; i += NTG) sty[i] = A.tab[1][(size_t)ey * 3 * Q * P1 + i];
+    gsync();
     const long long slot = slot_base + (long long)ly_ * NE + el;
     const int fx = evalid ? br.first[0][ex] : 0;
+    // this element's factors in the row tile [factor][q1][element][q0]: factor k of
+    // point (q0, q1) at Grow[k * GST + q1 * NE * Q + q0]
+    constexpr int GST = NE * NQE;
+    const T* Grow = A.geo + (size_t)(slot_base + (long long)ly_ * NE) * NG * NQE + (size_t)el * Q;
     T g[VEC][NCH][Q];  // channel order (v, g0, g1, h00, h01, h11) at q1
 
     if constexpr (MODE == MODE_APPLY) {
@@ -115,7 +149,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
               dst[(k * Q + q0) * SX + i1] = s;
             }
         }
-        __syncthreads();
+        gsync();
         if (evalid) {  // Y in registers: q0 = t
           const int q0 = t;
           const T* src = bufX + el * NK * Q * SX;
@@ -144,16 +178,16 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             for (int k = 0; k < NCH; ++k) g[c][k][q1] = ch[k];
           }
         }
-        __syncthreads();
+        gsync();
       }
       if (evalid) {
-        const T* G = A.geo + (size_t)slot * NG * NQE;
 #pragma unroll
         for (int q1 = 0; q1 < Q; ++q1) {
           const int q = t + Q * q1;
+          const T* G = Grow + (size_t)q1 * (NE * Q) + t;
           if constexpr (OPK == OPK_SCALAR) {
             if constexpr (!RAT) {
-              T k0 = G[q], k1 = G[NQE + q], k2 = G[2 * NQE + q];
+              T k0 = G[0], k1 = G[GST], k2 = G[(2) * GST];
               T gx = g[0][1][q1], gy = g[0][2][q1];
               g[0][1][q1] = k0 * gx + k1 * gy;
               g[0][2][q1] = k1 * gx + k2 * gy;
@@ -161,7 +195,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             } else {
               T m[6];
 #pragma unroll
-              for (int k = 0; k < 6; ++k) m[k] = G[k * NQE + q];
+              for (int k = 0; k < 6; ++k) m[k] = G[(k) * GST];
               T v = g[0][0][q1], gx = g[0][1][q1], gy = g[0][2][q1];
               g[0][0][q1] = m[0] * v + m[1] * gx + m[2] * gy;
               g[0][1][q1] = m[1] * v + m[3] * gx + m[4] * gy;
@@ -178,20 +212,20 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             for (int i = 0; i < n; ++i)
 #pragma unroll
               for (int j = i; j < n; ++j) {
-                T m = G[(k++) * NQE + q];
+                T m = G[((k++)) * GST];
                 o[i + off] += m * s[j + off];
                 if (j != i) o[j + off] += m * s[i + off];
               }
 #pragma unroll
             for (int kk = 0; kk < 6; ++kk) g[0][kk][q1] = o[kk];
           } else {  // 2D elasticity
-            T Ji[2][2] = {{G[q], G[NQE + q]}, {G[2 * NQE + q], G[3 * NQE + q]}};
-            T om = G[4 * NQE + q];
+            T Ji[2][2] = {{G[0], G[GST]}, {G[(2) * GST], G[(3) * GST]}};
+            T om = G[(4) * GST];
             T iW = 1, gW[2] = {0, 0};
             if constexpr (RAT) {
-              iW = G[5 * NQE + q];
-              gW[0] = G[6 * NQE + q];
-              gW[1] = G[7 * NQE + q];
+              iW = G[(5) * GST];
+              gW[0] = G[(6) * GST];
+              gW[1] = G[(7) * GST];
             }
             T gp[2][2];
 #pragma unroll
@@ -207,8 +241,8 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             T lam = (T)A.lam, mu = (T)A.mu;
             T Sh[2][2];  // hyperelastic: om dP at the stored state
             if constexpr (OPK == OPK_HYPER) {
-              const T M[2][2] = {{G[E0 * NQE + q], G[(E0 + 1) * NQE + q]}, {G[(E0 + 2) * NQE + q], G[(E0 + 3) * NQE + q]}};
-              hyper_dP<T, 2>(M, G[(E0 + 4) * NQE + q], lam, mu, om, Gx, Sh);
+              const T M[2][2] = {{G[(E0) * GST], G[((E0 + 1)) * GST]}, {G[((E0 + 2)) * GST], G[((E0 + 3)) * GST]}};
+              hyper_dP<T, 2>(M, G[((E0 + 4)) * GST], lam, mu, om, Gx, Sh);
             }
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
@@ -246,19 +280,19 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
       }
     } else if constexpr (MODE == MODE_RESID) {  // hyperelastic: the stored flux w P J^-T
       if (evalid) {
-        const T* G = A.geo + (size_t)slot * NG * NQE;
 #pragma unroll
         for (int q1 = 0; q1 < Q; ++q1) {
           const int q = t + Q * q1;
+          const T* G = Grow + (size_t)q1 * (NE * Q) + t;
           T iW = 1, gW[2] = {0, 0};
           if constexpr (RAT) {
-            iW = G[5 * NQE + q];
-            gW[0] = G[6 * NQE + q];
-            gW[1] = G[7 * NQE + q];
+            iW = G[(5) * GST];
+            gW[0] = G[(6) * GST];
+            gW[1] = G[(7) * GST];
           }
 #pragma unroll
           for (int c = 0; c < VEC; ++c) {
-            const T F0 = G[(E0 + 5 + 2 * c) * NQE + q], F1 = G[(E0 + 6 + 2 * c) * NQE + q];
+            const T F0 = G[((E0 + 5 + 2 * c)) * GST], F1 = G[((E0 + 6 + 2 * c)) * GST];
 #pragma unroll
             for (int k = 0; k < NCH; ++k) g[c][k][q1] = T(0);
             if constexpr (RAT) {
@@ -301,7 +335,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             if constexpr (HESS) dst[(2 * Q + q0) * SX + i1] = a2;
           }
         }
-        __syncthreads();
+        gsync();
         if (evalid && t < P1) {  // X^T: row i1 = t
           const int i1 = t;
           const T* src = bufX + el * NK * Q * SX;
@@ -317,7 +351,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             dst[i0 * P1 + i1] = r;
           }
         }
-        __syncthreads();
+        gsync();
       }
     } else {  // MODE_DIAG
       if (evalid) {
@@ -331,7 +365,7 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
             T vx = nx_v[q0 * P1 + a0], dx = nx_v[(Q + q0) * P1 + a0], hx = nx_v[(2 * Q + q0) * P1 + a0];
             T vy = sty[q1 * P1 + a1], dy = sty[(Q + q1) * P1 + a1], hy = sty[(2 * Q + q1) * P1 + a1];
             T s[6] = {vx * vy, dx * vy, vx * dy, hx * vy, dx * dy, vx * hy};
-            const T* G = A.geo + (size_t)slot * NG * NQE + q;
+            const T* G = Grow + (size_t)q1 * (NE * Q) + q0;
             if constexpr (OPK == OPK_SCALAR || OPK == OPK_PLATE) {
               constexpr int n = OPK == OPK_SCALAR ? (RAT ? 3 : 2) : (RAT ? 6 : 5);
               constexpr int off = RAT ? 0 : 1;
@@ -341,27 +375,27 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
               for (int i = 0; i < n; ++i)
 #pragma unroll
                 for (int j = i; j < n; ++j) {
-                  T m = G[(k++) * NQE];
+                  T m = G[((k++)) * GST];
                   acc_ += (i == j ? T(1) : T(2)) * m * s[i + off] * s[j + off];
                 }
               d[0] += acc_;
             } else {
-              T Ji[2][2] = {{G[0], G[NQE]}, {G[2 * NQE], G[3 * NQE]}};
-              T om = G[4 * NQE];
+              T Ji[2][2] = {{G[0], G[GST]}, {G[(2) * GST], G[(3) * GST]}};
+              T om = G[(4) * GST];
               T gp[2] = {s[1], s[2]};
               if constexpr (RAT) {
-                T iW = G[5 * NQE];
-                gp[0] = (gp[0] - s[0] * G[6 * NQE]) * iW;
-                gp[1] = (gp[1] - s[0] * G[7 * NQE]) * iW;
+                T iW = G[(5) * GST];
+                gp[0] = (gp[0] - s[0] * G[(6) * GST]) * iW;
+                gp[1] = (gp[1] - s[0] * G[(7) * GST]) * iW;
               }
               T gx[2] = {Ji[0][0] * gp[0] + Ji[0][1] * gp[1], Ji[1][0] * gp[0] + Ji[1][1] * gp[1]};
               T n2 = gx[0] * gx[0] + gx[1] * gx[1];
               if constexpr (OPK == OPK_HYPER) {
                 // mu |g|^2 + (c + lambda) (F^-T_c . g)^2 at the stored state
-                const T ch = G[(E0 + 4) * NQE] + (T)A.lam;
+                const T ch = G[((E0 + 4)) * GST] + (T)A.lam;
 #pragma unroll
                 for (int c = 0; c < VEC; ++c) {
-                  const T mg = G[(E0 + 2 * c) * NQE] * gx[0] + G[(E0 + 2 * c + 1) * NQE] * gx[1];
+                  const T mg = G[((E0 + 2 * c)) * GST] * gx[0] + G[((E0 + 2 * c + 1)) * GST] * gx[1];
                   d[c] += om * ((T)A.mu * n2 + ch * mg * mg);
                 }
               } else {
@@ -379,12 +413,12 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
           for (int c = 0; c < VEC; ++c) stage[(el * VEC + c) * PP + a0 * P1 + a1] = d[c] * wsq;
         }
       }
-      __syncthreads();
+      gsync();
     }
     // gather the row into the brick footprint
     {
       const int nfoot = VEC * fp0 * P1;
-      for (int i = tid; i < nfoot; i += NTH) {
+      for (int i = tg; i < nfoot; i += NTG) {
         const int jx = i % fp0;
         const int jyl = (i / fp0) % P1;
         const int c = i / (fp0 * P1);
@@ -398,22 +432,33 @@ __device__ __forceinline__ void brick2_body(const BrickArgs<T>& A, const long lo
         acc[(c * fp1 + offy + jyl) * fp0 + jx] += s;
       }
     }
-    __syncthreads();
+    gsync();
   }
   T* out = A.scratch + (size_t)b * accn;
-  for (int i = tid; i < accn; i += NTH) out[i] = acc[i];
+  if constexpr (RG == 1) {
+    for (int i = tid; i < accn; i += NTH) out[i] = acc[i];
+  } else {
+    __syncthreads();
+    const T* acc0 = stx + TX * 3 * Q * P1 + 3 * Q * P1 + NE * NK * Q * SX + NE * VEC * PP;  // group 0's footprint
+    for (int i = tid; i < accn; i += NTH) {
+      T v = acc0[i];
+#pragma unroll
+      for (int r = 1; r < RG; ++r) v += acc0[(size_t)r * gsz + i];
+      out[i] = v;
+    }
+  }
 }
 
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
-__global__ void __launch_bounds__(TX* Q) k_brick2(BrickArgs<T> A) {
-  brick2_body<T, P, Q, OPK, RAT, MODE, TX>(A, blockIdx.x);
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int RG>
+__global__ void __launch_bounds__(brick2_threads(TX, Q, RG)) k_brick2(BrickArgs<T> A) {
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX, false, RG>(A, blockIdx.x);
 }
 
 // Many instances in one launch: block i processes brick work[i].y of instance
 // work[i].x, whose arguments are args[work[i].x]; instances already converged
 // (states[inst].done) are skipped.
-template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX>
-__global__ void __launch_bounds__(TX* Q)
+template <typename T, int P, int Q, int OPK, bool RAT, int MODE, int TX, int RG>
+__global__ void __launch_bounds__(brick2_threads(TX, Q, RG))
     k_brick2_batch(const BrickArgs<T>* __restrict__ args, const int2* __restrict__ work,
                    const CgState* __restrict__ states) {
   __shared__ BrickArgs<T> sA;
@@ -421,7 +466,7 @@ __global__ void __launch_bounds__(TX* Q)
   if (states && states[w.x].done) return;
   if (threadIdx.x == 0) sA = args[w.x];
   __syncthreads();
-  brick2_body<T, P, Q, OPK, RAT, MODE, TX>(sA, w.y);
+  brick2_body<T, P, Q, OPK, RAT, MODE, TX, false, RG>(sA, w.y);
 }
 
 

@@ -267,12 +267,14 @@ __global__ void k_factors(FactorArgs A) {
   long long slot = idx / nqe;
   int q = (int)(idx % nqe);
   int q0 = q % Q, q1 = (q / Q) % Q, q2 = dim == 3 ? q / (Q * Q) : 0;
-  double* g = A.geo + (size_t)slot * A.ngeo * nqe + q;
+  const GeoAt ga = geo_at(dim, slot, q, Q, A.ngeo, nqe, br.te[0]);
+  double* g = A.geo + ga.base;
+  const size_t gs = ga.stride;
   int ex, ey, ez;
   bool valid;
   elem_of_slot(br, slot, ex, ey, ez, valid);
   if (!valid) {
-    for (int k = 0; k < A.ngeo; ++k) g[k * nqe] = 0.0;
+    for (int k = 0; k < A.ngeo; ++k) g[k * gs] = 0.0;
     A.wq[slot * nqe + q] = 0.0;
     if (A.invW) A.invW[slot * nqe + q] = 0.0;
     return;
@@ -326,21 +328,21 @@ __global__ void k_factors(FactorArgs A) {
         for (int k = 0; k < dim; ++k) s += Lg[k][r] * Lg[k][c];
         M[r][c] = a0 * om * s;
       }
-    store_sym(g, nqe, nc, M, off);
+    store_sym(g, gs, nc, M, off);
   } else if (A.op == JXB_OP_ELASTICITY || A.op == JXB_OP_HYPERELASTIC) {
     int k = 0;
     for (int i = 0; i < dim; ++i)
-      for (int a = 0; a < dim; ++a) g[nqe * (k++)] = Ji[i][a];
-    g[nqe * (k++)] = om;
+      for (int a = 0; a < dim; ++a) g[gs * (k++)] = Ji[i][a];
+    g[gs * (k++)] = om;
     if (A.rational) {
-      g[nqe * (k++)] = iW;
-      for (int a = 0; a < dim; ++a) g[nqe * (k++)] = S.Wd[a] * iW;
+      g[gs * (k++)] = iW;
+      for (int a = 0; a < dim; ++a) g[gs * (k++)] = S.Wd[a] * iW;
     }
     if (A.op == JXB_OP_HYPERELASTIC) {  // the state of u = 0: F^-T = I, mu - lambda ln J = mu, no flux
       for (int i = 0; i < dim; ++i)
-        for (int a = 0; a < dim; ++a) g[nqe * (k++)] = i == a ? 1.0 : 0.0;
-      g[nqe * (k++)] = A.coef[0];
-      for (int i = 0; i < dim * dim; ++i) g[nqe * (k++)] = 0.0;
+        for (int a = 0; a < dim; ++a) g[gs * (k++)] = i == a ? 1.0 : 0.0;
+      g[gs * (k++)] = A.coef[0];
+      for (int i = 0; i < dim * dim; ++i) g[gs * (k++)] = 0.0;
     }
   } else {  // plate (2D): channels (v, v0, v1, v00, v01, v11)
     double E = A.coef[0], nu = A.coef[1], t = A.coef[2];
@@ -410,7 +412,7 @@ __global__ void k_factors(FactorArgs A) {
           for (int j = 0; j < 3; ++j) s += L[i][r] * D[i][j] * L[j][c];
         M[r][c] = om * s;
       }
-    store_sym(g, nqe, A.rational ? 6 : 5, M, A.rational ? 0 : 1);
+    store_sym(g, gs, A.rational ? 6 : 5, M, A.rational ? 0 : 1);
   }
 }
 
@@ -1022,15 +1024,17 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
     bool valid;
     elem_of_slot(br, slot, ex, ey, ez, valid);
     if (!valid) continue;
-    double* g = A.geo + (size_t)slot * A.ngeo * nqe + q;
+    const GeoAt ga = geo_at(dim, slot, q, Q, A.ngeo, nqe, br.te[0]);
+    double* g = A.geo + ga.base;
+    const size_t gs = ga.stride;
     double Ji[3][3];
     for (int i = 0; i < dim; ++i)
-      for (int a = 0; a < dim; ++a) Ji[i][a] = g[nqe * (i * dim + a)];
-    const double om = g[nqe * (dim * dim)];
+      for (int a = 0; a < dim; ++a) Ji[i][a] = g[gs * (i * dim + a)];
+    const double om = g[gs * (dim * dim)];
     double iW = 1.0, gW[3] = {0, 0, 0};
     if (A.rational) {
-      iW = g[nqe * (dim * dim + 1)];
-      for (int a = 0; a < dim; ++a) gW[a] = g[nqe * (dim * dim + 2 + a)];
+      iW = g[gs * (dim * dim + 1)];
+      for (int a = 0; a < dim; ++a) gW[a] = g[gs * (dim * dim + 2 + a)];
     }
     const int sp[3] = {ex, ey, ez};
     const int qq[3] = {q % Q, (q / Q) % Q, dim == 3 ? q / (Q * Q) : 0};
@@ -1081,8 +1085,8 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
     wsum += om * (0.5 * mu * (I1 - dim) - mu * lnJ + 0.5 * lam * lnJ * lnJ);
     int k = e0;
     for (int i = 0; i < dim; ++i)
-      for (int a = 0; a < dim; ++a) g[nqe * (k++)] = Fi[a][i];  // F^-T
-    g[nqe * (k++)] = mu - lam * lnJ;
+      for (int a = 0; a < dim; ++a) g[gs * (k++)] = Fi[a][i];  // F^-T
+    g[gs * (k++)] = mu - lam * lnJ;
     for (int i = 0; i < dim; ++i)
       for (int a = 0; a < dim; ++a) {  // w P J^-T, P_ik = mu (F_ik - F^-T_ik) + lambda ln J F^-T_ik
         double f = 0;
@@ -1090,7 +1094,7 @@ __global__ void __launch_bounds__(256) k_hyper_state(FactorArgs A, const double*
           const double Pik = mu * (F[i][kk] - Fi[kk][i]) + lam * lnJ * Fi[kk][i];
           f += Pik * Ji[kk][a];
         }
-        g[nqe * (k++)] = om * f;
+        g[gs * (k++)] = om * f;
       }
   }
   // fixed-order block sum

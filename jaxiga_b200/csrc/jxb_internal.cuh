@@ -156,6 +156,28 @@ constexpr int TILE2_MAX_ROWS = 64;
 constexpr int PERSIST2_TX = 32;
 
 // ---------------------------------------------------------------------------
+// Where the per-point factors live. ngeo factors per Gauss point, nqe points
+// per element, one geometry slot per element position of a brick.
+//   3D: slot-major, [slot][factor][point]: one element layer of a brick (te[0]
+//       x te[1] slots) is one contiguous tile.
+//   2D: each brick row (te[0] consecutive slots) is one contiguous tile laid
+//       out [factor][q1][element][q0], so the threads of a row, one per
+//       (element, q0), read consecutive values for every (factor, q1).
+// base: offset of factor 0 of point q of `slot`; stride: from one factor to
+// the next.
+// ---------------------------------------------------------------------------
+struct GeoAt {
+  size_t base, stride;
+};
+
+__host__ __device__ inline GeoAt geo_at(int dim, long long slot, int q, int Q, int ngeo, long long nqe, int te0) {
+  if (dim == 3) return {(size_t)slot * ngeo * nqe + q, (size_t)nqe};
+  const long long row = slot / te0;
+  const int el = (int)(slot - row * te0), q0 = q % Q, q1 = q / Q;
+  return {(size_t)row * te0 * ngeo * nqe + ((size_t)q1 * te0 + el) * Q + q0, (size_t)te0 * nqe};
+}
+
+// ---------------------------------------------------------------------------
 // The combine's sum at one control point: y_i = the sum, over the bricks whose
 // footprint holds control point i, of their footprint values -- bricks taken
 // in the fixed order (z, then y, then x, each in cover-list order), so the

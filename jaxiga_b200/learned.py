@@ -302,8 +302,14 @@ class LearnedPreconditioner:
 
     # -- solve -------------------------------------------------------------------
     def solve(self, b, tol=1e-8, maxiter=None, stall=50, depth=4, mixed=False, inner_tol=None, check_every=16,
-              use_network=True, two_level=False, refinement="reliable"):
+              use_network=True, two_level=False, refinement="reliable", restarts=3):
         """Flexible CG with this preconditioner (Jacobi fallback); returns (x, stats).
+
+        ``restarts``: when the flexible CG's recursive residual met ``tol`` but
+        the true FP64 residual did not, up to this many correction solves on the
+        true residual, each to half the remaining target, on a shared iteration
+        budget -- the rule of the reference's CPU CG
+        (src/jaxiga/solvers/linear.py:261-321). ``stats["restarts"]`` counts them.
 
         ``mixed``: the flexible CG runs in FP32 with FP64 corrections. With
         ``refinement="reliable"`` the FP32 iterate is folded into the FP64
@@ -321,6 +327,44 @@ class LearnedPreconditioner:
         """
         if refinement not in ("reliable", "restart"):
             raise ValueError(f"refinement must be 'reliable' or 'restart', got {refinement!r}")
+        if isinstance(restarts, bool) or not isinstance(restarts, (int, np.integer)) or not 0 <= restarts <= 8:
+            raise ValueError("restarts must be an integer in 0..8")
+        kw = dict(stall=stall, depth=depth, mixed=mixed, inner_tol=inner_tol, check_every=check_every,
+                  use_network=use_network, two_level=two_level, refinement=refinement)
+        x, out = self._solve_once(b, tol, maxiter, **kw)
+        out["restarts"] = 0
+        if restarts == 0 or out["converged"] or not out["finite"]:
+            return x, out
+        import torch
+
+        op = self.op
+        keep = torch.as_tensor(~op.prescribed_mask, device=op.device)
+        b = torch.where(keep, op._vec(b), 0.0)  # the solve's right-hand side: its free rows
+        bn = float(torch.linalg.norm(b))
+        budget = (maxiter if maxiter is not None else 10 * int(op.info["n_free"])) - out["iterations"]
+        rel = out["relative_residual"]
+        for _ in range(restarts):
+            if budget <= 0 or rel <= tol:
+                break
+            r = b - op.apply(x)
+            rn = float(torch.linalg.norm(r))
+            dx, o = self._solve_once(r, min(0.5, 0.5 * tol * bn / rn), budget, **kw)
+            budget -= o["iterations"]
+            cand = x + dx
+            rc = float(torch.linalg.norm(b - op.apply(cand)))
+            out["iterations"] += o["iterations"]
+            out["learned_iterations"] += o["learned_iterations"]
+            out["seconds"] += o["seconds"]
+            out["restarts"] += 1
+            if not o["finite"] or rc >= rn:  # the correction did not help: keep x
+                break
+            x, rel = cand, rc / bn
+            out["residual"], out["relative_residual"] = rc, rel
+        out["converged"] = int(rel <= tol)
+        return x, out
+
+    def _solve_once(self, b, tol, maxiter, stall, depth, mixed, inner_tol, check_every, use_network, two_level,
+                    refinement):
         if two_level not in (False, True, "multiplicative", "additive"):
             raise ValueError(f"two_level must be False, True, 'multiplicative' or 'additive', got {two_level!r}")
         additive = two_level == "additive"
