@@ -23,6 +23,7 @@ from .csr import CSRPattern, DeviceCG
 from .forms import (ClampedBC, DirichletBC, Hyperelasticity, KirchhoffPlate, LinearElasticity, Neumann, PointField,
                     Poisson, Problem)
 from .geometry import Patch, primitives
+from .hierarchical import HierarchicalSpace, Hierarchy, HierarchyError, dorfler_mark, refine_elements
 from .newton import history_list
 from .operator import Operator
 from .pointset import PointSet, gauss
@@ -37,4 +38,5 @@ __all__ = [
     "KirchhoffPlate", "solve", "LinearOptions", "Solution", "errornorm", "norm", "integrate", "Operator",
     "PointSet", "gauss", "value_and_grad", "adjoint_solve", "parameter_gradients", "SOLVE_COUNTER",
     "reset_solve_counter", "DeviceCG", "CSRPattern", "Hyperelasticity", "history_list",
+    "HierarchicalSpace", "Hierarchy", "HierarchyError", "refine_elements", "dorfler_mark",
 ]
