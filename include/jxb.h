@@ -285,6 +285,42 @@ int jxb_hyper_residual(jxb_plan* plan, jxb_stream stream, double* r);
 int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_to_global, int64_t n_global_scalar,
                   const uint8_t* prescribed, jxb_plan** out);
 
+/* ---- truncated hierarchical (THB) spaces -----------------------------------
+ * Poisson, -div(a grad u) = f, on a space in the padded-element form of the
+ * reference (src/jaxiga/space/function_space.py:23-38, built by
+ * src/jaxiga/space/hierarchical.py:891-980): per leaf element, n_local_max
+ * hierarchical functions (padding index n_scalar) and the extraction rows
+ * (zero for the padding) that map the element's Bernstein polynomials on
+ * [-1, 1]^dim to them. Replaces the reference's element tangents and CSR scatter
+ * on such spaces (src/jaxiga/methods/galerkin.py:82-148, src/jaxiga/forms/
+ * library.py:54-65) by a matrix-free element apply. All arrays are host arrays:
+ *   elem_dofs  (n_elem, n_local_max) int64;
+ *   extraction (n_elem, n_local_max, nb), nb = (degree + 1)^dim;
+ *   wgts       (n_scalar) NURBS weights of the hierarchical basis;
+ *   tables     (dim + 1, nq, nb): Bernstein values, then the derivative along
+ *              each reference direction, at the nq = (degree + 1)^dim Gauss
+ *              points (first direction fastest);
+ *   factors    (n_elem, nq, nf), nf = (dim + 1)(dim + 2) / 2: per point the
+ *              symmetric metric M = a w L^T L of the channels (numerator value,
+ *              its reference gradient), L = J^-T (1/W) [-grad W / W | I],
+ *              packed upper triangle row by row;
+ *   wq         (n_elem, nq): quadrature weight over the weight function W;
+ *   prescribed (n_scalar) 1 = Dirichlet DOF, or NULL.
+ * The plan works with jxb_apply, jxb_diag, jxb_load (f_qp: (n_elem, nq)),
+ * jxb_dot, jxb_pcg and jxb_plan_destroy; the other entry points reject it. */
+typedef struct jxb_thb_desc {
+  int dim, degree, n_local_max;
+  int64_t n_elem, n_scalar;
+  const int64_t* elem_dofs;
+  const double* extraction;
+  const double* wgts;
+  const double* tables;
+  const double* factors;
+  const double* wq;
+  const uint8_t* prescribed;
+} jxb_thb_desc;
+int jxb_thb_create(const jxb_thb_desc* desc, jxb_plan** out);
+
 /* ---- batches of independent problems -------------------------------------
  * The B200 form of the reference's vmap-over-params batching
  * (tests/test_advanced.py:338-356; host SciPy solves run once per member,

@@ -49,6 +49,25 @@ class Desc(ctypes.Structure):
     ]
 
 
+class ThbDesc(ctypes.Structure):
+    """jxb_thb_desc (include/jxb.h)."""
+
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("degree", ctypes.c_int),
+        ("n_local_max", ctypes.c_int),
+        ("n_elem", ctypes.c_int64),
+        ("n_scalar", ctypes.c_int64),
+        ("elem_dofs", ctypes.c_void_p),
+        ("extraction", ctypes.c_void_p),
+        ("wgts", ctypes.c_void_p),
+        ("tables", ctypes.c_void_p),
+        ("factors", ctypes.c_void_p),
+        ("wq", ctypes.c_void_p),
+        ("prescribed", ctypes.c_void_p),
+    ]
+
+
 class Info(ctypes.Structure):
     _fields_ = [
         ("n_dofs", ctypes.c_int64),
@@ -139,6 +158,7 @@ SIGNATURES = [
     ("jxb_batch_destroy", [ctypes.c_void_p]),
     ("jxb_mp_create", [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                        ctypes.POINTER(ctypes.c_void_p)]),
+    ("jxb_thb_create", [ctypes.POINTER(ThbDesc), ctypes.POINTER(ctypes.c_void_p)]),
     ("jxb_hyper_state", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("jxb_hyper_residual", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("jxb_batch_size", [ctypes.c_void_p, c_int64_p, c_int64_p]),

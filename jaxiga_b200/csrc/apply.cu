@@ -896,6 +896,12 @@ int launch_bricks(jxb_plan* plan, cudaStream_t s, int mode, const T* x, const do
     else
       return fail(JXB_ERR_INVALID, "multipatch plans have no FP32 copy");
   }
+  if (plan->thb) {  // hierarchical plan: the padded-element apply
+    if constexpr (sizeof(T) == 8)
+      return thb_bricks(plan, s, mode, x, f_qp, state, masked);
+    else
+      return fail(JXB_ERR_INVALID, "hierarchical plans have no FP32 copy");
+  }
   BrickArgs<T> A;
   A.br = plan->br;
   constexpr bool F32 = sizeof(T) == 4;
@@ -940,6 +946,12 @@ int launch_combine(jxb_plan* plan, cudaStream_t s, T* y, int masked, const T* do
       return mp_combine(plan, s, y, masked, dot_with, partials, state);
     else
       return fail(JXB_ERR_INVALID, "multipatch plans have no FP32 copy");
+  }
+  if (plan->thb) {  // hierarchical: the fixed-order sum of the element copies of every DOF
+    if constexpr (sizeof(T) == 8)
+      return thb_combine(plan, s, y, masked, dot_with, partials, state);
+    else
+      return fail(JXB_ERR_INVALID, "hierarchical plans have no FP32 copy");
   }
   const T* scratch;
   if constexpr (sizeof(T) == 4)

@@ -59,7 +59,7 @@ int scratch_address(double** out) {
 }  // namespace
 
 extern "C" int jxb_apply_static(jxb_plan* plan, jxb_stream stream, const double* x, double* y, int masked) {
-  if (plan && plan->mp) return jxb::fail(JXB_ERR_INVALID, "jxb_apply_static: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return jxb::fail(JXB_ERR_INVALID, "jxb_apply_static: not available on a multipatch or hierarchical plan");
   if (!plan || !x || !y) return jxb::fail(JXB_ERR_INVALID, "jxb_apply_static: null argument");
   const size_t need = plan->scratch_elems * sizeof(double);
   if (need > JXB_STATIC_SCRATCH_BYTES)

@@ -284,7 +284,7 @@ extern "C" int jxb_batch_create(jxb_plan* const* plans, int n, jxb_batch** out) 
                                        " appears more than once; create one plan per instance");
   }
   for (int i = 0; i < n; ++i) {
-    if (plans[i]->mp) return fail(JXB_ERR_INVALID, "jxb_batch_create: not available on a multipatch plan");
+    if (plans[i]->mp || plans[i]->thb) return fail(JXB_ERR_INVALID, "jxb_batch_create: not available on a multipatch or hierarchical plan");
     if (plans[i]->dim != 2 || plans[i]->op != JXB_OP_POISSON)
       return fail(JXB_ERR_INVALID, "jxb_batch_create: batches take 2D Poisson plans");
     if (plans[i]->rational != plans[0]->rational)

@@ -635,7 +635,7 @@ using namespace jxb;
 extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const double* b, double* x,
                                const float* features, int n_features, float in_scale, double out_scale, int stall,
                                int depth, int mode, const jxb_solve_opts* opts, jxb_stats* stats) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: not available on a multipatch or hierarchical plan");
   const int mixed = mode & 1;
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: null argument");
   if (n_features < 0 || (n_features > 0 && !features)) return fail(JXB_ERR_INVALID, "jxb_fcg_learned: bad features");
@@ -776,7 +776,7 @@ extern "C" int jxb_fcg_learned(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, 
 extern "C" int jxb_cnn_accumulate_energy(jxb_plan* plan, jxb_cnn* cnn, jxb_stream stream, const float* in,
                                          const float* e, const float* r, float out_scale, double weight, int angle,
                                          double* loss) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: not available on a multipatch or hierarchical plan");
   if (!plan || !cnn || !in || !e || (angle && !r)) return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: null argument");
   if (cnn_out_channels(cnn) != plan->vec)
     return fail(JXB_ERR_INVALID, "jxb_cnn_accumulate_energy: the network's outputs must equal the plan's vec");

@@ -289,6 +289,7 @@ __device__ __forceinline__ void combine_point(const Bricks& br, const T* __restr
 
 struct jxb_krylov_ws;  // BiCGSTAB workspace (krylov.cu)
 struct jxb_mp_data;    // composite multipatch plan (mp.cu)
+struct jxb_thb_data;   // padded-element (THB) Poisson plan (thb.cu)
 
 struct jxb_plan {
   int device = 0;  // the CUDA device that was current at creation; its buffers live there
@@ -338,6 +339,7 @@ struct jxb_plan {
   cudaStream_t graph_stream[2] = {nullptr, nullptr};
   size_t scratch_elems = 0;
   jxb_mp_data* mp = nullptr;  // set on a composite plan over several patch plans
+  jxb_thb_data* thb = nullptr;  // set on a plan over a hierarchical (padded-element) space
 };
 
 namespace jxb {
@@ -375,6 +377,12 @@ int mp_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const d
 int mp_combine(jxb_plan* plan, cudaStream_t s, double* y, int masked, const double* dot_with, double* partials,
                const CgState* state);
 void free_mp(jxb_plan* plan);
+// thb.cu: the hierarchical plan's hooks in launch_bricks / launch_combine
+int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const double* f_qp, const CgState* state,
+               int masked);
+int thb_combine(jxb_plan* plan, cudaStream_t s, double* y, int masked, const double* dot_with, double* partials,
+                const CgState* state);
+void free_thb(jxb_plan* plan);
 
 size_t smem2_scalar_apply(int p, bool rational, int tx, int fp0, int fp1);
 int persist2_grid(bool rational, size_t smem, int* grid);

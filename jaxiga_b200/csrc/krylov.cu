@@ -287,7 +287,7 @@ using namespace jxb;
 
 extern "C" int jxb_bicgstab(jxb_plan* plan, jxb_stream stream, const double* b, double* x, const jxb_solve_opts* opts,
                             jxb_stats* stats) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_bicgstab: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_bicgstab: not available on a multipatch or hierarchical plan");
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_bicgstab: null argument");
   if (!(opts->tol > 0) || !isfinite(opts->tol)) return fail(JXB_ERR_INVALID, "jxb_bicgstab: tol must be finite and positive");
   cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);

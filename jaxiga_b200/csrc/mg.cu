@@ -451,7 +451,7 @@ extern "C" int jxb_mg_create(jxb_plan* const* plans, int n_levels, const jxb_tra
   if (!plans || !out || n_levels < 2 || n_levels > 12 || !transfer_ || !coarse_inv)
     return fail(JXB_ERR_INVALID, "jxb_mg_create: bad argument");
   for (int l = 0; l < n_levels; ++l)
-    if (plans[l] && plans[l]->mp) return fail(JXB_ERR_INVALID, "jxb_mg_create: not available on a multipatch plan");
+    if (plans[l] && (plans[l]->mp || plans[l]->thb)) return fail(JXB_ERR_INVALID, "jxb_mg_create: not available on a multipatch or hierarchical plan");
   if (degree < 1 || degree > 8 || !(smooth_range > 1.0))
     return fail(JXB_ERR_INVALID, "jxb_mg_create: degree must be in 1..8 and smooth_range > 1");
   *out = nullptr;

@@ -120,7 +120,7 @@ extern "C" int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* con
   for (int i = 0; i < n; ++i) {
     const jxb_plan* P = patches[i];
     if (!P || !local_to_global[i]) return fail(JXB_ERR_INVALID, "jxb_mp_create: null patch plan or map");
-    if (P->mp) return fail(JXB_ERR_INVALID, "jxb_mp_create: a patch plan is itself composite");
+    if (P->mp || P->thb) return fail(JXB_ERR_INVALID, "jxb_mp_create: a patch plan is itself composite or hierarchical");
     if (P->dim != P0->dim || P->vec != P0->vec || P->op != P0->op || P->p != P0->p)
       return fail(JXB_ERR_INVALID, "jxb_mp_create: patches differ in dimension, components, operator or degree");
     if (P->op == JXB_OP_HYPERELASTIC) return fail(JXB_ERR_INVALID, "jxb_mp_create: hyperelastic patches are not supported");

@@ -546,7 +546,7 @@ extern "C" int jxb_pcg(jxb_plan* plan, jxb_stream stream, const double* b, doubl
 
 extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                                 const jxb_solve_opts* opts, jxb_stats* stats) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_refine_solve: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_refine_solve: not available on a multipatch or hierarchical plan");
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_refine_solve: null argument");
   if (!plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_refine_solve: plan was created without want_f32");
   if (!(opts->tol > 0) || !isfinite(opts->tol))
@@ -613,7 +613,7 @@ extern "C" int jxb_refine_solve(jxb_plan* plan, jxb_stream stream, const double*
 // to that of FP64 CG while every K p but one per update is an FP32 apply.
 extern "C" int jxb_mixed_pcg(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                              const jxb_solve_opts* opts, jxb_stats* stats) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: not available on a multipatch or hierarchical plan");
   if (!plan || !b || !x || !opts) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: null argument");
   if (!plan->d_geo32) return fail(JXB_ERR_INVALID, "jxb_mixed_pcg: plan was created without want_f32");
   if (!(opts->tol > 0) || !isfinite(opts->tol))
@@ -685,7 +685,7 @@ extern "C" int jxb_dot(jxb_plan* plan, jxb_stream stream, const double* a, const
 extern "C" int jxb_pcg_snapshots(jxb_plan* plan, jxb_stream stream, const double* b, double* x,
                                  const jxb_solve_opts* opts, int every, double* snaps, int64_t max_snaps,
                                  int64_t* n_snaps, jxb_stats* stats) {
-  if (plan && plan->mp) return fail(JXB_ERR_INVALID, "jxb_pcg_snapshots: not available on a multipatch plan");
+  if (plan && (plan->mp || plan->thb)) return fail(JXB_ERR_INVALID, "jxb_pcg_snapshots: not available on a multipatch or hierarchical plan");
   if (!plan || !b || !x || !opts || !snaps || !n_snaps || every < 1 || max_snaps < 0)
     return fail(JXB_ERR_INVALID, "jxb_pcg_snapshots: bad argument");
   cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);

@@ -48,6 +48,7 @@ static int upload(T** d, const T* h, size_t n, cudaStream_t s) {
 static void free_plan(jxb_plan* p) {
   if (!p) return;
   free_mp(p);
+  free_thb(p);
   free_krylov(p);
   for (int d = 0; d < 3; ++d) {
     cudaFree(p->d_first[d]);
@@ -346,7 +347,7 @@ extern "C" int jxb_apply(jxb_plan* P, jxb_stream stream, const double* x, double
 }
 
 extern "C" int jxb_apply_f32(jxb_plan* P, jxb_stream stream, const float* x, float* y) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_apply_f32: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_apply_f32: not available on a multipatch or hierarchical plan");
   if (!P || !x || !y) return fail(JXB_ERR_INVALID, "jxb_apply_f32: null argument");
   if (!P->d_geo32) return fail(JXB_ERR_INVALID, "jxb_apply_f32: plan was created without want_f32");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -364,13 +365,13 @@ extern "C" int jxb_diag(jxb_plan* P, jxb_stream stream, double* d) {
 }
 
 extern "C" int jxb_hyper_state(jxb_plan* P, jxb_stream stream, const double* u, double* energy) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_hyper_state: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_hyper_state: not available on a multipatch or hierarchical plan");
   if (!P || !u) return fail(JXB_ERR_INVALID, "jxb_hyper_state: null argument");
   return hyper_state(P, reinterpret_cast<cudaStream_t>(stream), u, energy);
 }
 
 extern "C" int jxb_hyper_residual(jxb_plan* P, jxb_stream stream, double* r) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: not available on a multipatch or hierarchical plan");
   if (!P || !r) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: null argument");
   if (P->op != JXB_OP_HYPERELASTIC) return fail(JXB_ERR_INVALID, "jxb_hyper_residual: not a hyperelastic plan");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -388,19 +389,19 @@ extern "C" int jxb_load(jxb_plan* P, jxb_stream stream, const double* f_qp, doub
 }
 
 extern "C" int jxb_qp_coords(jxb_plan* P, jxb_stream stream, double* x) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_qp_coords: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_qp_coords: not available on a multipatch or hierarchical plan");
   if (!P || !x) return fail(JXB_ERR_INVALID, "jxb_qp_coords: null argument");
   return qp_coords(P, reinterpret_cast<cudaStream_t>(stream), x);
 }
 
 extern "C" int jxb_interpolate(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, double* out) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_interpolate: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_interpolate: not available on a multipatch or hierarchical plan");
   if (!P || !coef || !out) return fail(JXB_ERR_INVALID, "jxb_interpolate: null argument");
   return interpolate(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, out);
 }
 
 extern "C" int jxb_interpolate_grad(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, double* out) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: not available on a multipatch or hierarchical plan");
   if (!P || !coef || !out) return fail(JXB_ERR_INVALID, "jxb_interpolate_grad: null argument");
   return interpolate_grad(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, out);
 }
@@ -408,7 +409,7 @@ extern "C" int jxb_interpolate_grad(jxb_plan* P, jxb_stream stream, const double
 extern "C" int jxb_eval_points(jxb_plan* P, jxb_stream stream, const double* coef, int ncomp, int64_t n,
                                const int64_t* elems, const double* ref, double* val, double* grad, double* x,
                                double* jac) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_eval_points: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_eval_points: not available on a multipatch or hierarchical plan");
   if (!P || (n > 0 && (!elems || !ref))) return fail(JXB_ERR_INVALID, "jxb_eval_points: null argument");
   if (!coef && (val || grad)) return fail(JXB_ERR_INVALID, "jxb_eval_points: values need a coefficient field");
   return eval_points(P, reinterpret_cast<cudaStream_t>(stream), coef, ncomp, n,
@@ -418,7 +419,7 @@ extern "C" int jxb_eval_points(jxb_plan* P, jxb_stream stream, const double* coe
 extern "C" int jxb_boundary_points(jxb_plan* P, jxb_stream stream, int64_t n_faces, int n_q, const int64_t* elems,
                                    const int32_t* sides, const double* ref, const double* wref, double* x,
                                    double* normal, double* w) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_boundary_points: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_boundary_points: not available on a multipatch or hierarchical plan");
   if (!P || (n_faces > 0 && (!elems || !sides || !ref || (w && !wref))))
     return fail(JXB_ERR_INVALID, "jxb_boundary_points: null argument");
   return boundary_points(P, reinterpret_cast<cudaStream_t>(stream), n_faces, n_q,
@@ -429,7 +430,7 @@ extern "C" int jxb_boundary_load(jxb_plan* P, jxb_stream stream, int64_t n_faces
                                  const double* ref, const double* w, const double* traction, int64_t n_touched,
                                  const int64_t* dofs, const int64_t* ptr, const int64_t* contrib, double* local,
                                  double* F) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_boundary_load: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_boundary_load: not available on a multipatch or hierarchical plan");
   if (!P || (n_faces > 0 && (!elems || !ref || !w || !traction || !local || !F)) ||
       (n_touched > 0 && (!dofs || !ptr || !contrib)))
     return fail(JXB_ERR_INVALID, "jxb_boundary_load: null argument");
@@ -440,14 +441,14 @@ extern "C" int jxb_boundary_load(jxb_plan* P, jxb_stream stream, int64_t n_faces
 }
 
 extern "C" int jxb_qp_weights(jxb_plan* P, jxb_stream stream, double* w) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_qp_weights: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_qp_weights: not available on a multipatch or hierarchical plan");
   if (!P || !w) return fail(JXB_ERR_INVALID, "jxb_qp_weights: null argument");
   return qp_weights(P, reinterpret_cast<cudaStream_t>(stream), w);
 }
 
 extern "C" int jxb_profile_apply(jxb_plan* P, jxb_stream stream, const void* x, void* y, int reps, int f32,
                                  double* ms_out) {
-  if (P && P->mp) return fail(JXB_ERR_INVALID, "jxb_profile_apply: not available on a multipatch plan");
+  if (P && (P->mp || P->thb)) return fail(JXB_ERR_INVALID, "jxb_profile_apply: not available on a multipatch or hierarchical plan");
   if (!P || !x || !y || !ms_out || reps < 1) return fail(JXB_ERR_INVALID, "jxb_profile_apply: bad argument");
   if (f32 && !P->d_geo32) return fail(JXB_ERR_INVALID, "jxb_profile_apply: plan was created without want_f32");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -448,6 +448,7 @@ class HierarchicalSpace:
         self.elem_vertex = np.array(boxes).reshape(self.n_elems, 2 * self.dim)
         self.elem_key = np.array(keys, dtype=np.int64).reshape(self.n_elems, 3)
         self._boundaries = self._classify()
+        self._plans = {}  # device operators and evaluation data cached by solve()
 
     # -- sizes -------------------------------------------------------------
     @property

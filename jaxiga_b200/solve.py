@@ -135,8 +135,14 @@ def geometry_operator(space) -> Operator:
     if op is None:
         from .multipatch import MultiPatchGeometry, MultiPatchSpace
 
+        from .hierarchical import HierarchicalSpace
+
         if isinstance(space, MultiPatchSpace):
             op = MultiPatchGeometry(space)
+        elif isinstance(space, HierarchicalSpace):
+            from .thb import ThbGeometry
+
+            op = ThbGeometry(space)
         else:
             op = Operator(space, "poisson", (1.0,), vec=1)
         space._plans["geometry"] = op
@@ -229,7 +235,14 @@ def cached_operator(space, op_name, coef, prescribed_mask=None, coef_qp=None, wa
         cache.pop(key).close()
     from .multipatch import MultiPatchOperator, MultiPatchSpace
 
-    cls = MultiPatchOperator if isinstance(space, MultiPatchSpace) else Operator
+    from .hierarchical import HierarchicalSpace
+
+    if isinstance(space, HierarchicalSpace):
+        from .thb import ThbOperator
+
+        cls = ThbOperator
+    else:
+        cls = MultiPatchOperator if isinstance(space, MultiPatchSpace) else Operator
     op = cls(space, op_name, coef, prescribed=prescribed_mask, coef_qp=coef_qp, want_f32=want_f32,
              plane_strain=plane_strain)
     cache[key] = op
@@ -358,6 +371,13 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     if isinstance(space, MultiPatchSpace):
         if linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none") or linear.method != "cg":
             raise NotImplementedError("multipatch spaces solve with FP64 Jacobi-PCG")
+    from .hierarchical import HierarchicalSpace
+
+    if isinstance(space, HierarchicalSpace):
+        if linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none") or linear.method != "cg":
+            raise NotImplementedError("hierarchical spaces solve with FP64 Jacobi-PCG")
+        if problem.neumann:
+            raise NotImplementedError("Neumann loads on hierarchical spaces")
 
     op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)

@@ -1,0 +1,213 @@
+"""Device operator of Poisson problems on truncated hierarchical spaces.
+
+A ``HierarchicalSpace`` (hierarchical.py) has elements with different numbers
+of basis functions, so the tensor-product brick kernels do not apply. Its plan
+(``jxb_thb_create``, csrc/thb.cu) runs K.u element by element through each
+element's extraction operator, and hooks into the same entry points, so
+``apply``, ``diag``, ``load``, ``dot`` and ``pcg`` are the single-patch
+``Operator``'s.
+
+The per-point data the device reads is made here once per operator: for every
+leaf element the Bernstein form of the geometry (the element's homogeneous
+control points pushed through its extraction operator), the Jacobian, its
+determinant and inverse at the Gauss points of [-1, 1]^dim, the rational
+weight function W and its gradient, and from them the metric M = a w L^T L of
+the channels (numerator value, reference gradient) with L = J^-T (1/W)
+[-grad W / W | I] -- the quotient rule of src/jaxiga/space/evaluation.py:95-172
+folded into the operator, as the tensor kernels do.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .hierarchical import HierarchicalSpace
+from .space import bernstein_basis, gauss_1d
+
+
+def _bernstein_deriv(u, p):
+    """d/du of the Bernstein polynomials on [-1, 1]: (p/2)(B^{p-1}_{k-1} - B^{p-1}_k)."""
+    if p == 0:
+        return np.zeros((len(u), 1))
+    lo = bernstein_basis(u, p - 1)
+    d = np.zeros((len(u), p + 1))
+    d[:, 1:] += lo
+    d[:, :-1] -= lo
+    return 0.5 * p * d
+
+
+def reference_tables(dim, p):
+    """Gauss points and weights of [-1, 1]^dim ((p+1)^dim, first direction
+    fastest) and the (dim + 1, nq, nb) table of the Bernstein polynomials and
+    their reference derivatives there (tensor order first direction fastest)."""
+    u, w1 = gauss_1d(p + 1)
+    B1, D1 = bernstein_basis(u, p), _bernstein_deriv(u, p)
+    n1 = p + 1
+
+    def tensor(fs):  # fs[d]: (n1 points, n1 functions) -> (n1^dim, n1^dim)
+        out = fs[0]
+        for d in range(1, dim):
+            out = np.einsum("qa,rb->rqba", out.reshape(-1, n1 ** d), fs[d]).reshape(n1 ** (d + 1), n1 ** (d + 1))
+        return out
+
+    T = [tensor([B1] * dim)]
+    for k in range(dim):
+        T.append(tensor([D1 if d == k else B1 for d in range(dim)]))
+    wq = w1
+    for d in range(1, dim):
+        wq = np.einsum("q,r->rq", wq, w1).ravel()
+    return np.stack(T), wq
+
+
+def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096):
+    """(factors (n_e, nq, nf), w / W (n_e, nq), x (n_e, nq, dim), w (n_e, nq))
+    of every leaf element's Gauss points; ``a0`` scalar or (n_e, nq)."""
+    dim, p = space.dim, space.degree[0]
+    if space.dim_phys != dim:
+        raise NotImplementedError("hierarchical operators need the physical and parametric dimensions equal")
+    T, gw = reference_tables(dim, p)
+    hom = np.concatenate([space.cpts * space.wgts[:, None], space.wgts[:, None]], 1)
+    hom = np.concatenate([hom, np.zeros((1, dim + 1))])  # the padding index reads zeros
+    ne, nq = space.n_elems, len(gw)
+    nf = (dim + 1) * (dim + 2) // 2
+    fac = np.zeros((ne, nq, nf))
+    wqW = np.zeros((ne, nq))
+    X = np.zeros((ne, nq, dim))
+    W8 = np.zeros((ne, nq))
+    iu = np.triu_indices(dim + 1)
+    for lo in range(0, ne, chunk):
+        el = slice(lo, min(lo + chunk, ne))
+        Pb = np.einsum("eia,eik->eak", space.extraction[el], hom[space.elem_dofs[el]])  # Bernstein homogeneous net
+        val = np.einsum("qa,eak->eqk", T[0], Pb)
+        grd = np.einsum("cqa,eak->ecqk", T[1:], Pb)  # (e, dir, q, k)
+        W = val[..., -1]
+        x = val[..., :-1] / W[..., None]
+        dW = grd[..., -1]  # (e, dir, q)
+        dx = (grd[..., :-1] - x[:, None] * dW[..., None]) / W[:, None, :, None]  # (e, dir a, q, i) = d x_i / d xi_a
+        J = np.moveaxis(dx, 1, -1)  # (e, q, i, a)
+        det = np.linalg.det(J)
+        Ji = np.linalg.inv(J)       # (e, q, a, k) = (J^-1)[a][k]
+        w = gw[None, :] * np.abs(det)
+        a = a0 if np.ndim(a0) == 0 else np.asarray(a0, dtype=float).reshape(ne, nq)[el]
+        L = np.zeros(J.shape[:2] + (dim, dim + 1))
+        iW = 1.0 / W
+        dWq = np.moveaxis(dW, 1, -1)  # (e, q, a)
+        for k in range(dim):
+            L[..., k, 0] = -np.einsum("eqa,eqa->eq", Ji[..., :, k], dWq) * iW * iW
+            for c in range(dim):
+                L[..., k, 1 + c] = Ji[..., c, k] * iW
+        M = (a * w)[..., None, None] * np.einsum("eqkr,eqks->eqrs", L, L)
+        fac[el] = M[..., iu[0], iu[1]]
+        wqW[el] = w * iW
+        X[el] = x
+        W8[el] = w
+    return fac, wqW, X, W8
+
+
+class ThbOperator:
+    """Device Poisson operator on a HierarchicalSpace (``jxb_thb_create``):
+    apply, diagonal, load, dot and Jacobi-PCG on the hierarchical DOFs."""
+
+    def __init__(self, space, op="poisson", coef=(1.0,), prescribed=None, coef_qp=None, want_f32=False,
+                 plane_strain=False):
+        import torch
+
+        if op != "poisson" or space.vec != 1:
+            raise NotImplementedError("hierarchical spaces run the Poisson operator (vec = 1)")
+        if want_f32:
+            raise NotImplementedError("hierarchical operators run in FP64")
+        if not torch.cuda.is_available():
+            raise RuntimeError("the B200 solver needs a CUDA device; none is visible")
+        self.lib = _lib.load()
+        self.space, self.op, self.vec = space, op, 1
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.want_f32, self.tile = False, None
+        a0 = float(coef[0]) if coef_qp is None else np.asarray(coef_qp, dtype=float)
+        fac, wqW, X, W = point_data(space, a0)
+        self.qp_x, self.qp_w = X, W
+        T, _ = reference_tables(space.dim, space.degree[0])
+        keep = [np.ascontiguousarray(space.elem_dofs, dtype=np.int64), np.ascontiguousarray(space.extraction),
+                np.ascontiguousarray(space.wgts, dtype=np.float64), np.ascontiguousarray(T),
+                np.ascontiguousarray(fac), np.ascontiguousarray(wqW)]
+        self.prescribed_mask = (np.zeros(space.n_dofs, bool) if prescribed is None
+                                else np.asarray(prescribed).astype(bool).copy())
+        pm = np.ascontiguousarray(self.prescribed_mask.astype(np.uint8))
+        d = _lib.ThbDesc()
+        d.dim, d.degree, d.n_local_max = space.dim, space.degree[0], space.n_local_max
+        d.n_elem, d.n_scalar = space.n_elems, space.n_scalar_basis
+        d.elem_dofs, d.extraction, d.wgts, d.tables, d.factors, d.wq = [k.ctypes.data for k in keep]
+        d.prescribed = pm.ctypes.data
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.jxb_thb_create(ctypes.byref(d), ctypes.byref(h)))
+        self.handle = h
+        info = _lib.Info()
+        _lib.check(self.lib.jxb_plan_info(h, ctypes.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in _lib.Info._fields_}
+        self.n_dofs = info.n_dofs
+        self.n_qp = info.n_qp
+        self.nqe = len(T[0])
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.jxb_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ThbGeometry:
+    """Gauss-point coordinates, weights and field interpolation on a
+    HierarchicalSpace (the read-back of src/jaxiga/post/solution.py:39-50 at
+    the interior Gauss set), from the host point data."""
+
+    def __init__(self, space):
+        import torch
+
+        self.space = space
+        _, _, self.x, self.w = point_data(space)
+        T, _ = reference_tables(space.dim, space.degree[0])
+        self.B = T[0]
+        self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
+
+    def qp_coords(self):
+        import torch
+
+        return torch.as_tensor(self.x)
+
+    def qp_weights(self):
+        import torch
+
+        return torch.as_tensor(self.w)
+
+    def interpolate(self, coef):
+        """u(x_q) = sum_i u_i R_i(x_q) per element, (n_e, nq, ncomp)."""
+        import torch
+
+        s = self.space
+        c = np.asarray(coef.cpu().numpy() if hasattr(coef, "cpu") else coef, dtype=float).reshape(s.n_scalar_basis, -1)
+        c = np.concatenate([c, np.zeros((1, c.shape[1]))])
+        w = np.concatenate([s.wgts, np.zeros(1)])
+        N = np.einsum("eia,qa->eqi", s.extraction, self.B)  # B-spline values of each element's functions
+        M = N * w[s.elem_dofs][:, None, :]
+        Wq = M.sum(-1)
+        return torch.as_tensor(np.einsum("eqi,eic->eqc", M, c[s.elem_dofs]) / Wq[..., None])
+
+    def close(self):
+        pass
+
+
+def _bind_operator_methods():
+    from .operator import Operator
+
+    for name in ("_vec", "_empty", "apply", "diag", "load", "dot", "_opts", "pcg"):
+        setattr(ThbOperator, name, getattr(Operator, name))
+
+
+_bind_operator_methods()

@@ -177,7 +177,7 @@ def test_struct_layouts_match_header(tmp_path):
     if cc is None:
         pytest.skip("no C compiler")
     structs = {"jxb_desc": _lib.Desc, "jxb_info": _lib.Info, "jxb_solve_opts": _lib.SolveOpts, "jxb_stats": _lib.Stats,
-               "jxb_transfer1d": _lib.Transfer1d}
+               "jxb_transfer1d": _lib.Transfer1d, "jxb_thb_desc": _lib.ThbDesc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "jxb.h"', "int main(void){"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
