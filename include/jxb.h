@@ -286,7 +286,8 @@ int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_t
                   const uint8_t* prescribed, jxb_plan** out);
 
 /* ---- truncated hierarchical (THB) spaces -----------------------------------
- * Poisson, -div(a grad u) = f, on a space in the padded-element form of the
+ * Poisson, -div(a grad u) = f, or isotropic linear elasticity (src/jaxiga/forms/
+ * library.py:174-181) on a space in the padded-element form of the
  * reference (src/jaxiga/space/function_space.py:23-38, built by
  * src/jaxiga/space/hierarchical.py:891-980): per leaf element, n_local_max
  * hierarchical functions (padding index n_scalar) and the extraction rows
@@ -300,17 +301,22 @@ int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_t
  *   tables     (dim + 1, nq, nb): Bernstein values, then the derivative along
  *              each reference direction, at the nq = (degree + 1)^dim Gauss
  *              points (first direction fastest);
- *   factors    (n_elem, nq, nf), nf = (dim + 1)(dim + 2) / 2: per point the
- *              symmetric metric M = a w L^T L of the channels (numerator value,
- *              its reference gradient), L = J^-T (1/W) [-grad W / W | I],
- *              packed upper triangle row by row;
+ *   factors    (n_elem, nq, nf), Poisson: nf = (dim + 1)(dim + 2) / 2, per point
+ *              the symmetric metric M = a w L^T L of the channels (numerator
+ *              value, its reference gradient), L = J^-T (1/W) [-grad W / W | I],
+ *              packed upper triangle row by row; elasticity: nf = dim^2 + 2 +
+ *              dim, per point J^-1 (row-major, [a][k] = d xi_a / d x_k in
+ *              reference coordinates), w |J|, 1/W and grad W / W;
  *   wq         (n_elem, nq): quadrature weight over the weight function W;
- *   prescribed (n_scalar) 1 = Dirichlet DOF, or NULL.
- * The plan works with jxb_apply, jxb_diag, jxb_load (f_qp: (n_elem, nq)),
+ *   prescribed (n_scalar * vec) 1 = Dirichlet DOF, or NULL.
+ * DOF c of function i is vec * i + c. The plan works with jxb_apply, jxb_diag,
+ * jxb_load (f_qp: (n_elem, nq, vec)),
  * jxb_dot, jxb_pcg and jxb_plan_destroy; the other entry points reject it. */
 typedef struct jxb_thb_desc {
   int dim, degree, n_local_max;
+  int op;                      /* JXB_OP_POISSON or JXB_OP_ELASTICITY (vec = dim) */
   int64_t n_elem, n_scalar;
+  double lam, mu;              /* elasticity: Lame parameters (plane stress or strain folded in) */
   const int64_t* elem_dofs;
   const double* extraction;
   const double* wgts;

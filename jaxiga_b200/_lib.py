@@ -56,8 +56,11 @@ class ThbDesc(ctypes.Structure):
         ("dim", ctypes.c_int),
         ("degree", ctypes.c_int),
         ("n_local_max", ctypes.c_int),
+        ("op", ctypes.c_int),
         ("n_elem", ctypes.c_int64),
         ("n_scalar", ctypes.c_int64),
+        ("lam", ctypes.c_double),
+        ("mu", ctypes.c_double),
         ("elem_dofs", ctypes.c_void_p),
         ("extraction", ctypes.c_void_p),
         ("wgts", ctypes.c_void_p),

@@ -25,15 +25,15 @@
 #include "jxb_internal.cuh"
 
 struct jxb_thb_data {
-  int nlm = 0, nb = 0, nq = 0, nf = 0;
+  int nlm = 0, nb = 0, nq = 0, nf = 0, vec = 1;
   long long* d_dofs = nullptr;   // (n_elem, nlm)
   double* d_ext = nullptr;       // (n_elem, nlm, nb)
   double* d_w = nullptr;         // (n_scalar + 1): weights, 0 at the padding index
   double* d_tab = nullptr;       // (dim + 1, nq, nb)
   double* d_fac = nullptr;       // (n_elem, nq, nf)
   double* d_wq = nullptr;        // (n_elem, nq)
-  double* d_yl = nullptr;        // (n_elem, nlm) element outputs
-  long long* d_sptr = nullptr;   // (n_scalar + 1)
+  double* d_yl = nullptr;        // (n_elem, nlm, vec) element outputs
+  long long* d_sptr = nullptr;   // (n_dofs + 1)
   long long* d_sidx = nullptr;   // element slots grouped by DOF, ascending
 };
 
@@ -43,8 +43,9 @@ namespace {
 constexpr int THB_THREADS = 128;
 
 struct ThbArgs {
-  long long n_elem, n;
-  int nlm, nb, nq, nf;
+  long long n_elem, n;  // n: scalar functions (the padding index)
+  int nlm, nb, nq, nf, vec;
+  double lam, mu;
   const long long* dofs;
   const double* ext;
   const double* w;
@@ -156,26 +157,196 @@ __global__ void __launch_bounds__(THB_THREADS) k_thb_diag(ThbArgs A) {
   }
 }
 
-// load: F_e[i] = w_i sum_a C[i][a] sum_q B_a(q) wq(q) f(q)
+// load: F_e[i][c] = w_i sum_a C[i][a] sum_q B_a(q) wq(q) f_c(q)
 __global__ void __launch_bounds__(THB_THREADS) k_thb_load(ThbArgs A, const double* __restrict__ f_qp) {
   extern __shared__ double sm[];
-  double* fb = sm;  // [nb]
+  double* fb = sm;  // [nb][vec]
+  const int V = A.vec;
   for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int a = threadIdx.x; a < A.nb; a += blockDim.x) {
+    for (int k = threadIdx.x; k < A.nb * V; k += blockDim.x) {
+      const int a = k / V, c = k - a * V;
       double s = 0.0;
-      for (int q = 0; q < A.nq; ++q) s += __ldg(A.tab + (size_t)q * A.nb + a) * A.wq[e * A.nq + q] * f_qp[e * A.nq + q];
-      fb[a] = s;
+      for (int q = 0; q < A.nq; ++q)
+        s += __ldg(A.tab + (size_t)q * A.nb + a) * A.wq[e * A.nq + q] * f_qp[(e * A.nq + q) * V + c];
+      fb[k] = s;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < A.nlm; i += blockDim.x) {
+    for (int k = threadIdx.x; k < A.nlm * V; k += blockDim.x) {
+      const int i = k / V, c = k - i * V;
       const long long g = dofs[i];
       double s = 0.0;
-      for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * fb[a];
-      A.yl[e * A.nlm + i] = g < A.n ? A.w[g] * s : 0.0;
+      for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * fb[a * V + c];
+      A.yl[e * A.nlm * V + k] = g < A.n ? A.w[g] * s : 0.0;
     }
     __syncthreads();
+  }
+}
+
+// Isotropic elasticity at one point. g[c][0] = numerator value, g[c][1 + a] its
+// reference gradient for component c; Fr (DIM^2 + 2 + DIM values) = J^-1 ([a][k]),
+// w |J|, 1/W, grad W / W. Writes the flux channels f[c][0..DIM] of the test
+// functions' (value, reference gradient), the quotient rule transposed.
+template <int DIM>
+__device__ __forceinline__ void thb_elastic_point(const double* __restrict__ Fr, double lam, double mu,
+                                                  const double (&g)[DIM][DIM + 1], double (&f)[DIM][DIM + 1]) {
+  double Ji[DIM][DIM];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a)
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) Ji[a][k] = Fr[a * DIM + k];
+  const double om = Fr[DIM * DIM], iW = Fr[DIM * DIM + 1];
+  const double* gW = Fr + DIM * DIM + 2;
+  double Gx[DIM][DIM];  // du_c / dx_k
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    double gp[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) gp[a] = (g[c][1 + a] - g[c][0] * gW[a]) * iW;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) s += Ji[a][k] * gp[a];
+      Gx[c][k] = s;
+    }
+  }
+  double tr = 0.0;
+#pragma unroll
+  for (int k = 0; k < DIM; ++k) tr += Gx[k][k];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    double S[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) S[k] = om * (mu * (Gx[c][k] + Gx[k][c]) + (c == k ? lam * tr : 0.0));
+    double fv = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      double Fa = 0.0;
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) Fa += S[k] * Ji[a][k];
+      f[c][1 + a] = Fa * iW;
+      fv -= Fa * gW[a];
+    }
+    f[c][0] = fv * iW;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(THB_THREADS)
+    k_thb_apply_el(ThbArgs A, const double* __restrict__ x, int masked, const CgState* st) {
+  if (st && st->done) return;
+  constexpr int NC = DIM + 1;
+  extern __shared__ double sm[];
+  double* loc = sm;                // [nlm][DIM]  w_i u_ic
+  double* cb = loc + A.nlm * DIM;  // [nb][DIM]   numerator coefficients, then the residual
+  double* fl = cb + A.nb * DIM;    // [DIM][NC][nq] fluxes
+  const int tid = threadIdx.x;
+  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+    const long long* dofs = A.dofs + e * A.nlm;
+    const double* C = A.ext + e * A.nlm * A.nb;
+    for (int k = tid; k < A.nlm * DIM; k += blockDim.x) {
+      const int i = k / DIM, c = k - i * DIM;
+      const long long g = dofs[i];
+      double v = 0.0;
+      if (g < A.n) {
+        const long long d = g * DIM + c;
+        if (!(masked && !A.keep[d])) v = A.w[g] * x[d];
+      }
+      loc[k] = v;
+    }
+    __syncthreads();
+    for (int k = tid; k < A.nb * DIM; k += blockDim.x) {
+      const int a = k / DIM, c = k - a * DIM;
+      double s = 0.0;
+      for (int i = 0; i < A.nlm; ++i) s += C[i * A.nb + a] * loc[i * DIM + c];
+      cb[k] = s;
+    }
+    __syncthreads();
+    for (int q = tid; q < A.nq; q += blockDim.x) {
+      double g[DIM][NC];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) g[c][ch] = 0.0;
+      for (int a = 0; a < A.nb; ++a) {
+        double t[NC];
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) t[ch] = __ldg(A.tab + ((size_t)ch * A.nq + q) * A.nb + a);
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+          const double v = cb[a * DIM + c];
+#pragma unroll
+          for (int ch = 0; ch < NC; ++ch) g[c][ch] += t[ch] * v;
+        }
+      }
+      double f[DIM][NC];
+      thb_elastic_point<DIM>(A.fac + (e * A.nq + q) * A.nf, A.lam, A.mu, g, f);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) fl[(c * NC + ch) * A.nq + q] = f[c][ch];
+    }
+    __syncthreads();
+    for (int k = tid; k < A.nb * DIM; k += blockDim.x) {
+      const int a = k / DIM, c = k - a * DIM;
+      double s = 0.0;
+      for (int q = 0; q < A.nq; ++q)
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) s += __ldg(A.tab + ((size_t)ch * A.nq + q) * A.nb + a) * fl[(c * NC + ch) * A.nq + q];
+      cb[k] = s;  // every thread is past its reads of cb (the barrier above)
+    }
+    __syncthreads();
+    for (int k = tid; k < A.nlm * DIM; k += blockDim.x) {
+      const int i = k / DIM, c = k - i * DIM;
+      const long long g = dofs[i];
+      double s = 0.0;
+      for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * cb[a * DIM + c];
+      A.yl[e * A.nlm * DIM + k] = g < A.n ? A.w[g] * s : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+// diag K_e for elasticity: w_i^2 sum_q w |J| ((lam + mu) gx_c^2 + mu |gx|^2), gx the
+// physical gradient of R_i / w_i with the quotient rule
+template <int DIM>
+__global__ void __launch_bounds__(THB_THREADS) k_thb_diag_el(ThbArgs A) {
+  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+    const long long* dofs = A.dofs + e * A.nlm;
+    const double* C = A.ext + e * A.nlm * A.nb;
+    for (int i = threadIdx.x; i < A.nlm; i += blockDim.x) {
+      const long long g = dofs[i];
+      double d[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) d[c] = 0.0;
+      for (int q = 0; q < A.nq; ++q) {
+        double G[DIM + 1];
+#pragma unroll
+        for (int ch = 0; ch <= DIM; ++ch) {
+          const double* T = A.tab + ((size_t)ch * A.nq + q) * A.nb;
+          double s = 0.0;
+          for (int a = 0; a < A.nb; ++a) s += __ldg(T + a) * C[i * A.nb + a];
+          G[ch] = s;
+        }
+        const double* Fr = A.fac + (e * A.nq + q) * A.nf;
+        const double om = Fr[DIM * DIM], iW = Fr[DIM * DIM + 1];
+        double gx[DIM], n2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+          double s = 0.0;
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) s += Fr[a * DIM + k] * (G[1 + a] - G[0] * Fr[DIM * DIM + 2 + a]) * iW;
+          gx[k] = s;
+          n2 += s * s;
+        }
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) d[c] += om * ((A.lam + A.mu) * gx[c] * gx[c] + A.mu * n2);
+      }
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) A.yl[(e * A.nlm + i) * DIM + c] = g < A.n ? A.w[g] * A.w[g] * d[c] : 0.0;
+    }
   }
 }
 
@@ -218,6 +389,9 @@ static ThbArgs thb_args(jxb_plan* plan) {
   A.nb = T->nb;
   A.nq = T->nq;
   A.nf = T->nf;
+  A.vec = T->vec;
+  A.lam = plan->mat.lam;
+  A.mu = plan->mat.mu;
   A.dofs = T->d_dofs;
   A.ext = T->d_ext;
   A.w = T->d_w;
@@ -236,20 +410,35 @@ int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const 
   jxb_thb_data* T = plan->thb;
   ThbArgs A = thb_args(plan);
   const unsigned grid = thb_grid(plan->n_elem);
+  const bool el = plan->op == JXB_OP_ELASTICITY;
+  const int V = T->vec, NC = plan->dim + 1;
   if (mode == MODE_APPLY) {
-    const size_t sm = (size_t)(T->nlm + T->nb + (plan->dim + 1) * T->nq) * sizeof(double);
-    if (plan->dim == 2)
+    const size_t sm = (size_t)((T->nlm + T->nb) * V + V * NC * T->nq) * sizeof(double);
+    if (sm > 48 * 1024) return fail(JXB_ERR_INVALID, "hierarchical plan: element too large for shared memory");
+    if (el) {
+      if (plan->dim == 2)
+        k_thb_apply_el<2><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+      else
+        k_thb_apply_el<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+    } else if (plan->dim == 2) {
       k_thb_apply<2><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
-    else
+    } else {
       k_thb_apply<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+    }
   } else if (mode == MODE_DIAG) {
-    if (plan->dim == 2)
+    if (el) {
+      if (plan->dim == 2)
+        k_thb_diag_el<2><<<grid, THB_THREADS, 0, s>>>(A);
+      else
+        k_thb_diag_el<3><<<grid, THB_THREADS, 0, s>>>(A);
+    } else if (plan->dim == 2) {
       k_thb_diag<2><<<grid, THB_THREADS, 0, s>>>(A);
-    else
+    } else {
       k_thb_diag<3><<<grid, THB_THREADS, 0, s>>>(A);
+    }
   } else if (mode == MODE_LOAD) {
     if (!f_qp) return fail(JXB_ERR_INVALID, "jxb_load: null f_qp");
-    k_thb_load<<<grid, THB_THREADS, (size_t)T->nb * sizeof(double), s>>>(A, f_qp);
+    k_thb_load<<<grid, THB_THREADS, (size_t)T->nb * V * sizeof(double), s>>>(A, f_qp);
   } else {
     return fail(JXB_ERR_INVALID, "hierarchical plans apply, load and give the diagonal only");
   }
@@ -287,29 +476,37 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   if (d->n_elem < 1 || d->n_scalar < 1 || d->n_local_max < 1 || !d->elem_dofs || !d->extraction || !d->wgts ||
       !d->tables || !d->factors || !d->wq)
     return fail(JXB_ERR_INVALID, "jxb_thb_create: bad sizes or null arrays");
+  if (d->op != JXB_OP_POISSON && d->op != JXB_OP_ELASTICITY)
+    return fail(JXB_ERR_INVALID, "jxb_thb_create: the Poisson and linear elasticity operators are supported");
   int nb = 1;
   for (int k = 0; k < d->dim; ++k) nb *= d->degree + 1;
-  const int nq = nb, nlm = d->n_local_max, nf = (d->dim + 1) * (d->dim + 2) / 2;
-  const long long ne = d->n_elem, n = d->n_scalar;
-  // the DOF -> element-slot lists, ascending slot order (the fixed summation order)
-  std::vector<long long> count(n + 1, 0);
+  const bool el = d->op == JXB_OP_ELASTICITY;
+  const int V = el ? d->dim : 1;
+  const int nq = nb, nlm = d->n_local_max;
+  const int nf = el ? d->dim * d->dim + 2 + d->dim : (d->dim + 1) * (d->dim + 2) / 2;
+  const long long ne = d->n_elem, n = d->n_scalar, nd = n * V;
+  // the DOF -> element-slot lists, ascending slot order (the fixed summation
+  // order); slot (e * nlm + i) * V + c holds component c of local function i
+  std::vector<long long> count(nd + 1, 0);
   for (long long k = 0; k < ne * nlm; ++k) {
     const long long g = d->elem_dofs[k];
     if (g < 0 || g > n) return fail(JXB_ERR_INVALID, "jxb_thb_create: elem_dofs entry out of range");
-    if (g < n) ++count[g + 1];
+    if (g < n)
+      for (int c = 0; c < V; ++c) ++count[g * V + c + 1];
   }
-  for (long long g = 0; g < n; ++g) count[g + 1] += count[g];
-  std::vector<long long> sidx(std::max<long long>(count[n], 1)), fill(count.begin(), count.end() - 1);
+  for (long long g = 0; g < nd; ++g) count[g + 1] += count[g];
+  std::vector<long long> sidx(std::max<long long>(count[nd], 1)), fill(count.begin(), count.end() - 1);
   for (long long k = 0; k < ne * nlm; ++k) {
     const long long g = d->elem_dofs[k];
-    if (g < n) sidx[fill[g]++] = k;
+    if (g < n)
+      for (int c = 0; c < V; ++c) sidx[fill[g * V + c]++] = k * V + c;
   }
   std::vector<double> w(n + 1, 0.0);
   for (long long g = 0; g < n; ++g) w[g] = d->wgts[g];
-  std::vector<uint8_t> keep(n, 1);
-  long long nfree = n;
+  std::vector<uint8_t> keep(nd, 1);
+  long long nfree = nd;
   if (d->prescribed)
-    for (long long g = 0; g < n; ++g)
+    for (long long g = 0; g < nd; ++g)
       if (d->prescribed[g]) {
         keep[g] = 0;
         --nfree;
@@ -323,20 +520,23 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   T->nb = nb;
   T->nq = nq;
   T->nf = nf;
+  T->vec = V;
   P->device = device;
   P->dim = d->dim;
-  P->vec = 1;
+  P->vec = V;
   P->p = d->degree;
   P->q = d->degree + 1;
-  P->op = JXB_OP_POISSON;
+  P->op = d->op;
   P->order = 1;
   P->nqe = nq;
   P->ngeo = nf;
   P->n_elem = ne;
   P->n_qp = ne * nq;
   P->n_scalar = n;
-  P->n_dofs = n;
+  P->n_dofs = nd;
   P->n_free = nfree;
+  P->mat.lam = el ? d->lam : 0.0;
+  P->mat.mu = el ? d->mu : 0.0;
   cudaError_t e = cudaSuccess;
   auto al = [&](void** p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 8));
@@ -350,10 +550,10 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   al((void**)&T->d_tab, (size_t)(d->dim + 1) * nq * nb * sizeof(double));
   al((void**)&T->d_fac, (size_t)ne * nq * nf * sizeof(double));
   al((void**)&T->d_wq, (size_t)ne * nq * sizeof(double));
-  al((void**)&T->d_yl, (size_t)ne * nlm * sizeof(double));
-  al((void**)&T->d_sptr, (n + 1) * sizeof(long long));
+  al((void**)&T->d_yl, (size_t)ne * nlm * V * sizeof(double));
+  al((void**)&T->d_sptr, (nd + 1) * sizeof(long long));
   al((void**)&T->d_sidx, sidx.size() * sizeof(long long));
-  al((void**)&P->d_keep, n);
+  al((void**)&P->d_keep, nd);
   al((void**)&P->d_red, (4 * JXB_RED_BLOCKS + 16) * sizeof(double));
   static_assert(sizeof(long long) == sizeof(int64_t), "int64 DOF indices");
   up(T->d_dofs, d->elem_dofs, ne * nlm * sizeof(long long));
@@ -362,9 +562,9 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   up(T->d_tab, d->tables, (size_t)(d->dim + 1) * nq * nb * sizeof(double));
   up(T->d_fac, d->factors, (size_t)ne * nq * nf * sizeof(double));
   up(T->d_wq, d->wq, (size_t)ne * nq * sizeof(double));
-  up(T->d_sptr, count.data(), (n + 1) * sizeof(long long));
+  up(T->d_sptr, count.data(), (nd + 1) * sizeof(long long));
   up(T->d_sidx, sidx.data(), sidx.size() * sizeof(long long));
-  up(P->d_keep, keep.data(), n);
+  up(P->d_keep, keep.data(), nd);
   if (e == cudaSuccess) e = cudaMemset(P->d_red, 0, (4 * JXB_RED_BLOCKS + 16) * sizeof(double));
   if (e != cudaSuccess) {
     free_thb(P);

@@ -1,4 +1,5 @@
-"""Device operator of Poisson problems on truncated hierarchical spaces.
+"""Device operator of Poisson and linear-elasticity problems on truncated
+hierarchical spaces.
 
 A ``HierarchicalSpace`` (hierarchical.py) has elements with different numbers
 of basis functions, so the tensor-product brick kernels do not apply. Its plan
@@ -14,7 +15,9 @@ determinant and inverse at the Gauss points of [-1, 1]^dim, the rational
 weight function W and its gradient, and from them the metric M = a w L^T L of
 the channels (numerator value, reference gradient) with L = J^-T (1/W)
 [-grad W / W | I] -- the quotient rule of src/jaxiga/space/evaluation.py:95-172
-folded into the operator, as the tensor kernels do.
+folded into the operator, as the tensor kernels do. For elasticity the device
+takes J^-1, w |J|, 1/W and grad W / W per point and forms the isotropic stress
+(src/jaxiga/forms/library.py:174-181, materials.py:53-112) itself.
 """
 
 from __future__ import annotations
@@ -62,9 +65,14 @@ def reference_tables(dim, p):
     return np.stack(T), wq
 
 
-def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096):
+def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096, op="poisson"):
     """(factors (n_e, nq, nf), w / W (n_e, nq), x (n_e, nq, dim), w (n_e, nq))
-    of every leaf element's Gauss points; ``a0`` scalar or (n_e, nq)."""
+    of every leaf element's Gauss points; ``a0`` scalar or (n_e, nq).
+
+    Poisson factors: the channel metric a w L^T L, packed upper triangle row by
+    row (nf = (dim+1)(dim+2)/2). Elasticity factors: J^-1 in reference
+    coordinates ([a][k] = d xi_a / d x_k), w |J|, 1/W, grad W / W
+    (nf = dim^2 + 2 + dim)."""
     dim, p = space.dim, space.degree[0]
     if space.dim_phys != dim:
         raise NotImplementedError("hierarchical operators need the physical and parametric dimensions equal")
@@ -72,15 +80,16 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096):
     hom = np.concatenate([space.cpts * space.wgts[:, None], space.wgts[:, None]], 1)
     hom = np.concatenate([hom, np.zeros((1, dim + 1))])  # the padding index reads zeros
     ne, nq = space.n_elems, len(gw)
-    nf = (dim + 1) * (dim + 2) // 2
+    el = op == "elasticity"
+    nf = dim * dim + 2 + dim if el else (dim + 1) * (dim + 2) // 2
     fac = np.zeros((ne, nq, nf))
     wqW = np.zeros((ne, nq))
     X = np.zeros((ne, nq, dim))
     W8 = np.zeros((ne, nq))
     iu = np.triu_indices(dim + 1)
     for lo in range(0, ne, chunk):
-        el = slice(lo, min(lo + chunk, ne))
-        Pb = np.einsum("eia,eik->eak", space.extraction[el], hom[space.elem_dofs[el]])  # Bernstein homogeneous net
+        sl = slice(lo, min(lo + chunk, ne))
+        Pb = np.einsum("eia,eik->eak", space.extraction[sl], hom[space.elem_dofs[sl]])  # Bernstein homogeneous net
         val = np.einsum("qa,eak->eqk", T[0], Pb)
         grd = np.einsum("cqa,eak->ecqk", T[1:], Pb)  # (e, dir, q, k)
         W = val[..., -1]
@@ -91,7 +100,7 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096):
         det = np.linalg.det(J)
         Ji = np.linalg.inv(J)       # (e, q, a, k) = (J^-1)[a][k]
         w = gw[None, :] * np.abs(det)
-        a = a0 if np.ndim(a0) == 0 else np.asarray(a0, dtype=float).reshape(ne, nq)[el]
+        a = a0 if np.ndim(a0) == 0 else np.asarray(a0, dtype=float).reshape(ne, nq)[sl]
         L = np.zeros(J.shape[:2] + (dim, dim + 1))
         iW = 1.0 / W
         dWq = np.moveaxis(dW, 1, -1)  # (e, q, a)
@@ -99,34 +108,42 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096):
             L[..., k, 0] = -np.einsum("eqa,eqa->eq", Ji[..., :, k], dWq) * iW * iW
             for c in range(dim):
                 L[..., k, 1 + c] = Ji[..., c, k] * iW
-        M = (a * w)[..., None, None] * np.einsum("eqkr,eqks->eqrs", L, L)
-        fac[el] = M[..., iu[0], iu[1]]
-        wqW[el] = w * iW
-        X[el] = x
-        W8[el] = w
+        if el:
+            fac[sl] = np.concatenate([Ji.reshape(Ji.shape[:2] + (dim * dim,)), w[..., None], iW[..., None],
+                                      dWq * iW[..., None]], axis=-1)
+        else:
+            M = (a * w)[..., None, None] * np.einsum("eqkr,eqks->eqrs", L, L)
+            fac[sl] = M[..., iu[0], iu[1]]
+        wqW[sl] = w * iW
+        X[sl] = x
+        W8[sl] = w
     return fac, wqW, X, W8
 
 
 class ThbOperator:
-    """Device Poisson operator on a HierarchicalSpace (``jxb_thb_create``):
-    apply, diagonal, load, dot and Jacobi-PCG on the hierarchical DOFs."""
+    """Device Poisson (coef (a0,)) or linear-elasticity (coef (E, nu), vec = dim)
+    operator on a HierarchicalSpace (``jxb_thb_create``): apply, diagonal,
+    load, dot and Jacobi-PCG on the hierarchical DOFs."""
 
     def __init__(self, space, op="poisson", coef=(1.0,), prescribed=None, coef_qp=None, want_f32=False,
                  plane_strain=False):
         import torch
 
-        if op != "poisson" or space.vec != 1:
-            raise NotImplementedError("hierarchical spaces run the Poisson operator (vec = 1)")
+        if not ((op == "poisson" and space.vec == 1) or (op == "elasticity" and space.vec == space.dim)):
+            raise NotImplementedError("hierarchical spaces run the Poisson (vec = 1) and linear elasticity "
+                                      "(vec = dim) operators")
+        if op == "elasticity" and coef_qp is not None:
+            raise NotImplementedError("elasticity on hierarchical spaces takes constant E and nu")
         if want_f32:
             raise NotImplementedError("hierarchical operators run in FP64")
         if not torch.cuda.is_available():
             raise RuntimeError("the B200 solver needs a CUDA device; none is visible")
         self.lib = _lib.load()
-        self.space, self.op, self.vec = space, op, 1
+        self.space, self.op, self.vec = space, op, space.vec
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.want_f32, self.tile = False, None
         a0 = float(coef[0]) if coef_qp is None else np.asarray(coef_qp, dtype=float)
-        fac, wqW, X, W = point_data(space, a0)
+        fac, wqW, X, W = point_data(space, a0, op=op)
         self.qp_x, self.qp_w = X, W
         T, _ = reference_tables(space.dim, space.degree[0])
         keep = [np.ascontiguousarray(space.elem_dofs, dtype=np.int64), np.ascontiguousarray(space.extraction),
@@ -138,6 +155,12 @@ class ThbOperator:
         d = _lib.ThbDesc()
         d.dim, d.degree, d.n_local_max = space.dim, space.degree[0], space.n_local_max
         d.n_elem, d.n_scalar = space.n_elems, space.n_scalar_basis
+        d.op = 1 if op == "elasticity" else 0
+        if op == "elasticity":  # the tensor plan's Lame pair (plane stress unless plane strain)
+            E, nu = float(coef[0]), float(coef[1])
+            d.mu = E / (2.0 * (1.0 + nu))
+            d.lam = (E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)) if space.dim == 3 or plane_strain
+                     else E * nu / (1.0 - nu * nu))
         d.elem_dofs, d.extraction, d.wgts, d.tables, d.factors, d.wq = [k.ctypes.data for k in keep]
         d.prescribed = pm.ctypes.data
         h = ctypes.c_void_p()

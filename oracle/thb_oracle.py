@@ -79,3 +79,30 @@ def assemble_poisson(S, a0, prescribed, source_qp=None, chunk=1024):
     free = np.setdiff1d(np.arange(n), np.asarray(prescribed, dtype=np.int64))
     K_ff = K[free][:, free].tocsr()
     return K_ff, F[:n], free, np.concatenate(xs), np.concatenate(ws)
+
+
+def assemble_elasticity(S, E, nu, prescribed, source_qp=None, chunk=512):
+    """(K_ff CSR, F on all DOFs, free DOFs) of small-strain isotropic
+    elasticity (library.py:174-181, plane stress in 2D) on the THB space ``S``
+    with vec = dim; ``source_qp`` (n_e, n_q, dim). DOF c of function i is
+    dim * i + c (function_space.py:300-312)."""
+    vec = S.dim
+    n = S.n_scalar * vec
+    rows, cols, vals = [], [], []
+    F = np.zeros(n + vec)
+    for lo in range(0, S.n_elems, chunk):
+        el = np.arange(lo, min(lo + chunk, S.n_elems))
+        basis = O.evaluate(S, el)
+        Ke = O.element_tangents("elasticity", basis, {"E": E, "nu": nu}, vec)
+        gd = (vec * S.elem_dofs[el][..., None] + np.arange(vec)).reshape(len(el), -1)
+        rows.append(np.repeat(gd, gd.shape[1], axis=1).ravel())
+        cols.append(np.tile(gd, (1, gd.shape[1])).ravel())
+        vals.append(Ke.ravel())
+        if source_qp is not None:
+            Fe = np.einsum("eq,eqc,eqi->eic", basis["w"], np.asarray(source_qp)[el], basis["R"]).reshape(len(el), -1)
+            np.add.at(F, gd.ravel(), Fe.ravel())
+    K = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n + vec, n + vec)).tocsr()[:n, :n]
+    K.sum_duplicates()
+    free = np.setdiff1d(np.arange(n), np.asarray(prescribed, dtype=np.int64))
+    return K[free][:, free].tocsr(), F[:n], free, K

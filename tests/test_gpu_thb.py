@@ -113,3 +113,66 @@ def test_adaptive_refinement_reduces_the_error():
     # marking on a 4 x 4 mesh leaves it within 1e-3 of the start, measured on a
     # B200); over the loop it falls well below the tensor-space error
     assert errs[2] < 0.5 * errs[0] and errs[2] < errs[1], errs
+
+
+def _elastic_spaces():
+    return {
+        "sq_p2": lambda: H.refine_elements(
+            jx.FunctionSpace(jx.primitives.quadrilateral(SQ).elevate(2).refine(2), vec=2), [0, 1, 4]),
+        "annulus_p3": lambda: H.refine_elements(
+            jx.FunctionSpace(jx.primitives.quarter_annulus(1.0, 2.0).elevate(3).refine(2), vec=2), [5, 6, 10]),
+        "cube_p2": lambda: H.refine_elements(
+            jx.FunctionSpace(jx.primitives.cuboid([0, 0, 0], [1, 1, 1]).elevate(2).refine(1), vec=3), [0, 1]),
+    }
+
+
+@pytest.mark.parametrize("tag", ["sq_p2", "annulus_p3", "cube_p2"])
+def test_elasticity_apply_diag_and_load_match_the_oracle(tag):
+    from jaxiga_b200.thb import ThbOperator
+
+    W = _elastic_spaces()[tag]()
+    d = W.dim
+    S = TO.ThbSpace.of(W)
+    n = W.n_dofs
+    rng = np.random.default_rng(11)
+    nq = (W.degree[0] + 1) ** d
+    f = rng.standard_normal((W.n_elems, nq, d))
+    _, F, _, K = TO.assemble_elasticity(S, 2.0, 0.3, np.zeros(0, dtype=np.int64), source_qp=f)
+    mask = np.zeros(n, bool)
+    mask[jx.expand_dofs(W.boundary(sorted(W.boundaries)[0]).dofs, d)] = True
+    op = ThbOperator(W, "elasticity", (2.0, 0.3), prescribed=mask)
+    try:
+        u = rng.standard_normal(n)
+        y = op.apply(u, masked=False).cpu().numpy()
+        ref = K @ u
+        assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max()
+        ym = op.apply(u).cpu().numpy()
+        refm = np.where(mask, 0.0, K @ np.where(mask, 0.0, u))
+        assert np.abs(ym - refm).max() <= 1e-12 * np.abs(refm).max()
+        dg = op.diag().cpu().numpy()
+        refd = np.where(mask, 0.0, K.diagonal())
+        assert np.abs(dg - refd).max() <= 1e-12 * np.abs(refd).max()
+        Fd = op.load(f.reshape(-1)).cpu().numpy()
+        assert np.abs(Fd - F).max() <= 1e-12 * np.abs(F).max()
+    finally:
+        op.close()
+
+
+def test_elasticity_solve_matches_the_oracle():
+    """A clamped plate under a body force on a refined THB space: jx.solve against
+    the oracle's SuperLU solution of the same assembled system."""
+    from oracle import iga_oracle as O
+
+    W = _elastic_spaces()["annulus_p3"]()
+    problem = jx.LinearElasticity(W, dirichlet=[jx.DirichletBC([0.0, 0.0], where="sym_x")],
+                                  source=lambda x, p: np.array([0.1 * np.ones_like(x[0]), -1.0 * np.ones_like(x[0])]))
+    pres, vals = problem.resolve_dirichlet({})
+    sol = jx.solve(problem, params={"E": 2.0, "nu": 0.3}, linear=jx.LinearOptions(tol=1e-12))
+    assert sol.stats["converged"]
+    S = TO.ThbSpace.of(W)
+    nq = (W.degree[0] + 1) ** 2
+    f = np.broadcast_to(np.array([0.1, -1.0]), (W.n_elems, nq, 2))
+    K_ff, F, free, _ = TO.assemble_elasticity(S, 2.0, 0.3, pres, source_qp=f)
+    u = np.zeros(W.n_dofs)
+    u[free] = O.scipy_superlu(K_ff, F[free])
+    assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
