@@ -222,6 +222,38 @@ class ThbGeometry:
         Wq = M.sum(-1)
         return torch.as_tensor(np.einsum("eqi,eic->eqc", M, c[s.elem_dofs]) / Wq[..., None])
 
+    def interpolate_grad(self, coef):
+        """Physical gradients of a control-point field at the Gauss points,
+        (n_e, nq, ncomp, dim): the quotient rule of R_i = w_i N_i / W, mapped by
+        J^-T (evaluation.py:95-152)."""
+        import torch
+
+        s = self.space
+        dim = s.dim
+        c = np.asarray(coef.cpu().numpy() if hasattr(coef, "cpu") else coef, dtype=float).reshape(s.n_scalar_basis, -1)
+        c = np.concatenate([c, np.zeros((1, c.shape[1]))])
+        w = np.concatenate([s.wgts, np.zeros(1)])
+        T, _ = reference_tables(dim, s.degree[0])
+        wl = w[s.elem_dofs]                                               # (e, i)
+        M = np.einsum("eia,qa->eqi", s.extraction, T[0]) * wl[:, None]    # w_i N_i
+        dM = np.einsum("eia,dqa->edqi", s.extraction, T[1:]) * wl[:, None, None]
+        W = M.sum(-1)
+        dW = dM.sum(-1)                                                   # (e, d, q)
+        cl = c[s.elem_dofs]                                               # (e, i, ncomp)
+        num = np.einsum("eqi,eic->eqc", M, cl)
+        dnum = np.einsum("edqi,eic->edqc", dM, cl)
+        gref = (dnum - num[:, None] * (dW / W[:, None])[..., None]) / W[:, None, :, None]  # (e, d, q, c)
+        hom = np.concatenate([s.cpts * s.wgts[:, None], s.wgts[:, None]], 1)
+        hom = np.concatenate([hom, np.zeros((1, dim + 1))])
+        Pb = np.einsum("eia,eik->eak", s.extraction, hom[s.elem_dofs])
+        val = np.einsum("qa,eak->eqk", T[0], Pb)
+        grd = np.einsum("cqa,eak->ecqk", T[1:], Pb)
+        x = val[..., :-1] / val[..., -1:]
+        J = np.moveaxis((grd[..., :-1] - x[:, None] * grd[..., -1:]) / val[:, None, :, -1:], 1, -1)  # (e, q, i, a)
+        Ji = np.linalg.inv(J)                                             # (e, q, a, k)
+        # grad_x u_c[k] = sum_a Ji[a][k] d u_c / d xi_a
+        return torch.as_tensor(np.einsum("eqak,eaqc->eqck", Ji, gref))
+
     def close(self):
         pass
 

@@ -78,6 +78,13 @@ def test_solve_matches_the_reference_superlu(tag):
     assert sol.stats["converged"] and sol.stats["relative_residual"] <= 1e-12
     ref = G[f"{tag}/u"]
     assert np.linalg.norm(sol.u - ref) <= 1e-9 * np.linalg.norm(ref)
+    if tag == "sq_p3_deep":  # the read-back path: relative L2 and H1 errors against the exact solution
+        a0 = float(G[f"{tag}/a0"])  # -a0 lap u = 8 pi^2 sin sin: u = sin sin / a0
+        exact = lambda x: np.sin(2 * np.pi * x[:, 0]) * np.sin(2 * np.pi * x[:, 1]) / a0  # noqa: E731
+        grad = lambda x: 2 * np.pi / a0 * np.stack([np.cos(2 * np.pi * x[:, 0]) * np.sin(2 * np.pi * x[:, 1]),  # noqa
+                                                    np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1])], -1)
+        l2, h1 = jx.errornorm(sol, exact, "L2"), jx.errornorm(sol, exact, "H1", exact_grad=grad)
+        assert 0.0 < l2 < h1 < 0.1, (l2, h1)
 
 
 def test_adaptive_refinement_reduces_the_error():

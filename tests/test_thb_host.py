@@ -121,3 +121,24 @@ def test_refinement_argument_checks_and_bulk_marking():
     assert H.dorfler_mark(np.zeros(4)).size == 0
     with pytest.raises(ValueError):
         H.dorfler_mark(eta, 0.0)
+
+
+def test_gauss_point_values_and_gradients_match_the_oracle():
+    """The host read-back of a field on a THB space (values and physical
+    gradients at the Gauss points, used by errornorm and Solution.at) against
+    the oracle's basis on the same padded view."""
+    from jaxiga_b200.thb import ThbGeometry
+
+    for tag in ("sq_p3_deep", "annulus_p2", "cube_p2"):
+        W = CASES[tag]()
+        S = TO.ThbSpace.of(W)
+        b = O.evaluate(S, np.arange(W.n_elems))
+        c = np.random.default_rng(2).standard_normal((W.n_scalar_basis, 2))
+        cp = np.concatenate([c, np.zeros((1, 2))])[W.elem_dofs]  # (e, i, comp)
+        g = ThbGeometry(W)
+        val = g.interpolate(c).numpy()
+        assert np.abs(val - np.einsum("eqi,eic->eqc", b["R"], cp)).max() <= 1e-12
+        grad = g.interpolate_grad(c).numpy()
+        ref = np.einsum("eqdi,eic->eqcd", b["dR"], cp)
+        assert np.abs(grad - ref).max() <= 1e-11 * np.abs(ref).max()
+        assert np.abs(g.qp_coords().numpy() - b["x"]).max() <= 1e-13
