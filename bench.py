@@ -9,10 +9,12 @@ free DOFs) of the 3D linear-elasticity workload: unit cube, cubic NURBS,
 (1.34 GB) exceed the 126 MB L2, so consecutive steps stream them from HBM.
 ``value`` is whole-job DOF/s (N_dof x steps x n_gpus / max-over-ranks time,
 CUDA events, barrier + synchronize on both sides). ``e2e`` is the same metric
-through the C ABI with host buffers: pinned host u -> device, apply, device
-y -> pinned host, every step. ``time_to_solution`` gives the solves to a
-1e-8 true relative residual: plain FP64 Jacobi-PCG (with the reference CPU
-CG's true-residual restarts), the two mixed-precision schemes and, when
+through the C ABI with host buffers: every step copies u from pinned host
+memory to the device, applies K and copies y back to pinned host memory, the
+copies on their own streams overlapping the neighbouring steps' applies.
+``time_to_solution`` gives the solves to a 1e-8 true relative residual: plain
+FP64 Jacobi-PCG (with the reference CPU CG's true-residual restarts), the two
+mixed-precision schemes, multigrid-preconditioned CG and, when
 jaxiga_b200/checkpoints holds a trained network for the workload
 (``python -m jaxiga_b200.train_pc``), flexible CG with the learned
 preconditioner in every map.
@@ -23,15 +25,18 @@ time to solution): Darcy 96^3 with a lognormal random coefficient, the
 clamped Kirchhoff plate 256^2, and 256 uneven quarter-annulus Poisson
 instances solved as one batch.
 
-``cpu_baseline`` times the reference's CPU path on the host cores: SciPy's
-CSR K.u and its Jacobi-CG with true-residual restarts
+``cpu_baseline`` times the reference's CPU path on the host cores, all of
+them: SciPy's CSR K.u on whole rows of the 64^3 elasticity operator (its
+assembled matrix restricted to the control points of an element box, built
+from that box's element tangents; the full assembly is infeasible on a CPU,
+77 GB of element matrices), and its Jacobi-CG with true-residual restarts
 (src/jaxiga/solvers/linear.py:261-321, restated in the oracle) on the same
-elasticity workload at 16^3 elements -- the 64^3 assembled operator is
-infeasible on a CPU (its element matrices alone are 77 GB) -- next to the
-GPU's time to solution at that same size.
+workload at 16^3 elements, next to the GPU's time to solution at that size.
 
-``--impl reference`` times that CPU path alone for the headline metric: each
-step one SciPy CSR K.u of the 16^3 sample; the line adds its time to solution.
+``--impl reference`` times that CPU path alone for the headline metric, on
+the same config: each step one threaded SciPy CSR product of the 64^3 row
+sample (caches flushed before each); the line adds the CPU time to solution
+at 16^3 and 24^3.
 
 With ``--gpus N > 1`` (torchrun) every rank runs an independent replica of
 the headline workload (weak scaling; the single-patch apply does not
