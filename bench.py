@@ -481,6 +481,35 @@ def workload_tag(name, span):
     return f"plate2d_p4_{span}^2" if name == "plate" else f"{'darcy3d' if name == 'darcy' else 'elasticity3d'}_p3_{span}^3"
 
 
+_FP64_PEAK = {}
+
+
+def fp64_peak_tflops():
+    """FP64 dense throughput of this GPU, measured once per run: the best of 5
+    cuBLAS DGEMMs of 8192^3 (torch.matmul in float64; 2 n^3 flops), CUDA events.
+    MEASURED_PEAKS.json carries HBM and BF16 peaks only; the FP64-bound brick
+    kernels are compared with this."""
+    if "tflops" not in _FP64_PEAK:
+        import torch
+
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        c = a @ b
+        best = float("inf")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(5):
+            e0.record()
+            torch.matmul(a, b, out=c)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        _FP64_PEAK["tflops"] = 2 * n**3 / (best * 1e-3) / 1e12
+        del a, b, c
+        torch.cuda.empty_cache()
+    return _FP64_PEAK["tflops"]
+
+
 def roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span):
     """Per-kernel device times (CUDA events on the launching stream) and the
     HBM roofline of the brick kernel: algorithmic bytes = u and y once plus the
@@ -515,6 +544,8 @@ def roofline_of(op, name, V, n_qp, x, peaks, peak_kind, span):
         "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"), "kernel": kernel,
         "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": ms_bricks, "combine_ms": ms_combine,
         "fp64_tflops_achieved": flops / (ms_bricks * 1e-3) / 1e12, "flops_per_launch": flops,
+        "fp64_peak_tflops": fp64_peak_tflops(), "fp64_peak_source": "measured here: cuBLAS DGEMM 8192^3",
+        "fp64_frac": flops / (ms_bricks * 1e-3) / 1e12 / fp64_peak_tflops(),
         "f32_kernel_ms": ms_b32, "f32_achieved_gbs": alg_bytes32 / (ms_b32 * 1e-3) / 1e9,
     }
 
