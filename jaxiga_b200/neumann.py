@@ -37,7 +37,13 @@ def _stream():
 
 def side_centres(space, elems, sides):
     """Physical centre of the side each boundary element presents (problem.py:364-381)."""
+    from .hierarchical import HierarchicalSpace
     from .solve import geometry_operator
+
+    if isinstance(space, HierarchicalSpace):
+        from .thb import side_centres as thb_side_centres
+
+        return thb_side_centres(space, elems, sides)
 
     ref = np.zeros((len(elems), space.dim))
     for i, code in enumerate(sides):
@@ -66,6 +72,11 @@ def resolve_set(space, where):
         raise ValueError("Neumann predicate selected no boundary elements; it is evaluated at the physical "
                          "centre of each boundary element side")
     ke, ks = elems[mask], sides[mask]
+    from .hierarchical import HierarchicalSpace
+
+    if isinstance(space, HierarchicalSpace):  # padded element rows
+        ed = space.elem_dofs[ke]
+        return BoundarySet(ke, ks, np.unique(ed[ed < space.n_scalar_basis]))
     return BoundarySet(ke, ks, np.unique(space.element_dofs(ke)))
 
 
@@ -116,6 +127,12 @@ def neumann_load(op, problem, params, F=None):
         from .multipatch import neumann_load_multipatch
 
         return neumann_load_multipatch(op, problem, params, F)
+    from .hierarchical import HierarchicalSpace
+
+    if isinstance(space, HierarchicalSpace):
+        from .thb import neumann_load as thb_neumann_load
+
+        return thb_neumann_load(op, problem, params, F)
     for bc in problem.neumann:
         bset = resolve_set(space, bc.where)
         ps = boundary_gauss(space, bset, problem.quadrature)

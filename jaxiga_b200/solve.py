@@ -376,8 +376,6 @@ def solve(problem, *, method: str = "galerkin", params=None, linear: LinearOptio
     if isinstance(space, HierarchicalSpace):
         if linear.precision != "fp64" or linear.preconditioner not in ("jacobi", "none") or linear.method != "cg":
             raise NotImplementedError("hierarchical spaces solve with FP64 Jacobi-PCG")
-        if problem.neumann:
-            raise NotImplementedError("Neumann loads on hierarchical spaces")
 
     op, prescribed, values = _problem_operator(problem, params, fp32_operator)
     b = _rhs(problem, params, op, prescribed, values)

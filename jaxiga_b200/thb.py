@@ -65,6 +65,44 @@ def reference_tables(dim, p):
     return np.stack(T), wq
 
 
+def tables_at(pts, p):
+    """(dim + 1, n_pts, nb) table of the tensor Bernstein polynomials of degree
+    ``p`` and their reference derivatives at points ``pts`` (n_pts, dim) of
+    [-1, 1]^dim, functions first direction fastest (the order of
+    ``reference_tables``)."""
+    pts = np.asarray(pts, dtype=float)
+    dim = pts.shape[1]
+    B1 = [bernstein_basis(pts[:, d], p) for d in range(dim)]
+    D1 = [_bernstein_deriv(pts[:, d], p) for d in range(dim)]
+
+    def tensor(fs):
+        out = fs[0]
+        for d in range(1, dim):
+            out = np.einsum("qa,qb->qba", out, fs[d]).reshape(len(pts), -1)
+        return out
+
+    return np.stack([tensor(B1)] + [tensor([D1[d] if d == k else B1[d] for d in range(dim)]) for k in range(dim)])
+
+
+def _bernstein_geometry(space, elems, T):
+    """Geometry of the elements ``elems`` at the points of table ``T``: x
+    (e, q, dim), J (e, q, i, a) = d x_i / d xi_a in reference coordinates, the
+    weight function W (e, q) and its reference gradient (e, q, a), from the
+    Bernstein form of the homogeneous control net (each element's extraction
+    rows applied to its functions' (w P, w))."""
+    dim = space.dim
+    hom = np.concatenate([space.cpts * space.wgts[:, None], space.wgts[:, None]], 1)
+    hom = np.concatenate([hom, np.zeros((1, dim + 1))])  # the padding index reads zeros
+    Pb = np.einsum("eia,eik->eak", space.extraction[elems], hom[space.elem_dofs[elems]])
+    val = np.einsum("qa,eak->eqk", T[0], Pb)
+    grd = np.einsum("cqa,eak->ecqk", T[1:], Pb)  # (e, dir, q, k)
+    W = val[..., -1]
+    x = val[..., :-1] / W[..., None]
+    dW = grd[..., -1]  # (e, dir, q)
+    dx = (grd[..., :-1] - x[:, None] * dW[..., None]) / W[:, None, :, None]  # (e, dir a, q, i) = d x_i / d xi_a
+    return x, np.moveaxis(dx, 1, -1), W, np.moveaxis(dW, 1, -1)
+
+
 def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096, op="poisson"):
     """(factors (n_e, nq, nf), w / W (n_e, nq), x (n_e, nq, dim), w (n_e, nq))
     of every leaf element's Gauss points; ``a0`` scalar or (n_e, nq).
@@ -77,8 +115,6 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096, op="poisson"):
     if space.dim_phys != dim:
         raise NotImplementedError("hierarchical operators need the physical and parametric dimensions equal")
     T, gw = reference_tables(dim, p)
-    hom = np.concatenate([space.cpts * space.wgts[:, None], space.wgts[:, None]], 1)
-    hom = np.concatenate([hom, np.zeros((1, dim + 1))])  # the padding index reads zeros
     ne, nq = space.n_elems, len(gw)
     el = op == "elasticity"
     nf = dim * dim + 2 + dim if el else (dim + 1) * (dim + 2) // 2
@@ -89,21 +125,13 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096, op="poisson"):
     iu = np.triu_indices(dim + 1)
     for lo in range(0, ne, chunk):
         sl = slice(lo, min(lo + chunk, ne))
-        Pb = np.einsum("eia,eik->eak", space.extraction[sl], hom[space.elem_dofs[sl]])  # Bernstein homogeneous net
-        val = np.einsum("qa,eak->eqk", T[0], Pb)
-        grd = np.einsum("cqa,eak->ecqk", T[1:], Pb)  # (e, dir, q, k)
-        W = val[..., -1]
-        x = val[..., :-1] / W[..., None]
-        dW = grd[..., -1]  # (e, dir, q)
-        dx = (grd[..., :-1] - x[:, None] * dW[..., None]) / W[:, None, :, None]  # (e, dir a, q, i) = d x_i / d xi_a
-        J = np.moveaxis(dx, 1, -1)  # (e, q, i, a)
+        x, J, W, dWq = _bernstein_geometry(space, sl, T)
         det = np.linalg.det(J)
         Ji = np.linalg.inv(J)       # (e, q, a, k) = (J^-1)[a][k]
         w = gw[None, :] * np.abs(det)
         a = a0 if np.ndim(a0) == 0 else np.asarray(a0, dtype=float).reshape(ne, nq)[sl]
         L = np.zeros(J.shape[:2] + (dim, dim + 1))
         iW = 1.0 / W
-        dWq = np.moveaxis(dW, 1, -1)  # (e, q, a)
         for k in range(dim):
             L[..., k, 0] = -np.einsum("eqa,eqa->eq", Ji[..., :, k], dWq) * iW * iW
             for c in range(dim):
@@ -118,6 +146,28 @@ def point_data(space: HierarchicalSpace, a0=1.0, chunk=4096, op="poisson"):
         X[sl] = x
         W8[sl] = w
     return fac, wqW, X, W8
+
+
+def _create_plan(lib, space, elems, T, fac, wq, op, lam=0.0, mu=0.0, prescribed=None):
+    """``jxb_thb_create`` over the elements ``elems`` of ``space`` with the point
+    table ``T`` ((dim + 1, (p+1)^dim, nb)), per-point factors and weights w / W."""
+    keep = [np.ascontiguousarray(space.elem_dofs[elems], dtype=np.int64),
+            np.ascontiguousarray(space.extraction[elems], dtype=np.float64),
+            np.ascontiguousarray(space.wgts, dtype=np.float64), np.ascontiguousarray(T, dtype=np.float64),
+            np.ascontiguousarray(fac, dtype=np.float64), np.ascontiguousarray(wq, dtype=np.float64)]
+    d = _lib.ThbDesc()
+    d.dim, d.degree, d.n_local_max = space.dim, space.degree[0], space.n_local_max
+    d.n_elem, d.n_scalar = len(keep[0]), space.n_scalar_basis
+    d.op = 1 if op == "elasticity" else 0
+    d.lam, d.mu = lam, mu
+    d.elem_dofs, d.extraction, d.wgts, d.tables, d.factors, d.wq = [k.ctypes.data for k in keep]
+    pm = None
+    if prescribed is not None:
+        pm = np.ascontiguousarray(np.asarray(prescribed).astype(np.uint8))
+        d.prescribed = pm.ctypes.data
+    h = ctypes.c_void_p()
+    _lib.check(lib.jxb_thb_create(ctypes.byref(d), ctypes.byref(h)))
+    return h
 
 
 class ThbOperator:
@@ -146,25 +196,14 @@ class ThbOperator:
         fac, wqW, X, W = point_data(space, a0, op=op)
         self.qp_x, self.qp_w = X, W
         T, _ = reference_tables(space.dim, space.degree[0])
-        keep = [np.ascontiguousarray(space.elem_dofs, dtype=np.int64), np.ascontiguousarray(space.extraction),
-                np.ascontiguousarray(space.wgts, dtype=np.float64), np.ascontiguousarray(T),
-                np.ascontiguousarray(fac), np.ascontiguousarray(wqW)]
         self.prescribed_mask = (np.zeros(space.n_dofs, bool) if prescribed is None
                                 else np.asarray(prescribed).astype(bool).copy())
-        pm = np.ascontiguousarray(self.prescribed_mask.astype(np.uint8))
-        d = _lib.ThbDesc()
-        d.dim, d.degree, d.n_local_max = space.dim, space.degree[0], space.n_local_max
-        d.n_elem, d.n_scalar = space.n_elems, space.n_scalar_basis
-        d.op = 1 if op == "elasticity" else 0
+        lam = mu = 0.0
         if op == "elasticity":  # the tensor plan's Lame pair (plane stress unless plane strain)
             E, nu = float(coef[0]), float(coef[1])
-            d.mu = E / (2.0 * (1.0 + nu))
-            d.lam = (E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)) if space.dim == 3 or plane_strain
-                     else E * nu / (1.0 - nu * nu))
-        d.elem_dofs, d.extraction, d.wgts, d.tables, d.factors, d.wq = [k.ctypes.data for k in keep]
-        d.prescribed = pm.ctypes.data
-        h = ctypes.c_void_p()
-        _lib.check(self.lib.jxb_thb_create(ctypes.byref(d), ctypes.byref(h)))
+            mu = E / (2.0 * (1.0 + nu))
+            lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)) if space.dim == 3 or plane_strain else E * nu / (1.0 - nu * nu)
+        h = _create_plan(self.lib, space, slice(None), T, fac, wqW, op, lam, mu, self.prescribed_mask)
         self.handle = h
         info = _lib.Info()
         _lib.check(self.lib.jxb_plan_info(h, ctypes.byref(info)))
@@ -256,6 +295,90 @@ class ThbGeometry:
 
     def close(self):
         pass
+
+
+def side_points(space, elems, code, pts, wref):
+    """Boundary data of side ``code`` (2 direction + end) of the elements
+    ``elems`` at reference points ``pts`` (nq, dim) with weights ``wref``: x
+    (e, q, dim), the outward unit normal grad xi_d / |grad xi_d| signed by the
+    end, the surface weight wref |tangent| (2D) or wref |t1 x t2| (3D) in
+    reference coordinates, W, and the point table
+    (src/jaxiga/space/evaluation.py:174-193, 432-455)."""
+    dim = space.dim
+    T = tables_at(pts, space.degree[0])
+    x, J, W, _ = _bernstein_geometry(space, np.asarray(elems), T)
+    direction, end = divmod(int(code), 2)
+    nrm = np.linalg.inv(J)[:, :, direction, :]
+    nrm = nrm / np.linalg.norm(nrm, axis=-1, keepdims=True) * (1.0 if end == 1 else -1.0)
+    tang = [a for a in range(dim) if a != direction]
+    if dim == 2:
+        sj = np.linalg.norm(J[..., tang[0]], axis=-1)
+    else:
+        sj = np.linalg.norm(np.cross(J[..., tang[0]], J[..., tang[1]]), axis=-1)
+    return x, nrm, np.asarray(wref, dtype=float)[None, :] * sj, W, T
+
+
+def side_centres(space, elems, sides):
+    """Physical centre of the side each leaf element presents (problem.py:364-381)."""
+    elems, sides = np.asarray(elems, dtype=np.int64), np.asarray(sides, dtype=np.int64)
+    out = np.zeros((len(elems), space.dim))
+    for code in np.unique(sides):
+        sel = np.flatnonzero(sides == code)
+        direction, end = divmod(int(code), 2)
+        ref = np.zeros((1, space.dim))
+        ref[0, direction] = -1.0 if end == 0 else 1.0
+        out[sel] = _bernstein_geometry(space, elems[sel], tables_at(ref, space.degree[0]))[0][:, 0]
+    return out
+
+
+def neumann_load(op, problem, params, F):
+    """F plus the loads F_i,c = sum_q w t_c(x, n) R_i of every Neumann condition
+    of ``problem`` on a HierarchicalSpace (methods/_common.py:312-318).
+
+    The faces of one side code share their reference points, so each code's
+    faces become a plan of their own whose points are the face Gauss points
+    (zero-padded to the plan's (p+1)^dim rows: padded points have zero table
+    rows and zero weight): ``jxb_load`` integrates and the plan's fixed-order
+    combine scatters them, as it does the volume load."""
+    import torch
+
+    from .neumann import _call_traction, resolve_set
+    from .pointset import boundary_gauss
+
+    space = problem.space
+    dim, vec, p = space.dim, space.vec, space.degree[0]
+    nb = (p + 1) ** dim
+    kind = "elasticity" if vec > 1 else "poisson"
+    nf = dim * dim + 2 + dim if vec > 1 else (dim + 1) * (dim + 2) // 2
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for bc in problem.neumann:
+        ps = boundary_gauss(space, resolve_set(space, bc.where), problem.quadrature)
+        sides = np.asarray(ps.sides, dtype=np.int64)
+        for code in np.unique(sides):
+            sel = np.flatnonzero(sides == code)
+            elems = np.asarray(ps.elems, dtype=np.int64)[sel]
+            x, nrm, w, W, T = side_points(space, elems, code, ps.ref[sel[0]], ps.weights[sel[0]])
+            ne, nq = w.shape
+            if nq > nb:
+                raise NotImplementedError("boundary rules of more than (p+1)^(dim-1) points on hierarchical spaces")
+            t = _call_traction(bc.value, x.reshape(-1, dim), nrm.reshape(-1, dim), params, vec)
+            Tp = np.zeros((dim + 1, nb, nb))
+            Tp[:, :nq] = T
+            wq = np.zeros((ne, nb))
+            wq[:, :nq] = w / W
+            fq = np.zeros((ne, nb, vec))
+            fq[:, :nq] = t.reshape(ne, nq, vec)
+            h = _create_plan(op.lib, space, elems, Tp, np.zeros((ne, nb, nf)), wq, kind)
+            try:
+                f_dev = torch.as_tensor(fq.reshape(-1), device=op.device)
+                Fs = torch.empty(space.n_dofs, dtype=torch.float64, device=op.device)
+                _lib.check(op.lib.jxb_load(h, stream, ctypes.c_void_p(f_dev.data_ptr()),
+                                           ctypes.c_void_p(Fs.data_ptr())))
+                F += Fs
+                torch.cuda.current_stream().synchronize()
+            finally:
+                op.lib.jxb_plan_destroy(h)
+    return F
 
 
 def _bind_operator_methods():

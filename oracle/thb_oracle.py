@@ -106,3 +106,18 @@ def assemble_elasticity(S, E, nu, prescribed, source_qp=None, chunk=512):
     K.sum_duplicates()
     free = np.setdiff1d(np.arange(n), np.asarray(prescribed, dtype=np.int64))
     return K[free][:, free].tocsr(), F[:n], free, K
+
+
+def neumann_load(S, vec, elems, sides, ref, wref, traction):
+    """F_i,c = sum_q w t_c(x, n) R_i over boundary faces of the THB space ``S``
+    (the negative gradient of neumann_work, src/jaxiga/methods/_common.py:312-318),
+    the tensor oracle's boundary evaluation on the padded view; traction(x, n)
+    -> (n_pts, vec); DOF c of function i is vec * i + c, the padding entry is
+    dropped."""
+    b = O.evaluate_boundary(S, elems, sides, ref, wref)
+    nf, nq = b["w"].shape
+    t = np.asarray(traction(b["x"].reshape(-1, S.dim), b["normal"].reshape(-1, S.dim)), dtype=float)
+    Fe = np.einsum("fq,fqc,fqi->fic", b["w"], t.reshape(nf, nq, vec), b["R"])
+    F = np.zeros((S.n_scalar + 1, vec))
+    np.add.at(F, b["dofs"], Fe)
+    return F[:-1].ravel()

@@ -183,3 +183,91 @@ def test_elasticity_solve_matches_the_oracle():
     u = np.zeros(W.n_dofs)
     u[free] = O.scipy_superlu(K_ff, F[free])
     assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
+
+
+def _neumann_reference(W, problem, params):
+    """The oracle's Neumann load of every condition of ``problem`` on the padded view."""
+    from jaxiga_b200.neumann import resolve_set
+    from jaxiga_b200.pointset import boundary_gauss
+
+    S = TO.ThbSpace.of(W)
+    F = np.zeros(W.n_dofs)
+    for bc in problem.neumann:
+        ps = boundary_gauss(W, resolve_set(W, bc.where))
+        F += TO.neumann_load(S, W.vec, ps.elems, ps.sides, ps.ref, ps.weights,
+                             lambda x, n, bc=bc: bc.value(x, n, params))
+    return F
+
+
+def test_neumann_loads_match_the_oracle():
+    """Fluxes and tractions on labelled sides and on sides chosen by a predicate
+    over their centres: 2D Poisson, 2D elasticity and 3D Poisson on refined
+    THB spaces, against the oracle's boundary integration."""
+    import torch
+
+    from jaxiga_b200.neumann import neumann_load
+    from jaxiga_b200.thb import ThbOperator
+
+    cases = [
+        (_cases()["annulus_p2"](), lambda W: jx.Poisson(W, neumann=[
+            jx.Neumann(lambda x, n, p: np.sin(x[:, :1]) * n[:, :1] + p["g"], where="inner"),
+            jx.Neumann(lambda x, n, p: x[:, 1:2], where=lambda c: c[:, 0] > 1.2)]), "poisson", (1.0,)),
+        (_elastic_spaces()["annulus_p3"](), lambda W: jx.LinearElasticity(W, neumann=[
+            jx.Neumann(lambda x, n, p: -p["g"] * n, where="inner"),
+            jx.Neumann(lambda x, n, p: np.stack([-n[:, 1], n[:, 0]], 1) * x[:, :1], where="outer")]),
+         "elasticity", (2.0, 0.3)),
+        (_cases()["cube_p2"](), lambda W: jx.Poisson(W, neumann=[
+            jx.Neumann(lambda x, n, p: np.sin(x[:, 1:2]) * n[:, :1], where=lambda c: np.isclose(c[:, 0], 1.0))]),
+         "poisson", (1.0,)),
+    ]
+    params = {"g": 2.5}
+    for W, make, kind, coef in cases:
+        problem = make(W)
+        op = ThbOperator(W, kind, coef)
+        try:
+            F = neumann_load(op, problem, params, torch.zeros(W.n_dofs, dtype=torch.float64, device=op.device))
+            ref = _neumann_reference(W, problem, params)
+            assert np.abs(ref).max() > 0
+            assert np.abs(F.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+        finally:
+            op.close()
+
+
+def test_pressurised_thick_cylinder_on_a_refined_space():
+    """The reference's Lame cylinder (tests/test_examples.py:22-60) on a THB
+    space refined twice along the pressurised inner arc: the solve matches the
+    oracle's SuperLU solution of the same system and beats the unrefined
+    space's error against the closed-form displacement."""
+    from oracle import iga_oracle as O
+
+    r_i, r_o, q, E, nu = 1.0, 4.0, 10.0, 1e5, 0.3
+
+    def disp(pts):
+        r, th = np.hypot(pts[:, 0], pts[:, 1]), np.arctan2(pts[:, 1], pts[:, 0])
+        ur = q * r_i**2 * r / (E * (r_o**2 - r_i**2)) * ((1 - nu) + (1 + nu) * r_o**2 / r**2)
+        return np.stack([ur * np.cos(th), ur * np.sin(th)], axis=1)
+
+    def problem(W):
+        return jx.LinearElasticity(W, plane="stress",
+                                   dirichlet=[jx.DirichletBC(0.0, where="sym_y", component=1),
+                                              jx.DirichletBC(0.0, where="sym_x", component=0)],
+                                   neumann=[jx.Neumann(lambda x, n, p: -q * n, where="inner")])
+
+    V = jx.FunctionSpace(jx.primitives.quarter_annulus(r_i, r_o).elevate(3).refine(2), vec=2)
+    W = H.refine_elements(V, V.boundary("inner").elems)
+    W = H.refine_elements(W, W.boundary("inner").elems)
+    params = {"E": E, "nu": nu}
+    opts = jx.LinearOptions(tol=1e-12)
+    base = jx.solve(problem(V), params=params, linear=opts)
+    sol = jx.solve(problem(W), params=params, linear=opts)
+    assert sol.stats["converged"]
+    pr = problem(W)
+    pres, _ = pr.resolve_dirichlet({})
+    S = TO.ThbSpace.of(W)
+    K_ff, _, free, _ = TO.assemble_elasticity(S, E, nu, pres)
+    F = _neumann_reference(W, pr, params)
+    u = np.zeros(W.n_dofs)
+    u[free] = O.scipy_superlu(K_ff, F[free])
+    assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
+    e_ref, e_thb = jx.errornorm(base, disp, "L2"), jx.errornorm(sol, disp, "L2")
+    assert e_thb < 0.5 * e_ref, (e_thb, e_ref)

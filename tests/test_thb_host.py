@@ -142,3 +142,29 @@ def test_gauss_point_values_and_gradients_match_the_oracle():
         ref = np.einsum("eqdi,eic->eqcd", b["dR"], cp)
         assert np.abs(grad - ref).max() <= 1e-11 * np.abs(ref).max()
         assert np.abs(g.qp_coords().numpy() - b["x"]).max() <= 1e-13
+
+
+@pytest.mark.parametrize("tag", ["annulus_p2", "cube_p2", "sq_p3_deep"])
+def test_boundary_points_match_the_oracle(tag):
+    """Face points, outward normals and surface weights of every labelled side
+    (host side data of the Neumann load) against the oracle's boundary
+    evaluation on the padded view; side centres lie on the sides' points."""
+    from jaxiga_b200.pointset import boundary_gauss
+    from jaxiga_b200.thb import reference_tables, side_centres, side_points, tables_at
+
+    W = CASES[tag]()
+    S = TO.ThbSpace.of(W)
+    u = np.polynomial.legendre.leggauss(W.degree[0] + 1)[0]
+    grid = np.stack([g.ravel(order="F") for g in np.meshgrid(*([u] * W.dim), indexing="ij")], -1)
+    assert np.array_equal(tables_at(grid, W.degree[0]), reference_tables(W.dim, W.degree[0])[0])
+    for label in sorted(W.boundaries):
+        ps = boundary_gauss(W, W.boundary(label))
+        b = O.evaluate_boundary(S, ps.elems, ps.sides, ps.ref, ps.weights)
+        for code in np.unique(ps.sides):
+            sel = np.flatnonzero(ps.sides == code)
+            x, n, w, _, _ = side_points(W, ps.elems[sel], code, ps.ref[sel[0]], ps.weights[sel[0]])
+            assert np.abs(x - b["x"][sel]).max() < 1e-14
+            assert np.abs(n - b["normal"][sel]).max() < 1e-13
+            assert np.abs(w - b["w"][sel]).max() < 1e-14 * np.abs(b["w"]).max()
+        c = side_centres(W, ps.elems, ps.sides)
+        assert c.shape == (len(ps.elems), W.dim) and np.isfinite(c).all()
