@@ -300,13 +300,17 @@ int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_t
  *   wgts       (n_scalar) NURBS weights of the hierarchical basis;
  *   tables     (dim + 1, nq, nb): Bernstein values, then the derivative along
  *              each reference direction, at the nq = (degree + 1)^dim Gauss
- *              points (first direction fastest);
+ *              points (first direction fastest); the plate adds the second
+ *              derivatives 11, 12, 22: (6, nq, nb);
  *   factors    (n_elem, nq, nf), Poisson: nf = (dim + 1)(dim + 2) / 2, per point
  *              the symmetric metric M = a w L^T L of the channels (numerator
  *              value, its reference gradient), L = J^-T (1/W) [-grad W / W | I],
  *              packed upper triangle row by row; elasticity: nf = dim^2 + 2 +
  *              dim, per point J^-1 (row-major, [a][k] = d xi_a / d x_k in
- *              reference coordinates), w |J|, 1/W and grad W / W;
+ *              reference coordinates), w |J|, 1/W and grad W / W; plate:
+ *              nf = 21, the metric w L^T D L of the six channels (numerator
+ *              value, gradient, second derivatives) with L mapping them to the
+ *              curvatures -(R_xx, R_yy, 2 R_xy), packed the same way;
  *   wq         (n_elem, nq): quadrature weight over the weight function W;
  *   prescribed (n_scalar * vec) 1 = Dirichlet DOF, or NULL.
  * DOF c of function i is vec * i + c. The plan works with jxb_apply, jxb_diag,
@@ -314,7 +318,7 @@ int jxb_mp_create(jxb_plan* const* patches, int n, const int64_t* const* local_t
  * jxb_dot, jxb_pcg and jxb_plan_destroy; the other entry points reject it. */
 typedef struct jxb_thb_desc {
   int dim, degree, n_local_max;
-  int op;                      /* JXB_OP_POISSON or JXB_OP_ELASTICITY (vec = dim) */
+  int op;                      /* JXB_OP_POISSON, JXB_OP_ELASTICITY (vec = dim) or JXB_OP_PLATE (dim 2) */
   int64_t n_elem, n_scalar;
   double lam, mu;              /* elasticity: Lame parameters (plane stress or strain folded in) */
   const int64_t* elem_dofs;

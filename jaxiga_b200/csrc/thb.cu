@@ -1,4 +1,5 @@
-// Poisson on truncated hierarchical (THB) spaces: a plan over padded elements.
+// Poisson, linear elasticity and the Kirchhoff plate on truncated hierarchical
+// (THB) spaces: a plan over padded elements.
 //
 // The reference evaluates a hierarchical space with the tensor code through its
 // padded-element contract (src/jaxiga/space/function_space.py:23-38): element e
@@ -29,7 +30,7 @@ struct jxb_thb_data {
   long long* d_dofs = nullptr;   // (n_elem, nlm)
   double* d_ext = nullptr;       // (n_elem, nlm, nb)
   double* d_w = nullptr;         // (n_scalar + 1): weights, 0 at the padding index
-  double* d_tab = nullptr;       // (dim + 1, nq, nb)
+  double* d_tab = nullptr;       // (dim + 1, nq, nb); the plate's (6, nq, nb)
   double* d_fac = nullptr;       // (n_elem, nq, nf)
   double* d_wq = nullptr;        // (n_elem, nq)
   double* d_yl = nullptr;        // (n_elem, nlm, vec) element outputs
@@ -56,11 +57,13 @@ struct ThbArgs {
   double* yl;
 };
 
-template <int DIM>
+// NC channels per point: the numerator's value and reference gradient (Poisson,
+// NC = dim + 1) or, for the plate, value, gradient and second derivatives
+// (11, 12, 22): NC = 6; the metric M_q is packed, nf = NC (NC + 1) / 2.
+template <int NC>
 __global__ void __launch_bounds__(THB_THREADS)
     k_thb_apply(ThbArgs A, const double* __restrict__ x, int masked, const CgState* st) {
   if (st && st->done) return;
-  constexpr int NC = DIM + 1;
   extern __shared__ double sm[];
   double* loc = sm;             // [nlm]  w_i u_i
   double* cb = loc + A.nlm;     // [nb]   numerator coefficients, then the residual r_a
@@ -127,9 +130,8 @@ __global__ void __launch_bounds__(THB_THREADS)
 }
 
 // diag K_e: for function i, w_i^2 sum_q G_i(q)^T M_q G_i(q), G_i = the channels of N_i
-template <int DIM>
+template <int NC>
 __global__ void __launch_bounds__(THB_THREADS) k_thb_diag(ThbArgs A) {
-  constexpr int NC = DIM + 1;
   for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
@@ -411,7 +413,7 @@ int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const 
   ThbArgs A = thb_args(plan);
   const unsigned grid = thb_grid(plan->n_elem);
   const bool el = plan->op == JXB_OP_ELASTICITY;
-  const int V = T->vec, NC = plan->dim + 1;
+  const int V = T->vec, NC = plan->op == JXB_OP_PLATE ? 6 : plan->dim + 1;
   if (mode == MODE_APPLY) {
     const size_t sm = (size_t)((T->nlm + T->nb) * V + V * NC * T->nq) * sizeof(double);
     if (sm > 48 * 1024) return fail(JXB_ERR_INVALID, "hierarchical plan: element too large for shared memory");
@@ -420,10 +422,12 @@ int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const 
         k_thb_apply_el<2><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
       else
         k_thb_apply_el<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
-    } else if (plan->dim == 2) {
-      k_thb_apply<2><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
-    } else {
+    } else if (NC == 3) {
       k_thb_apply<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+    } else if (NC == 4) {
+      k_thb_apply<4><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+    } else {
+      k_thb_apply<6><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
     }
   } else if (mode == MODE_DIAG) {
     if (el) {
@@ -431,10 +435,12 @@ int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const 
         k_thb_diag_el<2><<<grid, THB_THREADS, 0, s>>>(A);
       else
         k_thb_diag_el<3><<<grid, THB_THREADS, 0, s>>>(A);
-    } else if (plan->dim == 2) {
-      k_thb_diag<2><<<grid, THB_THREADS, 0, s>>>(A);
-    } else {
+    } else if (NC == 3) {
       k_thb_diag<3><<<grid, THB_THREADS, 0, s>>>(A);
+    } else if (NC == 4) {
+      k_thb_diag<4><<<grid, THB_THREADS, 0, s>>>(A);
+    } else {
+      k_thb_diag<6><<<grid, THB_THREADS, 0, s>>>(A);
     }
   } else if (mode == MODE_LOAD) {
     if (!f_qp) return fail(JXB_ERR_INVALID, "jxb_load: null f_qp");
@@ -476,14 +482,16 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   if (d->n_elem < 1 || d->n_scalar < 1 || d->n_local_max < 1 || !d->elem_dofs || !d->extraction || !d->wgts ||
       !d->tables || !d->factors || !d->wq)
     return fail(JXB_ERR_INVALID, "jxb_thb_create: bad sizes or null arrays");
-  if (d->op != JXB_OP_POISSON && d->op != JXB_OP_ELASTICITY)
-    return fail(JXB_ERR_INVALID, "jxb_thb_create: the Poisson and linear elasticity operators are supported");
+  if (d->op != JXB_OP_POISSON && d->op != JXB_OP_ELASTICITY && !(d->op == JXB_OP_PLATE && d->dim == 2))
+    return fail(JXB_ERR_INVALID,
+                "jxb_thb_create: the Poisson, linear elasticity and (2D) Kirchhoff plate operators are supported");
   int nb = 1;
   for (int k = 0; k < d->dim; ++k) nb *= d->degree + 1;
-  const bool el = d->op == JXB_OP_ELASTICITY;
+  const bool el = d->op == JXB_OP_ELASTICITY, pl = d->op == JXB_OP_PLATE;
   const int V = el ? d->dim : 1;
   const int nq = nb, nlm = d->n_local_max;
-  const int nf = el ? d->dim * d->dim + 2 + d->dim : (d->dim + 1) * (d->dim + 2) / 2;
+  const int ntab = pl ? 6 : d->dim + 1;  // point tables: value, gradient (and second derivatives)
+  const int nf = el ? d->dim * d->dim + 2 + d->dim : ntab * (ntab + 1) / 2;
   const long long ne = d->n_elem, n = d->n_scalar, nd = n * V;
   // the DOF -> element-slot lists, ascending slot order (the fixed summation
   // order); slot (e * nlm + i) * V + c holds component c of local function i
@@ -527,7 +535,7 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   P->p = d->degree;
   P->q = d->degree + 1;
   P->op = d->op;
-  P->order = 1;
+  P->order = pl ? 2 : 1;
   P->nqe = nq;
   P->ngeo = nf;
   P->n_elem = ne;
@@ -547,7 +555,7 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   al((void**)&T->d_dofs, ne * nlm * sizeof(long long));
   al((void**)&T->d_ext, (size_t)ne * nlm * nb * sizeof(double));
   al((void**)&T->d_w, (n + 1) * sizeof(double));
-  al((void**)&T->d_tab, (size_t)(d->dim + 1) * nq * nb * sizeof(double));
+  al((void**)&T->d_tab, (size_t)ntab * nq * nb * sizeof(double));
   al((void**)&T->d_fac, (size_t)ne * nq * nf * sizeof(double));
   al((void**)&T->d_wq, (size_t)ne * nq * sizeof(double));
   al((void**)&T->d_yl, (size_t)ne * nlm * V * sizeof(double));
@@ -559,7 +567,7 @@ extern "C" int jxb_thb_create(const jxb_thb_desc* d, jxb_plan** out) {
   up(T->d_dofs, d->elem_dofs, ne * nlm * sizeof(long long));
   up(T->d_ext, d->extraction, (size_t)ne * nlm * nb * sizeof(double));
   up(T->d_w, w.data(), (n + 1) * sizeof(double));
-  up(T->d_tab, d->tables, (size_t)(d->dim + 1) * nq * nb * sizeof(double));
+  up(T->d_tab, d->tables, (size_t)ntab * nq * nb * sizeof(double));
   up(T->d_fac, d->factors, (size_t)ne * nq * nf * sizeof(double));
   up(T->d_wq, d->wq, (size_t)ne * nq * sizeof(double));
   up(T->d_sptr, count.data(), (nd + 1) * sizeof(long long));

@@ -65,11 +65,30 @@ def reference_tables(dim, p):
     return np.stack(T), wq
 
 
-def tables_at(pts, p):
+def _bernstein_deriv2(u, p):
+    """d^2/du^2 of the Bernstein polynomials on [-1, 1]: (p/2)(dB^{p-1}_{k-1} - dB^{p-1}_k)."""
+    if p < 2:
+        return np.zeros((len(u), p + 1))
+    lo = _bernstein_deriv(u, p - 1)
+    d = np.zeros((len(u), p + 1))
+    d[:, 1:] += lo
+    d[:, :-1] -= lo
+    return 0.5 * p * d
+
+
+def gauss_points(dim, p):
+    """The (p+1)^dim Gauss points of [-1, 1]^dim, first direction fastest, and their weights."""
+    u, _ = gauss_1d(p + 1)
+    pts = np.stack([g.ravel(order="F") for g in np.meshgrid(*([u] * dim), indexing="ij")], -1)
+    return pts, reference_tables(dim, p)[1]
+
+
+def tables_at(pts, p, order=1):
     """(dim + 1, n_pts, nb) table of the tensor Bernstein polynomials of degree
     ``p`` and their reference derivatives at points ``pts`` (n_pts, dim) of
     [-1, 1]^dim, functions first direction fastest (the order of
-    ``reference_tables``)."""
+    ``reference_tables``); ``order=2`` appends the second derivatives of the
+    pairs (a, b), a <= b, in row order (11, 12, 22 in 2D)."""
     pts = np.asarray(pts, dtype=float)
     dim = pts.shape[1]
     B1 = [bernstein_basis(pts[:, d], p) for d in range(dim)]
@@ -81,7 +100,13 @@ def tables_at(pts, p):
             out = np.einsum("qa,qb->qba", out, fs[d]).reshape(len(pts), -1)
         return out
 
-    return np.stack([tensor(B1)] + [tensor([D1[d] if d == k else B1[d] for d in range(dim)]) for k in range(dim)])
+    T = [tensor(B1)] + [tensor([D1[d] if d == k else B1[d] for d in range(dim)]) for k in range(dim)]
+    if order >= 2:
+        D2 = [_bernstein_deriv2(pts[:, d], p) for d in range(dim)]
+        for a in range(dim):
+            for b in range(a, dim):
+                T.append(tensor([(D2[d] if a == b else D1[d]) if d in (a, b) else B1[d] for d in range(dim)]))
+    return np.stack(T)
 
 
 def _bernstein_geometry(space, elems, T):
@@ -158,7 +183,7 @@ def _create_plan(lib, space, elems, T, fac, wq, op, lam=0.0, mu=0.0, prescribed=
     d = _lib.ThbDesc()
     d.dim, d.degree, d.n_local_max = space.dim, space.degree[0], space.n_local_max
     d.n_elem, d.n_scalar = len(keep[0]), space.n_scalar_basis
-    d.op = 1 if op == "elasticity" else 0
+    d.op = {"poisson": _lib.OP_POISSON, "elasticity": _lib.OP_ELASTICITY, "plate": _lib.OP_PLATE}[op]
     d.lam, d.mu = lam, mu
     d.elem_dofs, d.extraction, d.wgts, d.tables, d.factors, d.wq = [k.ctypes.data for k in keep]
     pm = None
@@ -170,6 +195,66 @@ def _create_plan(lib, space, elems, T, fac, wq, op, lam=0.0, mu=0.0, prescribed=
     return h
 
 
+def plate_point_data(space: HierarchicalSpace, E, nu, t, chunk=4096):
+    """(factors (n_e, nq, 21), w / W, x, w) of the Kirchhoff plate
+    (library.py:68-143) at every leaf element's Gauss points: per point the
+    metric w L^T D L of the six channels g = (n, n_1, n_2, n_11, n_12, n_22) of
+    the rational numerator n = sum_i w_i u_i N_i in reference coordinates, L
+    the linear map from g to the curvatures -(R_xx, R_yy, 2 R_xy), D the
+    bending stiffness E t^3 / (12 (1 - nu^2)) [[1, nu, 0], [nu, 1, 0], [0, 0,
+    (1 - nu) / 2]]. L is the second-order quotient rule of R = n / W followed
+    by the push-forward of second derivatives through the geometry's first
+    and second derivatives (evaluation.py:95-172)."""
+    if space.dim != 2 or space.vec != 1 or space.dim_phys != 2:
+        raise NotImplementedError("the Kirchhoff plate runs on 2D scalar spaces")
+    p = space.degree[0]
+    pts, gw = gauss_points(2, p)
+    T = tables_at(pts, p, order=2)  # (6, nq, nb)
+    D = E * t**3 / (12.0 * (1.0 - nu**2)) * np.array([[1.0, nu, 0.0], [nu, 1.0, 0.0], [0.0, 0.0, (1.0 - nu) / 2.0]])
+    pairs = [(0, 0), (0, 1), (1, 1)]
+    hom = np.concatenate([space.cpts * space.wgts[:, None], space.wgts[:, None]], 1)
+    hom = np.concatenate([hom, np.zeros((1, 3))])
+    ne, nq = space.n_elems, len(gw)
+    fac = np.zeros((ne, nq, 21))
+    wqW, X, W8 = np.zeros((ne, nq)), np.zeros((ne, nq, 2)), np.zeros((ne, nq))
+    iu = np.triu_indices(6)
+    for lo in range(0, ne, chunk):
+        sl = slice(lo, min(lo + chunk, ne))
+        Pb = np.einsum("eia,eik->eak", space.extraction[sl], hom[space.elem_dofs[sl]])
+        ch = np.einsum("cqa,eak->eqck", T, Pb)     # (e, q, channel, (wx, wy, w))
+        W = ch[:, :, 0, 2]
+        x = ch[:, :, 0, :2] / W[..., None]
+        Wa = ch[:, :, 1:3, 2]                       # (e, q, a)
+        xa = (ch[:, :, 1:3, :2] - Wa[..., None] * x[:, :, None]) / W[..., None, None]  # (e, q, a, i)
+        xab = np.stack([(ch[:, :, 3 + k, :2] - xa[:, :, a] * Wa[..., b, None] - xa[:, :, b] * Wa[..., a, None]
+                         - x * ch[:, :, 3 + k, 2, None]) / W[..., None] for k, (a, b) in enumerate(pairs)], 2)
+        e_, q_ = W.shape
+        iW = 1.0 / W
+        dR = np.zeros((e_, q_, 2, 6))   # reference first derivatives of R in the channels
+        d2R = np.zeros((e_, q_, 3, 6))  # reference second derivatives
+        for a in range(2):
+            dR[..., a, 0] = -Wa[..., a] * iW**2
+            dR[..., a, 1 + a] = iW
+        for k, (a, b) in enumerate(pairs):
+            d2R[..., k, 3 + k] = iW
+            d2R[..., k, 1 + a] -= Wa[..., b] * iW**2
+            d2R[..., k, 1 + b] -= Wa[..., a] * iW**2
+            d2R[..., k, 0] = -ch[:, :, 3 + k, 2] * iW**2 + 2.0 * Wa[..., a] * Wa[..., b] * iW**3
+        J = xa                                      # [a][i] = d x_i / d xi_a
+        dRx = np.linalg.solve(J, dR)                # physical gradient channels
+        Tm = np.zeros((e_, q_, 3, 3))
+        for r, (a, b) in enumerate(pairs):
+            for c, (i, j) in enumerate(pairs):
+                Tm[..., r, c] = J[..., a, i] * J[..., b, j] + (J[..., a, j] * J[..., b, i] if i != j else 0.0)
+        d2Rx = np.linalg.solve(Tm, d2R - np.einsum("eqki,eqin->eqkn", xab, dRx))  # (xx, xy, yy)
+        L = -np.stack([d2Rx[..., 0, :], d2Rx[..., 2, :], 2.0 * d2Rx[..., 1, :]], axis=2)
+        w = gw[None, :] * np.abs(np.linalg.det(J))
+        M = w[..., None, None] * np.einsum("eqsc,st,eqtd->eqcd", L, D, L)
+        fac[sl] = M[..., iu[0], iu[1]]
+        wqW[sl], X[sl], W8[sl] = w * iW, x, w
+    return fac, wqW, X, W8, T
+
+
 class ThbOperator:
     """Device Poisson (coef (a0,)) or linear-elasticity (coef (E, nu), vec = dim)
     operator on a HierarchicalSpace (``jxb_thb_create``): apply, diagonal,
@@ -179,9 +264,12 @@ class ThbOperator:
                  plane_strain=False):
         import torch
 
-        if not ((op == "poisson" and space.vec == 1) or (op == "elasticity" and space.vec == space.dim)):
-            raise NotImplementedError("hierarchical spaces run the Poisson (vec = 1) and linear elasticity "
-                                      "(vec = dim) operators")
+        if not ((op == "poisson" and space.vec == 1) or (op == "elasticity" and space.vec == space.dim)
+                or (op == "plate" and space.vec == 1 and space.dim == 2)):
+            raise NotImplementedError("hierarchical spaces run the Poisson (vec = 1), linear elasticity "
+                                      "(vec = dim) and 2D Kirchhoff plate operators")
+        if op == "plate" and coef_qp is not None:
+            raise NotImplementedError("the plate on hierarchical spaces takes constant E, nu and t")
         if op == "elasticity" and coef_qp is not None:
             raise NotImplementedError("elasticity on hierarchical spaces takes constant E and nu")
         if want_f32:
@@ -192,10 +280,13 @@ class ThbOperator:
         self.space, self.op, self.vec = space, op, space.vec
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.want_f32, self.tile = False, None
-        a0 = float(coef[0]) if coef_qp is None else np.asarray(coef_qp, dtype=float)
-        fac, wqW, X, W = point_data(space, a0, op=op)
+        if op == "plate":
+            fac, wqW, X, W, T = plate_point_data(space, float(coef[0]), float(coef[1]), float(coef[2]))
+        else:
+            a0 = float(coef[0]) if coef_qp is None else np.asarray(coef_qp, dtype=float)
+            fac, wqW, X, W = point_data(space, a0, op=op)
+            T, _ = reference_tables(space.dim, space.degree[0])
         self.qp_x, self.qp_w = X, W
-        T, _ = reference_tables(space.dim, space.degree[0])
         self.prescribed_mask = (np.zeros(space.n_dofs, bool) if prescribed is None
                                 else np.asarray(prescribed).astype(bool).copy())
         lam = mu = 0.0

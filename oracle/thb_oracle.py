@@ -81,6 +81,32 @@ def assemble_poisson(S, a0, prescribed, source_qp=None, chunk=1024):
     return K_ff, F[:n], free, np.concatenate(xs), np.concatenate(ws)
 
 
+def assemble_plate(S, E, nu, t, prescribed, source_qp=None, chunk=1024):
+    """(K_ff CSR, F on all DOFs, free DOFs) of the Kirchhoff plate
+    (library.py:68-143: K_e = sum_q w B^T D B, B = -(R_xx, R_yy, 2 R_xy)) on the
+    2D THB space ``S``, through the tensor oracle's second-derivative
+    evaluation on the padded view; ``source_qp`` (n_e, n_q) is the load."""
+    n = S.n_scalar
+    rows, cols, vals = [], [], []
+    F = np.zeros(n + 1)
+    for lo in range(0, S.n_elems, chunk):
+        el = np.arange(lo, min(lo + chunk, S.n_elems))
+        basis = O.evaluate(S, el, order=2)
+        Ke = O.element_tangents("plate", basis, {"E": E, "nu": nu, "t": t})
+        gd = S.elem_dofs[el]
+        rows.append(np.repeat(gd, gd.shape[1], axis=1).ravel())
+        cols.append(np.tile(gd, (1, gd.shape[1])).ravel())
+        vals.append(Ke.ravel())
+        if source_qp is not None:
+            Fe = np.einsum("eq,eq,eqi->ei", basis["w"], np.asarray(source_qp)[el], basis["R"])
+            np.add.at(F, gd.ravel(), Fe.ravel())
+    K = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n + 1, n + 1)).tocsr()[:n, :n]
+    K.sum_duplicates()
+    free = np.setdiff1d(np.arange(n), np.asarray(prescribed, dtype=np.int64))
+    return K[free][:, free].tocsr(), F[:n], free, K
+
+
 def assemble_elasticity(S, E, nu, prescribed, source_qp=None, chunk=512):
     """(K_ff CSR, F on all DOFs, free DOFs) of small-strain isotropic
     elasticity (library.py:174-181, plane stress in 2D) on the THB space ``S``

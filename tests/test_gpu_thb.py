@@ -271,3 +271,50 @@ def test_pressurised_thick_cylinder_on_a_refined_space():
     assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
     e_ref, e_thb = jx.errornorm(base, disp, "L2"), jx.errornorm(sol, disp, "L2")
     assert e_thb < 0.5 * e_ref, (e_thb, e_ref)
+
+
+@pytest.mark.parametrize("tag", ["sq_p2", "sq_p3_deep", "annulus_p2"])
+def test_plate_apply_diag_and_load_match_the_oracle(tag):
+    """The Kirchhoff plate (six channels per point) on THB spaces against the
+    oracle's assembly through its second-derivative evaluation."""
+    from jaxiga_b200.thb import ThbOperator
+
+    W = _cases()[tag]()
+    S = TO.ThbSpace.of(W)
+    n = W.n_scalar_basis
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((W.n_elems, (W.degree[0] + 1) ** 2))
+    _, F, _, K = TO.assemble_plate(S, 2.0, 0.3, 0.1, np.zeros(0, dtype=np.int64), source_qp=f)
+    mask = np.zeros(n, bool)
+    mask[W.boundary(sorted(W.boundaries)[0]).dofs] = True
+    op = ThbOperator(W, "plate", (2.0, 0.3, 0.1), prescribed=mask)
+    try:
+        u = rng.standard_normal(n)
+        ref = K @ u
+        assert np.abs(op.apply(u, masked=False).cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+        refm = np.where(mask, 0.0, K @ np.where(mask, 0.0, u))
+        assert np.abs(op.apply(u).cpu().numpy() - refm).max() <= 1e-12 * np.abs(refm).max()
+        refd = np.where(mask, 0.0, K.diagonal())
+        assert np.abs(op.diag().cpu().numpy() - refd).max() <= 1e-12 * np.abs(refd).max()
+        assert np.abs(op.load(f).cpu().numpy() - F).max() <= 1e-12 * np.abs(F).max()
+    finally:
+        op.close()
+
+
+def test_simply_supported_plate_solve_matches_the_oracle():
+    """A uniformly loaded, simply supported square plate on a THB space refined
+    towards a corner: jx.solve against the oracle's SuperLU solution."""
+    from oracle import iga_oracle as O
+
+    W = _cases()["sq_p3_deep"]()
+    ALL = lambda x: np.full(len(x), True)  # noqa: E731
+    problem = jx.KirchhoffPlate(W, dirichlet=[jx.DirichletBC(0.0, where=ALL)], source=lambda x, p: np.ones_like(x[0]))
+    params = {"E": 1e4, "nu": 0.3, "t": 0.1}
+    sol = jx.solve(problem, params=params, linear=jx.LinearOptions(tol=1e-12, maxiter=20000))
+    assert sol.stats["converged"]
+    pres, _ = problem.resolve_dirichlet(params)
+    nq = (W.degree[0] + 1) ** 2
+    K_ff, F, free, _ = TO.assemble_plate(TO.ThbSpace.of(W), 1e4, 0.3, 0.1, pres, source_qp=np.ones((W.n_elems, nq)))
+    u = np.zeros(W.n_scalar_basis)
+    u[free] = O.scipy_superlu(K_ff, F[free])
+    assert np.linalg.norm(sol.u - u) <= 1e-8 * np.linalg.norm(u)

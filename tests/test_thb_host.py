@@ -168,3 +168,26 @@ def test_boundary_points_match_the_oracle(tag):
             assert np.abs(w - b["w"][sel]).max() < 1e-14 * np.abs(b["w"]).max()
         c = side_centres(W, ps.elems, ps.sides)
         assert c.shape == (len(ps.elems), W.dim) and np.isfinite(c).all()
+
+
+@pytest.mark.parametrize("tag", ["sq_p2", "sq_p3_deep", "annulus_p2"])
+def test_plate_metric_reproduces_the_oracle_tangents(tag):
+    """The Kirchhoff plate's per-point metric (the channels of the rational
+    numerator mapped to the curvatures) contracted with the element's channel
+    values gives the oracle's element tangents (library.py:68-143), on the
+    rational annulus too."""
+    from jaxiga_b200.thb import plate_point_data
+
+    W = CASES[tag]()
+    fac, _, X, w, T = plate_point_data(W, 2.0, 0.3, 0.1)
+    iu = np.triu_indices(6)
+    M = np.zeros(fac.shape[:2] + (6, 6))
+    M[..., iu[0], iu[1]] = fac
+    M[..., iu[1], iu[0]] = fac
+    wl = np.concatenate([W.wgts, [0.0]])[W.elem_dofs]
+    G = np.einsum("cqa,eia->eqci", T, W.extraction) * wl[:, None, None, :]
+    Ke = np.einsum("eqci,eqcd,eqdj->eij", G, M, G)
+    b = O.evaluate(TO.ThbSpace.of(W), np.arange(W.n_elems), order=2)
+    Ko = O.element_tangents("plate", b, {"E": 2.0, "nu": 0.3, "t": 0.1})
+    assert np.abs(Ke - Ko).max() <= 1e-12 * np.abs(Ko).max()
+    assert np.abs(X - b["x"]).max() < 1e-14 and np.abs(w - b["w"]).max() < 1e-14 * np.abs(b["w"]).max()
