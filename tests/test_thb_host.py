@@ -191,3 +191,13 @@ def test_plate_metric_reproduces_the_oracle_tangents(tag):
     Ko = O.element_tangents("plate", b, {"E": 2.0, "nu": 0.3, "t": 0.1})
     assert np.abs(Ke - Ko).max() <= 1e-12 * np.abs(Ko).max()
     assert np.abs(X - b["x"]).max() < 1e-14 and np.abs(w - b["w"]).max() < 1e-14 * np.abs(b["w"]).max()
+
+
+def test_clamped_conditions_are_rejected_on_hierarchical_spaces():
+    """A clamped side needs the second control-point layer of every level; the
+    reference rejects it on hierarchical spaces (src/jaxiga/forms/problem.py:249-262)
+    and so does this package, while the simply supported plate is accepted."""
+    W = CASES["sq_p2"]()
+    with pytest.raises(NotImplementedError):
+        jx.KirchhoffPlate(W, dirichlet=[jx.ClampedBC(where=sorted(W.boundaries)[0])])
+    jx.KirchhoffPlate(W, dirichlet=[jx.DirichletBC(0.0, where=sorted(W.boundaries)[0])])
