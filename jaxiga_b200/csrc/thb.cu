@@ -9,7 +9,8 @@
 // K_e = sum_q w a0 dR^T dR (src/jaxiga/forms/library.py:54-65) and scatters
 // them into CSR (src/jaxiga/methods/galerkin.py:122-148).
 //
-// Here K.u runs matrix-free per element, one CTA per element (grid-stride):
+// Here K.u runs matrix-free per element, one warp per element (grid-stride,
+// several warps per CTA):
 //   c_a = sum_i C[i][a] w_i u_i          (the numerator's Bernstein coefficients)
 //   g(q) = (sum_a B_a c_a, sum_a dB_a c_a)  at every Gauss point
 //   f(q) = M_q g(q)                        (M_q: the metric a w L^T L, host-made)
@@ -41,11 +42,21 @@ struct jxb_thb_data {
 namespace jxb {
 namespace {
 
+// One warp per element: a CTA of up to THB_THREADS runs blockDim / 32 elements
+// side by side (grid-stride), each warp on its own slice of A.sg doubles of
+// dynamic shared memory and synchronised by __syncwarp alone; lanes stride over
+// the element's functions, Bernstein coefficients and points (mostly one pass).
 constexpr int THB_THREADS = 128;
+
+__device__ __forceinline__ long long thb_first() {
+  return (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+}
+__device__ __forceinline__ long long thb_stride() { return (long long)gridDim.x * (blockDim.x >> 5); }
 
 struct ThbArgs {
   long long n_elem, n;  // n: scalar functions (the padding index)
   int nlm, nb, nq, nf, vec;
+  int sg;  // dynamic shared memory per warp (doubles)
   double lam, mu;
   const long long* dofs;
   const double* ext;
@@ -64,28 +75,29 @@ template <int NC>
 __global__ void __launch_bounds__(THB_THREADS)
     k_thb_apply(ThbArgs A, const double* __restrict__ x, int masked, const CgState* st) {
   if (st && st->done) return;
-  extern __shared__ double sm[];
+  extern __shared__ double smem[];
+  double* sm = smem + (threadIdx.x >> 5) * A.sg;  // this warp's slice
   double* loc = sm;             // [nlm]  w_i u_i
   double* cb = loc + A.nlm;     // [nb]   numerator coefficients, then the residual r_a
   double* fl = cb + A.nb;       // [NC][nq] fluxes
-  const int tid = threadIdx.x;
-  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+  const int tid = threadIdx.x & 31;
+  for (long long e = thb_first(); e < A.n_elem; e += thb_stride()) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int i = tid; i < A.nlm; i += blockDim.x) {
+    for (int i = tid; i < A.nlm; i += 32) {
       const long long g = dofs[i];
       double v = 0.0;
       if (g < A.n && !(masked && !A.keep[g])) v = A.w[g] * x[g];
       loc[i] = v;
     }
-    __syncthreads();
-    for (int a = tid; a < A.nb; a += blockDim.x) {
+    __syncwarp();
+    for (int a = tid; a < A.nb; a += 32) {
       double s = 0.0;
       for (int i = 0; i < A.nlm; ++i) s += C[i * A.nb + a] * loc[i];
       cb[a] = s;
     }
-    __syncthreads();
-    for (int q = tid; q < A.nq; q += blockDim.x) {
+    __syncwarp();
+    for (int q = tid; q < A.nq; q += 32) {
       double g[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
@@ -110,32 +122,32 @@ __global__ void __launch_bounds__(THB_THREADS)
 #pragma unroll
       for (int c = 0; c < NC; ++c) fl[c * A.nq + q] = f[c];
     }
-    __syncthreads();
-    for (int a = tid; a < A.nb; a += blockDim.x) {
+    __syncwarp();
+    for (int a = tid; a < A.nb; a += 32) {
       double s = 0.0;
       for (int q = 0; q < A.nq; ++q)
 #pragma unroll
         for (int c = 0; c < NC; ++c) s += __ldg(A.tab + ((size_t)c * A.nq + q) * A.nb + a) * fl[c * A.nq + q];
-      cb[a] = s;  // every thread is past its reads of cb (the barrier above)
+      cb[a] = s;  // every lane is past its reads of cb (the warp barrier above)
     }
-    __syncthreads();
-    for (int i = tid; i < A.nlm; i += blockDim.x) {
+    __syncwarp();
+    for (int i = tid; i < A.nlm; i += 32) {
       const long long g = dofs[i];
       double s = 0.0;
       for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * cb[a];
       A.yl[e * A.nlm + i] = g < A.n ? A.w[g] * s : 0.0;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
 // diag K_e: for function i, w_i^2 sum_q G_i(q)^T M_q G_i(q), G_i = the channels of N_i
 template <int NC>
 __global__ void __launch_bounds__(THB_THREADS) k_thb_diag(ThbArgs A) {
-  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+  for (long long e = thb_first(); e < A.n_elem; e += thb_stride()) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int i = threadIdx.x; i < A.nlm; i += blockDim.x) {
+    for (int i = threadIdx.x & 31; i < A.nlm; i += 32) {
       const long long g = dofs[i];
       double d = 0.0;
       for (int q = 0; q < A.nq; ++q) {
@@ -161,28 +173,29 @@ __global__ void __launch_bounds__(THB_THREADS) k_thb_diag(ThbArgs A) {
 
 // load: F_e[i][c] = w_i sum_a C[i][a] sum_q B_a(q) wq(q) f_c(q)
 __global__ void __launch_bounds__(THB_THREADS) k_thb_load(ThbArgs A, const double* __restrict__ f_qp) {
-  extern __shared__ double sm[];
+  extern __shared__ double smem[];
+  double* sm = smem + (threadIdx.x >> 5) * A.sg;  // this warp's slice
   double* fb = sm;  // [nb][vec]
   const int V = A.vec;
-  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+  for (long long e = thb_first(); e < A.n_elem; e += thb_stride()) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int k = threadIdx.x; k < A.nb * V; k += blockDim.x) {
+    for (int k = threadIdx.x & 31; k < A.nb * V; k += 32) {
       const int a = k / V, c = k - a * V;
       double s = 0.0;
       for (int q = 0; q < A.nq; ++q)
         s += __ldg(A.tab + (size_t)q * A.nb + a) * A.wq[e * A.nq + q] * f_qp[(e * A.nq + q) * V + c];
       fb[k] = s;
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < A.nlm * V; k += blockDim.x) {
+    __syncwarp();
+    for (int k = threadIdx.x & 31; k < A.nlm * V; k += 32) {
       const int i = k / V, c = k - i * V;
       const long long g = dofs[i];
       double s = 0.0;
       for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * fb[a * V + c];
       A.yl[e * A.nlm * V + k] = g < A.n ? A.w[g] * s : 0.0;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -240,15 +253,16 @@ __global__ void __launch_bounds__(THB_THREADS)
     k_thb_apply_el(ThbArgs A, const double* __restrict__ x, int masked, const CgState* st) {
   if (st && st->done) return;
   constexpr int NC = DIM + 1;
-  extern __shared__ double sm[];
+  extern __shared__ double smem[];
+  double* sm = smem + (threadIdx.x >> 5) * A.sg;  // this warp's slice
   double* loc = sm;                // [nlm][DIM]  w_i u_ic
   double* cb = loc + A.nlm * DIM;  // [nb][DIM]   numerator coefficients, then the residual
   double* fl = cb + A.nb * DIM;    // [DIM][NC][nq] fluxes
-  const int tid = threadIdx.x;
-  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+  const int tid = threadIdx.x & 31;
+  for (long long e = thb_first(); e < A.n_elem; e += thb_stride()) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int k = tid; k < A.nlm * DIM; k += blockDim.x) {
+    for (int k = tid; k < A.nlm * DIM; k += 32) {
       const int i = k / DIM, c = k - i * DIM;
       const long long g = dofs[i];
       double v = 0.0;
@@ -258,15 +272,15 @@ __global__ void __launch_bounds__(THB_THREADS)
       }
       loc[k] = v;
     }
-    __syncthreads();
-    for (int k = tid; k < A.nb * DIM; k += blockDim.x) {
+    __syncwarp();
+    for (int k = tid; k < A.nb * DIM; k += 32) {
       const int a = k / DIM, c = k - a * DIM;
       double s = 0.0;
       for (int i = 0; i < A.nlm; ++i) s += C[i * A.nb + a] * loc[i * DIM + c];
       cb[k] = s;
     }
-    __syncthreads();
-    for (int q = tid; q < A.nq; q += blockDim.x) {
+    __syncwarp();
+    for (int q = tid; q < A.nq; q += 32) {
       double g[DIM][NC];
 #pragma unroll
       for (int c = 0; c < DIM; ++c)
@@ -290,24 +304,24 @@ __global__ void __launch_bounds__(THB_THREADS)
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) fl[(c * NC + ch) * A.nq + q] = f[c][ch];
     }
-    __syncthreads();
-    for (int k = tid; k < A.nb * DIM; k += blockDim.x) {
+    __syncwarp();
+    for (int k = tid; k < A.nb * DIM; k += 32) {
       const int a = k / DIM, c = k - a * DIM;
       double s = 0.0;
       for (int q = 0; q < A.nq; ++q)
 #pragma unroll
         for (int ch = 0; ch < NC; ++ch) s += __ldg(A.tab + ((size_t)ch * A.nq + q) * A.nb + a) * fl[(c * NC + ch) * A.nq + q];
-      cb[k] = s;  // every thread is past its reads of cb (the barrier above)
+      cb[k] = s;  // every lane is past its reads of cb (the warp barrier above)
     }
-    __syncthreads();
-    for (int k = tid; k < A.nlm * DIM; k += blockDim.x) {
+    __syncwarp();
+    for (int k = tid; k < A.nlm * DIM; k += 32) {
       const int i = k / DIM, c = k - i * DIM;
       const long long g = dofs[i];
       double s = 0.0;
       for (int a = 0; a < A.nb; ++a) s += C[i * A.nb + a] * cb[a * DIM + c];
       A.yl[e * A.nlm * DIM + k] = g < A.n ? A.w[g] * s : 0.0;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -315,10 +329,10 @@ __global__ void __launch_bounds__(THB_THREADS)
 // physical gradient of R_i / w_i with the quotient rule
 template <int DIM>
 __global__ void __launch_bounds__(THB_THREADS) k_thb_diag_el(ThbArgs A) {
-  for (long long e = blockIdx.x; e < A.n_elem; e += gridDim.x) {
+  for (long long e = thb_first(); e < A.n_elem; e += thb_stride()) {
     const long long* dofs = A.dofs + e * A.nlm;
     const double* C = A.ext + e * A.nlm * A.nb;
-    for (int i = threadIdx.x; i < A.nlm; i += blockDim.x) {
+    for (int i = threadIdx.x & 31; i < A.nlm; i += 32) {
       const long long g = dofs[i];
       double d[DIM];
 #pragma unroll
@@ -392,6 +406,7 @@ static ThbArgs thb_args(jxb_plan* plan) {
   A.nq = T->nq;
   A.nf = T->nf;
   A.vec = T->vec;
+  A.sg = 0;
   A.lam = plan->mat.lam;
   A.mu = plan->mat.mu;
   A.dofs = T->d_dofs;
@@ -411,40 +426,45 @@ int thb_bricks(jxb_plan* plan, cudaStream_t s, int mode, const double* x, const 
                int masked) {
   jxb_thb_data* T = plan->thb;
   ThbArgs A = thb_args(plan);
-  const unsigned grid = thb_grid(plan->n_elem);
   const bool el = plan->op == JXB_OP_ELASTICITY;
   const int V = T->vec, NC = plan->op == JXB_OP_PLATE ? 6 : plan->dim + 1;
+  // per-warp shared memory; as many warps (elements) per CTA as 48 KB holds, at most 4
+  A.sg = mode == MODE_APPLY ? (T->nlm + T->nb) * V + V * NC * T->nq : mode == MODE_LOAD ? T->nb * V : 0;
+  const size_t sg_bytes = (size_t)A.sg * sizeof(double);
+  if (sg_bytes > 48 * 1024) return fail(JXB_ERR_INVALID, "hierarchical plan: element too large for shared memory");
+  const int warps = sg_bytes ? (int)std::min<size_t>(THB_THREADS / 32, (48 * 1024) / sg_bytes) : THB_THREADS / 32;
+  const unsigned threads = 32u * (unsigned)warps;
+  const unsigned grid = thb_grid((plan->n_elem + warps - 1) / warps);
+  const size_t sm = sg_bytes * warps;
   if (mode == MODE_APPLY) {
-    const size_t sm = (size_t)((T->nlm + T->nb) * V + V * NC * T->nq) * sizeof(double);
-    if (sm > 48 * 1024) return fail(JXB_ERR_INVALID, "hierarchical plan: element too large for shared memory");
     if (el) {
       if (plan->dim == 2)
-        k_thb_apply_el<2><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+        k_thb_apply_el<2><<<grid, threads, sm, s>>>(A, x, masked, state);
       else
-        k_thb_apply_el<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+        k_thb_apply_el<3><<<grid, threads, sm, s>>>(A, x, masked, state);
     } else if (NC == 3) {
-      k_thb_apply<3><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+      k_thb_apply<3><<<grid, threads, sm, s>>>(A, x, masked, state);
     } else if (NC == 4) {
-      k_thb_apply<4><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+      k_thb_apply<4><<<grid, threads, sm, s>>>(A, x, masked, state);
     } else {
-      k_thb_apply<6><<<grid, THB_THREADS, sm, s>>>(A, x, masked, state);
+      k_thb_apply<6><<<grid, threads, sm, s>>>(A, x, masked, state);
     }
   } else if (mode == MODE_DIAG) {
     if (el) {
       if (plan->dim == 2)
-        k_thb_diag_el<2><<<grid, THB_THREADS, 0, s>>>(A);
+        k_thb_diag_el<2><<<grid, threads, 0, s>>>(A);
       else
-        k_thb_diag_el<3><<<grid, THB_THREADS, 0, s>>>(A);
+        k_thb_diag_el<3><<<grid, threads, 0, s>>>(A);
     } else if (NC == 3) {
-      k_thb_diag<3><<<grid, THB_THREADS, 0, s>>>(A);
+      k_thb_diag<3><<<grid, threads, 0, s>>>(A);
     } else if (NC == 4) {
-      k_thb_diag<4><<<grid, THB_THREADS, 0, s>>>(A);
+      k_thb_diag<4><<<grid, threads, 0, s>>>(A);
     } else {
-      k_thb_diag<6><<<grid, THB_THREADS, 0, s>>>(A);
+      k_thb_diag<6><<<grid, threads, 0, s>>>(A);
     }
   } else if (mode == MODE_LOAD) {
     if (!f_qp) return fail(JXB_ERR_INVALID, "jxb_load: null f_qp");
-    k_thb_load<<<grid, THB_THREADS, (size_t)T->nb * V * sizeof(double), s>>>(A, f_qp);
+    k_thb_load<<<grid, threads, sm, s>>>(A, f_qp);
   } else {
     return fail(JXB_ERR_INVALID, "hierarchical plans apply, load and give the diagonal only");
   }
