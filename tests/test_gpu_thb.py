@@ -318,3 +318,26 @@ def test_simply_supported_plate_solve_matches_the_oracle():
     u = np.zeros(W.n_scalar_basis)
     u[free] = O.scipy_superlu(K_ff, F[free])
     assert np.linalg.norm(sol.u - u) <= 1e-8 * np.linalg.norm(u)
+
+
+def test_variable_coefficient_solve_matches_the_oracle():
+    """A callable a0(x) reaches the THB plan as per-point values (the metric
+    scaled point by point): jx.solve against the oracle's SuperLU solution with
+    a0 evaluated at the oracle's own Gauss points."""
+    from oracle import iga_oracle as O
+
+    W = _cases()["annulus_p2"]()
+    ALL = lambda x: np.full(len(x), True)  # noqa: E731
+    problem = jx.Poisson(W, dirichlet=[jx.DirichletBC(0.0, where=ALL)], source=lambda x, p: np.ones_like(x[0]))
+    sol = jx.solve(problem, params={"a0": lambda x, p: 1.0 + x[0] ** 2 * x[1]}, linear=jx.LinearOptions(tol=1e-12))
+    assert sol.stats["converged"]
+    S = TO.ThbSpace.of(W)
+    xq = O.evaluate(S, np.arange(W.n_elems))["x"]
+    a_qp = 1.0 + xq[..., 0] ** 2 * xq[..., 1]
+    pres, _ = problem.resolve_dirichlet({})
+    K_ff, F, free, _, _ = TO.assemble_poisson(S, a_qp, pres, source_qp=np.ones(a_qp.shape))
+    u = np.zeros(W.n_scalar_basis)
+    u[free] = O.scipy_superlu(K_ff, F[free])
+    assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
+    const = jx.solve(problem, params={"a0": 1.0}, linear=jx.LinearOptions(tol=1e-12))
+    assert np.linalg.norm(const.u - u) > 1e-3 * np.linalg.norm(u)  # the coefficient made a difference
