@@ -282,23 +282,51 @@ def _relevant(L, l, elems):
     """Level-l functions supported on at least one of ``elems`` (sorted)."""
     if not elems:
         return np.zeros(0, dtype=np.int64)
-    flat = np.array(sorted(elems), dtype=np.int64)
-    idx = np.array(_unravel(flat, L.n_elem[l]))
-    out = set()
-    for k in range(len(flat)):
-        out.update(_tensor([L.funcs_of_elem(l, d, idx[d, k]) for d in range(L.dim)], L.n_func[l]).tolist())
-    return np.array(sorted(out), dtype=np.int64)
+    return np.unique(_elem_funcs(L, l, np.fromiter(elems, dtype=np.int64, count=len(elems))))
+
+
+def _elem_funcs(L, l, elems):
+    """(n, (p+1)^dim) level-l tensor functions of each element, first direction fastest."""
+    dim, n1 = L.dim, L.degree[0] + 1
+    idx = np.array(_unravel(elems, L.n_elem[l]))
+    strides = np.concatenate([[1], np.cumprod(np.asarray(L.n_func[l][:-1], dtype=np.int64))])
+    t = np.arange(n1 ** dim)
+    out = np.zeros((len(elems), n1 ** dim), dtype=np.int64)
+    for d in range(dim):
+        out += (L.spans[l][d][2][idx[d]][:, None] + (t // n1 ** d) % n1) * strides[d]
+    return out
+
+
+def _box_counts(L, l, marked, lo, hi):
+    """Per box [lo, hi) of level-l element indices (dim, n), how many of its
+    elements are in ``marked`` (a set of flat indices): summed-area table."""
+    shape = tuple(L.n_elem[l])
+    flag = np.zeros(int(np.prod(shape)), dtype=np.int64)
+    if marked:
+        flag[np.fromiter(marked, dtype=np.int64, count=len(marked))] = 1
+    P = np.zeros(tuple(s + 1 for s in shape), dtype=np.int64)
+    A = flag.reshape(shape, order="F")
+    for d in range(len(shape)):
+        A = np.cumsum(A, axis=d)
+    P[tuple(slice(1, None) for _ in shape)] = A
+    total = np.zeros(lo.shape[1], dtype=np.int64)
+    for corner in np.ndindex(*([2] * len(shape))):
+        sign = (-1) ** (len(shape) - sum(corner))
+        total += sign * P[tuple(hi[d] if c else lo[d] for d, c in enumerate(corner))]
+    return total
 
 
 def _active(L, l, cand, dom, leaf):
     """Candidates whose support lies in the level-l domain and meets a leaf."""
-    out = []
-    for j in cand:
-        idx = np.array(_unravel([int(j)], L.n_func[l]))[:, 0]
-        supp = _tensor([L.elems_of_func(l, d, idx[d]) for d in range(L.dim)], L.n_elem[l]).tolist()
-        if all(e in dom for e in supp) and any(e in leaf for e in supp):
-            out.append(int(j))
-    return np.array(out, dtype=np.int64)
+    cand = np.asarray(cand, dtype=np.int64)
+    if not len(cand):
+        return cand
+    jd = np.array(_unravel(cand, L.n_func[l]))
+    lo = np.stack([np.searchsorted(L.spans[l][d][2], jd[d] - L.degree[d], side="left") for d in range(L.dim)])
+    hi = np.stack([np.searchsorted(L.spans[l][d][2], jd[d], side="right") for d in range(L.dim)])
+    size = np.prod(hi - lo, axis=0)
+    keep = (_box_counts(L, l, dom, lo, hi) == size) & (_box_counts(L, l, leaf, lo, hi) > 0)
+    return cand[keep]
 
 
 def _two_scale(L, l, coarse, fine):
@@ -354,23 +382,49 @@ def _thb_coefficients(relevant, active, S, truncate):
     return Q, columns
 
 
-def _kron_extraction(ops):
-    """kron(... kron(C_1, C_0)): the last direction outermost (function_space.py:315-323)."""
-    C = ops[-1]
-    for d in range(len(ops) - 2, -1, -1):
-        C = np.kron(C, ops[d])
-    return C
-
-
-def _element_rows(Q, rows):
-    """(columns, values) of the named CSR rows over the columns they touch."""
-    blk = Q[rows]
-    blk.eliminate_zeros()
-    cols = np.unique(blk.indices)
-    V = np.zeros((len(rows), len(cols)))
-    coo = blk.tocoo()
-    V[coo.row, np.searchsorted(cols, coo.col)] = coo.data
-    return cols, V
+def _level_elements(L, l, elems, Q, relevant):
+    """Connectivity and extraction of the leaf elements ``elems`` (sorted) of
+    level l, all at once: per element the active functions that its level-l
+    tensor functions touch through the THB rows Q (ascending), the values V of
+    those rows, and the extraction V^T kron(C_{dim-1}, ..., C_0) from the
+    element's Bernstein polynomials to them (function_space.py:315-323).
+    Returns (columns per element as a padded (n, m) array with counts, the
+    extraction (n, m, nb), the parametric boxes (n, 2 dim))."""
+    dim, p = L.dim, L.degree[0]
+    n1 = p + 1
+    nb = n1 ** dim
+    E = np.asarray(elems, dtype=np.int64)
+    n = len(E)
+    idx = np.array(_unravel(E, L.n_elem[l]))                      # (dim, n)
+    loc = _elem_funcs(L, l, E)                                     # level-l tensor functions
+    rows = np.searchsorted(relevant, loc)                          # rows of Q (relevant is sorted)
+    ip, ind, dat = Q.indptr, Q.indices, Q.data
+    r = rows.ravel()
+    cnt = ip[r + 1] - ip[r]
+    src = np.repeat(ip[r], cnt) + (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+    ent = np.repeat(np.arange(n * nb), cnt)
+    col, val = ind[src].astype(np.int64), dat[src]
+    nz = val != 0.0
+    ent, col, val = ent[nz], col[nz], val[nz]
+    el, lrow = ent // nb, ent % nb
+    key = el * Q.shape[1] + col
+    uk, inv = np.unique(key, return_inverse=True)                  # per element, its columns ascending
+    ue, uc = uk // Q.shape[1], uk % Q.shape[1]
+    count = np.bincount(ue, minlength=n)
+    lcol = np.arange(len(uk)) - (np.cumsum(count) - count)[ue]
+    m = int(count.max()) if n else 0
+    cols = np.zeros((n, m), dtype=np.int64)
+    cols[ue, lcol] = uc
+    V = np.zeros((n, nb, m))
+    V[el, lrow, lcol[inv]] = val
+    C = np.asarray(L.ext[l][dim - 1])[idx[dim - 1]]
+    for d in range(dim - 2, -1, -1):                               # kron, the last direction outermost
+        Ed = np.asarray(L.ext[l][d])[idx[d]]
+        C = np.einsum("eij,ekl->eikjl", C, Ed).reshape(n, C.shape[1] * Ed.shape[1], C.shape[2] * Ed.shape[2])
+    ops = np.matmul(V.transpose(0, 2, 1), C)
+    boxes = np.concatenate([np.stack([L.spans[l][d][0][idx[d]] for d in range(dim)], 1),
+                            np.stack([L.spans[l][d][1][idx[d]] for d in range(dim)], 1)], 1)
+    return cols, count, ops, boxes
 
 
 # --------------------------------------------------------------------------
@@ -417,36 +471,32 @@ class HierarchicalSpace:
         self.wgts = control[:, -1].copy()
         self.cpts = control[:, :-1] / control[:, -1:]
         nb = int(np.prod([p + 1 for p in self.degree]))
-        keys, boxes, rows, ops = [], [], [], []
+        parts = []  # per level with leaves: (level, elements, columns, counts, extraction, boxes)
         for l in range(nl):
-            if not leaf[l]:
-                continue
-            for e in sorted(leaf[l]):
-                idx = np.array(_unravel([e], L.n_elem[l]))[:, 0]
-                loc = _tensor([L.funcs_of_elem(l, d, idx[d]) for d in range(self.dim)], L.n_func[l])
-                cols, V = _element_rows(Q[l], np.array([rowof[l][int(j)] for j in loc]))
-                C = _kron_extraction([L.ext[l][d][idx[d]] for d in range(self.dim)])
-                ops.append(V.T @ C)
-                rows.append(cols)
-                box = np.zeros(2 * self.dim)
-                for d in range(self.dim):
-                    box[d], box[self.dim + d] = L.spans[l][d][0][idx[d]], L.spans[l][d][1][idx[d]]
-                boxes.append(box)
-                keys.append((0, l, int(e)))
-        n_loc = max(max((len(r) for r in rows), default=nb), nb)
+            if leaf[l]:
+                E = np.array(sorted(leaf[l]), dtype=np.int64)
+                parts.append((l, E) + _level_elements(L, l, E, Q[l], relevant[l]))
+        n_loc = max([nb] + [int(c.max()) for *_, c, _, _ in parts if len(c)])
         if n_loc > MAX_LOCAL_GROWTH * nb:
             raise HierarchyError(f"an element gathers {n_loc} functions where a tensor-product element of this "
                                  f"degree gathers {nb}; refine with admissible=True, or mark fewer elements")
-        self.n_elems = len(keys)
+        self.n_elems = sum(len(E) for _, E, *_ in parts)
         self.n_local_max = n_loc
         self.n_local = nb
         self.elem_dofs = np.full((self.n_elems, n_loc), self.n_scalar_basis, dtype=np.int64)
         self.extraction = np.zeros((self.n_elems, n_loc, nb))
-        for k, (r, op) in enumerate(zip(rows, ops)):
-            self.elem_dofs[k, :len(r)] = r
-            self.extraction[k, :len(r)] = op
-        self.elem_vertex = np.array(boxes).reshape(self.n_elems, 2 * self.dim)
-        self.elem_key = np.array(keys, dtype=np.int64).reshape(self.n_elems, 3)
+        self.elem_vertex = np.zeros((self.n_elems, 2 * self.dim))
+        self.elem_key = np.zeros((self.n_elems, 3), dtype=np.int64)
+        k = 0
+        for l, E, cols, count, ops, boxes in parts:
+            sl = slice(k, k + len(E))
+            m = cols.shape[1]
+            pad = np.arange(m)[None, :] >= count[:, None]
+            self.elem_dofs[sl, :m] = np.where(pad, self.n_scalar_basis, cols)
+            self.extraction[sl, :m] = np.where(pad[..., None], 0.0, ops)
+            self.elem_vertex[sl] = boxes
+            self.elem_key[sl, 1], self.elem_key[sl, 2] = l, E
+            k += len(E)
         self._boundaries = self._classify()
         self._plans = {}  # device operators and evaluation data cached by solve()
 
