@@ -517,20 +517,25 @@ class HierarchicalSpace:
         """label -> BoundarySet: the leaf elements on a patch side and the
         active functions whose tensor index sits on it (hierarchical.py:982-1039)."""
         L, labels = self._levels, self.patch.label_map
+        nd = self.dim
         lev = np.array([l for l, _ in self.columns], dtype=np.int64)
-        fidx = [np.array(_unravel([j], L.n_func[l]))[:, 0] for l, j in self.columns]
+        fnum = np.array([j for _, j in self.columns], dtype=np.int64)
+        # per function and per element: its tensor index at its level and that level's extent
+        fidx, fext = np.zeros((nd, len(fnum)), dtype=np.int64), np.zeros((nd, len(fnum)), dtype=np.int64)
+        eidx, eext = np.zeros((nd, self.n_elems), dtype=np.int64), np.zeros((nd, self.n_elems), dtype=np.int64)
+        for l in np.unique(np.concatenate([lev, self.elem_key[:, 1]])):
+            f, e = lev == l, self.elem_key[:, 1] == l
+            fidx[:, f] = np.array(_unravel(fnum[f], L.n_func[l])).reshape(nd, -1)
+            fext[:, f] = np.asarray(L.n_func[l])[:, None]
+            eidx[:, e] = np.array(_unravel(self.elem_key[e, 2], L.n_elem[l])).reshape(nd, -1)
+            eext[:, e] = np.asarray(L.n_elem[l])[:, None]
         out = {}
         for d in range(self.dim):
             for end in (0, 1):
                 side = f"{'uvw'[d]}{end}"
                 label = labels.get(side, f"patch0/{side}")
-                elems = []
-                for k, (_, l, e) in enumerate(self.elem_key):
-                    i = np.array(_unravel([e], L.n_elem[l]))[d, 0]
-                    if i == (0 if end == 0 else L.n_elem[l][d] - 1):
-                        elems.append(k)
-                dofs = [c for c in range(len(self.columns))
-                        if fidx[c][d] == (0 if end == 0 else L.n_func[lev[c]][d] - 1)]
+                elems = np.flatnonzero(eidx[d] == (0 if end == 0 else eext[d] - 1))
+                dofs = np.flatnonzero(fidx[d] == (0 if end == 0 else fext[d] - 1))
                 entry = out.setdefault(label, ([], [], []))
                 entry[0].append(np.asarray(elems, dtype=np.int64))
                 entry[1].append(np.full(len(elems), 2 * d + end, dtype=np.int64))
