@@ -219,6 +219,9 @@ def test_neumann_loads_match_the_oracle():
         (_cases()["cube_p2"](), lambda W: jx.Poisson(W, neumann=[
             jx.Neumann(lambda x, n, p: np.sin(x[:, 1:2]) * n[:, :1], where=lambda c: np.isclose(c[:, 0], 1.0))]),
          "poisson", (1.0,)),
+        (_cases()["sq_p3_deep"](), lambda W: jx.KirchhoffPlate(W, neumann=[  # an edge shear on the plate
+            jx.Neumann(lambda x, n, p: np.cos(x[:, :1]) + p["g"], where=sorted(W.boundaries)[1])]),
+         "plate", (1.0, 0.3, 0.1)),
     ]
     params = {"g": 2.5}
     for W, make, kind, coef in cases:
@@ -271,6 +274,17 @@ def test_pressurised_thick_cylinder_on_a_refined_space():
     assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
     e_ref, e_thb = jx.errornorm(base, disp, "L2"), jx.errornorm(sol, disp, "L2")
     assert e_thb < 0.5 * e_ref, (e_thb, e_ref)
+
+    def stress(pts):  # the closed-form plane stress field, Voigt (xx, yy, xy)
+        r, th = np.hypot(pts[:, 0], pts[:, 1]), np.arctan2(pts[:, 1], pts[:, 0])
+        srr = q * r_i**2 / (r_o**2 - r_i**2) * (1 - r_o**2 / r**2)
+        stt = q * r_i**2 / (r_o**2 - r_i**2) * (1 + r_o**2 / r**2)
+        c, s = np.cos(th), np.sin(th)
+        return np.stack([srr * c**2 + stt * s**2, srr * s**2 + stt * c**2, (srr - stt) * s * c], axis=1)
+
+    en_ref, en_thb = (jx.errornorm(base, disp, "energy", exact_grad=stress),
+                      jx.errornorm(sol, disp, "energy", exact_grad=stress))
+    assert en_thb < en_ref, (en_thb, en_ref)
 
 
 @pytest.mark.parametrize("tag", ["sq_p2", "sq_p3_deep", "annulus_p2"])
