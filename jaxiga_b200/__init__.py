@@ -24,6 +24,7 @@ from .forms import (ClampedBC, DirichletBC, Hyperelasticity, KirchhoffPlate, Lin
                     Poisson, Problem)
 from .geometry import Patch, primitives
 from .hierarchical import HierarchicalSpace, Hierarchy, HierarchyError, dorfler_mark, refine_elements
+from .estimators import adapt, residual_indicator
 from .newton import history_list
 from .operator import Operator
 from .pointset import PointSet, gauss
@@ -39,4 +40,5 @@ __all__ = [
     "PointSet", "gauss", "value_and_grad", "adjoint_solve", "parameter_gradients", "SOLVE_COUNTER",
     "reset_solve_counter", "DeviceCG", "CSRPattern", "Hyperelasticity", "history_list",
     "HierarchicalSpace", "Hierarchy", "HierarchyError", "refine_elements", "dorfler_mark",
+    "residual_indicator", "adapt",
 ]

@@ -808,3 +808,34 @@ def interpolate_qp(space, coef, n_q=None, chunk=4096):
         basis = evaluate(space, el, n_q=n_q)
         out.append(np.einsum("eqn,enc->eqc", basis["R"], coef2[basis["dofs"]]))
     return np.concatenate(out)
+
+
+def residual_indicator(space, u, problem_kind, params, source=None, n_q=None, elems=None):
+    """Explicit residual indicators (post/estimators.py:33-88): eta_e^2 = h_e^2
+    sum_q w |r|^2, h_e = |e|^(1/dim), on n_q = p + 2 Gauss points per
+    direction, r = -a0 lap u - f (Poisson) or r = -((lam + mu) grad div u +
+    mu lap u) - f (isotropic elasticity; plane stress in 2D); ``source(x)`` ->
+    (n_pts, vec); ``space`` any view ``evaluate`` takes (tensor or padded THB)."""
+    dim, vec = space.dim, (1 if problem_kind == "poisson" else space.dim)
+    n_q = max(space.degree) + 2 if n_q is None else n_q
+    elems = np.arange(space.n_elems) if elems is None else np.asarray(elems)
+    b = evaluate(space, elems, n_q=n_q, order=2)
+    pairs = voigt_pairs(dim)
+    U = np.concatenate([np.asarray(u, dtype=float).reshape(-1, vec), np.zeros((1, vec))])[b["dofs"]]  # (e, n, vec)
+    H = np.zeros(b["w"].shape + (vec, dim, dim))
+    for k, (a, c) in enumerate(pairs):
+        H[..., a, c] = H[..., c, a] = np.einsum("eqn,enc->eqc", b["d2R"][:, :, k], U)[..., None][..., 0]
+    f = np.zeros(b["w"].shape + (vec,))
+    if source is not None:
+        f = np.asarray(source(b["x"].reshape(-1, dim)), dtype=float).reshape(f.shape)
+    lap = np.trace(H, axis1=-2, axis2=-1)                                   # (e, q, vec)
+    if problem_kind == "poisson":
+        r = -params["a0"] * lap - f
+    else:
+        E, nu = params["E"], params["nu"]
+        mu = E / (2 * (1 + nu))
+        lam = E * nu / ((1 + nu) * (1 - 2 * nu)) if dim == 3 else E * nu / (1 - nu**2)
+        graddiv = np.einsum("eqjij->eqi", H)                                # d_i sum_j d_j u_j
+        r = -((lam + mu) * graddiv + mu * lap) - f
+    h = b["w"].sum(1) ** (1.0 / dim)
+    return np.sqrt(h**2 * np.sum(b["w"] * np.sum(r**2, -1), 1))

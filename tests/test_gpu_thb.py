@@ -355,3 +355,27 @@ def test_variable_coefficient_solve_matches_the_oracle():
     assert np.linalg.norm(sol.u - u) <= 1e-9 * np.linalg.norm(u)
     const = jx.solve(problem, params={"a0": 1.0}, linear=jx.LinearOptions(tol=1e-12))
     assert np.linalg.norm(const.u - u) > 1e-3 * np.linalg.norm(u)  # the coefficient made a difference
+
+
+def test_adapt_drives_the_estimate_and_the_error_down():
+    """The reference's solve-estimate-mark-refine driver (post/estimators.py:91-183)
+    on a Gaussian peak: four cycles, every solve on the device; the residual
+    estimate and the L2 error fall while the THB space grows."""
+    a, c = 50.0, 0.5
+
+    def peak(x):
+        return np.exp(-a * ((x[:, 0] - c) ** 2 + (x[:, 1] - c) ** 2))
+
+    def src(x, p):  # -lap of the peak
+        r2 = (x[0] - c) ** 2 + (x[1] - c) ** 2
+        return -np.exp(-a * r2) * (4 * a * a * r2 - 4 * a)
+
+    ALL = lambda x: np.full(len(x), True)  # noqa: E731
+    V = jx.FunctionSpace(jx.primitives.quadrilateral(SQ).elevate(2).refine(3))
+    sol, W, hist = jx.adapt(lambda S: jx.Poisson(S, dirichlet=[jx.DirichletBC(0.0, where=ALL)], source=src),
+                            {"a0": 1.0}, space=V, n_cycles=4, frac=0.5, exact=peak,
+                            solve_kwargs={"linear": jx.LinearOptions(tol=1e-10)})
+    assert isinstance(W, H.HierarchicalSpace) and sol.space is W and len(hist) == 4
+    assert [h["n_elems"] for h in hist] == sorted(h["n_elems"] for h in hist) and hist[-1]["n_elems"] > 64
+    assert hist[-1]["eta"] < 0.5 * hist[0]["eta"], hist
+    assert hist[-1]["L2"] < hist[0]["L2"], hist
