@@ -30,15 +30,18 @@ from .space import gauss_1d
 
 
 def _element_data(space):
-    """(elem_dofs with a padding index, extraction (n_e, n_loc, nb)) of a tensor or THB space."""
+    """(elem_dofs, extraction (n_e, n_loc, nb)) of a tensor, multipatch or THB space (THB rows padded)."""
     from .hierarchical import HierarchicalSpace
+    from .multipatch import MultiPatchSpace
     from .space import FunctionSpace
 
     if isinstance(space, HierarchicalSpace):
         return space.elem_dofs, space.extraction
+    if isinstance(space, MultiPatchSpace):  # elements patch by patch, global (conforming) DOFs
+        return space.elem_dofs, np.concatenate([s.extraction() for s in space.spaces])
     if isinstance(space, FunctionSpace):
         return space.elem_dofs, space.extraction()
-    raise NotImplementedError("residual indicators run on single-patch tensor and THB spaces")
+    raise NotImplementedError("residual indicators run on tensor, multipatch and THB spaces")
 
 
 def second_derivatives(space, u, n=None, chunk=2048):

@@ -72,3 +72,17 @@ def test_adapt_argument_checks():
     with pytest.raises(NotImplementedError):
         jx.residual_indicator(Solution(V, np.zeros(V.n_dofs), {"E": 1.0, "nu": 0.3, "t": 0.1},
                                        jx.KirchhoffPlate(V)))
+
+
+def test_multipatch_indicators_are_the_patches_own():
+    """On a conforming two-patch space the indicators are, patch by patch, the
+    oracle's on each patch with its share of the global coefficients."""
+    rect = jx.primitives.rectangle
+    V = jx.FunctionSpace([rect(0, 0, 1, 1).elevate(2).refine(2), rect(1, 0, 2, 1).elevate(2).refine(2)])
+    u = np.random.default_rng(3).standard_normal(V.n_dofs)
+    eta = jx.residual_indicator(Solution(V, u, {"a0": 1.0}, jx.Poisson(V, source=lambda x, p: x[0] * x[1])))
+    ref = np.concatenate([
+        O.residual_indicator(O.Space(s.knots, s.degree, s.cpts, s.wgts, 1), u[V.topology.local_to_global[i]],
+                             "poisson", {"a0": 1.0}, source=lambda x: x[:, 0] * x[:, 1])
+        for i, s in enumerate(V.spaces)])
+    assert np.abs(eta - ref).max() <= 1e-12 * np.abs(ref).max()
