@@ -384,6 +384,45 @@ class ThbGeometry:
         # grad_x u_c[k] = sum_a Ji[a][k] d u_c / d xi_a
         return torch.as_tensor(np.einsum("eqak,eaqc->eqck", Ji, gref))
 
+    def eval_points(self, elems, ref, coef=None, val=True, grad=False, x=False, jac=False):
+        """Values, physical gradients of a control-point field, coordinates and
+        |det J| (reference coordinates) at points given by element indices (n,)
+        and reference coordinates (n, dim) in [-1, 1]^dim; the interface of the
+        tensor ``Operator.eval_points`` (evaluation.py:305-467)."""
+        import torch
+
+        s = self.space
+        dim = s.dim
+        e = np.asarray(elems, dtype=np.int64).reshape(-1)
+        r = np.asarray(ref, dtype=float).reshape(len(e), dim)
+        if coef is None and (val or grad):
+            raise ValueError("values and gradients need a coefficient field")
+        T = tables_at(r, s.degree[0])                                      # (dim + 1, n, nb): row k is point k
+        hom = np.concatenate([s.cpts * s.wgts[:, None], s.wgts[:, None]], 1)
+        hom = np.concatenate([hom, np.zeros((1, dim + 1))])
+        C, d = s.extraction[e], s.elem_dofs[e]
+        geo = np.einsum("cka,kia,kij->kcj", T, C, hom[d])                  # (n, channel, (w x, w))
+        W, Wa = geo[:, 0, dim], geo[:, 1:, dim]
+        xp = geo[:, 0, :dim] / W[:, None]
+        J = (geo[:, 1:, :dim] - Wa[..., None] * xp[:, None]) / W[:, None, None]  # [a][i]
+        out = {}
+        if coef is not None:
+            c = np.asarray(coef.cpu().numpy() if hasattr(coef, "cpu") else coef, dtype=float)
+            c = c.reshape(s.n_scalar_basis, -1)
+            cw = np.concatenate([c * s.wgts[:, None], np.zeros((1, c.shape[1]))])
+            num = np.einsum("cka,kia,kij->kcj", T, C, cw[d])                # (n, channel, ncomp)
+            f = num[:, 0] / W[:, None]
+            if val:
+                out["val"] = torch.as_tensor(f)
+            if grad:
+                fa = (num[:, 1:] - Wa[..., None] * f[:, None]) / W[:, None, None]  # (n, a, ncomp)
+                out["grad"] = torch.as_tensor(np.moveaxis(np.linalg.solve(J, fa), 1, 2))
+        if x:
+            out["x"] = torch.as_tensor(xp)
+        if jac:
+            out["jac"] = torch.as_tensor(np.abs(np.linalg.det(J)))
+        return out
+
     def close(self):
         pass
 

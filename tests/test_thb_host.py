@@ -201,3 +201,29 @@ def test_clamped_conditions_are_rejected_on_hierarchical_spaces():
     with pytest.raises(NotImplementedError):
         jx.KirchhoffPlate(W, dirichlet=[jx.ClampedBC(where=sorted(W.boundaries)[0])])
     jx.KirchhoffPlate(W, dirichlet=[jx.DirichletBC(0.0, where=sorted(W.boundaries)[0])])
+
+
+@pytest.mark.parametrize("tag", ["annulus_p2", "cube_p2", "sq_p3_deep"])
+def test_point_evaluation_matches_the_oracle(tag):
+    """Values, physical gradients, coordinates and |det J| of a field at random
+    points of random leaf elements (Solution.at / grad on any PointSet) against
+    the oracle's evaluation on the padded view."""
+    from jaxiga_b200.solve import Solution
+    from jaxiga_b200.thb import ThbGeometry
+
+    W = CASES[tag]()
+    S = TO.ThbSpace.of(W)
+    rng = np.random.default_rng(2)
+    el, ref = rng.integers(0, W.n_elems, 40), rng.uniform(-1, 1, (40, W.dim))
+    c = rng.standard_normal((W.n_scalar_basis, 2))
+    out = ThbGeometry(W).eval_points(el, ref, c, val=True, grad=True, x=True, jac=True)
+    cp = np.concatenate([c, np.zeros((1, 2))])
+    b = [O.evaluate(S, [e], ref=r[None], weights=np.ones(1)) for e, r in zip(el, ref)]
+    val = np.array([bk["R"][0, 0] @ cp[bk["dofs"][0]] for bk in b])
+    grad = np.array([(bk["dR"][0, 0] @ cp[bk["dofs"][0]]).T for bk in b])
+    assert np.abs(out["val"].numpy() - val).max() <= 1e-13 * np.abs(val).max()
+    assert np.abs(out["grad"].numpy() - grad).max() <= 1e-12 * np.abs(grad).max()
+    assert np.abs(out["x"].numpy() - np.array([bk["x"][0, 0] for bk in b])).max() < 1e-14
+    assert np.abs(out["jac"].numpy() - np.array([bk["w"][0, 0] for bk in b])).max() < 1e-15
+    ps = jx.gauss(W, 3)
+    assert Solution(W, c[:, 0]).at(ps).shape == (W.n_elems, 3 ** W.dim, 1)
